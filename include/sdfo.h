@@ -1,0 +1,279 @@
+/*
+ * sdfo.h -- C ABI of libsdfo_cuda.so, the B200 (sm_100a) implementation of
+ * the SdfOracle hot path: SDF construction from a triangle mesh (dense and
+ * sparse narrow-band), batched SDF queries with their backward, and the fused
+ * per-quadrature-point penalty contact with its 6-DoF pose Jacobian.
+ *
+ * Conventions
+ *  - Plain C: no C++ types, no exceptions cross this boundary.  Every
+ *    function returns an int status: SDFO_OK (0) or a negative SDFO_ERR_*;
+ *    sdfo_last_error() returns the message of the calling thread's last error.
+ *  - Pointers named d_* are device pointers (CUDA global memory, e.g. a torch
+ *    tensor's data_ptr()); pointers named h_* are host pointers.  `stream` is
+ *    a cudaStream_t passed as void* (NULL = legacy default stream).  Calls
+ *    taking d_* buffers are asynchronous on `stream` unless stated.
+ *  - Buffers are owned by the caller.  The library owns only the storage
+ *    behind an sdfo_grid handle.  A handle is immutable after creation, so
+ *    concurrent queries on different streams are safe.
+ *  - Grid index convention (reference GridSpec, GridSpec.h:17-60): voxel
+ *    centre = bmin + voxel * (ijk + 0.5); linear index i + nx*(j + ny*k).
+ *
+ * The reference (W-Moorer/sdf-contact-module) has no FFI; each entry point
+ * below names the reference interface whose behaviour it reproduces.
+ */
+#ifndef SDFO_H
+#define SDFO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SDFO_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define SDFO_OK 0
+#define SDFO_ERR_INVALID_ARGUMENT (-1) /* bad pointer, size, mode or params */
+#define SDFO_ERR_CUDA (-2)             /* a CUDA runtime call failed */
+#define SDFO_ERR_OUT_OF_MEMORY (-3)
+#define SDFO_ERR_EMPTY_MESH (-4)       /* "Empty mesh provided to SdfBuilder" */
+#define SDFO_ERR_DEVICE_STATUS (-5)    /* a kernel reported a failure (see message) */
+#define SDFO_ERR_UNSUPPORTED (-6)      /* mode/layout combination not provided */
+#define SDFO_ERR_NO_DEVICE (-7)        /* no CUDA device / not an sm_100 device */
+
+/* ---- enums --------------------------------------------------------------- */
+/* QueryMode (SdfOracle.h:11-18). */
+#define SDFO_FIRST_ORDER 0
+#define SDFO_SECOND_ORDER 1
+#define SDFO_TRILINEAR 2
+#define SDFO_TRICUBIC 3
+#define SDFO_CONTACT_AWARE 4
+
+/* Storage layouts, numbered as the SDFO 0.1.0 header's layout field
+ * (SdfIO.cpp:30-33). */
+#define SDFO_LAYOUT_DENSE 1
+#define SDFO_LAYOUT_SPARSE 2
+
+/* Device storage precision of the query payload. */
+#define SDFO_STORAGE_FP32 0
+#define SDFO_STORAGE_FP16 1 /* sparse only: per-brick affine phi + fp16 normal */
+
+/* Point precision for query inputs. */
+#define SDFO_POINTS_F32 0
+#define SDFO_POINTS_F64 1
+
+typedef struct sdfo_grid sdfo_grid;
+
+/* GridSpec (GridSpec.h:17-27) plus the sparse header fields of
+ * SparseSdfData (SdfData.h:154-163). */
+typedef struct
+{
+    double bmin[3];
+    double bmax[3];
+    double voxel[3];
+    int32_t shape[3];       /* nx, ny, nz */
+    int32_t layout;         /* SDFO_LAYOUT_* */
+    int32_t storage;        /* SDFO_STORAGE_* */
+    int32_t has_hessian;
+    int32_t block_dim;      /* sparse */
+    int32_t halo_voxels;    /* sparse */
+    int32_t block_count;    /* sparse: number of stored blocks */
+    int32_t reserved0;
+    double band_distance;   /* sparse */
+} sdfo_grid_info;
+
+/* BuilderParams (SdfBuilder.h:24-31); the log callback stays on the host. */
+typedef struct
+{
+    double padding;            /* fraction of the bbox diagonal, default 0.1 */
+    double voxel_size;         /* 0 = longest padded side / target_resolution */
+    int32_t target_resolution; /* default 128 */
+    int32_t max_resolution;    /* default 512 */
+} sdfo_build_params;
+
+/* SparseBuilderParams (SdfBuilder.h:33-40). */
+typedef struct
+{
+    sdfo_build_params base;
+    int32_t block_dim;     /* default 8 */
+    int32_t halo_voxels;   /* default 2 */
+    int32_t band_voxels;   /* default 8 */
+    int32_t store_hessian; /* default 1 */
+    double band_distance;  /* 0 = band_voxels * voxel */
+} sdfo_sparse_build_params;
+
+/* Body state for contact: position r, rotation R (row-major 3x3, body to
+ * world), linear velocity v and angular velocity w (world frame). */
+typedef struct
+{
+    double r[3];
+    double R[9];
+    double v[3];
+    double w[3];
+} sdfo_body_state;
+
+/* ContactPair fields used by SDFContactEngine.evaluate
+ * (prototype/src/ir/contact.py:1-18, contacts_sdf.py:296-302). */
+typedef struct
+{
+    double stiffness;           /* k_n */
+    double order;               /* k_order (n in k * delta^n) */
+    double damping;             /* c_n, quadrature_settings['damping'] */
+    double friction;            /* mu */
+    double regularizer;         /* quadrature_settings['regularizer'] */
+    double activation_distance; /* read but unused by the reference law */
+} sdfo_contact_params;
+
+/* Build statistics of the last build on a handle. */
+typedef struct
+{
+    double setup_ms, bvh_ms, fill_ms, hessian_ms, total_ms;
+    int64_t voxels_filled;    /* voxels whose distance was computed */
+    int64_t candidate_blocks; /* sparse: blocks tested for activation */
+    int32_t triangles;
+    int32_t bvh_nodes;
+} sdfo_build_stats;
+
+/* Raw device views of a grid (for interop, e.g. torch autograd on the
+ * payload).  Dense: phin = float4[nx*ny*nz] {phi, nx, ny, nz}.  Sparse:
+ * phin = float4[block_count * block_dim^3], table = int32[nbx*nby*nbz]
+ * (block slot or -1), block_ijk = int32[block_count*3]. */
+typedef struct
+{
+    void* phin;
+    void* hessian6; /* float[6] per stored voxel, or NULL */
+    void* table;
+    void* block_ijk;
+    int64_t stored_voxels;
+    int32_t table_dims[3];
+    int32_t reserved0;
+} sdfo_device_views;
+
+/* ---- library ------------------------------------------------------------ */
+const char* sdfo_version(void);
+int sdfo_abi_version(void);
+/* Copies the calling thread's last error message (NUL-terminated). */
+int sdfo_last_error(char* buf, size_t len);
+/* Checks that device `device` is usable (compute capability 10.x). */
+int sdfo_device_check(int device);
+
+void sdfo_build_params_default(sdfo_build_params* p);
+void sdfo_sparse_build_params_default(sdfo_sparse_build_params* p);
+
+/* Host-only grid setup: SdfBuilder::setupGrid (SdfBuilder.cpp:994-1035) with
+ * snapToStandardResolution (GridSpec.h:65-74). */
+int sdfo_setup_grid(const double* h_verts, int64_t nv, const sdfo_build_params* p,
+                    sdfo_grid_info* out);
+
+/* ---- build (SdfBuilder) --------------------------------------------------- */
+/* SdfBuilder::build (SdfBuilder.cpp:364-407, SdfBuilder.h:62-70): dense SDF,
+ * normals, witness points and symmetrised Hessian.  h_verts (nv,3) float64,
+ * h_tris (nt,3) int32, both host.  Synchronous. */
+int sdfo_grid_build_dense(const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
+                          const sdfo_build_params* p, void* stream, sdfo_grid** out);
+
+/* SdfBuilder::buildSparse (SdfBuilder.cpp:823-983, SdfBuilder.h:83-91):
+ * narrow-band blocks in (bk, bj, bi) order, FP32 payload.  Synchronous. */
+int sdfo_grid_build_sparse(const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
+                           const sdfo_sparse_build_params* p, void* stream, sdfo_grid** out);
+
+int sdfo_grid_build_stats(const sdfo_grid* g, sdfo_build_stats* out);
+
+/* ---- grid from / to host data (SdfData / SparseSdfData, SdfData.h) ------- */
+/* SdfOracle(SdfData) (SdfOracle.cpp:154-157): dense FP64 arrays, x-fastest:
+ * phi (N), normal (N,3), hessian6 (N,6: xx,xy,xz,yy,yz,zz, may be NULL),
+ * witness (N,3, may be NULL).  info supplies bmin/bmax/voxel/shape. */
+int sdfo_grid_create_dense(const sdfo_grid_info* info, const double* h_phi,
+                           const double* h_normal, const double* h_hessian6,
+                           const double* h_witness, void* stream, sdfo_grid** out);
+/* SdfOracle(SparseSdfData) (SdfOracle.cpp:159-163): block_count blocks of
+ * block_dim^3 voxels: ijk (B,3), phi (B,V), normal (B,V,3), hessian6 (B,V,6)
+ * or NULL.  Blocks are kept in the given order. */
+int sdfo_grid_create_sparse(const sdfo_grid_info* info, const int32_t* h_block_ijk,
+                            const float* h_phi, const float* h_normal, const float* h_hessian6,
+                            void* stream, sdfo_grid** out);
+/* Re-encodes a sparse FP32 grid as FP16 with a per-brick phi scale/offset
+ * (new storage form; the SDFO file format is unchanged). */
+int sdfo_grid_to_fp16(const sdfo_grid* src, void* stream, sdfo_grid** out);
+
+/* Export to host in the SdfData / SparseSdfData layouts above.  Dense grids
+ * built on the device keep their FP64 build results, so the export is
+ * exact; dense grids created from FP32-only data widen to FP64. */
+int sdfo_grid_export_dense(const sdfo_grid* g, double* h_phi, double* h_normal,
+                           double* h_hessian6, double* h_witness);
+int sdfo_grid_export_sparse(const sdfo_grid* g, int32_t* h_block_ijk, float* h_phi,
+                            float* h_normal, float* h_hessian6);
+
+/* Copies the grid's FP32 query payload (float4 {phi, n} per stored voxel,
+ * dense x-fastest or sparse brick order) into d_dst. */
+int sdfo_grid_copy_payload(const sdfo_grid* g, void* d_dst, void* stream);
+/* A handle that shares g's structure (spec, block table) but reads its FP32
+ * payload from caller-owned device memory d_phin (stored_voxels float4, not
+ * copied, not freed).  Used to differentiate w.r.t. the payload held in a
+ * framework tensor.  Must be destroyed before g and before d_phin is freed. */
+int sdfo_grid_create_view(const sdfo_grid* g, void* d_phin, sdfo_grid** out);
+
+int sdfo_grid_get_info(const sdfo_grid* g, sdfo_grid_info* out);
+int sdfo_grid_device_views(const sdfo_grid* g, sdfo_device_views* out);
+int sdfo_grid_destroy(sdfo_grid* g);
+
+/* ---- queries (SdfOracle::queryFast / queryBatch) ------------------------- */
+/* SdfOracle::queryFast + queryBatch (SdfOracle.cpp:226-444) for n points.
+ * d_points: (n,3) float32 or float64 (points_f64).  Outputs (device, any may
+ * be NULL except d_gap):
+ *   d_gap[n]          interpolated signed distance ("gap")
+ *   d_grad[n*3]       raw gradient of the interpolant (FirstOrder: n0;
+ *                     SecondOrder: n0 + H0 dx, as the reference's normal)
+ *   d_unit[n*3]       the reference's gapNormal: grad/|grad|, UnitX when
+ *                     |grad| <= 1e-15 (SecondOrder: falls back to n0)
+ *   d_witness[n*3]    p - gap * gapNormal
+ *   d_valid[n]        1 if the query is inside the stored domain
+ *   d_hess[n*9]       d grad / d p of the interpolant (row-major), the
+ *                     forward-mode Jacobian of (gap, grad) w.r.t. p
+ * Invalid queries write gap 0, grad 0, unit (1,0,0), witness 0, hess 0.
+ * ContactAware on grids without candidates behaves as Tricubic, as the
+ * reference does (SdfOracle.cpp:209-212). */
+int sdfo_query(const sdfo_grid* g, int32_t mode, const void* d_points, int32_t points_f64,
+               int64_t n, float* d_gap, float* d_grad, float* d_unit, float* d_witness,
+               uint8_t* d_valid, float* d_hess, void* stream);
+
+/* Same with host buffers (pageable or pinned): copies in, queries, copies
+ * out; synchronous. */
+int sdfo_query_host(const sdfo_grid* g, int32_t mode, const void* h_points, int32_t points_f64,
+                    int64_t n, float* h_gap, float* h_grad, float* h_unit, float* h_witness,
+                    uint8_t* h_valid, void* stream);
+
+/* Backward of sdfo_query (no reference counterpart): given upstream
+ * d_dgap[n] and d_dgrad[n*3] (either may be NULL = zero), writes
+ *   d_dpoints[n*3] = dgap * grad + H * dgrad        (may be NULL)
+ * and accumulates into d_dgrid (float4 per stored voxel: d phi, d n) the
+ * gradient w.r.t. the stored payload (may be NULL).  Trilinear and Tricubic
+ * on FP32 storage; float32 points. */
+int sdfo_query_backward(const sdfo_grid* g, int32_t mode, const float* d_points, int64_t n,
+                        const float* d_dgap, const float* d_dgrad, float* d_dpoints,
+                        float* d_dgrid, void* stream);
+
+/* ---- contact (SDFContactEngine.evaluate) --------------------------------- */
+/* Batched SDFContactEngine.evaluate (prototype/src/dynamics/contacts_sdf.py:
+ * 225-385) for P poses of body A (the quadrature body) against the grid of
+ * body B: Y = R_B^T R_A X + R_B^T (r_A - r_B); penalty p = k max(-g,0)^n
+ * along R_B grad g; damping c (-v_n) R_B grad g when g < 0; regularised
+ * Coulomb friction -mu p |grad g| u_t / sqrt(|u_t|^2 + reg^2).
+ *   d_quad_x (Q,3) float32 body-A-local points, d_quad_w (Q) float32 weights
+ *   d_pose_a (P) body A states, d_body_b (1) body B state (device)
+ *   d_ft (P,6) float64: F_A, tau_A (tau about r_A)
+ *   d_jac (P,36) float64 or NULL: row-major d(F_A,tau_A)/d(dx,dtheta) for
+ *   r_A += dx, R_A = exp([dtheta]x) R_A (forward-mode, in-kernel).
+ * Mode: Trilinear or Tricubic. */
+int sdfo_contact_eval(const sdfo_grid* g, int32_t mode, const float* d_quad_x,
+                      const float* d_quad_w, int64_t nq, const sdfo_body_state* d_pose_a,
+                      int64_t np, const sdfo_body_state* d_body_b,
+                      const sdfo_contact_params* h_params, double* d_ft, double* d_jac,
+                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SDFO_H */

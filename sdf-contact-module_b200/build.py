@@ -1,0 +1,82 @@
+"""Builds libsdfo_cuda.so (sm_100a) in-tree from csrc/*.cu.
+
+    python sdf-contact-module_b200/build.py [--force] [--verbose]
+
+Each translation unit is compiled with
+``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``; build.cu (the FP64
+distance / sign path) additionally with ``-fmad=false`` so its FP64
+expressions are evaluated exactly in source order.  The static CUDA runtime
+is linked in so the library does not depend on the toolkit's libcudart at
+run time.  Objects go to _build/, the library to lib/.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+BUILD = os.path.join(PKG, "_build")
+LIBDIR = os.path.join(PKG, "lib")
+LIB = os.path.join(LIBDIR, "libsdfo_cuda.so")
+INCLUDE = os.path.join(ROOT, "include")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
+          "-ffp-contract=off", "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
+PER_FILE = {"build.cu": ["-fmad=false"]}
+SOURCES = ["grid.cu", "capi.cu", "query.cu", "build.cu", "contact.cu"]
+HEADERS = ["sdfo_internal.cuh", "interp.cuh"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _newer(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    os.makedirs(LIBDIR, exist_ok=True)
+    hdr = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "sdfo.h"),
+                                                    os.path.abspath(__file__)]
+    objs = []
+    for src in SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        objs.append(o)
+        if force or _newer(o, [s] + hdr):
+            cmd = [nvcc(), "-c", s, "-o", o] + ARCH + COMMON + PER_FILE.get(src, []) + (extra_flags or [])
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+    if force or _newer(LIB, objs):
+        cmd = [nvcc(), "-shared", "-o", LIB] + objs + ARCH + ["-cudart", "static",
+                                                            "-Xcompiler", "-fPIC"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--ptxas-v", action="store_true", help="print register/spill usage")
+    a = ap.parse_args()
+    extra = ["-Xptxas", "-v"] if a.ptxas_v else None
+    print(build(force=a.force or a.ptxas_v, verbose=a.verbose, extra_flags=extra))
+    sys.exit(0)

@@ -1,0 +1,221 @@
+// extern "C" entry points for builds, queries and contact (see include/sdfo.h).
+#include <cmath>
+#include <cstring>
+
+#include "sdfo_internal.cuh"
+
+using namespace sdfo;
+
+namespace {
+
+void check_grid(const sdfo_grid* g)
+{
+    SDFO_REQUIRE(g != nullptr, SDFO_ERR_INVALID_ARGUMENT, "grid is NULL");
+    SDFO_REQUIRE(g->stored_voxels > 0 || g->info.layout == SDFO_LAYOUT_SPARSE,
+                 SDFO_ERR_INVALID_ARGUMENT, "grid is empty");
+}
+
+void check_mesh(const double* verts, int64_t nv, const int32_t* tris, int64_t nt)
+{
+    SDFO_REQUIRE(nv > 0 && nt > 0 && verts && tris, SDFO_ERR_EMPTY_MESH,
+                 "Empty mesh provided to SdfBuilder");
+    SDFO_REQUIRE(nt < (int64_t(1) << 31) && nv < (int64_t(1) << 31), SDFO_ERR_INVALID_ARGUMENT,
+                 "mesh too large");
+    for (int64_t i = 0; i < 3 * nt; ++i)
+        SDFO_REQUIRE(tris[i] >= 0 && tris[i] < nv, SDFO_ERR_INVALID_ARGUMENT,
+                     "triangle references invalid vertex");
+    for (int64_t i = 0; i < 3 * nv; ++i)
+        SDFO_REQUIRE(std::isfinite(verts[i]), SDFO_ERR_INVALID_ARGUMENT,
+                     "vertex coordinates must be finite");
+}
+
+void check_build_params(const sdfo_build_params* p)
+{
+    SDFO_REQUIRE(p != nullptr, SDFO_ERR_INVALID_ARGUMENT, "build params are NULL");
+    SDFO_REQUIRE(p->max_resolution > 0, SDFO_ERR_INVALID_ARGUMENT, "maxResolution must be positive");
+    SDFO_REQUIRE(p->voxel_size > 0.0 || p->target_resolution > 0, SDFO_ERR_INVALID_ARGUMENT,
+                 "targetResolution must be positive when voxelSize is 0");
+    SDFO_REQUIRE(std::isfinite(p->padding) && std::isfinite(p->voxel_size),
+                 SDFO_ERR_INVALID_ARGUMENT, "padding and voxelSize must be finite");
+}
+
+} // namespace
+
+extern "C" {
+
+const char* sdfo_version(void) { return "sdfo-b200 0.1.0 (SDFO format 0.1.0)"; }
+
+int sdfo_abi_version(void) { return SDFO_ABI_VERSION; }
+
+int sdfo_device_check(int device)
+{
+    return guarded([&] {
+        int count = 0;
+        const cudaError_t e = cudaGetDeviceCount(&count);
+        if (e != cudaSuccess || count == 0)
+        {
+            (void)cudaGetLastError();
+            throw Error(SDFO_ERR_NO_DEVICE, "no CUDA device available");
+        }
+        SDFO_REQUIRE(device >= 0 && device < count, SDFO_ERR_NO_DEVICE, "device index out of range");
+        cudaDeviceProp prop;
+        SDFO_CUDA(cudaGetDeviceProperties(&prop, device));
+        SDFO_REQUIRE(prop.major == 10, SDFO_ERR_NO_DEVICE,
+                     std::string("libsdfo_cuda is built for sm_100a; device is ") + prop.name);
+    });
+}
+
+void sdfo_build_params_default(sdfo_build_params* p)
+{
+    if (!p) return;
+    p->padding = 0.1;
+    p->voxel_size = 0.0;
+    p->target_resolution = 128;
+    p->max_resolution = 512;
+}
+
+void sdfo_sparse_build_params_default(sdfo_sparse_build_params* p)
+{
+    if (!p) return;
+    sdfo_build_params_default(&p->base);
+    p->block_dim = 8;
+    p->halo_voxels = 2;
+    p->band_voxels = 8;
+    p->store_hessian = 1;
+    p->band_distance = 0.0;
+}
+
+int sdfo_setup_grid(const double* h_verts, int64_t nv, const sdfo_build_params* p,
+                    sdfo_grid_info* out)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(out != nullptr, SDFO_ERR_INVALID_ARGUMENT, "out is NULL");
+        SDFO_REQUIRE(h_verts && nv > 0, SDFO_ERR_EMPTY_MESH, "Empty mesh provided to SdfBuilder");
+        check_build_params(p);
+        *out = setup_grid(h_verts, nv, *p);
+    });
+}
+
+int sdfo_grid_build_dense(const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
+                          const sdfo_build_params* p, void* stream, sdfo_grid** out)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(out != nullptr, SDFO_ERR_INVALID_ARGUMENT, "out is NULL");
+        *out = nullptr;
+        check_mesh(h_verts, nv, h_tris, nt);
+        check_build_params(p);
+        *out = build_dense(h_verts, nv, h_tris, nt, *p, as_stream(stream));
+    });
+}
+
+int sdfo_grid_build_sparse(const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
+                           const sdfo_sparse_build_params* p, void* stream, sdfo_grid** out)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(out != nullptr, SDFO_ERR_INVALID_ARGUMENT, "out is NULL");
+        *out = nullptr;
+        check_mesh(h_verts, nv, h_tris, nt);
+        SDFO_REQUIRE(p != nullptr, SDFO_ERR_INVALID_ARGUMENT, "build params are NULL");
+        check_build_params(&p->base);
+        SDFO_REQUIRE(p->block_dim > 0, SDFO_ERR_INVALID_ARGUMENT,
+                     "Sparse SDF blockDim must be positive");
+        SDFO_REQUIRE(p->block_dim <= 16, SDFO_ERR_UNSUPPORTED, "blockDim above 16 is not provided");
+        *out = build_sparse(h_verts, nv, h_tris, nt, *p, as_stream(stream));
+    });
+}
+
+int sdfo_query(const sdfo_grid* g, int32_t mode, const void* d_points, int32_t points_f64,
+               int64_t n, float* d_gap, float* d_grad, float* d_unit, float* d_witness,
+               uint8_t* d_valid, float* d_hess, void* stream)
+{
+    return guarded([&] {
+        check_grid(g);
+        SDFO_REQUIRE(n >= 0, SDFO_ERR_INVALID_ARGUMENT, "negative query count");
+        if (n == 0) return;
+        SDFO_REQUIRE(d_points && d_gap, SDFO_ERR_INVALID_ARGUMENT, "points and gap are required");
+        SDFO_REQUIRE(mode >= SDFO_FIRST_ORDER && mode <= SDFO_CONTACT_AWARE,
+                     SDFO_ERR_INVALID_ARGUMENT, "unknown query mode");
+        SDFO_REQUIRE(n <= (int64_t)65535 * 256 * 4096, SDFO_ERR_INVALID_ARGUMENT, "too many queries");
+        const QueryOutputs o{d_gap, d_grad, d_unit, d_witness, d_valid, d_hess};
+        launch_query(make_view(g), mode, d_points, points_f64 != 0, n, o, as_stream(stream));
+    });
+}
+
+int sdfo_query_host(const sdfo_grid* g, int32_t mode, const void* h_points, int32_t points_f64,
+                    int64_t n, float* h_gap, float* h_grad, float* h_unit, float* h_witness,
+                    uint8_t* h_valid, void* stream)
+{
+    return guarded([&] {
+        check_grid(g);
+        SDFO_REQUIRE(n >= 0, SDFO_ERR_INVALID_ARGUMENT, "negative query count");
+        if (n == 0) return;
+        SDFO_REQUIRE(h_points && h_gap, SDFO_ERR_INVALID_ARGUMENT, "points and gap are required");
+        SDFO_REQUIRE(mode >= SDFO_FIRST_ORDER && mode <= SDFO_CONTACT_AWARE,
+                     SDFO_ERR_INVALID_ARGUMENT, "unknown query mode");
+        cudaStream_t s = as_stream(stream);
+        const size_t pb = (size_t)n * 3 * (points_f64 ? sizeof(double) : sizeof(float));
+        DeviceBuffer<unsigned char> pts(pb);
+        DeviceBuffer<float> gap((size_t)n), grad(h_grad ? 3 * (size_t)n : 0),
+            unit(h_unit ? 3 * (size_t)n : 0), wit(h_witness ? 3 * (size_t)n : 0);
+        DeviceBuffer<uint8_t> valid(h_valid ? (size_t)n : 0);
+        SDFO_CUDA(cudaMemcpyAsync(pts.get(), h_points, pb, cudaMemcpyHostToDevice, s));
+        const QueryOutputs o{gap.get(), grad.get(), unit.get(), wit.get(), valid.get(), nullptr};
+        launch_query(make_view(g), mode, pts.get(), points_f64 != 0, n, o, s);
+        SDFO_CUDA(cudaMemcpyAsync(h_gap, gap.get(), sizeof(float) * n, cudaMemcpyDeviceToHost, s));
+        if (h_grad)
+            SDFO_CUDA(cudaMemcpyAsync(h_grad, grad.get(), sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
+        if (h_unit)
+            SDFO_CUDA(cudaMemcpyAsync(h_unit, unit.get(), sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
+        if (h_witness)
+            SDFO_CUDA(cudaMemcpyAsync(h_witness, wit.get(), sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
+        if (h_valid)
+            SDFO_CUDA(cudaMemcpyAsync(h_valid, valid.get(), n, cudaMemcpyDeviceToHost, s));
+        SDFO_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int sdfo_query_backward(const sdfo_grid* g, int32_t mode, const float* d_points, int64_t n,
+                        const float* d_dgap, const float* d_dgrad, float* d_dpoints,
+                        float* d_dgrid, void* stream)
+{
+    return guarded([&] {
+        check_grid(g);
+        SDFO_REQUIRE(n >= 0, SDFO_ERR_INVALID_ARGUMENT, "negative query count");
+        if (n == 0) return;
+        SDFO_REQUIRE(d_points != nullptr, SDFO_ERR_INVALID_ARGUMENT, "points are required");
+        SDFO_REQUIRE(mode == SDFO_TRILINEAR || mode == SDFO_TRICUBIC, SDFO_ERR_UNSUPPORTED,
+                     "query backward supports Trilinear and Tricubic");
+        SDFO_REQUIRE(d_dgrid == nullptr || g->info.storage == SDFO_STORAGE_FP32, SDFO_ERR_UNSUPPORTED,
+                     "grid gradients need FP32 storage");
+        SDFO_REQUIRE((reinterpret_cast<uintptr_t>(d_dgrid) & 15) == 0, SDFO_ERR_INVALID_ARGUMENT,
+                     "grid gradient buffer must be 16-byte aligned");
+        launch_query_backward(make_view(g), mode, d_points, n, d_dgap, d_dgrad, d_dpoints, d_dgrid,
+                              as_stream(stream));
+    });
+}
+
+int sdfo_contact_eval(const sdfo_grid* g, int32_t mode, const float* d_quad_x,
+                      const float* d_quad_w, int64_t nq, const sdfo_body_state* d_pose_a,
+                      int64_t np, const sdfo_body_state* d_body_b,
+                      const sdfo_contact_params* h_params, double* d_ft, double* d_jac,
+                      void* stream)
+{
+    return guarded([&] {
+        check_grid(g);
+        SDFO_REQUIRE(h_params != nullptr, SDFO_ERR_INVALID_ARGUMENT, "contact params are NULL");
+        SDFO_REQUIRE(mode == SDFO_TRILINEAR || mode == SDFO_TRICUBIC, SDFO_ERR_UNSUPPORTED,
+                     "contact supports Trilinear and Tricubic");
+        SDFO_REQUIRE(nq >= 0 && np >= 0, SDFO_ERR_INVALID_ARGUMENT, "negative count");
+        if (np == 0) return;
+        SDFO_REQUIRE(d_pose_a && d_body_b && d_ft, SDFO_ERR_INVALID_ARGUMENT,
+                     "poses, body B and the force output are required");
+        SDFO_REQUIRE(nq == 0 || (d_quad_x && d_quad_w), SDFO_ERR_INVALID_ARGUMENT,
+                     "quadrature points and weights are required");
+        SDFO_REQUIRE(np <= 0x7fffffff && nq <= 0x7fffffff, SDFO_ERR_INVALID_ARGUMENT,
+                     "too many poses or points");
+        launch_contact(make_view(g), mode, d_quad_x, d_quad_w, nq, d_pose_a, np, d_body_b,
+                       *h_params, d_ft, d_jac, as_stream(stream));
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,316 @@
+// Device-side grid addressing and interpolants shared by the query, backward
+// and contact kernels.
+//
+// Interpolants restate the reference's SdfOracle query modes:
+//   trilinear  - SdfOracle.cpp:524-596 (8-corner lerp of phi, analytic gradient)
+//   tricubic   - SdfOracle.cpp:932-1092 (tensor cubic Hermite over the 8 cell
+//                corners with values phi and slopes n*h; no cross terms)
+//   first/second order - SdfOracle.cpp:448-520 (Taylor at the nearest voxel)
+// Arithmetic is FP32 (storage is FP32/FP16); the cell index and fractional
+// coordinate are computed in FP64 exactly as the reference does,
+// f = (p - bmin) / voxel - 0.5, so every query selects the reference's cell.
+#pragma once
+
+#include "sdfo_internal.cuh"
+
+namespace sdfo {
+
+struct Cell
+{
+    int i0, j0, k0;  // lower corner (trilinear/tricubic) or nearest voxel
+    float u, v, w;   // fractional position in the cell
+    bool ok;         // inside the index domain
+};
+
+// Fractional grid coordinate as in GridSpec/trilinearQuery:
+// f = (p - bmin).cwiseQuotient(voxel) - 0.5.
+__device__ __forceinline__ double frac_coord(double p, double bmin, double voxel)
+{
+    return (p - bmin) / voxel - 0.5;
+}
+
+// Lower-corner cell of p; ok iff i0 >= 0 and i0 + 1 < n on every axis.
+__device__ __forceinline__ Cell cell_of(const GridView& g, const double p[3])
+{
+    Cell c;
+    double f[3];
+    int lo[3];
+    bool ok = true;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    float fr[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        f[a] = frac_coord(p[a], g.bmin[a], g.voxel[a]);
+        // NaN / huge coordinates are outside the domain.
+        if (!(f[a] >= -1.0 && f[a] < (double)n[a]))
+        {
+            ok = false;
+            lo[a] = 0;
+            fr[a] = 0.f;
+            continue;
+        }
+        const double fl = floor(f[a]);
+        lo[a] = (int)fl;
+        fr[a] = (float)(f[a] - fl);
+        ok = ok && lo[a] >= 0 && lo[a] + 1 < n[a];
+    }
+    c.i0 = lo[0];
+    c.j0 = lo[1];
+    c.k0 = lo[2];
+    c.u = fr[0];
+    c.v = fr[1];
+    c.w = fr[2];
+    c.ok = ok;
+    return c;
+}
+
+// Nearest voxel (GridSpec::indexFromWorld, GridSpec.h:37-45) with its
+// in-bounds flag; dx = p - centre (FP64 then FP32).
+__device__ __forceinline__ bool nearest_voxel(const GridView& g, const double p[3], int ijk[3],
+                                              float dx[3])
+{
+    const int n[3] = {g.nx, g.ny, g.nz};
+    bool ok = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        const double f = frac_coord(p[a], g.bmin[a], g.voxel[a]);
+        if (!(f > -1.0 && f < (double)n[a] + 1.0))
+        {
+            ok = false;
+            ijk[a] = 0;
+            dx[a] = 0.f;
+            continue;
+        }
+        ijk[a] = (int)round(f);
+        ok = ok && ijk[a] >= 0 && ijk[a] < n[a];
+        const double c = g.bmin[a] + g.voxel[a] * (ijk[a] + 0.5);
+        dx[a] = (float)(p[a] - c);
+    }
+    return ok;
+}
+
+__device__ __forceinline__ int64_t dense_index(const GridView& g, int i, int j, int k)
+{
+    return (int64_t)i + (int64_t)g.nx * ((int64_t)j + (int64_t)g.ny * (int64_t)k);
+}
+
+// Stored-voxel index of (i,j,k) in a sparse grid or -1 when its block is not
+// stored (SparseSdfData::blockForVoxel + sampleFromBlock, SdfData.h:224-302).
+// BD = block_dim when known at compile time, 0 for the runtime value.
+template <int BD>
+__device__ __forceinline__ int64_t sparse_index(const GridView& g, int i, int j, int k)
+{
+    const int bd = BD > 0 ? BD : g.bd;
+    const int bi = i / bd, bj = j / bd, bk = k / bd;
+    const int slot = __ldg(g.table + bi + g.nbx * (bj + g.nby * bk));
+    if (slot < 0) return -1;
+    const int local = (i - bi * bd) + bd * ((j - bj * bd) + bd * (k - bk * bd));
+    return (int64_t)slot * (bd * bd * bd) + local;
+}
+
+// FP16 payload: {phi_q, nx, ny, nz} halves; phi = phi_q * scale + offset.
+__device__ __forceinline__ float4 decode_fp16(ushort4 q, float2 aff)
+{
+    float4 r;
+    r.x = __half2float(__ushort_as_half(q.x)) * aff.x + aff.y;
+    r.y = __half2float(__ushort_as_half(q.y));
+    r.z = __half2float(__ushort_as_half(q.z));
+    r.w = __half2float(__ushort_as_half(q.w));
+    return r;
+}
+
+template <int BD>
+__device__ __forceinline__ float4 load_stored(const GridView& g, int64_t idx)
+{
+    if (g.storage == SDFO_STORAGE_FP16)
+    {
+        const int V = (BD > 0 ? BD : g.bd);
+        const int64_t brick = idx / (V * V * V);
+        return decode_fp16(__ldg(g.phin16 + idx), __ldg(g.brick_affine + brick));
+    }
+    return __ldg(g.phin + idx);
+}
+
+// Gathers the 8 cell corners (corner c = di + 2 dj + 4 dk) as {phi, n}.
+// Returns false when a sparse corner's block is missing.
+template <bool SPARSE, int BD>
+__device__ __forceinline__ bool gather_corners(const GridView& g, const Cell& c, float4 out[8],
+                                               int64_t idx[8])
+{
+    if (!SPARSE)
+    {
+        const int64_t base = dense_index(g, c.i0, c.j0, c.k0);
+        const int64_t sx = 1, sy = g.nx, sz = (int64_t)g.nx * g.ny;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+        {
+            idx[q] = base + ((q & 1) ? sx : 0) + ((q & 2) ? sy : 0) + ((q & 4) ? sz : 0);
+            out[q] = __ldg(g.phin + idx[q]);
+        }
+        return true;
+    }
+    bool ok = true;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+    {
+        idx[q] = sparse_index<BD>(g, c.i0 + (q & 1), c.j0 + ((q >> 1) & 1), c.k0 + (q >> 2));
+        ok = ok && idx[q] >= 0;
+    }
+    if (!ok) return false;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) out[q] = load_stored<BD>(g, idx[q]);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// cubic Hermite basis: h00, h10, h01, h11 and their first/second derivatives
+// (SdfOracle.cpp:976-1012 for the values and first derivatives).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void hermite(float t, float b[4], float d[4])
+{
+    const float t2 = t * t;
+    b[0] = t2 * (2.f * t - 3.f) + 1.f;
+    b[1] = t * (t * (t - 2.f) + 1.f);
+    b[2] = t2 * (3.f - 2.f * t);
+    b[3] = t2 * (t - 1.f);
+    d[0] = 6.f * t * (t - 1.f);
+    d[1] = t * (3.f * t - 4.f) + 1.f;
+    d[2] = 6.f * t * (1.f - t);
+    d[3] = t * (3.f * t - 2.f);
+}
+__device__ __forceinline__ void hermite2(float t, float s[4])
+{
+    s[0] = 12.f * t - 6.f;
+    s[1] = 6.f * t - 4.f;
+    s[2] = 6.f - 12.f * t;
+    s[3] = 6.f * t - 2.f;
+}
+
+// x-collapse of the tensor Hermite interpolant for each (dj,dk) corner pair:
+// X0 = sum_di P0 phi + P1 gx,  Xy = sum_di P0 gy,  Xz = sum_di P0 gz.
+struct XColl
+{
+    float x0[4], xy[4], xz[4];
+};
+
+__device__ __forceinline__ XColl collapse_x(const float bx[4], const float phi[8],
+                                            const float gx[8], const float gy[8],
+                                            const float gz[8])
+{
+    XColl r;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+    {
+        const int c0 = 2 * q, c1 = 2 * q + 1;
+        r.x0[q] = bx[0] * phi[c0] + bx[1] * gx[c0] + bx[2] * phi[c1] + bx[3] * gx[c1];
+        r.xy[q] = bx[0] * gy[c0] + bx[2] * gy[c1];
+        r.xz[q] = bx[0] * gz[c0] + bx[2] * gz[c1];
+    }
+    return r;
+}
+
+// yz-collapse: sum_dk R0 (sum_dj Q0 X0 + Q1 Xy) + R1 (sum_dj Q0 Xz).
+__device__ __forceinline__ float collapse_yz(const XColl& x, const float by[4], const float bz[4])
+{
+    float y0[2], yz[2];
+#pragma unroll
+    for (int dk = 0; dk < 2; ++dk)
+    {
+        const int q0 = 2 * dk, q1 = 2 * dk + 1;
+        y0[dk] = by[0] * x.x0[q0] + by[1] * x.xy[q0] + by[2] * x.x0[q1] + by[3] * x.xy[q1];
+        yz[dk] = by[0] * x.xz[q0] + by[2] * x.xz[q1];
+    }
+    return bz[0] * y0[0] + bz[1] * yz[0] + bz[2] * y0[1] + bz[3] * yz[1];
+}
+
+struct Interp
+{
+    float gap;
+    float g[3];   // raw gradient
+    float H[6];   // xx, xy, xz, yy, yz, zz
+};
+
+// Tricubic Hermite (SdfOracle.cpp:932-1092) over corners {phi, n}; slopes
+// n * h; gradient = d/du / h; optional Hessian.
+template <bool HESS>
+__device__ __forceinline__ Interp tricubic(const float4 c[8], float u, float v, float w,
+                                           const float h[3])
+{
+    float phi[8], gx[8], gy[8], gz[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+    {
+        phi[q] = c[q].x;
+        gx[q] = c[q].y * h[0];
+        gy[q] = c[q].z * h[1];
+        gz[q] = c[q].w * h[2];
+    }
+    float bx[4], dx[4], by[4], dy[4], bz[4], dz[4];
+    hermite(u, bx, dx);
+    hermite(v, by, dy);
+    hermite(w, bz, dz);
+    const XColl xa = collapse_x(bx, phi, gx, gy, gz);
+    const XColl xd = collapse_x(dx, phi, gx, gy, gz);
+    Interp r;
+    r.gap = collapse_yz(xa, by, bz);
+    r.g[0] = collapse_yz(xd, by, bz) / h[0];
+    r.g[1] = collapse_yz(xa, dy, bz) / h[1];
+    r.g[2] = collapse_yz(xa, by, dz) / h[2];
+    if (HESS)
+    {
+        float sx[4], sy[4], sz[4];
+        hermite2(u, sx);
+        hermite2(v, sy);
+        hermite2(w, sz);
+        const XColl xs = collapse_x(sx, phi, gx, gy, gz);
+        r.H[0] = collapse_yz(xs, by, bz) / (h[0] * h[0]);
+        r.H[1] = collapse_yz(xd, dy, bz) / (h[0] * h[1]);
+        r.H[2] = collapse_yz(xd, by, dz) / (h[0] * h[2]);
+        r.H[3] = collapse_yz(xa, sy, bz) / (h[1] * h[1]);
+        r.H[4] = collapse_yz(xa, dy, dz) / (h[1] * h[2]);
+        r.H[5] = collapse_yz(xa, by, sz) / (h[2] * h[2]);
+    }
+    else
+    {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) r.H[q] = 0.f;
+    }
+    return r;
+}
+
+__device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(t, b - a, a); }
+
+// Trilinear (SdfOracle.cpp:551-583) over corner phi; optional mixed second
+// derivatives (the diagonal ones are zero).
+template <bool HESS>
+__device__ __forceinline__ Interp trilinear(const float c[8], float u, float v, float w,
+                                            const float h[3])
+{
+    Interp r;
+    const float c00 = lerpf(c[0], c[1], u), c10 = lerpf(c[2], c[3], u);
+    const float c01 = lerpf(c[4], c[5], u), c11 = lerpf(c[6], c[7], u);
+    r.gap = lerpf(lerpf(c00, c10, v), lerpf(c01, c11, v), w);
+    // x differences at (j,k), y differences at (i,k), z differences at (i,j)
+    const float dx00 = c[1] - c[0], dx10 = c[3] - c[2], dx01 = c[5] - c[4], dx11 = c[7] - c[6];
+    const float dy00 = c[2] - c[0], dy10 = c[3] - c[1], dy01 = c[6] - c[4], dy11 = c[7] - c[5];
+    const float dz00 = c[4] - c[0], dz10 = c[5] - c[1], dz01 = c[6] - c[2], dz11 = c[7] - c[3];
+    r.g[0] = lerpf(lerpf(dx00, dx10, v), lerpf(dx01, dx11, v), w) / h[0];
+    r.g[1] = lerpf(lerpf(dy00, dy10, u), lerpf(dy01, dy11, u), w) / h[1];
+    r.g[2] = lerpf(lerpf(dz00, dz10, u), lerpf(dz01, dz11, u), v) / h[2];
+    r.H[0] = r.H[3] = r.H[5] = 0.f;
+    if (HESS)
+    {
+        r.H[1] = lerpf(dx10 - dx00, dx11 - dx01, w) / (h[0] * h[1]);
+        r.H[2] = lerpf(dx01 - dx00, dx11 - dx10, v) / (h[0] * h[2]);
+        r.H[4] = lerpf(dy01 - dy00, dy11 - dy10, u) / (h[1] * h[2]);
+    }
+    else
+    {
+        r.H[1] = r.H[2] = r.H[4] = 0.f;
+    }
+    return r;
+}
+
+} // namespace sdfo

@@ -1,0 +1,192 @@
+// Internal declarations shared by the libsdfo_cuda translation units.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "sdfo.h"
+
+namespace sdfo {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+struct Error
+{
+    int code;
+    std::string msg;
+    Error(int c, std::string m) : code(c), msg(std::move(m)) {}
+};
+
+void set_last_error(const std::string& msg);
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line);
+
+#define SDFO_CUDA(call)                                                                  \
+    do                                                                                   \
+    {                                                                                    \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) ::sdfo::throw_cuda(e_, #call, __FILE__, __LINE__);        \
+    } while (0)
+
+#define SDFO_CHECK_LAUNCH() SDFO_CUDA(cudaGetLastError())
+
+#define SDFO_REQUIRE(cond, code, msg)                                                    \
+    do                                                                                   \
+    {                                                                                    \
+        if (!(cond)) throw ::sdfo::Error((code), (msg));                                 \
+    } while (0)
+
+// Runs f() and converts exceptions into a status code + last-error message.
+template <class F>
+int guarded(F&& f)
+{
+    try
+    {
+        f();
+        return SDFO_OK;
+    }
+    catch (const Error& e)
+    {
+        set_last_error(e.msg);
+        return e.code;
+    }
+    catch (const std::bad_alloc&)
+    {
+        set_last_error("host out of memory");
+        return SDFO_ERR_OUT_OF_MEMORY;
+    }
+    catch (const std::exception& e)
+    {
+        set_last_error(e.what());
+        return SDFO_ERR_INVALID_ARGUMENT;
+    }
+}
+
+// Device allocation owned by a grid handle.
+void* device_alloc(size_t bytes);
+void device_free(void* p);
+
+template <class T>
+T* dalloc(size_t count)
+{
+    return static_cast<T*>(device_alloc(count * sizeof(T)));
+}
+
+inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+// Scoped device buffer for temporaries inside one call.
+template <class T>
+struct DeviceBuffer
+{
+    T* p = nullptr;
+    size_t n = 0;
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(size_t count) { reset(count); }
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { device_free(p); }
+    void reset(size_t count)
+    {
+        device_free(p);
+        p = count ? dalloc<T>(count) : nullptr;
+        n = count;
+    }
+    T* get() const { return p; }
+};
+
+// ---------------------------------------------------------------------------
+// grid storage
+// ---------------------------------------------------------------------------
+// Device payload of a grid.  Dense: one float4 {phi, n} per voxel, x-fastest,
+// plus optional FP32 Hessians and the FP64 build results for exact export.
+// Sparse: bricks of block_dim^3 voxels in stored order (local index
+// lx + bd*(ly + bd*lz)), a dense int32 table over block coordinates, and the
+// block coordinates.  FP16 sparse storage keeps {phi_q, nx, ny, nz} as four
+// halves per voxel and a float2 {scale, offset} per brick.
+struct GridStorage
+{
+    float4* phin = nullptr;
+    float* hess6 = nullptr;
+    double* phi64 = nullptr;
+    double* n64 = nullptr;
+    double* w64 = nullptr;
+    double* h64 = nullptr;
+    int32_t* table = nullptr;
+    int32_t* ijk = nullptr;
+    ushort4* phin16 = nullptr;
+    float2* brick_affine = nullptr;
+};
+
+} // namespace sdfo
+
+struct sdfo_grid
+{
+    sdfo_grid_info info{};
+    sdfo::GridStorage d{};
+    sdfo_build_stats stats{};
+    int device = 0;
+    int64_t stored_voxels = 0;
+    int32_t nb[3] = {0, 0, 0};
+    bool borrowed = false; // a view: storage belongs to another handle / caller
+    ~sdfo_grid();
+};
+
+namespace sdfo {
+
+// Kernel-side view of a grid (passed by value).
+struct GridView
+{
+    double bmin[3];
+    double voxel[3];
+    int nx, ny, nz;
+    int layout;  // SDFO_LAYOUT_*
+    int storage; // SDFO_STORAGE_*
+    int has_hessian;
+    const float4* phin;
+    const float* hess6;
+    const int32_t* table;
+    int nbx, nby, nbz;
+    int bd;
+    const ushort4* phin16;
+    const float2* brick_affine;
+};
+
+GridView make_view(const sdfo_grid* g);
+
+// Query launch (query.cu).
+struct QueryOutputs
+{
+    float* gap;
+    float* grad;
+    float* unit;
+    float* witness;
+    uint8_t* valid;
+    float* hess;
+};
+void launch_query(const GridView& v, int mode, const void* pts, bool f64, int64_t n,
+                  const QueryOutputs& o, cudaStream_t s);
+void launch_query_backward(const GridView& v, int mode, const float* pts, int64_t n,
+                           const float* dgap, const float* dgrad, float* dpts, float* dgrid,
+                           cudaStream_t s);
+
+// Builders (build.cu).
+sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
+                       const sdfo_build_params& p, cudaStream_t s);
+sdfo_grid* build_sparse(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
+                        const sdfo_sparse_build_params& p, cudaStream_t s);
+sdfo_grid_info setup_grid(const double* verts, int64_t nv, const sdfo_build_params& p);
+
+// Contact (contact.cu).
+void launch_contact(const GridView& v, int mode, const float* qx, const float* qw, int64_t nq,
+                    const sdfo_body_state* pose_a, int64_t np, const sdfo_body_state* body_b,
+                    const sdfo_contact_params& prm, double* ft, double* jac, cudaStream_t s);
+
+// FP16 re-encoding (grid.cu).
+void encode_fp16(const sdfo_grid* src, sdfo_grid* dst, cudaStream_t s);
+
+} // namespace sdfo

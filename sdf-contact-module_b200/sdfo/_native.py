@@ -1,0 +1,156 @@
+"""ctypes binding to libsdfo_cuda.so (the C ABI declared in include/sdfo.h).
+
+The library is built in-tree (``sdf-contact-module_b200/lib``) by
+``__graft_entry__.build()`` or ``python sdf-contact-module_b200/build.py``.
+There is no CPU fallback: every entry point raises when the library is
+missing or the call fails.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libsdfo_cuda.so")
+
+SDFO_OK = 0
+FIRST_ORDER, SECOND_ORDER, TRILINEAR, TRICUBIC, CONTACT_AWARE = 0, 1, 2, 3, 4
+LAYOUT_DENSE, LAYOUT_SPARSE = 1, 2
+STORAGE_FP32, STORAGE_FP16 = 0, 1
+
+MODE_NAMES = {"first_order": FIRST_ORDER, "second_order": SECOND_ORDER,
+              "trilinear": TRILINEAR, "tricubic": TRICUBIC, "contact_aware": CONTACT_AWARE,
+              "FirstOrder": FIRST_ORDER, "SecondOrder": SECOND_ORDER, "Trilinear": TRILINEAR,
+              "Tricubic": TRICUBIC, "ContactAware": CONTACT_AWARE}
+
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+
+
+class GridInfo(ctypes.Structure):
+    _fields_ = [("bmin", _D * 3), ("bmax", _D * 3), ("voxel", _D * 3), ("shape", _I32 * 3),
+                ("layout", _I32), ("storage", _I32), ("has_hessian", _I32), ("block_dim", _I32),
+                ("halo_voxels", _I32), ("block_count", _I32), ("reserved0", _I32),
+                ("band_distance", _D)]
+
+
+class BuildParams(ctypes.Structure):
+    _fields_ = [("padding", _D), ("voxel_size", _D), ("target_resolution", _I32),
+                ("max_resolution", _I32)]
+
+
+class SparseBuildParams(ctypes.Structure):
+    _fields_ = [("base", BuildParams), ("block_dim", _I32), ("halo_voxels", _I32),
+                ("band_voxels", _I32), ("store_hessian", _I32), ("band_distance", _D)]
+
+
+class BodyState(ctypes.Structure):
+    _fields_ = [("r", _D * 3), ("R", _D * 9), ("v", _D * 3), ("w", _D * 3)]
+
+
+class ContactParams(ctypes.Structure):
+    _fields_ = [("stiffness", _D), ("order", _D), ("damping", _D), ("friction", _D),
+                ("regularizer", _D), ("activation_distance", _D)]
+
+
+class BuildStats(ctypes.Structure):
+    _fields_ = [("setup_ms", _D), ("bvh_ms", _D), ("fill_ms", _D), ("hessian_ms", _D),
+                ("total_ms", _D), ("voxels_filled", _I64), ("candidate_blocks", _I64),
+                ("triangles", _I32), ("bvh_nodes", _I32)]
+
+
+class DeviceViews(ctypes.Structure):
+    _fields_ = [("phin", _P), ("hessian6", _P), ("table", _P), ("block_ijk", _P),
+                ("stored_voxels", _I64), ("table_dims", _I32 * 3), ("reserved0", _I32)]
+
+
+# (name, restype, argtypes) of every exported function in include/sdfo.h
+SIGNATURES = [
+    ("sdfo_version", ctypes.c_char_p, []),
+    ("sdfo_abi_version", ctypes.c_int, []),
+    ("sdfo_last_error", ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
+    ("sdfo_device_check", ctypes.c_int, [ctypes.c_int]),
+    ("sdfo_build_params_default", None, [ctypes.POINTER(BuildParams)]),
+    ("sdfo_sparse_build_params_default", None, [ctypes.POINTER(SparseBuildParams)]),
+    ("sdfo_setup_grid", ctypes.c_int, [_P, _I64, ctypes.POINTER(BuildParams), ctypes.POINTER(GridInfo)]),
+    ("sdfo_grid_build_dense", ctypes.c_int,
+     [_P, _I64, _P, _I64, ctypes.POINTER(BuildParams), _P, ctypes.POINTER(_P)]),
+    ("sdfo_grid_build_sparse", ctypes.c_int,
+     [_P, _I64, _P, _I64, ctypes.POINTER(SparseBuildParams), _P, ctypes.POINTER(_P)]),
+    ("sdfo_grid_build_stats", ctypes.c_int, [_P, ctypes.POINTER(BuildStats)]),
+    ("sdfo_grid_create_dense", ctypes.c_int,
+     [ctypes.POINTER(GridInfo), _P, _P, _P, _P, _P, ctypes.POINTER(_P)]),
+    ("sdfo_grid_create_sparse", ctypes.c_int,
+     [ctypes.POINTER(GridInfo), _P, _P, _P, _P, _P, ctypes.POINTER(_P)]),
+    ("sdfo_grid_to_fp16", ctypes.c_int, [_P, _P, ctypes.POINTER(_P)]),
+    ("sdfo_grid_export_dense", ctypes.c_int, [_P, _P, _P, _P, _P]),
+    ("sdfo_grid_export_sparse", ctypes.c_int, [_P, _P, _P, _P, _P]),
+    ("sdfo_grid_copy_payload", ctypes.c_int, [_P, _P, _P]),
+    ("sdfo_grid_create_view", ctypes.c_int, [_P, _P, ctypes.POINTER(_P)]),
+    ("sdfo_grid_get_info", ctypes.c_int, [_P, ctypes.POINTER(GridInfo)]),
+    ("sdfo_grid_device_views", ctypes.c_int, [_P, ctypes.POINTER(DeviceViews)]),
+    ("sdfo_grid_destroy", ctypes.c_int, [_P]),
+    ("sdfo_query", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P, _P, _P, _P]),
+    ("sdfo_query_host", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P, _P, _P]),
+    ("sdfo_query_backward", ctypes.c_int, [_P, _I32, _P, _I64, _P, _P, _P, _P, _P]),
+    ("sdfo_contact_eval", ctypes.c_int,
+     [_P, _I32, _P, _P, _I64, _P, _I64, _P, ctypes.POINTER(ContactParams), _P, _P, _P]),
+]
+
+_lib = None
+
+
+class SdfoError(RuntimeError):
+    """A libsdfo_cuda call returned a non-zero status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[sdfo {code}] {msg}")
+        self.code = code
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def load(path: str | None = None):
+    """Loads libsdfo_cuda.so (raises FileNotFoundError when it is not built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise FileNotFoundError(
+            f"libsdfo_cuda.so not found at {p}; build it with "
+            "`python sdf-contact-module_b200/build.py` (no CPU fallback exists)")
+    lib = ctypes.CDLL(p)
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(1024)
+    load().sdfo_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(code: int) -> None:
+    if code != SDFO_OK:
+        raise SdfoError(code, last_error())
+
+
+def mode_id(mode) -> int:
+    if isinstance(mode, str):
+        if mode not in MODE_NAMES:
+            raise ValueError(f"unknown query mode {mode!r}")
+        return MODE_NAMES[mode]
+    m = int(mode)
+    if m < 0 or m > 4:
+        raise ValueError(f"unknown query mode {mode!r}")
+    return m

@@ -1,0 +1,117 @@
+"""Seeded synthetic inputs of the five benchmark configurations.
+
+No dataset or mesh ships with the reference for these workloads, so every
+input is generated here from a fixed seed (numpy default_rng):
+
+  C1 cube64      cube 0.1 m, 12 tris, dense 64^3 with 4 voxels of padding;
+                 100k uniform points in the padded box (seed 0), Trilinear.
+  C2 cylinder    hollow cylinder R 50 / r 40 / H 20 mm, 512 x 16 segments
+                 (34,816 tris); dense 128^3 (snapped to 128x128x64) and
+                 sparse band 3 voxels, 8^3 bricks; 1M Tricubic points on the
+                 surface offset along the normal by N(0, (2h)^2) (seed 1).
+  C3 ring-cube   cube 100 mm at 128^3; torus R 50 / r 10 mm, 192 x 20
+                 (7,680 tris) as quadrature body; 4096 poses (seed 2).
+  C4 gears       256 star-profile gear prisms, sparse grids (seed 3).
+  C5 icosphere   perturbed icosphere (1.31M tris), sparse 512^3 (seed 4).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import meshes as M
+
+CUBE_SIDE = 0.1
+
+
+def c1_cube64(n_points=100_000, seed=0):
+    v, t = M.cube(CUBE_SIDE)
+    h = CUBE_SIDE / 56.0
+    params = dict(voxel_size=h, padding=4.0 * h / (CUBE_SIDE * math.sqrt(3.0)),
+                  target_resolution=64, max_resolution=64)
+    return dict(name="cube64", verts=v, tris=t, build=params, n_points=n_points, seed=seed)
+
+
+def c1_points(grid_bmin, grid_bmax, n=100_000, seed=0):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(grid_bmin, grid_bmax, size=(n, 3)).astype(np.float32)
+
+
+def c2_cylinder():
+    v, t = M.hollow_cylinder(0.05, 0.04, 0.02, n_az=512, n_vert=16, n_rad=1)
+    dense = dict(target_resolution=128, max_resolution=128, padding=0.1)
+    sparse = dict(dense, block_dim=8, band_voxels=3, halo_voxels=2)
+    return dict(name="hollow_cylinder", verts=v, tris=t, dense=dense, sparse=sparse)
+
+
+def c2_points(verts, tris, voxel, n=1_000_000, seed=1):
+    rng = np.random.default_rng(seed)
+    return M.surface_points(verts, tris, n, 2.0 * voxel, rng).astype(np.float32)
+
+
+def c3_ring_cube(n_poses=4096, seed=2):
+    cv, ct = M.cube(CUBE_SIDE)
+    tv, tt = M.torus(0.05, 0.01, 192, 20)
+    qx, qw = M.centroid_quadrature(tv, tt)
+    rng = np.random.default_rng(seed)
+    z = rng.uniform(0.060, 0.070, n_poses)
+    phi = rng.uniform(0.0, 2.0 * np.pi, n_poses)
+    ang = np.deg2rad(5.0) * rng.uniform(0.0, 1.0, n_poses)
+    axis = np.stack([np.cos(phi), np.sin(phi), np.zeros(n_poses)], 1)
+    R = _axis_angle(axis, ang)
+
+    def ball(radius):
+        d = rng.normal(size=(n_poses, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        return d * (radius * rng.uniform(0.0, 1.0, n_poses) ** (1.0 / 3.0))[:, None]
+
+    v = ball(0.1)
+    w = ball(1.0)
+    r = np.stack([np.zeros(n_poses), np.zeros(n_poses), z], 1)
+    return dict(name="ring_on_cube", cube=(cv, ct), torus=(tv, tt), quad_x=qx, quad_w=qw,
+                build=dict(target_resolution=128, max_resolution=128, padding=0.1),
+                r=r, R=R, v=v, w=w,
+                params=dict(stiffness=1e11, order=2.0, damping=1e4, friction=0.3,
+                            regularizer=1e-4, activation_distance=1e-5))
+
+
+def _axis_angle(axis, ang):
+    k = axis / np.maximum(np.linalg.norm(axis, axis=1, keepdims=True), 1e-300)
+    K = np.zeros((len(k), 3, 3))
+    K[:, 0, 1], K[:, 0, 2] = -k[:, 2], k[:, 1]
+    K[:, 1, 0], K[:, 1, 2] = k[:, 2], -k[:, 0]
+    K[:, 2, 0], K[:, 2, 1] = -k[:, 1], k[:, 0]
+    s, c = np.sin(ang)[:, None, None], np.cos(ang)[:, None, None]
+    return np.eye(3)[None] + s * K + (1 - c) * (K @ K)
+
+
+def c4_gears(n_gears=256, seed=3):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_gears):
+        teeth = int(rng.integers(20, 61))
+        r_out = float(rng.uniform(0.020, 0.080))
+        thick = float(rng.uniform(0.005, 0.020))
+        target = int(round(math.exp(rng.uniform(math.log(2000), math.log(60000)))))
+        res = int(rng.choice([64, 96, 128, 192, 256]))
+        v, t = M.gear_prism(teeth, r_out, thick, target)
+        out.append(dict(verts=v, tris=t, teeth=teeth, r_outer=r_out, thickness=thick,
+                        resolution=res,
+                        sparse=dict(target_resolution=res, max_resolution=res, padding=0.1,
+                                    block_dim=8, band_voxels=3, halo_voxels=2)))
+    return out
+
+
+def c5_icosphere(subdivisions=8, seed=4):
+    v, t = M.perturbed_icosphere(subdivisions, 0.1, 0.002, 8, 1, 6, seed)
+    return dict(name="perturbed_icosphere", verts=v, tris=t,
+                sparse=dict(target_resolution=512, max_resolution=512, padding=0.1, block_dim=8,
+                            band_voxels=3, halo_voxels=2))
+
+
+def near_surface_points(verts, tris, voxel, n, seed, band_voxels=4.0):
+    """Surface points offset along the normal by U(-band*h, band*h)."""
+    rng = np.random.default_rng(seed)
+    return M.surface_points(verts, tris, n, band_voxels * voxel, rng,
+                            uniform_offset=True).astype(np.float32)
