@@ -60,6 +60,15 @@ extern "C" {
 #define SDFO_STORAGE_FP32 0
 #define SDFO_STORAGE_FP16 1 /* sparse only: per-brick affine phi + fp16 normal */
 
+/* Triangle acceleration structure used by the builders. */
+#define SDFO_BVH_REFERENCE 0 /* the reference's median-split tree (host-built),
+                                traversed on the device in its order: results
+                                identical to the reference incl. exact ties */
+#define SDFO_BVH_LBVH 1      /* device-built linear BVH: fastest build; exactly
+                                equidistant triangles resolve to the lowest
+                                index, so witness/normal at such ties and the
+                                face-normal sign fallback may differ */
+
 /* Point precision for query inputs. */
 #define SDFO_POINTS_F32 0
 #define SDFO_POINTS_F64 1
@@ -180,6 +189,12 @@ int sdfo_grid_build_sparse(const double* h_verts, int64_t nv, const int32_t* h_t
                            const sdfo_sparse_build_params* p, void* stream, sdfo_grid** out);
 
 int sdfo_grid_build_stats(const sdfo_grid* g, sdfo_build_stats* out);
+
+/* Selects the acceleration structure of subsequent builds (process-wide;
+ * default SDFO_BVH_REFERENCE).  No reference counterpart: the reference has
+ * only its own tree. */
+int sdfo_set_bvh_mode(int32_t mode);
+int sdfo_get_bvh_mode(void);
 
 /* ---- grid from / to host data (SdfData / SparseSdfData, SdfData.h) ------- */
 /* SdfOracle(SdfData) (SdfOracle.cpp:154-157): dense FP64 arrays, x-fastest:

@@ -7,23 +7,31 @@
 // reference's order (KdTree.h, SdfBuilder.cpp), so distances, witness points,
 // normals and signs are bit-identical to the reference's FP64 arithmetic.
 //
-// Acceleration structure (own design; the reference uses a serial
-// median-split BVH, KdTree.h:91-121, 188-242):
-//   - 63-bit Morton codes of triangle centroids, radix-sorted (CUB),
-//   - Karras (2012) binary radix tree, one thread per internal node,
-//   - bottom-up FP64 box refit with per-node arrival counters,
-//   - packed 64-byte nodes holding both child boxes in FP32, rounded outward
-//     and widened by a margin so FP32 culling is conservative; the FP64
-//     triangle tests decide.
-// Ties in the nearest search (equal FP64 squared distance) resolve to the
-// lowest triangle index (the reference keeps its first-visited triangle).
+// Two acceleration structures (sdfo_set_bvh_mode):
+//  * SDFO_BVH_REFERENCE (default): the reference's median-split tree
+//    (KdTree.h:91-121, 188-242) built on the host with std::nth_element and
+//    traversed on the device in the reference's near-first order with FP64
+//    boxes.  Exactly equidistant triangles then resolve to the same triangle
+//    as in the reference, which matters: for points the parity ray misses the
+//    sign comes from that triangle's face normal (KdTree.h:156-163).
+//  * SDFO_BVH_LBVH: a device-built linear BVH --
+//      63-bit Morton codes of triangle centroids, radix-sorted (CUB),
+//      Karras (2012) binary radix tree, one thread per internal node,
+//      bottom-up FP64 box refit with per-node arrival counters,
+//      packed 64-byte nodes holding both child boxes in FP32, rounded outward
+//      and widened by a margin so FP32 culling is conservative.
+//    Ties resolve to the lowest triangle index.
+// Both decide every distance and every ray hit with the FP64 triangle tests.
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
+#include <cfloat>
 #include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <vector>
 
 #include "sdfo_internal.cuh"
 
@@ -87,6 +95,13 @@ sdfo_grid_info setup_grid(const double* verts, int64_t nv, const sdfo_build_para
     info.has_hessian = 1;
     return info;
 }
+
+namespace {
+std::atomic<int> g_bvh_mode{SDFO_BVH_REFERENCE};
+} // namespace
+
+int bvh_mode() { return g_bvh_mode.load(); }
+void set_bvh_mode(int m) { g_bvh_mode.store(m); }
 
 namespace {
 
@@ -174,7 +189,7 @@ __device__ bool ray_hits(const d3& o, const d3& dir, const d3& a, const d3& b, c
 // ---------------------------------------------------------------------------
 // LBVH
 // ---------------------------------------------------------------------------
-struct BvhView
+struct LbvhView
 {
     const float4* nodes;  // 4 float4 per internal node
     const double* tri9;   // leaf order, 9 doubles per triangle
@@ -184,7 +199,8 @@ struct BvhView
     float inv_dir[3];
 };
 
-__device__ __forceinline__ d3 tri_vertex(const BvhView& b, int slot, int v)
+template <class Tree>
+__device__ __forceinline__ d3 tri_vertex(const Tree& b, int slot, int v)
 {
     const double* t = b.tri9 + 9 * (int64_t)slot + 3 * v;
     return mk(__ldg(t), __ldg(t + 1), __ldg(t + 2));
@@ -366,7 +382,7 @@ struct Nearest
     d3 cp;
 };
 
-__device__ __forceinline__ void test_triangle(const BvhView& b, const d3& p, int slot, Nearest& best)
+__device__ __forceinline__ void test_triangle(const LbvhView& b, const d3& p, int slot, Nearest& best)
 {
     const d3 a = tri_vertex(b, slot, 0), bb = tri_vertex(b, slot, 1), c = tri_vertex(b, slot, 2);
     const d3 cp = closest_point(p, a, bb, c);
@@ -389,7 +405,7 @@ __device__ __forceinline__ float cull_limit(double sq)
     return sq >= 3.0e38 ? INFINITY : __double2float_ru(sq) * 1.000002f;
 }
 
-__device__ Nearest nearest_triangle(const BvhView& b, const d3& p, int* status)
+__device__ Nearest tree_nearest(const LbvhView& b, const d3& p, int* status)
 {
     Nearest best;
     best.sq = 1.0e308 * 10.0; // +inf
@@ -486,7 +502,7 @@ __device__ __forceinline__ bool ray_box(const float o[3], const float inv[3], fl
 
 // countRayIntersections (KdTree.h:398-441): number of triangles the fixed
 // ray hits (exact FP64 test on every triangle whose widened box it crosses).
-__device__ int ray_count(const BvhView& b, const d3& p, int* status)
+__device__ int tree_ray_count(const LbvhView& b, const d3& p, int* status)
 {
     const d3 dir = mk(b.dir[0], b.dir[1], b.dir[2]);
     if (b.n == 1)
@@ -538,6 +554,199 @@ __device__ int ray_count(const BvhView& b, const d3& p, int* status)
     return hits;
 }
 
+// ---------------------------------------------------------------------------
+// reference-order tree: the reference's median-split BVH, traversed on the
+// device in the reference's order with FP64 boxes
+// ---------------------------------------------------------------------------
+struct RefNode
+{
+    double lo[3];
+    double hi[3];
+    int left, right; // internal: children (node ids)
+    int start, count; // leaf: range of slots (count > 0)
+};
+static_assert(sizeof(RefNode) == 64, "RefNode is one 64-byte record");
+
+struct RefTreeView
+{
+    const RefNode* nodes;
+    const double* tri9;    // slot order (m_indices), 9 doubles per triangle
+    const int32_t* tri_id; // slot -> original triangle index
+    int n;
+    int nnodes;
+    double dir[3];
+};
+
+__device__ __forceinline__ void load_box(const RefNode* nd, double lo[3], double hi[3])
+{
+    const double2* q = reinterpret_cast<const double2*>(nd);
+    const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    lo[0] = a.x;
+    lo[1] = a.y;
+    lo[2] = b.x;
+    hi[0] = b.y;
+    hi[1] = c.x;
+    hi[2] = c.y;
+}
+
+// squaredDistanceToAabb (KdTree.h:244-264), same branches and order.
+__device__ __forceinline__ double box_dist_sq(const d3& p, const double lo[3], const double hi[3])
+{
+    const double pp[3] = {p.x, p.y, p.z};
+    double sq = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        if (pp[a] < lo[a])
+        {
+            const double d = lo[a] - pp[a];
+            sq += d * d;
+        }
+        else if (pp[a] > hi[a])
+        {
+            const double d = pp[a] - hi[a];
+            sq += d * d;
+        }
+    }
+    return sq;
+}
+
+// searchNearest (KdTree.h:266-328) without recursion: the explicit stack pops
+// subtrees in the same near-first depth-first order and applies the same
+// "box distance > best" cut when a subtree is entered, and triangles replace
+// the best only on a strictly smaller squared distance -- so the triangle
+// found is the reference's, ties included.
+__device__ Nearest tree_nearest(const RefTreeView& b, const d3& p, int* status)
+{
+    Nearest best;
+    best.sq = DBL_MAX;
+    best.slot = -1;
+    best.id = -1;
+    best.cp = mk(0.0, 0.0, 0.0);
+    if (b.nnodes == 0) return best;
+    int stack[kStackDepth];
+    double sdist[kStackDepth];
+    int sp = 0;
+    {
+        double lo[3], hi[3];
+        load_box(b.nodes, lo, hi);
+        stack[0] = 0;
+        sdist[0] = box_dist_sq(p, lo, hi);
+        sp = 1;
+    }
+    while (sp > 0)
+    {
+        --sp;
+        const int node = stack[sp];
+        if (sdist[sp] > best.sq) continue;
+        const RefNode* nd = b.nodes + node;
+        const int4 meta = __ldg(reinterpret_cast<const int4*>(nd) + 3);
+        if (meta.w > 0)
+        {
+            for (int s = meta.z; s < meta.z + meta.w; ++s)
+            {
+                const d3 a = tri_vertex(b, s, 0), bb = tri_vertex(b, s, 1), c = tri_vertex(b, s, 2);
+                const d3 cp = closest_point(p, a, bb, c);
+                const d3 d = sub(p, cp);
+                const double sq = dot(d, d);
+                if (sq < best.sq)
+                {
+                    best.sq = sq;
+                    best.slot = s;
+                    best.cp = cp;
+                }
+            }
+            continue;
+        }
+        double llo[3], lhi[3], rlo[3], rhi[3];
+        load_box(b.nodes + meta.x, llo, lhi);
+        load_box(b.nodes + meta.y, rlo, rhi);
+        const double dl = box_dist_sq(p, llo, lhi);
+        const double dr = box_dist_sq(p, rlo, rhi);
+        int first = meta.x, second = meta.y;
+        double df = dl, ds = dr;
+        if (dr < dl)
+        {
+            first = meta.y;
+            second = meta.x;
+            df = dr;
+            ds = dl;
+        }
+        if (sp + 2 > kStackDepth)
+        {
+            atomicOr(status, kStatusStackOverflow);
+            break;
+        }
+        stack[sp] = second;
+        sdist[sp] = ds;
+        ++sp;
+        stack[sp] = first;
+        sdist[sp] = df;
+        ++sp;
+    }
+    if (best.slot >= 0) best.id = __ldg(b.tri_id + best.slot);
+    return best;
+}
+
+// rayIntersectsAabb (KdTree.h:335-360), same arithmetic.
+__device__ __forceinline__ bool ray_box_ref(const d3& o, const double dir[3], const double lo[3],
+                                            const double hi[3])
+{
+    const double oo[3] = {o.x, o.y, o.z};
+    double tmin = 0.0, tmax = DBL_MAX;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        const double invD = 1.0 / dir[a];
+        double t0 = (lo[a] - oo[a]) * invD;
+        double t1 = (hi[a] - oo[a]) * invD;
+        if (t0 > t1)
+        {
+            const double t = t0;
+            t0 = t1;
+            t1 = t;
+        }
+        tmin = tmin < t0 ? t0 : tmin;
+        tmax = t1 < tmax ? t1 : tmax;
+        if (tmax < tmin) return false;
+    }
+    return true;
+}
+
+// countRayIntersectionsRecursive (KdTree.h:398-441) over the same tree.
+__device__ int tree_ray_count(const RefTreeView& b, const d3& p, int* status)
+{
+    if (b.nnodes == 0) return 0;
+    const d3 dir = mk(b.dir[0], b.dir[1], b.dir[2]);
+    int stack[kStackDepth];
+    int sp = 0;
+    stack[sp++] = 0;
+    int hits = 0;
+    while (sp > 0)
+    {
+        const int node = stack[--sp];
+        const RefNode* nd = b.nodes + node;
+        double lo[3], hi[3];
+        load_box(nd, lo, hi);
+        if (!ray_box_ref(p, b.dir, lo, hi)) continue;
+        const int4 meta = __ldg(reinterpret_cast<const int4*>(nd) + 3);
+        if (meta.w > 0)
+        {
+            for (int s = meta.z; s < meta.z + meta.w; ++s)
+                hits += ray_hits(p, dir, tri_vertex(b, s, 0), tri_vertex(b, s, 1), tri_vertex(b, s, 2)) ? 1 : 0;
+            continue;
+        }
+        if (sp + 2 > kStackDepth)
+        {
+            atomicOr(status, kStatusStackOverflow);
+            break;
+        }
+        stack[sp++] = meta.y;
+        stack[sp++] = meta.x;
+    }
+    return hits;
+}
+
 struct SignedResult
 {
     double sd;
@@ -546,16 +755,17 @@ struct SignedResult
 };
 
 // findSignedNearest (KdTree.h:143-165).
-__device__ SignedResult signed_nearest(const BvhView& b, const d3& p, int* status)
+template <class Tree>
+__device__ SignedResult signed_nearest(const Tree& b, const d3& p, int* status)
 {
-    const Nearest best = nearest_triangle(b, p, status);
+    const Nearest best = tree_nearest(b, p, status);
     SignedResult r;
     const double dist = sqrt(best.sq);
     r.cp = best.cp;
     r.fn = best.slot >= 0 ? face_normal(tri_vertex(b, best.slot, 0), tri_vertex(b, best.slot, 1),
                                         tri_vertex(b, best.slot, 2))
                           : mk(0.0, 0.0, 1.0);
-    const int hits = ray_count(b, p, status);
+    const int hits = tree_ray_count(b, p, status);
     if (hits > 0)
         r.sd = (hits % 2) == 1 ? -dist : dist;
     else
@@ -589,7 +799,8 @@ __device__ __forceinline__ d3 voxel_center(const SpecD& s, int i, int j, int k)
 }
 
 // Dense fill: CTA = 8x8x4 voxel tile (coherent traversals), thread = voxel.
-__global__ void __launch_bounds__(256) k_dense_fill(BvhView b, SpecD s, double* __restrict__ phi64,
+template <class Tree>
+__global__ void __launch_bounds__(256) k_dense_fill(Tree b, SpecD s, double* __restrict__ phi64,
                                                     double* __restrict__ n64, double* __restrict__ w64,
                                                     float4* __restrict__ phin, int* status)
 {
@@ -658,7 +869,8 @@ __global__ void k_dense_hessian(SpecD s, const double* __restrict__ n64, double*
 
 // Sparse block activation (SdfBuilder.cpp:869-890): distance from the block's
 // geometric centre to the mesh against band + halo*h + (sqrt(3)/2)*bd*h.
-__global__ void k_sparse_activate(BvhView b, SpecD s, int bd, int nbx, int nby, int nbz,
+template <class Tree>
+__global__ void k_sparse_activate(Tree b, SpecD s, int bd, int nbx, int nby, int nbz,
                                   double activation, int32_t* __restrict__ flags, int* status)
 {
     const int bl = blockIdx.x * blockDim.x + threadIdx.x;
@@ -669,7 +881,7 @@ __global__ void k_sparse_activate(BvhView b, SpecD s, int bd, int nbx, int nby, 
     const d3 c = mk(s.bmin[0] + s.voxel[0] * (0.5 * (double)(i0 + i1)),
                     s.bmin[1] + s.voxel[1] * (0.5 * (double)(j0 + j1)),
                     s.bmin[2] + s.voxel[2] * (0.5 * (double)(k0 + k1)));
-    const Nearest best = nearest_triangle(b, c, status);
+    const Nearest best = tree_nearest(b, c, status);
     const double dist = sqrt(best.sq);
     flags[bl] = fabs(dist) <= activation ? 1 : 0;
 }
@@ -696,7 +908,8 @@ __global__ void k_sparse_table(int total, int nbx, int nby, const int32_t* __res
 
 // Brick fill (SdfBuilder.cpp:925-965): one CTA per stored block; voxels
 // outside the grid get phi 0, n (1,0,0).
-__global__ void __launch_bounds__(256) k_sparse_fill(BvhView b, SpecD s, int bd,
+template <class Tree>
+__global__ void __launch_bounds__(256) k_sparse_fill(Tree b, SpecD s, int bd,
                                                      const int32_t* __restrict__ ijk,
                                                      float4* __restrict__ phin, int* status)
 {
@@ -809,36 +1022,175 @@ struct Timer
     }
 };
 
-// Device-side BVH with its storage.
-struct DeviceBvh
+// KdTree::rayDirection (KdTree.h:330-333): the fixed vector normalised.
+void parity_ray(double dir[3])
+{
+    const double r[3] = {1.0, 0.3713906763541037, 0.52999894000318};
+    volatile double n2 = r[0] * r[0];
+    n2 = n2 + r[1] * r[1];
+    n2 = n2 + r[2] * r[2];
+    const double len = std::sqrt((double)n2);
+    for (int a = 0; a < 3; ++a) dir[a] = r[a] / len;
+}
+
+// Device-side LBVH with its storage.
+struct DeviceLbvh
 {
     DeviceBuffer<float4> nodes;
     DeviceBuffer<double> tri9;
     DeviceBuffer<int32_t> tri_id;
     int n = 0;
-    BvhView view() const
+    LbvhView view() const
     {
-        BvhView v{};
+        LbvhView v{};
         v.nodes = nodes.get();
         v.tri9 = tri9.get();
         v.tri_id = tri_id.get();
         v.n = n;
-        // KdTree::rayDirection (KdTree.h:330-333): the fixed vector normalised.
-        const double r[3] = {1.0, 0.3713906763541037, 0.52999894000318};
-        volatile double n2 = r[0] * r[0];
-        n2 = n2 + r[1] * r[1];
-        n2 = n2 + r[2] * r[2];
-        const double len = std::sqrt((double)n2);
-        for (int a = 0; a < 3; ++a)
-        {
-            v.dir[a] = r[a] / len;
-            v.inv_dir[a] = (float)(1.0 / v.dir[a]);
-        }
+        parity_ray(v.dir);
+        for (int a = 0; a < 3; ++a) v.inv_dir[a] = (float)(1.0 / v.dir[a]);
         return v;
     }
 };
 
-void build_bvh(DeviceBvh& bvh, const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
+// Host build of the reference's tree (KdTree::build / buildRecursive,
+// KdTree.h:91-121, 188-242): median split of the centroids on the longest
+// centroid-extent axis with std::nth_element, leaves of <= 8 triangles, nodes
+// numbered in creation (pre-)order.  Restated because tie resolution of the
+// nearest search (and with it the face-normal sign fallback) depends on this
+// exact tree.
+struct HostRefTree
+{
+    std::vector<RefNode> nodes;
+    std::vector<int32_t> order;
+    std::vector<double> lo, hi, cen;
+
+    int build(int lo_i, int hi_i)
+    {
+        const int id = (int)nodes.size();
+        nodes.emplace_back();
+        double bmin[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, bmax[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+        double cmin[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, cmax[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+        for (int i = lo_i; i < hi_i; ++i)
+        {
+            const int t = order[(size_t)i];
+            for (int a = 0; a < 3; ++a)
+            {
+                const double l = lo[3 * (size_t)t + a], h = hi[3 * (size_t)t + a],
+                             c = cen[3 * (size_t)t + a];
+                bmin[a] = l < bmin[a] ? l : bmin[a];
+                bmax[a] = bmax[a] < h ? h : bmax[a];
+                cmin[a] = c < cmin[a] ? c : cmin[a];
+                cmax[a] = cmax[a] < c ? c : cmax[a];
+            }
+        }
+        RefNode n{};
+        for (int a = 0; a < 3; ++a)
+        {
+            n.lo[a] = bmin[a];
+            n.hi[a] = bmax[a];
+        }
+        n.left = n.right = -1;
+        n.start = -1;
+        n.count = 0;
+        const int count = hi_i - lo_i;
+        if (count <= 8)
+        {
+            n.start = lo_i;
+            n.count = count;
+            nodes[(size_t)id] = n;
+            return id;
+        }
+        const double ext[3] = {cmax[0] - cmin[0], cmax[1] - cmin[1], cmax[2] - cmin[2]};
+        int axis = 0;
+        if (ext[1] > ext[0]) axis = 1;
+        if (ext[2] > ext[axis]) axis = 2;
+        const int mid = lo_i + count / 2;
+        const double* c = cen.data();
+        std::nth_element(order.begin() + lo_i, order.begin() + mid, order.begin() + hi_i,
+                         [c, axis](int x, int y) { return c[3 * x + axis] < c[3 * y + axis]; });
+        nodes[(size_t)id] = n;
+        const int l = build(lo_i, mid);
+        const int r = build(mid, hi_i);
+        nodes[(size_t)id].left = l;
+        nodes[(size_t)id].right = r;
+        return id;
+    }
+};
+
+struct DeviceRefTree
+{
+    DeviceBuffer<RefNode> nodes;
+    DeviceBuffer<double> tri9;
+    DeviceBuffer<int32_t> tri_id;
+    int n = 0;
+    int nnodes = 0;
+    RefTreeView view() const
+    {
+        RefTreeView v{};
+        v.nodes = nodes.get();
+        v.tri9 = tri9.get();
+        v.tri_id = tri_id.get();
+        v.n = n;
+        v.nnodes = nnodes;
+        parity_ray(v.dir);
+        return v;
+    }
+};
+
+void build_ref_tree(DeviceRefTree& t, const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
+                    cudaStream_t s)
+{
+    (void)nv;
+    HostRefTree h;
+    const size_t n = (size_t)nt;
+    h.lo.resize(3 * n);
+    h.hi.resize(3 * n);
+    h.cen.resize(3 * n);
+    h.order.resize(n);
+    for (size_t i = 0; i < n; ++i)
+    {
+        const double* a = verts + 3 * (size_t)tris[3 * i];
+        const double* b = verts + 3 * (size_t)tris[3 * i + 1];
+        const double* c = verts + 3 * (size_t)tris[3 * i + 2];
+        for (int q = 0; q < 3; ++q)
+        {
+            // a.cwiseMin(b).cwiseMin(c), a.cwiseMax(b).cwiseMax(c), (a + b + c) / 3.0
+            double mn = b[q] < a[q] ? b[q] : a[q];
+            mn = c[q] < mn ? c[q] : mn;
+            double mx = a[q] < b[q] ? b[q] : a[q];
+            mx = mx < c[q] ? c[q] : mx;
+            h.lo[3 * i + q] = mn;
+            h.hi[3 * i + q] = mx;
+            volatile double sum = a[q] + b[q];
+            sum = sum + c[q];
+            h.cen[3 * i + q] = sum / 3.0;
+        }
+        h.order[i] = (int32_t)i;
+    }
+    h.nodes.reserve(2 * n);
+    h.build(0, (int)nt);
+    std::vector<double> tri9(9 * n);
+    for (size_t sl = 0; sl < n; ++sl)
+    {
+        const int32_t ti = h.order[sl];
+        for (int v = 0; v < 3; ++v)
+            for (int q = 0; q < 3; ++q) tri9[9 * sl + 3 * v + q] = verts[3 * (size_t)tris[3 * (size_t)ti + v] + q];
+    }
+    t.n = (int)nt;
+    t.nnodes = (int)h.nodes.size();
+    t.nodes.reset(h.nodes.size());
+    t.tri9.reset(9 * n);
+    t.tri_id.reset(n);
+    SDFO_CUDA(cudaMemcpyAsync(t.nodes.get(), h.nodes.data(), sizeof(RefNode) * h.nodes.size(),
+                              cudaMemcpyHostToDevice, s));
+    SDFO_CUDA(cudaMemcpyAsync(t.tri9.get(), tri9.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, s));
+    SDFO_CUDA(cudaMemcpyAsync(t.tri_id.get(), h.order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    // the host vectors above are freed on return: finish the copies first
+    SDFO_CUDA(cudaStreamSynchronize(s));
+}
+
+void build_lbvh(DeviceLbvh& bvh, const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
                double extent, cudaStream_t s)
 {
     const int n = (int)nt;
@@ -890,6 +1242,34 @@ void build_bvh(DeviceBvh& bvh, const double* h_verts, int64_t nv, const int32_t*
     SDFO_CHECK_LAUNCH();
 }
 
+// The acceleration structure selected by sdfo_set_bvh_mode.
+struct AnyTree
+{
+    int mode;
+    DeviceRefTree ref;
+    DeviceLbvh lbvh;
+    void build(const double* verts, int64_t nv, const int32_t* tris, int64_t nt, double extent,
+               cudaStream_t s)
+    {
+        if (mode == SDFO_BVH_LBVH)
+            build_lbvh(lbvh, verts, nv, tris, nt, extent, s);
+        else
+            build_ref_tree(ref, verts, nv, tris, nt, s);
+    }
+    int node_count(int64_t nt) const
+    {
+        return mode == SDFO_BVH_LBVH ? (int)(nt > 1 ? nt - 1 : 0) : ref.nnodes;
+    }
+    template <class F>
+    void visit(F&& f) const
+    {
+        if (mode == SDFO_BVH_LBVH)
+            f(lbvh.view());
+        else
+            f(ref.view());
+    }
+};
+
 double scene_extent(const double* verts, int64_t nv, const sdfo_grid_info& info)
 {
     double e = 0.0;
@@ -931,12 +1311,12 @@ sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int
     const int64_t N = (int64_t)g->info.shape[0] * g->info.shape[1] * g->info.shape[2];
     g->stored_voxels = N;
     g->stats.triangles = (int32_t)nt;
-    g->stats.bvh_nodes = (int32_t)(nt > 1 ? nt - 1 : 0);
     g->stats.setup_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     Timer tm(s);
-    DeviceBvh bvh;
-    build_bvh(bvh, verts, nv, tris, nt, scene_extent(verts, nv, g->info), s);
+    AnyTree tree{bvh_mode()};
+    tree.build(verts, nv, tris, nt, scene_extent(verts, nv, g->info), s);
+    g->stats.bvh_nodes = tree.node_count(nt);
     g->stats.bvh_ms = tm.lap();
     g->d.phin = dalloc<float4>((size_t)N);
     g->d.phi64 = dalloc<double>((size_t)N);
@@ -948,8 +1328,10 @@ sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int
     SDFO_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), s));
     const SpecD sp = spec_of(g->info);
     const dim3 grid((sp.n[0] + 7) / 8, (sp.n[1] + 7) / 8, (sp.n[2] + 3) / 4);
-    k_dense_fill<<<grid, 256, 0, s>>>(bvh.view(), sp, g->d.phi64, g->d.n64, g->d.w64, g->d.phin,
-                                      status.get());
+    tree.visit([&](auto view) {
+        k_dense_fill<<<grid, 256, 0, s>>>(view, sp, g->d.phi64, g->d.n64, g->d.w64, g->d.phin,
+                                          status.get());
+    });
     SDFO_CHECK_LAUNCH();
     g->stats.fill_ms = tm.lap();
     k_dense_hessian<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(sp, g->d.n64, g->d.h64, g->d.hess6);
@@ -985,21 +1367,23 @@ sdfo_grid* build_sparse(const double* verts, int64_t nv, const int32_t* tris, in
     for (int a = 0; a < 3; ++a) g->nb[a] = (g->info.shape[a] + bd - 1) / bd;
     const int total = g->nb[0] * g->nb[1] * g->nb[2];
     g->stats.triangles = (int32_t)nt;
-    g->stats.bvh_nodes = (int32_t)(nt > 1 ? nt - 1 : 0);
     g->stats.candidate_blocks = total;
     g->stats.setup_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     Timer tm(s);
-    DeviceBvh bvh;
-    build_bvh(bvh, verts, nv, tris, nt, scene_extent(verts, nv, g->info), s);
+    AnyTree tree{bvh_mode()};
+    tree.build(verts, nv, tris, nt, scene_extent(verts, nv, g->info), s);
+    g->stats.bvh_nodes = tree.node_count(nt);
     g->stats.bvh_ms = tm.lap();
     DeviceBuffer<int> status(1);
     SDFO_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), s));
     const SpecD sp = spec_of(g->info);
     DeviceBuffer<int32_t> flags(total), slots(total);
     const int T = 256;
-    k_sparse_activate<<<(total + T - 1) / T, T, 0, s>>>(bvh.view(), sp, bd, g->nb[0], g->nb[1], g->nb[2],
-                                                         activation, flags.get(), status.get());
+    tree.visit([&](auto view) {
+        k_sparse_activate<<<(total + T - 1) / T, T, 0, s>>>(view, sp, bd, g->nb[0], g->nb[1], g->nb[2],
+                                                             activation, flags.get(), status.get());
+    });
     SDFO_CHECK_LAUNCH();
     size_t temp = 0;
     SDFO_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, flags.get(), slots.get(), total, s));
@@ -1021,7 +1405,9 @@ sdfo_grid* build_sparse(const double* verts, int64_t nv, const int32_t* tris, in
     if (B > 0)
     {
         g->d.phin = dalloc<float4>((size_t)B * V);
-        k_sparse_fill<<<B, 256, 0, s>>>(bvh.view(), sp, bd, g->d.ijk, g->d.phin, status.get());
+        tree.visit([&](auto view) {
+            k_sparse_fill<<<B, 256, 0, s>>>(view, sp, bd, g->d.ijk, g->d.phin, status.get());
+        });
         SDFO_CHECK_LAUNCH();
     }
     g->stats.fill_ms = tm.lap();

@@ -124,6 +124,17 @@ int sdfo_grid_build_sparse(const double* h_verts, int64_t nv, const int32_t* h_t
     });
 }
 
+int sdfo_set_bvh_mode(int32_t mode)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(mode == SDFO_BVH_REFERENCE || mode == SDFO_BVH_LBVH, SDFO_ERR_INVALID_ARGUMENT,
+                     "unknown BVH mode");
+        set_bvh_mode(mode);
+    });
+}
+
+int sdfo_get_bvh_mode(void) { return bvh_mode(); }
+
 int sdfo_query(const sdfo_grid* g, int32_t mode, const void* d_points, int32_t points_f64,
                int64_t n, float* d_gap, float* d_grad, float* d_unit, float* d_witness,
                uint8_t* d_valid, float* d_hess, void* stream)

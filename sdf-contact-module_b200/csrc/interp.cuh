@@ -233,16 +233,20 @@ struct Interp
 };
 
 // Tricubic Hermite (SdfOracle.cpp:932-1092) over corners {phi, n}; slopes
-// n * h; gradient = d/du / h; optional Hessian.
+// n * h; gradient = d/du / h; optional Hessian.  The value weights sum to 1
+// and every derivative's weights sum to 0, so phi is interpolated relative to
+// corner 0 (phi_c - phi_0) and phi_0 added back to the value only: the FP32
+// derivative sums then carry errors of order ulp(h), not ulp(|phi|).
 template <bool HESS>
 __device__ __forceinline__ Interp tricubic(const float4 c[8], float u, float v, float w,
                                            const float h[3])
 {
     float phi[8], gx[8], gy[8], gz[8];
+    const float phi0 = c[0].x;
 #pragma unroll
     for (int q = 0; q < 8; ++q)
     {
-        phi[q] = c[q].x;
+        phi[q] = c[q].x - phi0;
         gx[q] = c[q].y * h[0];
         gy[q] = c[q].z * h[1];
         gz[q] = c[q].w * h[2];
@@ -254,7 +258,7 @@ __device__ __forceinline__ Interp tricubic(const float4 c[8], float u, float v, 
     const XColl xa = collapse_x(bx, phi, gx, gy, gz);
     const XColl xd = collapse_x(dx, phi, gx, gy, gz);
     Interp r;
-    r.gap = collapse_yz(xa, by, bz);
+    r.gap = collapse_yz(xa, by, bz) + phi0;
     r.g[0] = collapse_yz(xd, by, bz) / h[0];
     r.g[1] = collapse_yz(xa, dy, bz) / h[1];
     r.g[2] = collapse_yz(xa, by, dz) / h[2];

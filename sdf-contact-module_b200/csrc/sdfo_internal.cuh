@@ -180,6 +180,8 @@ sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int
 sdfo_grid* build_sparse(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
                         const sdfo_sparse_build_params& p, cudaStream_t s);
 sdfo_grid_info setup_grid(const double* verts, int64_t nv, const sdfo_build_params& p);
+int bvh_mode();
+void set_bvh_mode(int m);
 
 // Contact (contact.cu).
 void launch_contact(const GridView& v, int mode, const float* qx, const float* qw, int64_t nq,

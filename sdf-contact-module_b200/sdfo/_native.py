@@ -17,6 +17,7 @@ SDFO_OK = 0
 FIRST_ORDER, SECOND_ORDER, TRILINEAR, TRICUBIC, CONTACT_AWARE = 0, 1, 2, 3, 4
 LAYOUT_DENSE, LAYOUT_SPARSE = 1, 2
 STORAGE_FP32, STORAGE_FP16 = 0, 1
+BVH_REFERENCE, BVH_LBVH = 0, 1
 
 MODE_NAMES = {"first_order": FIRST_ORDER, "second_order": SECOND_ORDER,
               "trilinear": TRILINEAR, "tricubic": TRICUBIC, "contact_aware": CONTACT_AWARE,
@@ -80,6 +81,8 @@ SIGNATURES = [
     ("sdfo_grid_build_sparse", ctypes.c_int,
      [_P, _I64, _P, _I64, ctypes.POINTER(SparseBuildParams), _P, ctypes.POINTER(_P)]),
     ("sdfo_grid_build_stats", ctypes.c_int, [_P, ctypes.POINTER(BuildStats)]),
+    ("sdfo_set_bvh_mode", ctypes.c_int, [_I32]),
+    ("sdfo_get_bvh_mode", ctypes.c_int, []),
     ("sdfo_grid_create_dense", ctypes.c_int,
      [ctypes.POINTER(GridInfo), _P, _P, _P, _P, _P, ctypes.POINTER(_P)]),
     ("sdfo_grid_create_sparse", ctypes.c_int,

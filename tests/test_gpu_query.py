@@ -1,0 +1,188 @@
+"""GPU queries (all four modes, dense and sparse) against the oracle.
+
+The oracle runs in FP64 on the same stored payload (the FP32 values the GPU
+holds, widened), so the comparison isolates the kernels' FP32 arithmetic:
+valid flags must match exactly; gap within 1e-5 * max(|gap|, h); gradient,
+unit normal within 1e-5 * max(|.|, 1); interpolant Hessian within
+2e-5 * (|H| + 1/h).  A second comparison against the FP64 grid states the
+storage rounding on top, with the same bounds."""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+MODES = [0, 1, 2, 3]
+
+
+def _dense_fp32(g):
+    phi = g["phi"].astype(np.float32).astype(np.float64)
+    nrm = g["normal"].astype(np.float32).astype(np.float64)
+    hes = g["hessian"].astype(np.float32).astype(np.float64)
+    return phi, nrm, hes
+
+
+def _check(gpu, ref, h, pts, modes_hess=True):
+    valid = ref["valid"]
+    assert np.array_equal(gpu["valid"].astype(bool), valid)
+    gap = gpu["gap"].astype(np.float64)
+    assert np.all(np.abs(gap - ref["gap"]) <= 1e-5 * np.maximum(np.abs(ref["gap"]), h))
+    grad = gpu["grad"].astype(np.float64)
+    assert np.all(np.abs(grad - ref["grad"]) <= 1e-5 * np.maximum(np.abs(ref["grad"]), 1.0))
+    if "unit" in gpu:
+        unit = gpu["unit"].astype(np.float64)
+        assert np.all(np.abs(unit - ref["unit"]) <= 1e-5 * np.maximum(np.abs(ref["unit"]), 1.0))
+    if "witness" in gpu:
+        w = gpu["witness"].astype(np.float64)
+        scale = np.abs(pts).max() + h
+        assert np.all(np.abs(w - ref["witness"]) <= 1e-6 * scale + 1e-5 * h)
+    if "hess" in gpu and modes_hess:
+        H = gpu["hess"].astype(np.float64)
+        assert np.all(np.abs(H - ref["hess"]) <= 2e-5 * (np.abs(ref["hess"]) + 1.0 / h))
+
+
+def _gpu_query(grid, pts, mode, f64=False):
+    import torch
+
+    t = torch.tensor(pts, dtype=torch.float64 if f64 else torch.float32, device="cuda")
+    out = grid.query_tensors(t, mode=mode, unit=True, witness=True, valid=True, hess=True)
+    return {k: v.cpu().numpy() for k, v in out.items()}
+
+
+@pytest.mark.parametrize("name", ["cube", "cyl", "torus"])
+@pytest.mark.parametrize("mode", MODES)
+def test_dense_query_vs_oracle(cuda, port, name, mode):
+    from sdfo import SdfGrid
+
+    g = golden(f"dense_{name}.npz")
+    spec = port.GridSpec(bmin=g["bmin"], bmax=g["bmax"], voxel=g["voxel"], shape=tuple(g["shape"]))
+    grid = SdfGrid.from_dense(spec, g["phi"], g["normal"], g["hessian"], g["witness"])
+    pts = g["pts"]  # FP32-representable, includes voxel centres and cell corners
+    h = float(g["voxel"][0])
+    phi, nrm, hes = _dense_fp32(g)
+    ref32 = port.query_dense(spec, phi, nrm, hes, mode, pts)
+    ref32["hess"] = ref32["hess"]
+    gpu = _gpu_query(grid, pts, mode)
+    gpu["hess"] = gpu["hess"].reshape(-1, 3, 3)
+    _check(gpu, ref32, h, pts)
+    # against the FP64 grid: storage rounding included
+    ref64 = port.query_dense(spec, g["phi"], g["normal"], g["hessian"], mode, pts)
+    _check({k: gpu[k] for k in ("valid", "gap", "grad", "unit")}, ref64, h, pts)
+    # float64 points give the same cells and values
+    gpu64 = _gpu_query(grid, pts, mode, f64=True)
+    assert np.array_equal(gpu64["valid"], gpu["valid"])
+    assert np.allclose(gpu64["gap"], gpu["gap"], rtol=0, atol=1e-6 * h)
+
+
+@pytest.mark.parametrize("name", ["cube", "cyl"])
+@pytest.mark.parametrize("mode", MODES)
+def test_sparse_query_vs_oracle(cuda, port, name, mode):
+    from sdfo import SdfGrid
+
+    g = golden(f"sparse_{name}.npz")
+    spec = port.GridSpec(bmin=g["bmin"], bmax=g["bmax"], voxel=g["voxel"], shape=tuple(g["shape"]))
+    bd = int(g["block_dim"])
+    grid = SdfGrid.from_sparse(spec, bd, g["ijk"], g["phi"], g["normal"], g["hessian"],
+                               int(g["halo"]), float(g["band"]))
+    pts = g["pts"]
+    h = float(g["voxel"][0])
+    ref = port.query_sparse(spec, bd, g["ijk"], g["phi"], g["normal"], g["hessian"], mode, pts)
+    gpu = _gpu_query(grid, pts, mode)
+    gpu["hess"] = gpu["hess"].reshape(-1, 3, 3)
+    _check(gpu, ref, h, pts)
+    assert ref["valid"].any() and not ref["valid"].all()
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_queries_match_reference_golden(cuda, mode):
+    """Straight against SdfOracle::queryFast results recorded from the reference."""
+    from sdfo import SdfGrid
+
+    g = golden("dense_torus.npz")
+    spec = dict(bmin=g["bmin"], bmax=g["bmax"], voxel=g["voxel"], shape=tuple(g["shape"]))
+    grid = SdfGrid.from_dense(spec, g["phi"], g["normal"], g["hessian"], g["witness"])
+    gpu = _gpu_query(grid, g["pts"], mode)
+    h = float(g["voxel"][0])
+    v = g[f"q{mode}_valid"]
+    assert np.array_equal(gpu["valid"].astype(bool), v)
+    assert np.all(np.abs(gpu["gap"] - g[f"q{mode}_gap"]) <= 1e-5 * np.maximum(np.abs(g[f"q{mode}_gap"]), h))
+    assert np.all(np.abs(gpu["unit"] - g[f"q{mode}_normal"]) <= 1e-5 * np.maximum(np.abs(g[f"q{mode}_normal"]), 1.0))
+
+
+def test_query_batch_duck_type_matches_prototype(cuda):
+    """SdfGrid.query_batch vs the prototype's TrilinearSDFGrid.query_batch."""
+    from sdfo import SdfGrid
+
+    g = golden("prototype_cube32.npz")
+    spec = dict(bmin=g["bmin"], bmax=g["bmax"], voxel=g["voxel"], shape=tuple(g["shape"]))
+    grid = SdfGrid.from_dense(spec, g["phi"], g["normal"])
+    gq, raw, gn, unit, valid = grid.query_batch(g["pts"])
+    h = float(g["voxel"][0])
+    assert np.array_equal(valid, g["valid"])
+    assert np.all(np.abs(gq - g["g"]) <= 1e-5 * np.maximum(np.abs(g["g"]), h))
+    assert np.all(np.abs(raw - g["raw_grad"]) <= 1e-5 * np.maximum(np.abs(g["raw_grad"]), 1.0))
+    assert np.all(np.abs(gn - g["grad_norm"]) <= 1e-5 * np.maximum(g["grad_norm"], 1.0))
+    assert np.all(np.abs(unit - g["unit"]) <= 1e-5)
+    assert np.all(unit[~valid] == np.array([0.0, 0.0, 1.0]))
+    s = grid.query(g["pts"][0])
+    assert len(s) == 5
+
+
+def test_invalid_points_and_edges(cuda, port):
+    from sdfo import SdfGrid
+
+    g = golden("dense_cube.npz")
+    spec = dict(bmin=g["bmin"], bmax=g["bmax"], voxel=g["voxel"], shape=tuple(g["shape"]))
+    grid = SdfGrid.from_dense(spec, g["phi"], g["normal"], g["hessian"])
+    pts = np.array([[np.nan, 0, 0], [np.inf, 0, 0], [-np.inf, 0, 0], [1e30, 0, 0], [0, 0, -1e30],
+                    g["bmin"], g["bmax"], [0.0, 0.0, 0.0]], dtype=np.float32)
+    for mode in MODES:
+        r = _gpu_query(grid, pts, mode)
+        assert not r["valid"][:6].any()
+        assert np.all(r["gap"][:6] == 0) and np.all(r["grad"][:6] == 0)
+        assert np.all(r["unit"][:6] == np.array([1, 0, 0], np.float32))
+        assert r["valid"][7]
+    # empty batch is a no-op
+    import torch
+
+    out = grid.query_tensors(torch.zeros((0, 3), device="cuda"), mode=3)
+    assert out["gap"].numel() == 0
+
+
+def test_host_path_matches_device_path(cuda):
+    from sdfo import SdfGrid
+
+    g = golden("dense_cyl.npz")
+    spec = dict(bmin=g["bmin"], bmax=g["bmax"], voxel=g["voxel"], shape=tuple(g["shape"]))
+    grid = SdfGrid.from_dense(spec, g["phi"], g["normal"], g["hessian"])
+    pts = g["pts"].astype(np.float32)
+    host = grid.query_host(pts, mode=3)
+    dev = _gpu_query(grid, pts, 3)
+    assert np.array_equal(host["gap"], dev["gap"])
+    assert np.array_equal(host["grad"], dev["grad"])
+    assert np.array_equal(host["valid"], dev["valid"].astype(bool))
+
+
+def test_fp16_sparse_storage_error_bound(cuda, port):
+    """FP16 brick payload: gap error stated against the FP64 oracle."""
+    from sdfo import SdfGrid
+
+    g = golden("sparse_cyl.npz")
+    spec = dict(bmin=g["bmin"], bmax=g["bmax"], voxel=g["voxel"], shape=tuple(g["shape"]))
+    bd = int(g["block_dim"])
+    grid = SdfGrid.from_sparse(spec, bd, g["ijk"], g["phi"], g["normal"], g["hessian"])
+    g16 = grid.to_fp16()
+    pts = g["pts"]
+    h = float(g["voxel"][0])
+    ref = port.query_sparse(port.GridSpec(**spec), bd, g["ijk"], g["phi"], g["normal"],
+                            g["hessian"], 3, pts)
+    r16 = _gpu_query(g16, pts, 3)
+    v = ref["valid"]
+    assert np.array_equal(r16["valid"].astype(bool), v)
+    # per-brick affine phi in FP16: |d phi| <= 2^-11 * half-range of the brick's
+    # phi (<= sqrt(3) * bd * h), normals to 2^-11
+    bound = 2.0 ** -11 * np.sqrt(3.0) * bd * h * 1.5
+    assert np.max(np.abs(r16["gap"][v] - ref["gap"][v])) <= bound
+    d = g16.export_sparse()
+    assert np.max(np.abs(d["phi"] - g["phi"])) <= bound
