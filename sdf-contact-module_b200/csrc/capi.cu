@@ -164,23 +164,42 @@ int sdfo_query_host(const sdfo_grid* g, int32_t mode, const void* h_points, int3
         SDFO_REQUIRE(mode >= SDFO_FIRST_ORDER && mode <= SDFO_CONTACT_AWARE,
                      SDFO_ERR_INVALID_ARGUMENT, "unknown query mode");
         cudaStream_t s = as_stream(stream);
+        // one staging allocation per handle, 256-byte aligned sub-buffers
+        auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
         const size_t pb = (size_t)n * 3 * (points_f64 ? sizeof(double) : sizeof(float));
-        DeviceBuffer<unsigned char> pts(pb);
-        DeviceBuffer<float> gap((size_t)n), grad(h_grad ? 3 * (size_t)n : 0),
-            unit(h_unit ? 3 * (size_t)n : 0), wit(h_witness ? 3 * (size_t)n : 0);
-        DeviceBuffer<uint8_t> valid(h_valid ? (size_t)n : 0);
-        SDFO_CUDA(cudaMemcpyAsync(pts.get(), h_points, pb, cudaMemcpyHostToDevice, s));
-        const QueryOutputs o{gap.get(), grad.get(), unit.get(), wit.get(), valid.get(), nullptr};
-        launch_query(make_view(g), mode, pts.get(), points_f64 != 0, n, o, s);
-        SDFO_CUDA(cudaMemcpyAsync(h_gap, gap.get(), sizeof(float) * n, cudaMemcpyDeviceToHost, s));
-        if (h_grad)
-            SDFO_CUDA(cudaMemcpyAsync(h_grad, grad.get(), sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
-        if (h_unit)
-            SDFO_CUDA(cudaMemcpyAsync(h_unit, unit.get(), sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
-        if (h_witness)
-            SDFO_CUDA(cudaMemcpyAsync(h_witness, wit.get(), sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
-        if (h_valid)
-            SDFO_CUDA(cudaMemcpyAsync(h_valid, valid.get(), n, cudaMemcpyDeviceToHost, s));
+        const size_t gb = sizeof(float) * (size_t)n, vb = sizeof(float) * 3 * (size_t)n;
+        const size_t need = up(pb) + up(gb) + (h_grad ? up(vb) : 0) + (h_unit ? up(vb) : 0) +
+                            (h_witness ? up(vb) : 0) + (h_valid ? up((size_t)n) : 0);
+        std::lock_guard<std::mutex> lock(g->ws_mutex);
+        if (g->ws_bytes < need)
+        {
+            SDFO_CUDA(cudaStreamSynchronize(s));
+            device_free(g->ws);
+            g->ws = nullptr;
+            g->ws_bytes = 0;
+            g->ws = device_alloc(need);
+            g->ws_bytes = need;
+        }
+        unsigned char* base = static_cast<unsigned char*>(g->ws);
+        auto take = [&](size_t b) {
+            unsigned char* p = base;
+            base += up(b);
+            return p;
+        };
+        void* pts = take(pb);
+        float* gap = reinterpret_cast<float*>(take(gb));
+        float* grad = h_grad ? reinterpret_cast<float*>(take(vb)) : nullptr;
+        float* unit = h_unit ? reinterpret_cast<float*>(take(vb)) : nullptr;
+        float* wit = h_witness ? reinterpret_cast<float*>(take(vb)) : nullptr;
+        uint8_t* valid = h_valid ? take((size_t)n) : nullptr;
+        SDFO_CUDA(cudaMemcpyAsync(pts, h_points, pb, cudaMemcpyHostToDevice, s));
+        const QueryOutputs o{gap, grad, unit, wit, valid, nullptr};
+        launch_query(make_view(g), mode, pts, points_f64 != 0, n, o, s);
+        SDFO_CUDA(cudaMemcpyAsync(h_gap, gap, gb, cudaMemcpyDeviceToHost, s));
+        if (h_grad) SDFO_CUDA(cudaMemcpyAsync(h_grad, grad, vb, cudaMemcpyDeviceToHost, s));
+        if (h_unit) SDFO_CUDA(cudaMemcpyAsync(h_unit, unit, vb, cudaMemcpyDeviceToHost, s));
+        if (h_witness) SDFO_CUDA(cudaMemcpyAsync(h_witness, wit, vb, cudaMemcpyDeviceToHost, s));
+        if (h_valid) SDFO_CUDA(cudaMemcpyAsync(h_valid, valid, (size_t)n, cudaMemcpyDeviceToHost, s));
         SDFO_CUDA(cudaStreamSynchronize(s));
     });
 }

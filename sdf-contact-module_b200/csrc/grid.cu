@@ -167,6 +167,7 @@ void encode_fp16(const sdfo_grid* src, sdfo_grid* dst, cudaStream_t s)
 sdfo_grid::~sdfo_grid()
 {
     using sdfo::device_free;
+    device_free(ws);
     if (borrowed) return;
     device_free(d.phin);
     device_free(d.hess6);

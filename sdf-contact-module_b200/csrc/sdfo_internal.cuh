@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -133,6 +134,11 @@ struct sdfo_grid
     int64_t stored_voxels = 0;
     int32_t nb[3] = {0, 0, 0};
     bool borrowed = false; // a view: storage belongs to another handle / caller
+    // Device staging for the host-buffer query path, grown on demand and
+    // reused across calls; calls on one handle serialise on the mutex.
+    mutable std::mutex ws_mutex;
+    mutable void* ws = nullptr;
+    mutable size_t ws_bytes = 0;
     ~sdfo_grid();
 };
 
