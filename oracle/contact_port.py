@@ -49,7 +49,10 @@ def evaluate_pose(query_batch, Xq, wq, rA, RA, vA, wA, rB, RB, vB, wB, k, order,
     u_rel = uA - uB
     if damping > 0:
         vn = np.sum(u_rel * rg, axis=1)
-        fn = fn + damping * (-vn)[:, None] * rg * (gv < 0.0)[:, None]
+        # the damping switch g < 0 is a step; with the active set frozen it is
+        # kept on for every frozen point (all had g < 0 at the base pose)
+        damp_on = np.ones_like(gv, bool) if freeze is not None else (gv < 0.0)
+        fn = fn + damping * (-vn)[:, None] * rg * damp_on[:, None]
     un = rg / np.maximum(gn[:, None], 1e-30)
     udotn = np.sum(u_rel * un, axis=1, keepdims=True)
     u_t = u_rel - udotn * un

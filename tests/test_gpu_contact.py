@@ -4,9 +4,11 @@ Forces/torques: the oracle (oracle/contact_port.py, pinned to the
 prototype's SDFContactEngine.evaluate) evaluated in FP64 on the same FP32
 grid payload; tolerance 1e-5 of the pose's force (torque) magnitude.
 Jacobian: central differences (h = 1e-7 m / 1e-6 rad) of the oracle with the
-active point set and each point's interpolation cell frozen at the base pose,
-i.e. the derivative of the smooth piece that forward-mode AD differentiates;
-tolerance 1e-4 of the Jacobian's magnitude."""
+active point set, the damping switch (g < 0) and each point's interpolation
+cell frozen at the base pose, i.e. the derivative of the smooth piece that
+forward-mode AD differentiates (the damping switch is a step at g = 0 and the
+trilinear gradient jumps across cell faces: unfrozen differences across
+either are not derivatives); tolerance 1e-4 of the Jacobian's magnitude."""
 import numpy as np
 import pytest
 

@@ -40,9 +40,13 @@ def _check(gpu, ref, h, pts, modes_hess=True):
         assert np.all(np.abs(unit - ref["unit"]) <= tol)
         assert np.allclose(np.linalg.norm(unit[valid], axis=1), 1.0, atol=1e-6)
     if "witness" in gpu:
+        # p - gap * unit: FP32 rounding of p plus |gap| times the unit bound
         w = gpu["witness"].astype(np.float64)
         scale = np.abs(pts).max() + h
-        assert np.all(np.abs(w - ref["witness"]) <= 1e-6 * scale + 1e-5 * h)
+        gn = np.linalg.norm(ref["grad"], axis=1, keepdims=True)
+        utol = 2e-5 * np.maximum(1.0, 1.0 / np.maximum(gn, 1e-30))
+        tol = 1e-6 * scale + 1e-5 * h + np.abs(ref["gap"])[:, None] * utol
+        assert np.all(np.abs(w - ref["witness"]) <= tol)
     if "hess" in gpu and modes_hess:
         H = gpu["hess"].astype(np.float64)
         assert np.all(np.abs(H - ref["hess"]) <= 2e-5 * (np.abs(ref["hess"]) + 1.0 / h))
