@@ -260,6 +260,26 @@ int sdfo_query_host(const sdfo_grid* g, int32_t mode, const void* h_points, int3
                     int64_t n, float* h_gap, float* h_grad, float* h_unit, float* h_witness,
                     uint8_t* h_valid, void* stream);
 
+/* sdfo_query_host without any device allocation.  No counterpart in the
+ * reference.  For callers that cannot let a library allocate device memory
+ * (applications that give all GPU memory to their own pool at start-up, or
+ * that forbid cudaMalloc and the synchronisation it implies inside their
+ * step loop): the host points and results are staged through one fixed
+ * device array of SDFO_STATIC_STAGING_BYTES that is part of the library image
+ * -- every GPU that loads libsdfo_cuda holds it until the process exits.
+ * Outputs: h_gap (required), h_grad and h_valid (may be NULL); points and
+ * outputs together must fit the array (about 1.1M float32 queries with all
+ * outputs), larger batches return SDFO_ERR_INVALID_ARGUMENT.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress) and
+ * should come before any stream capture.  Every call shares the array and
+ * leaves its contents behind: calls that overlap on the GPU (from several
+ * host threads or streams at once) race on it, so callers must serialise
+ * them.  Synchronous; the grid's device must be current. */
+#define SDFO_STATIC_STAGING_BYTES (32u << 20)
+int sdfo_query_host_static(const sdfo_grid* g, int32_t mode, const void* h_points,
+                           int32_t points_f64, int64_t n, float* h_gap, float* h_grad,
+                           uint8_t* h_valid, void* stream);
+
 /* Backward of sdfo_query (no reference counterpart): given upstream
  * d_dgap[n] and d_dgrad[n*3] (either may be NULL = zero), writes
  *   d_dpoints[n*3] = dgap * grad + H * dgrad        (may be NULL)

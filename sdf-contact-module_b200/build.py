@@ -29,7 +29,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
           "-ffp-contract=off", "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
 PER_FILE = {"build.cu": ["-fmad=false"]}
-SOURCES = ["grid.cu", "capi.cu", "query.cu", "build.cu", "contact.cu"]
+SOURCES = ["grid.cu", "capi.cu", "query.cu", "build.cu", "contact.cu", "static_staging.cu"]
 HEADERS = ["sdfo_internal.cuh", "interp.cuh"]
 
 

@@ -97,6 +97,7 @@ SIGNATURES = [
     ("sdfo_grid_destroy", ctypes.c_int, [_P]),
     ("sdfo_query", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P, _P, _P, _P]),
     ("sdfo_query_host", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P, _P, _P]),
+    ("sdfo_query_host_static", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P]),
     ("sdfo_query_backward", ctypes.c_int, [_P, _I32, _P, _I64, _P, _P, _P, _P, _P]),
     ("sdfo_contact_eval", ctypes.c_int,
      [_P, _I32, _P, _P, _I64, _P, _I64, _P, ctypes.POINTER(ContactParams), _P, _P, _P]),
