@@ -68,7 +68,45 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    build_host(force, verbose)
     return LIB
+
+
+HOST = os.path.join(PKG, "host")
+HOST_LIB = os.path.join(LIBDIR, "libsdfo_host.so")
+HOST_CHECK = os.path.join(LIBDIR, "sdfo_host_check")
+HOST_SOURCES = ["SdfIO.cpp", "SdfSurfaceMesh.cpp", "SdfBuilder.cpp", "SdfOracle.cpp"]
+
+
+def host_cxx() -> str:
+    for cand in ("/usr/bin/g++", shutil.which("g++")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("g++ not found")
+
+
+def build_host(force: bool = False, verbose: bool = False) -> str:
+    """The C++ plugin API (libsdfo_host.so) and its check program, linked
+    against libsdfo_cuda.so with an $ORIGIN run path."""
+    hdrs = [os.path.join(HOST, "include", "SdfOracle", h)
+            for h in os.listdir(os.path.join(HOST, "include", "SdfOracle"))]
+    hdrs += [os.path.join(INCLUDE, "sdfo.h"), os.path.join(HOST, "compat", "Eigen", "Dense")]
+    flags = ["-std=c++17", "-O2", "-fPIC", "-Wall", "-I", os.path.join(HOST, "include"),
+             "-I", os.path.join(HOST, "compat"), "-I", INCLUDE]
+    srcs = [os.path.join(HOST, "src", s) for s in HOST_SOURCES]
+    link = ["-L", LIBDIR, "-lsdfo_cuda", "-Wl,-rpath,$ORIGIN"]
+    if force or _newer(HOST_LIB, srcs + hdrs + [LIB]):
+        cmd = [host_cxx(), "-shared", "-o", HOST_LIB] + flags + srcs + link
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    app = os.path.join(HOST, "app", "sdfo_host_check.cpp")
+    if force or _newer(HOST_CHECK, [app, HOST_LIB] + hdrs):
+        cmd = [host_cxx(), "-o", HOST_CHECK, app] + flags + ["-L", LIBDIR, "-lsdfo_host"] + link
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return HOST_LIB
 
 
 if __name__ == "__main__":
