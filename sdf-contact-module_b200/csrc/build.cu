@@ -1336,6 +1336,7 @@ sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int
     g->stats.fill_ms = tm.lap();
     k_dense_hessian<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(sp, g->d.n64, g->d.h64, g->d.hess6);
     SDFO_CHECK_LAUNCH();
+    build_stencil_layouts(g.get(), s);
     g->stats.hessian_ms = tm.lap();
     check_status(status, s);
     g->stats.voxels_filled = N;

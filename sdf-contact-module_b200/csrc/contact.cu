@@ -58,21 +58,43 @@ __device__ __forceinline__ bool sample(const GridView& g, const double Y[3], flo
 {
     const Cell c = cell_of(g, Y);
     if (!c.ok) return false;
-    float4 cs[8];
-    int64_t idx[8];
-    if (!gather_corners<SPARSE, BD>(g, c, cs, idx)) return false;
     const float h[3] = {(float)g.voxel[0], (float)g.voxel[1], (float)g.voxel[2]};
     Interp r;
-    if (MODE == SDFO_TRICUBIC)
+    if (!SPARSE && MODE == SDFO_TRILINEAR && g.cell8 != nullptr)
     {
-        r = tricubic<JAC>(cs, c.u, c.v, c.w, h);
+        float4 a, b;
+        ld256(g.cell8 + 2 * dense_index(g, c.i0, c.j0, c.k0), a, b);
+        const float phi[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        r = trilinear<JAC>(phi, c.u, c.v, c.w, h);
     }
     else
     {
-        float phi[8];
+        float4 cs[8];
+        if (!SPARSE && g.xpair != nullptr)
+        {
+            const int64_t base = dense_index(g, c.i0, c.j0, c.k0);
+            const int64_t sy = g.nx, sz = (int64_t)g.nx * g.ny;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) phi[q] = cs[q].x;
-        r = trilinear<JAC>(phi, c.u, c.v, c.w, h);
+            for (int q = 0; q < 4; ++q)
+                ld256(g.xpair + 2 * (base + ((q & 1) ? sy : 0) + ((q & 2) ? sz : 0)), cs[2 * q],
+                      cs[2 * q + 1]);
+        }
+        else
+        {
+            int64_t idx[8];
+            if (!gather_corners<SPARSE, BD>(g, c, cs, idx)) return false;
+        }
+        if (MODE == SDFO_TRICUBIC)
+        {
+            r = tricubic<JAC>(cs, c.u, c.v, c.w, h);
+        }
+        else
+        {
+            float phi[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) phi[q] = cs[q].x;
+            r = trilinear<JAC>(phi, c.u, c.v, c.w, h);
+        }
     }
     gap = r.gap;
     grad = V(r.g[0], r.g[1], r.g[2]);
@@ -88,87 +110,109 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+// Per-point contact state of one quadrature point at one pose.
+struct PointState
+{
+    double p, gn, vn, udn, den, phat, dgdd, wq;
+    v3 off, rg, gl, u, un, ut, fq;
+    double Hl[6];
+    bool damp, fric;
+};
+
 template <int MODE, bool SPARSE, int BD, bool JAC>
 __global__ void __launch_bounds__(kContactThreads)
     k_contact(GridView g, const float* __restrict__ qx, const float* __restrict__ qw, int nq,
               const sdfo_body_state* __restrict__ poses, const sdfo_body_state* __restrict__ body_b,
               sdfo_contact_params prm, double* __restrict__ ft, double* __restrict__ jac)
 {
-    constexpr int NACC = JAC ? 42 : 6;
+    constexpr int kWarps = kContactThreads / 32;
     const int pose = blockIdx.x;
     __shared__ sdfo_body_state sA, sB;
-    __shared__ double red[kContactThreads / 32][NACC];
+    __shared__ double red[kWarps][6];
+    __shared__ double sjac[JAC ? kWarps : 1][JAC ? 36 : 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0)
     {
         sA = poses[pose];
         sB = *body_b;
     }
+    if (JAC)
+        for (int t = lane; t < 36; t += 32) sjac[warp][t] = 0.0;
     __syncthreads();
     const v3 rA = V(sA.r[0], sA.r[1], sA.r[2]), rB = V(sB.r[0], sB.r[1], sB.r[2]);
     const v3 vA = V(sA.v[0], sA.v[1], sA.v[2]), wA = V(sA.w[0], sA.w[1], sA.w[2]);
     const v3 vB = V(sB.v[0], sB.v[1], sB.v[2]), wB = V(sB.w[0], sB.w[1], sB.w[2]);
     const v3 tl = mulT(sB.R, rA - rB); // R_B^T (r_A - r_B)
-    double acc[NACC];
-#pragma unroll
-    for (int q = 0; q < NACC; ++q) acc[q] = 0.0;
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 
-    for (int i = threadIdx.x; i < nq; i += kContactThreads)
+    // block-uniform trip count so whole warps stay converged for the
+    // warp-level Jacobian reduction below
+    for (int i0 = 0; i0 < nq; i0 += kContactThreads)
     {
-        const v3 X = V(__ldg(qx + 3 * i), __ldg(qx + 3 * i + 1), __ldg(qx + 3 * i + 2));
-        const v3 off = mul(sA.R, X);           // x_w - r_A
-        const v3 Yv = mulT(sB.R, off) + tl;    // body-B local point
-        const double Y[3] = {Yv.x, Yv.y, Yv.z};
-        float gapf;
-        v3 gl;
-        double Hl[6];
-        if (!sample<MODE, SPARSE, BD, JAC>(g, Y, gapf, gl, Hl)) continue;
-        const double gap = gapf;
-        const double delta = gap < 0.0 ? -gap : 0.0;
-        const double dpow = prm.order == 2.0 ? delta * delta
-                          : prm.order == 1.0 ? delta
-                                             : pow(delta, prm.order);
-        const double p = prm.stiffness * dpow;
-        if (!(p > 1e-30)) continue;
-        const double wq = (double)__ldg(qw + i);
-        const v3 xw = rA + off;
-        const v3 rg = mul(sB.R, gl);
-        const double gn = sqrt(dot(gl, gl));
-        v3 fq = p * rg;
-        const v3 uA = vA + cross(wA, off);
-        const v3 offB = xw - rB;
-        const v3 uB = vB + cross(wB, offB);
-        const v3 u = uA - uB;
-        const bool damp = prm.damping > 0.0 && gap < 0.0;
-        const double vn = dot(u, rg);
-        if (damp) fq = fq + (prm.damping * (-vn)) * rg;
-        const double gsafe = gn > 1e-30 ? gn : 1e-30;
-        const v3 un = (1.0 / gsafe) * rg;
-        const double udn = dot(u, un);
-        const v3 ut = u - udn * un;
-        const double utn2 = dot(ut, ut);
-        const double den = sqrt(utn2 + prm.regularizer * prm.regularizer);
-        const double phat = p * gn;
-        const bool fric = prm.friction * phat > 0.0;
-        if (fric) fq = fq + (-prm.friction * phat / den) * ut;
-        const v3 tq = cross(off, fq);
-        acc[0] += wq * fq.x;
-        acc[1] += wq * fq.y;
-        acc[2] += wq * fq.z;
-        acc[3] += wq * tq.x;
-        acc[4] += wq * tq.y;
-        acc[5] += wq * tq.z;
-        if (JAC)
+        const int i = i0 + threadIdx.x;
+        PointState st;
+        bool act = false;
+        if (i < nq)
         {
-            // world Hessian of g: H_w = R_B H_l R_B^T
-            const double Hm[9] = {Hl[0], Hl[1], Hl[2], Hl[1], Hl[3], Hl[4], Hl[2], Hl[4], Hl[5]};
-            const double dgdd = -prm.stiffness *
-                                (prm.order == 2.0 ? 2.0 * delta
-                                 : prm.order == 1.0 ? 1.0
-                                                    : prm.order * pow(delta, prm.order - 1.0));
-#pragma unroll 1
-            for (int j = 0; j < 6; ++j)
+            const v3 X = V(__ldg(qx + 3 * i), __ldg(qx + 3 * i + 1), __ldg(qx + 3 * i + 2));
+            st.off = mul(sA.R, X);               // x_w - r_A
+            const v3 Yv = mulT(sB.R, st.off) + tl; // body-B local point
+            const double Y[3] = {Yv.x, Yv.y, Yv.z};
+            float gapf;
+            if (sample<MODE, SPARSE, BD, JAC>(g, Y, gapf, st.gl, st.Hl))
             {
-                // dx_w and d(off) for parameter j
+                const double gap = gapf;
+                const double delta = gap < 0.0 ? -gap : 0.0;
+                const double dpow = prm.order == 2.0 ? delta * delta
+                                  : prm.order == 1.0 ? delta
+                                                     : pow(delta, prm.order);
+                st.p = prm.stiffness * dpow;
+                act = st.p > 1e-30;
+                if (act)
+                {
+                    st.wq = (double)__ldg(qw + i);
+                    const v3 xw = rA + st.off;
+                    st.rg = mul(sB.R, st.gl);
+                    st.gn = sqrt(dot(st.gl, st.gl));
+                    st.fq = st.p * st.rg;
+                    const v3 uA = vA + cross(wA, st.off);
+                    const v3 uB = vB + cross(wB, xw - rB);
+                    st.u = uA - uB;
+                    st.damp = prm.damping > 0.0 && gap < 0.0;
+                    st.vn = dot(st.u, st.rg);
+                    if (st.damp) st.fq = st.fq + (prm.damping * (-st.vn)) * st.rg;
+                    const double gsafe = st.gn > 1e-30 ? st.gn : 1e-30;
+                    st.un = (1.0 / gsafe) * st.rg;
+                    st.udn = dot(st.u, st.un);
+                    st.ut = st.u - st.udn * st.un;
+                    st.den = sqrt(dot(st.ut, st.ut) + prm.regularizer * prm.regularizer);
+                    st.phat = st.p * st.gn;
+                    st.fric = prm.friction * st.phat > 0.0;
+                    if (st.fric) st.fq = st.fq + (-prm.friction * st.phat / st.den) * st.ut;
+                    const v3 tq = cross(st.off, st.fq);
+                    acc[0] += st.wq * st.fq.x;
+                    acc[1] += st.wq * st.fq.y;
+                    acc[2] += st.wq * st.fq.z;
+                    acc[3] += st.wq * tq.x;
+                    acc[4] += st.wq * tq.y;
+                    acc[5] += st.wq * tq.z;
+                    st.dgdd = -prm.stiffness * (prm.order == 2.0 ? 2.0 * delta
+                                                : prm.order == 1.0 ? 1.0
+                                                                   : prm.order * pow(delta, prm.order - 1.0));
+                }
+            }
+        }
+        if (!JAC || !__any_sync(0xffffffffu, act)) continue;
+        // Forward-mode derivatives of this point's force / torque w.r.t. the 6
+        // pose parameters, one column at a time, summed over the warp.
+        const double Hm[9] = {st.Hl[0], st.Hl[1], st.Hl[2], st.Hl[1], st.Hl[3],
+                              st.Hl[4], st.Hl[2], st.Hl[4], st.Hl[5]};
+#pragma unroll 1
+        for (int j = 0; j < 6; ++j)
+        {
+            double col[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            if (act)
+            {
                 v3 dxw, doff;
                 if (j < 3)
                 {
@@ -177,65 +221,71 @@ __global__ void __launch_bounds__(kContactThreads)
                 }
                 else
                 {
-                    const v3 e = V(j == 3, j == 4, j == 5);
-                    doff = cross(e, off);
+                    doff = cross(V(j == 3, j == 4, j == 5), st.off);
                     dxw = doff;
                 }
                 const v3 dYl = mulT(sB.R, dxw);
                 const v3 dgl = V(Hm[0] * dYl.x + Hm[1] * dYl.y + Hm[2] * dYl.z,
                                  Hm[3] * dYl.x + Hm[4] * dYl.y + Hm[5] * dYl.z,
                                  Hm[6] * dYl.x + Hm[7] * dYl.y + Hm[8] * dYl.z);
-                const double dg = dot(gl, dYl);
+                const double dg = dot(st.gl, dYl);
                 const v3 drg = mul(sB.R, dgl);
-                const double dp = dgdd * dg; // p = k delta^n, delta = -g
-                v3 dfq = dp * rg + p * drg;
-                const v3 duA = cross(wA, doff);
-                const v3 duB = cross(wB, dxw);
-                const v3 du = duA - duB;
-                if (damp)
+                const double dp = st.dgdd * dg; // p = k delta^n, delta = -g
+                v3 dfq = dp * st.rg + st.p * drg;
+                const v3 du = cross(wA, doff) - cross(wB, dxw);
+                if (st.damp)
                 {
-                    const double dvn = dot(du, rg) + dot(u, drg);
-                    dfq = dfq + (-prm.damping) * (dvn * rg + vn * drg);
+                    const double dvn = dot(du, st.rg) + dot(st.u, drg);
+                    dfq = dfq + (-prm.damping) * (dvn * st.rg + st.vn * drg);
                 }
-                if (fric)
+                if (st.fric)
                 {
-                    const double dgn = gn > 1e-30 ? dot(gl, dgl) / gn : 0.0;
-                    const double dphat = dp * gn + p * dgn;
-                    const v3 dun = gn > 1e-30 ? (1.0 / gn) * (drg - dot(un, drg) * un)
-                                              : (1.0 / gsafe) * drg;
-                    const double dudn = dot(du, un) + dot(u, dun);
-                    const v3 dut = du - dudn * un - udn * dun;
-                    const double dden = dot(ut, dut) / den;
-                    dfq = dfq + (-prm.friction) * ((dphat / den) * ut + (phat / den) * dut -
-                                                   (phat * dden / (den * den)) * ut);
+                    const double gsafe = st.gn > 1e-30 ? st.gn : 1e-30;
+                    const double dgn = st.gn > 1e-30 ? dot(st.gl, dgl) / st.gn : 0.0;
+                    const double dphat = dp * st.gn + st.p * dgn;
+                    const v3 dun = (1.0 / gsafe) * (st.gn > 1e-30 ? drg - dot(st.un, drg) * st.un : drg);
+                    const double dudn = dot(du, st.un) + dot(st.u, dun);
+                    const v3 dut = du - dudn * st.un - st.udn * dun;
+                    const double dden = dot(st.ut, dut) / st.den;
+                    dfq = dfq + (-prm.friction) * ((dphat / st.den) * st.ut + (st.phat / st.den) * dut -
+                                                   (st.phat * dden / (st.den * st.den)) * st.ut);
                 }
-                const v3 dtq = cross(doff, fq) + cross(off, dfq);
-                acc[6 + 0 * 6 + j] += wq * dfq.x;
-                acc[6 + 1 * 6 + j] += wq * dfq.y;
-                acc[6 + 2 * 6 + j] += wq * dfq.z;
-                acc[6 + 3 * 6 + j] += wq * dtq.x;
-                acc[6 + 4 * 6 + j] += wq * dtq.y;
-                acc[6 + 5 * 6 + j] += wq * dtq.z;
+                const v3 dtq = cross(doff, st.fq) + cross(st.off, dfq);
+                col[0] = st.wq * dfq.x;
+                col[1] = st.wq * dfq.y;
+                col[2] = st.wq * dfq.z;
+                col[3] = st.wq * dtq.x;
+                col[4] = st.wq * dtq.y;
+                col[5] = st.wq * dtq.z;
+            }
+#pragma unroll
+            for (int r = 0; r < 6; ++r)
+            {
+                const double sum = warp_sum(col[r]);
+                if (lane == 0) sjac[warp][6 * r + j] += sum;
             }
         }
     }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
-    for (int q = 0; q < NACC; ++q)
+    for (int q = 0; q < 6; ++q)
     {
         const double s = warp_sum(acc[q]);
         if (lane == 0) red[warp][q] = s;
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < NACC; q += kContactThreads)
+    if (threadIdx.x < 6)
     {
         double s = 0.0;
 #pragma unroll
-        for (int w = 0; w < kContactThreads / 32; ++w) s += red[w][q];
-        if (q < 6)
-            ft[6 * (int64_t)pose + q] = s;
-        else if (jac)
-            jac[36 * (int64_t)pose + (q - 6)] = s;
+        for (int w = 0; w < kWarps; ++w) s += red[w][threadIdx.x];
+        ft[6 * (int64_t)pose + threadIdx.x] = s;
+    }
+    if (JAC && jac != nullptr && threadIdx.x < 36)
+    {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) s += sjac[w][threadIdx.x];
+        jac[36 * (int64_t)pose + threadIdx.x] = s;
     }
 }
 

@@ -69,6 +69,8 @@ GridView make_view(const sdfo_grid* g)
     v.bd = g->info.block_dim;
     v.phin16 = g->d.phin16;
     v.brick_affine = g->d.brick_affine;
+    v.xpair = g->d.xpair;
+    v.cell8 = g->d.cell8;
     return v;
 }
 
@@ -148,6 +150,80 @@ __global__ void k_encode_fp16(const float4* __restrict__ phin, int V, ushort4* _
 
 } // namespace
 
+namespace {
+
+// Dense stencil records from the voxel payload: xpair[v] = {phin[v],
+// phin[v+1]} (x neighbour clamped at the last column), cell8[v] = phi of the
+// 8 cell corners (neighbours clamped at the upper faces; cells there are never
+// interpolated because their upper corners are outside the grid).
+__global__ void k_stencil_layouts(const float4* __restrict__ phin, int nx, int ny, int nz,
+                                  float4* __restrict__ xpair, float4* __restrict__ cell8)
+{
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t N = (int64_t)nx * ny * nz;
+    if (v >= N) return;
+    const int i = (int)(v % nx), j = (int)((v / nx) % ny), k = (int)(v / ((int64_t)nx * ny));
+    const int64_t dx = i + 1 < nx ? 1 : 0;
+    const int64_t dy = j + 1 < ny ? nx : 0;
+    const int64_t dz = k + 1 < nz ? (int64_t)nx * ny : 0;
+    const float4 a = phin[v];
+    xpair[2 * v] = a;
+    xpair[2 * v + 1] = phin[v + dx];
+    cell8[2 * v] = make_float4(a.x, phin[v + dx].x, phin[v + dy].x, phin[v + dx + dy].x);
+    cell8[2 * v + 1] = make_float4(phin[v + dz].x, phin[v + dx + dz].x, phin[v + dy + dz].x,
+                                   phin[v + dx + dy + dz].x);
+}
+
+// Sparse stencil records, per stored voxel: neighbours are found through the
+// block table; a neighbour whose block is not stored gets phi = NaN, which
+// makes any query touching it invalid (as a missing block does in the
+// reference); neighbours outside the grid repeat the voxel (never read).
+__global__ void k_sparse_stencil_layouts(const float4* __restrict__ phin,
+                                         const int32_t* __restrict__ ijk,
+                                         const int32_t* __restrict__ table, int nx, int ny, int nz,
+                                         int bd, int nbx, int nby, int64_t stored,
+                                         float4* __restrict__ xpair, float4* __restrict__ cell8)
+{
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= stored) return;
+    const int V = bd * bd * bd;
+    const int blk = (int)(v / V), local = (int)(v % V);
+    const int i = ijk[3 * blk] * bd + local % bd;
+    const int j = ijk[3 * blk + 1] * bd + (local / bd) % bd;
+    const int k = ijk[3 * blk + 2] * bd + local / (bd * bd);
+    const float4 self = phin[v];
+    auto at = [&](int di, int dj, int dk) -> float4 {
+        const int ii = i + di, jj = j + dj, kk = k + dk;
+        if (ii >= nx || jj >= ny || kk >= nz) return self;
+        const int b2 = table[ii / bd + nbx * (jj / bd + nby * (kk / bd))];
+        if (b2 < 0) return make_float4(NAN, NAN, NAN, NAN);
+        return phin[(int64_t)b2 * V + (ii % bd) + bd * ((jj % bd) + bd * (kk % bd))];
+    };
+    xpair[2 * v] = self;
+    xpair[2 * v + 1] = at(1, 0, 0);
+    cell8[2 * v] = make_float4(self.x, at(1, 0, 0).x, at(0, 1, 0).x, at(1, 1, 0).x);
+    cell8[2 * v + 1] = make_float4(at(0, 0, 1).x, at(1, 0, 1).x, at(0, 1, 1).x, at(1, 1, 1).x);
+}
+
+} // namespace
+
+void build_stencil_layouts(sdfo_grid* g, cudaStream_t s)
+{
+    if (g->stored_voxels == 0 || g->info.storage != SDFO_STORAGE_FP32 || g->d.phin == nullptr)
+        return;
+    const int64_t N = g->stored_voxels;
+    if (!g->d.xpair) g->d.xpair = dalloc<float4>((size_t)N * 2);
+    if (!g->d.cell8) g->d.cell8 = dalloc<float4>((size_t)N * 2);
+    if (g->info.layout == SDFO_LAYOUT_DENSE)
+        k_stencil_layouts<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
+            g->d.phin, g->info.shape[0], g->info.shape[1], g->info.shape[2], g->d.xpair, g->d.cell8);
+    else
+        k_sparse_stencil_layouts<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
+            g->d.phin, g->d.ijk, g->d.table, g->info.shape[0], g->info.shape[1], g->info.shape[2],
+            g->info.block_dim, g->nb[0], g->nb[1], N, g->d.xpair, g->d.cell8);
+    SDFO_CHECK_LAUNCH();
+}
+
 void encode_fp16(const sdfo_grid* src, sdfo_grid* dst, cudaStream_t s)
 {
     const int V = src->info.block_dim * src->info.block_dim * src->info.block_dim;
@@ -179,6 +255,8 @@ sdfo_grid::~sdfo_grid()
     device_free(d.ijk);
     device_free(d.phin16);
     device_free(d.brick_affine);
+    device_free(d.xpair);
+    device_free(d.cell8);
 }
 
 using namespace sdfo;
@@ -240,6 +318,7 @@ int sdfo_grid_create_dense(const sdfo_grid_info* info, const double* h_phi,
             g->d.w64 = dalloc<double>((size_t)N * 3);
             SDFO_CUDA(cudaMemcpyAsync(g->d.w64, h_witness, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, s));
         }
+        build_stencil_layouts(g.get(), s);
         SDFO_CUDA(cudaStreamSynchronize(s));
         *out = g.release();
     });
@@ -517,6 +596,7 @@ int sdfo_grid_create_view(const sdfo_grid* g, void* d_phin, sdfo_grid** out)
         v->d = g->d;
         v->d.phin = static_cast<float4*>(d_phin);
         v->d.phi64 = v->d.n64 = v->d.w64 = v->d.h64 = nullptr; // export reads the live payload
+        v->d.xpair = v->d.cell8 = nullptr; // stencil copies would go stale: read the payload
         v->borrowed = true;
         *out = v.release();
     });

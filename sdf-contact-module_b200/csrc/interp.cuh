@@ -91,6 +91,15 @@ __device__ __forceinline__ bool nearest_voxel(const GridView& g, const double p[
     return ok;
 }
 
+// One 256-bit read-only load (sm_100: ld.global.nc.v8.f32) of a 32-byte
+// aligned record: a single L1 request and one 32-byte sector.
+__device__ __forceinline__ void ld256(const float4* p, float4& a, float4& b)
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(p));
+}
+
 __device__ __forceinline__ int64_t dense_index(const GridView& g, int i, int j, int k)
 {
     return (int64_t)i + (int64_t)g.nx * ((int64_t)j + (int64_t)g.ny * (int64_t)k);

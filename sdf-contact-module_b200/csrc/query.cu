@@ -53,9 +53,34 @@ __device__ __forceinline__ bool evaluate(const GridView& g, const double p[3], I
     {
         const Cell c = cell_of(g, p);
         if (!c.ok) return false;
+        if (!SPARSE && MODE == SDFO_TRILINEAR && g.cell8 != nullptr)
+        {
+            // one 32-byte load: the 8 corner phi of the cell
+            float4 a, b;
+            ld256(g.cell8 + 2 * dense_index(g, c.i0, c.j0, c.k0), a, b);
+            const float phi[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+            r = trilinear<HESS>(phi, c.u, c.v, c.w, h);
+            unit_of(r.g, unit);
+            return true;
+        }
         float4 cs[8];
-        int64_t idx[8];
-        if (!gather_corners<SPARSE, BD>(g, c, cs, idx)) return false;
+        if (!SPARSE && MODE == SDFO_TRICUBIC && g.xpair != nullptr)
+        {
+            // four 32-byte loads: the x-pairs of the 4 (dj, dk) corner rows
+            const int64_t base = dense_index(g, c.i0, c.j0, c.k0);
+            const int64_t sy = g.nx, sz = (int64_t)g.nx * g.ny;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                const int64_t v = base + ((q & 1) ? sy : 0) + ((q & 2) ? sz : 0);
+                ld256(g.xpair + 2 * v, cs[2 * q], cs[2 * q + 1]);
+            }
+        }
+        else
+        {
+            int64_t idx[8];
+            if (!gather_corners<SPARSE, BD>(g, c, cs, idx)) return false;
+        }
         if (MODE == SDFO_TRICUBIC)
         {
             r = tricubic<HESS>(cs, c.u, c.v, c.w, h);
@@ -126,18 +151,55 @@ __device__ __forceinline__ bool evaluate(const GridView& g, const double p[3], I
     return true;
 }
 
-template <int MODE, bool SPARSE, int BD, typename PT, bool HESS>
+// Block-cooperative I/O of 3-float records (points in, gradient / unit /
+// witness out): the block's 256 records are one contiguous 3 KB range, moved
+// with 16-byte accesses through shared memory instead of three 4-byte
+// accesses per thread at a 12-byte stride.  Used when the pointers are
+// 16-byte aligned (the host checks); `cnt` = records of this block.
+__device__ __forceinline__ void stage_in3(float* sbuf, const float* src, int cnt)
+{
+    const int nf = 3 * cnt, nv = nf >> 2;
+    for (int t = threadIdx.x; t < nv; t += kThreads)
+        reinterpret_cast<float4*>(sbuf)[t] = __ldcs(reinterpret_cast<const float4*>(src) + t);
+    for (int t = 4 * nv + threadIdx.x; t < nf; t += kThreads) sbuf[t] = __ldcs(src + t);
+}
+
+__device__ __forceinline__ void stage_out3(float* sbuf, float* dst, int cnt)
+{
+    const int nf = 3 * cnt, nv = nf >> 2;
+    for (int t = threadIdx.x; t < nv; t += kThreads)
+        __stcs(reinterpret_cast<float4*>(dst) + t, reinterpret_cast<const float4*>(sbuf)[t]);
+    for (int t = 4 * nv + threadIdx.x; t < nf; t += kThreads) __stcs(dst + t, sbuf[t]);
+}
+
+template <int MODE, bool SPARSE, int BD, typename PT, bool HESS, bool STAGED>
 __global__ void __launch_bounds__(kThreads) k_query(GridView g, const PT* __restrict__ pts,
                                                   int64_t n, QueryOutputs o)
 {
-    const int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x;
-    if (q >= n) return;
-    double p[3];
-    load_point(pts, q, p);
+    __shared__ __align__(16) float sbuf[STAGED ? 3 * kThreads : 1];
+    const int64_t q0 = (int64_t)blockIdx.x * kThreads;
+    const int64_t q = q0 + threadIdx.x;
+    const bool active = q < n;
+    const int cnt = (int)(n - q0 < kThreads ? n - q0 : kThreads);
+    double p[3] = {0.0, 0.0, 0.0};
+    if (STAGED)
+    {
+        stage_in3(sbuf, reinterpret_cast<const float*>(pts) + 3 * q0, cnt);
+        __syncthreads();
+        if (active)
+        {
+            p[0] = sbuf[3 * threadIdx.x];
+            p[1] = sbuf[3 * threadIdx.x + 1];
+            p[2] = sbuf[3 * threadIdx.x + 2];
+        }
+    }
+    else if (active)
+    {
+        load_point(pts, q, p);
+    }
     Interp r;
     float unit[3];
-    bool valid;
-    valid = evaluate<MODE, SPARSE, BD, HESS>(g, p, r, unit);
+    const bool valid = active && evaluate<MODE, SPARSE, BD, HESS>(g, p, r, unit);
     if (!valid)
     {
         r.gap = 0.f;
@@ -147,27 +209,44 @@ __global__ void __launch_bounds__(kThreads) k_query(GridView g, const PT* __rest
 #pragma unroll
         for (int a = 0; a < 6; ++a) r.H[a] = 0.f;
     }
-    __stcs(o.gap + q, r.gap);
-    if (o.grad)
+    if (active)
     {
-        __stcs(o.grad + 3 * q + 0, r.g[0]);
-        __stcs(o.grad + 3 * q + 1, r.g[1]);
-        __stcs(o.grad + 3 * q + 2, r.g[2]);
+        __stcs(o.gap + q, r.gap);
+        if (o.valid) o.valid[q] = valid ? 1 : 0;
     }
-    if (o.unit)
-    {
-        __stcs(o.unit + 3 * q + 0, unit[0]);
-        __stcs(o.unit + 3 * q + 1, unit[1]);
-        __stcs(o.unit + 3 * q + 2, unit[2]);
-    }
-    if (o.witness)
-    {
+    float w[3];
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-            __stcs(o.witness + 3 * q + a, valid ? (float)(p[a] - (double)r.gap * unit[a]) : 0.f);
+    for (int a = 0; a < 3; ++a) w[a] = valid ? (float)(p[a] - (double)r.gap * unit[a]) : 0.f;
+    if (STAGED)
+    {
+        // o.grad / o.unit / o.witness are uniform over the block
+        const float* outs[3] = {r.g, unit, w};
+        float* dsts[3] = {o.grad, o.unit, o.witness};
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            if (dsts[k] == nullptr) continue;
+            __syncthreads();
+            sbuf[3 * threadIdx.x] = outs[k][0];
+            sbuf[3 * threadIdx.x + 1] = outs[k][1];
+            sbuf[3 * threadIdx.x + 2] = outs[k][2];
+            __syncthreads();
+            stage_out3(sbuf, dsts[k] + 3 * q0, cnt);
+        }
     }
-    if (o.valid) o.valid[q] = valid ? 1 : 0;
-    if (HESS)
+    else if (active)
+    {
+        if (o.grad)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) __stcs(o.grad + 3 * q + a, r.g[a]);
+        if (o.unit)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) __stcs(o.unit + 3 * q + a, unit[a]);
+        if (o.witness)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) __stcs(o.witness + 3 * q + a, w[a]);
+    }
+    if (HESS && active)
     {
         const float H9[9] = {r.H[0], r.H[1], r.H[2], r.H[1], r.H[3], r.H[4], r.H[2], r.H[4], r.H[5]};
 #pragma unroll
@@ -276,29 +355,34 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+template <int MODE, bool SPARSE, int BD, bool HESS>
+void launch_pt2(const GridView& v, const void* pts, bool f64, bool staged, int64_t n,
+                const QueryOutputs& o, cudaStream_t s)
+{
+    const unsigned blocks = (unsigned)((n + kThreads - 1) / kThreads);
+    if (f64)
+        k_query<MODE, SPARSE, BD, double, HESS, false><<<blocks, kThreads, 0, s>>>(
+            v, static_cast<const double*>(pts), n, o);
+    else if (staged)
+        k_query<MODE, SPARSE, BD, float, HESS, true><<<blocks, kThreads, 0, s>>>(
+            v, static_cast<const float*>(pts), n, o);
+    else
+        k_query<MODE, SPARSE, BD, float, HESS, false><<<blocks, kThreads, 0, s>>>(
+            v, static_cast<const float*>(pts), n, o);
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 template <int MODE, bool SPARSE, int BD>
 void launch_pt(const GridView& v, const void* pts, bool f64, int64_t n, const QueryOutputs& o,
                cudaStream_t s)
 {
-    const unsigned blocks = (unsigned)((n + kThreads - 1) / kThreads);
-    if (f64)
-    {
-        if (o.hess)
-            k_query<MODE, SPARSE, BD, double, true><<<blocks, kThreads, 0, s>>>(
-                v, static_cast<const double*>(pts), n, o);
-        else
-            k_query<MODE, SPARSE, BD, double, false><<<blocks, kThreads, 0, s>>>(
-                v, static_cast<const double*>(pts), n, o);
-    }
+    const bool staged = !f64 && aligned16(pts) && aligned16(o.grad) && aligned16(o.unit) &&
+                        aligned16(o.witness);
+    if (o.hess)
+        launch_pt2<MODE, SPARSE, BD, true>(v, pts, f64, staged, n, o, s);
     else
-    {
-        if (o.hess)
-            k_query<MODE, SPARSE, BD, float, true><<<blocks, kThreads, 0, s>>>(
-                v, static_cast<const float*>(pts), n, o);
-        else
-            k_query<MODE, SPARSE, BD, float, false><<<blocks, kThreads, 0, s>>>(
-                v, static_cast<const float*>(pts), n, o);
-    }
+        launch_pt2<MODE, SPARSE, BD, false>(v, pts, f64, staged, n, o, s);
 }
 
 template <int MODE>

@@ -121,6 +121,8 @@ struct GridStorage
     int32_t* ijk = nullptr;
     ushort4* phin16 = nullptr;
     float2* brick_affine = nullptr;
+    float4* xpair = nullptr; // 2 float4 per voxel
+    float4* cell8 = nullptr; // 2 float4 per voxel
 };
 
 } // namespace sdfo
@@ -160,9 +162,16 @@ struct GridView
     int bd;
     const ushort4* phin16;
     const float2* brick_affine;
+    // Dense stencil layouts (32-byte records, one 256-bit load each), or NULL:
+    //   xpair[v] = {phin[v], phin[v + 1]}             Tricubic: 4 loads / query
+    //   cell8[v] = phi of the 8 corners of cell v       Trilinear: 1 load / query
+    const float4* xpair;
+    const float4* cell8;
 };
 
 GridView make_view(const sdfo_grid* g);
+// Fills the dense stencil layouts from phin (grid.cu).
+void build_stencil_layouts(sdfo_grid* g, cudaStream_t s);
 
 // Query launch (query.cu).
 struct QueryOutputs
