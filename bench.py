@@ -57,6 +57,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--skip-c4", action="store_true",
+                    help="leave out the 256-gear batched build / query section")
+    ap.add_argument("--skip-c5", action="store_true",
+                    help="leave out the 512^3 icosphere section (about 30 s of setup)")
     return ap.parse_args()
 
 
@@ -254,6 +258,237 @@ def timed(torch, fn, steps, warmup, flush, stream):
     return sum(s.elapsed_time(e) for s, e in evs)
 
 
+# algorithmic bytes per C5 query (sparse, 8^3 bricks): forward = point 12 +
+# gap 4 + grad 12 + valid 1 + 8 corners x {phi, n} (16 B FP32 / 8 B FP16) +
+# brick-table entry 4 (+ FP16 per-brick scale/offset 8); the saved-Hessian
+# forward adds 24 B (hess6 write).  Backward: dgap 4 + dgrad 12 + grad 12 +
+# hess6 24 + dpts 12 (points) and point 12 + valid 1 + table 4 + 8 corners x
+# 16 B read-modify-write (grid).
+C5_FWD_BYTES = {"fp32": 12 + 4 + 12 + 1 + 8 * 16 + 4, "fp16": 12 + 4 + 12 + 1 + 8 * 8 + 4 + 8}
+C5_LIN_EXTRA = 24
+C5_BWD_POINTS_BYTES = 4 + 12 + 12 + 24 + 12
+C5_BWD_GRID_BYTES = 12 + 1 + 4 + 8 * 16 * 2
+
+
+def c5_section(torch, lib, N, dev, stream, flush, steps, warmup, peak):
+    """Config 5: perturbed icosphere (1.31M tris) sparse 512^3, FP32 and FP16
+    storage; 16M Tricubic queries within 4 voxels of the surface; forward,
+    differentiable forward + backward w.r.t. points and grid, and the
+    forward + central-difference baseline."""
+    import ctypes
+
+    from sdfo import SdfGrid
+    from sdfo import workloads as W
+
+    def P(t):
+        return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+    def sp():
+        return ctypes.c_void_p(stream.cuda_stream)
+
+    c = W.c5_icosphere()
+    N.check(lib.sdfo_set_bvh_mode(N.BVH_REFERENCE))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g32 = SdfGrid.build_sparse(c["verts"], c["tris"], mode=TRICUBIC, **c["sparse"])
+    t_build = time.perf_counter() - t0
+    st = g32.build_stats()
+    N.check(lib.sdfo_set_bvh_mode(N.BVH_LBVH))
+    t0 = time.perf_counter()
+    gl = SdfGrid.build_sparse(c["verts"], c["tris"], mode=TRICUBIC, **c["sparse"])
+    t_lbvh = time.perf_counter() - t0
+    st_l = gl.build_stats()
+    same_occupancy = bool(gl.block_count == g32.block_count)
+    gl.close()
+    N.check(lib.sdfo_set_bvh_mode(N.BVH_REFERENCE))
+    g16 = g32.to_fp16()
+    h = float(g32.voxel[0])
+    pts = torch.tensor(W.c5_points(c["verts"], c["tris"], h), device=dev)
+    n = pts.shape[0]
+    f32 = dict(device=dev, dtype=torch.float32)
+    gap, grad = torch.empty(n, **f32), torch.empty((n, 3), **f32)
+    gap16, grad16 = torch.empty(n, **f32), torch.empty((n, 3), **f32)
+    valid = torch.empty(n, dtype=torch.uint8, device=dev)
+    valid16 = torch.empty(n, dtype=torch.uint8, device=dev)
+    hess6 = torch.empty((n, 6), **f32)
+    gen = torch.Generator(device=dev).manual_seed(7)
+    dgap = torch.randn(n, generator=gen, **f32)
+    dgrad = torch.randn((n, 3), generator=gen, **f32)
+    dpts = torch.empty((n, 3), **f32)
+    dgrid = torch.empty((g32.stored_voxels, 4), **f32)
+
+    def fwd(g, gp, gr, va):
+        N.check(lib.sdfo_query(g.handle, TRICUBIC, P(pts), 0, n, P(gp), P(gr), None, None,
+                               P(va), None, sp()))
+
+    def ad(g, with_grid):
+        N.check(lib.sdfo_query_linearize(g.handle, TRICUBIC, P(pts), n, P(gap), P(grad),
+                                         P(valid), P(hess6), sp()))
+        if with_grid:
+            dgrid.zero_()
+        N.check(lib.sdfo_query_backward_saved(g.handle, TRICUBIC, P(pts), n, P(grad), P(hess6),
+                                              P(valid), P(dgap), P(dgrad), P(dpts),
+                                              P(dgrid) if with_grid else None, sp()))
+
+    fd_h = 1e-3 * h
+    shifts = torch.zeros((6, 1, 3), **f32)
+    for a in range(3):
+        shifts[2 * a, 0, a] = fd_h
+        shifts[2 * a + 1, 0, a] = -fd_h
+    xfd = torch.empty((6, n, 3), **f32)
+    gfd = torch.empty(6 * n, **f32)
+    nfd = torch.empty((6 * n, 3), **f32)
+
+    def fd(g):
+        fwd(g, gap, grad, valid)
+        torch.add(pts.unsqueeze(0), shifts, out=xfd)
+        N.check(lib.sdfo_query(g.handle, TRICUBIC, P(xfd), 0, 6 * n, P(gfd), P(nfd), None, None,
+                               None, None, sp()))
+        gg = gfd.view(3, 2, n)
+        nn = nfd.view(3, 2, n, 3)
+        return (gg[:, 0] - gg[:, 1]) / (2 * fd_h), (nn[:, 0] - nn[:, 1]) / (2 * fd_h)
+
+    ms = {}
+    ms["fwd_fp32"] = timed(torch, lambda: fwd(g32, gap, grad, valid), steps, warmup, flush,
+                           stream) / steps
+    ms["fwd_fp16"] = timed(torch, lambda: fwd(g16, gap16, grad16, valid16), steps, warmup, flush,
+                           stream) / steps
+    ms["ad_points_fp32"] = timed(torch, lambda: ad(g32, False), steps, warmup, flush,
+                                 stream) / steps
+    ms["ad_points_grid_fp32"] = timed(torch, lambda: ad(g32, True), steps, warmup, flush,
+                                      stream) / steps
+    ms["ad_points_fp16"] = timed(torch, lambda: ad(g16, False), steps, warmup, flush,
+                                 stream) / steps
+    ms["fd_fp32"] = timed(torch, lambda: fd(g32), steps, warmup, flush, stream) / steps
+    # FP16 storage against FP32 storage on the same points (the FP32 grid's
+    # own error against the FP64 oracle is pinned by the tests)
+    fwd(g32, gap, grad, valid)
+    fwd(g16, gap16, grad16, valid16)
+    torch.cuda.synchronize()
+    both = (valid > 0) & (valid16 > 0)
+    dg = (gap16 - gap)[both].abs()
+    dn = (grad16 - grad)[both].abs().amax(dim=1)
+    gb = C5_FWD_BYTES["fp32"] + C5_LIN_EXTRA + C5_BWD_POINTS_BYTES
+    gbg = gb + C5_BWD_GRID_BYTES
+    rate = {k: n / (v * 1e-3) for k, v in ms.items()}
+    ach = {
+        "fwd_fp32": C5_FWD_BYTES["fp32"] * rate["fwd_fp32"] / 1e9,
+        "fwd_fp16": C5_FWD_BYTES["fp16"] * rate["fwd_fp16"] / 1e9,
+        "ad_points_fp32": gb * rate["ad_points_fp32"] / 1e9,
+        "ad_points_grid_fp32": gbg * rate["ad_points_grid_fp32"] / 1e9,
+    }
+    out = {
+        "workload": "perturbed_icosphere_1310720tris_sparse512_band3_16M_tricubic",
+        "grid": list(g32.shape), "bricks": g32.block_count, "stored_voxels": g32.stored_voxels,
+        "pool_mb_fp32": round(16 * g32.stored_voxels / 2**20, 1),
+        "pool_mb_fp16": round(8 * g32.stored_voxels / 2**20, 1),
+        "queries_per_step": n, "valid_fraction": float(valid.float().mean()),
+        "build_ms": 1e3 * t_build, "build_fill_ms": st["fill_ms"], "build_bvh_ms": st["bvh_ms"],
+        "build_stored_voxels_per_s": g32.stored_voxels / t_build,
+        "build_candidate_blocks": st["candidate_blocks"],
+        "lbvh_build_ms": 1e3 * t_lbvh, "lbvh_fill_ms": st_l["fill_ms"],
+        "lbvh_same_block_count": same_occupancy,
+        "queries_per_s": rate,
+        "ad_vs_fd_speedup_fp32": ms["fd_fp32"] / ms["ad_points_fp32"],
+        "gather_model_gbs": ach,
+        "hbm_frac": {k: v / peak for k, v in ach.items()},
+        "bytes_per_query": {"fwd_fp32": C5_FWD_BYTES["fp32"], "fwd_fp16": C5_FWD_BYTES["fp16"],
+                            "ad_points_fp32": gb, "ad_points_grid_fp32": gbg},
+        "fp16_vs_fp32": {"max_abs_gap_over_h": float(dg.max()) / h,
+                         "mean_abs_gap_over_h": float(dg.mean()) / h,
+                         "max_abs_grad": float(dn.max()), "mean_abs_grad": float(dn.mean())},
+        "l2": "flushed (256 MB write) before every timed step; brick pool exceeds L2",
+    }
+    for g in (g16, g32):
+        g.close()
+    return out
+
+
+def c4_section(torch, lib, N, dev, stream, flush, steps, warmup):
+    """Config 4: 256 gear prisms (2k-60k tris, sparse 64^3..256^3, band 3):
+    one batched build against 256 single builds, then 256 x 65,536 Tricubic
+    queries under random poses as one captured CUDA graph (the launch shape
+    picked by the autotuner) against 256 per-grid launches."""
+    from sdfo import SdfGrid
+    from sdfo import workloads as W
+    from sdfo.batch import QueryBatch, pack_poses
+    from sdfo.tune import tune_query_batch
+
+    gears = W.c4_gears()
+    args = [dict(verts=g["verts"], tris=g["tris"], **g["sparse"]) for g in gears]
+    N.check(lib.sdfo_set_bvh_mode(N.BVH_REFERENCE))
+    for g in SdfGrid.build_sparse_batched(args[:8]):  # warm
+        g.close()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    grids = SdfGrid.build_sparse_batched(args, mode=TRICUBIC)
+    t_batch = time.perf_counter() - t0
+    st = grids[0].build_stats()
+    t0 = time.perf_counter()
+    for a in args:
+        SdfGrid.build_sparse(a["verts"], a["tris"], mode=TRICUBIC,
+                             **{k: v for k, v in a.items() if k not in ("verts", "tris")}).close()
+    torch.cuda.synchronize()
+    t_single = time.perf_counter() - t0
+    stored = sum(g.stored_voxels for g in grids)
+    n_per = 65_536
+    rng = np.random.default_rng(3)
+    world, R, t = [], [], []
+    for g, grid in zip(gears, grids):
+        p = W.near_surface_points(g["verts"], g["tris"], float(grid.voxel[0]), n_per,
+                                  int(rng.integers(1 << 30)))
+        k = rng.normal(size=3)
+        k /= np.linalg.norm(k)
+        ang = rng.uniform(0.0, np.pi)
+        K = np.array([[0.0, -k[2], k[1]], [k[2], 0.0, -k[0]], [-k[1], k[0], 0.0]])
+        Rg = np.eye(3) + np.sin(ang) * K + (1.0 - np.cos(ang)) * (K @ K)
+        tg = rng.uniform(-0.5, 0.5, 3)
+        world.append((p.astype(np.float64) @ Rg.T + tg).astype(np.float32))
+        R.append(Rg)
+        t.append(tg)
+    x = torch.tensor(np.concatenate(world), device=dev)
+    poses = pack_poses(np.array(R), np.array(t), device=dev)
+    qb = QueryBatch(grids, [n_per] * len(grids))
+    tuned = tune_query_batch(qb, x, poses, reps=10, warmup=2)
+    graph, out = qb.capture(x, poses)
+    total = qb.total
+    graph_ms = timed(torch, graph.replay, steps, warmup, flush, stream) / steps
+    # the same queries as 256 separate single-grid launches (local points)
+    import ctypes
+
+    xs = [x[i * n_per:(i + 1) * n_per] for i in range(len(grids))]
+    gap = torch.empty(n_per, device=dev)
+    grad = torch.empty((n_per, 3), device=dev)
+
+    def per_grid():
+        for grid, xi in zip(grids, xs):
+            N.check(lib.sdfo_query(grid.handle, TRICUBIC, ctypes.c_void_p(xi.data_ptr()), 0, n_per,
+                                   ctypes.c_void_p(gap.data_ptr()), ctypes.c_void_p(grad.data_ptr()),
+                                   None, None, None, None, ctypes.c_void_p(stream.cuda_stream)))
+
+    per_grid_ms = timed(torch, per_grid, max(3, steps // 4), warmup, flush, stream) / max(3, steps // 4)
+    valid = float(out[2].float().mean())
+    res = {
+        "workload": "256_gear_prisms_sparse64-256_band3_65536q_each_tricubic_posed",
+        "meshes": len(grids), "triangles": int(sum(len(g["tris"]) for g in gears)),
+        "stored_voxels": int(stored), "bricks": int(sum(g.block_count for g in grids)),
+        "batched_build_ms": 1e3 * t_batch, "single_builds_ms": 1e3 * t_single,
+        "batched_build_speedup": t_single / t_batch,
+        "batched_fill_ms": st["fill_ms"], "batched_bvh_ms": st["bvh_ms"],
+        "batched_stored_voxels_per_s": stored / t_batch,
+        "queries": total, "valid_fraction": valid,
+        "graph_queries_per_s": total / (graph_ms * 1e-3),
+        "per_grid_launches_queries_per_s": total / (per_grid_ms * 1e-3),
+        "graph_vs_per_grid_speedup": per_grid_ms / graph_ms,
+        "autotuned_threads": tuned["threads"],
+        "autotune_ms": {str(k): v for k, v in tuned["ms"].items()},
+    }
+    qb.close()
+    for g in grids:
+        g.close()
+    return res
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -344,12 +579,24 @@ def run_ours(args, rank, world, local_rank):
     dgrad = torch.randn((n, 3), device=dev)
     dpts = torch.empty((n, 3), device=dev)
 
+    hess6 = torch.empty((n, 6), device=dev)
+
     def ad_step():
+        # what sdfo.autograd runs for float32 points: forward + saved Hessian,
+        # then the elementwise backward (no second stencil gather)
+        N.check(lib.sdfo_query_linearize(dense.handle, TRICUBIC, P(pts), n, P(gap), P(grad),
+                                         P(valid), P(hess6), sptr()))
+        N.check(lib.sdfo_query_backward_saved(dense.handle, TRICUBIC, P(pts), n, P(grad),
+                                              P(hess6), P(valid), P(dgap), P(dgrad), P(dpts),
+                                              None, sptr()))
+
+    def ad_regather_step():
         query(dense)
         N.check(lib.sdfo_query_backward(dense.handle, TRICUBIC, P(pts), n, P(dgap), P(dgrad),
                                         P(dpts), None, sptr()))
 
     ad_ms = timed(torch, ad_step, args.steps, args.warmup, flush, stream) / args.steps
+    ad_rg_ms = timed(torch, ad_regather_step, args.steps, args.warmup, flush, stream) / args.steps
     hess = torch.empty((n, 3, 3), device=dev)
     jac_ms = timed(torch, lambda: query(dense, out_hess=hess), args.steps, args.warmup, flush,
                    stream) / args.steps
@@ -413,6 +660,14 @@ def run_ours(args, rank, world, local_rank):
     batch3 = ContactBatch(cube, cc["quad_x"], cc["quad_w"], mode=3, **cc["params"])
     ct_ad3 = timed(torch, lambda: batch3.evaluate(poses, body_b, jacobian=True), csteps,
                    args.warmup, flush, stream) / csteps
+    peak, peak_src = measured_peaks()
+    c4 = None
+    if not args.skip_c4:
+        c4 = c4_section(torch, lib, N, dev, stream, flush, max(3, args.steps // 20), args.warmup)
+    c5 = None
+    if not args.skip_c5:
+        c5 = c5_section(torch, lib, N, dev, stream, flush, max(3, args.steps // 20),
+                        args.warmup, peak)
     clk = clocks.stop()
 
     # ---- CPU baseline (reference OpenMP loop), rank 0 only ----
@@ -425,7 +680,6 @@ def run_ours(args, rank, world, local_rank):
                          f"({secs:.2f} s of CPU time)"}
         cpu_build = cpu_build_rate(c)
 
-    peak, peak_src = measured_peaks()
     achieved = BYTES_PER_QUERY * n / per_launch_s / 1e9
     traffic = ncu_traffic("tricubic_dense_c2")
     line = {
@@ -466,6 +720,7 @@ def run_ours(args, rank, world, local_rank):
             "dense_tricubic_fwd_per_s": n / per_launch_s,
             "sparse_tricubic_fwd_per_s": n / (sparse_ms * 1e-3),
             "ad_fwd_bwd_per_s": n / (ad_ms * 1e-3),
+            "ad_fwd_bwd_regather_per_s": n / (ad_rg_ms * 1e-3),
             "fused_jacobian_per_s": n / (jac_ms * 1e-3),
             "fd_jacobian_per_s": n / (fd_ms * 1e-3),
             "ad_vs_fd_speedup": fd_ms / ad_ms,
@@ -479,6 +734,8 @@ def run_ours(args, rank, world, local_rank):
             "ad_vs_fd_speedup": ct_fd / ct_ad,
             "tricubic_fwd_jac_poses_per_s": 4096 / (ct_ad3 * 1e-3),
         },
+        "c4": c4,
+        "c5": c5,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -188,6 +188,31 @@ int sdfo_grid_build_dense(const double* h_verts, int64_t nv, const int32_t* h_tr
 int sdfo_grid_build_sparse(const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
                            const sdfo_sparse_build_params* p, void* stream, sdfo_grid** out);
 
+/* One mesh of a batched build: host arrays as for sdfo_grid_build_sparse. */
+typedef struct
+{
+    const double* h_verts; /* (nv, 3) float64 */
+    int64_t nv;
+    const int32_t* h_tris; /* (nt, 3) int32 */
+    int64_t nt;
+    sdfo_sparse_build_params params;
+} sdfo_mesh_desc;
+
+/* Many sparse builds in one pass (no reference counterpart as a single
+ * call; each grid equals SdfBuilder::buildSparse of its mesh and params):
+ * the per-mesh trees are built on host threads (or on the device in LBVH
+ * mode), then ONE block-activation launch over every mesh's candidate
+ * blocks, one scan, ONE persistent brick-fill launch whose CTAs take bricks
+ * of any mesh from a shared work counter (meshes of very different sizes
+ * load-balance), and one Hessian launch.  All meshes must use the same
+ * block_dim.  out[n] receives one handle per mesh; the handles share one
+ * device allocation, released with the last of them.  Synchronous. */
+int sdfo_grid_build_sparse_batched(const sdfo_mesh_desc* meshes, int32_t n, void* stream,
+                                   sdfo_grid** out);
+/* CTAs per SM of the persistent brick fill of batched builds (process-wide;
+ * 0 = as many as fit, the default) -- a knob of the autotuner. */
+int sdfo_set_fill_ctas_per_sm(int32_t ctas);
+
 int sdfo_grid_build_stats(const sdfo_grid* g, sdfo_build_stats* out);
 
 /* Selects the acceleration structure of subsequent builds (process-wide;
@@ -284,11 +309,67 @@ int sdfo_query_host_static(const sdfo_grid* g, int32_t mode, const void* h_point
  * d_dgap[n] and d_dgrad[n*3] (either may be NULL = zero), writes
  *   d_dpoints[n*3] = dgap * grad + H * dgrad        (may be NULL)
  * and accumulates into d_dgrid (float4 per stored voxel: d phi, d n) the
- * gradient w.r.t. the stored payload (may be NULL).  Trilinear and Tricubic
- * on FP32 storage; float32 points. */
+ * gradient w.r.t. the stored payload (may be NULL; for FP16 storage, w.r.t.
+ * the decoded values).  Trilinear and Tricubic; float32 points. */
 int sdfo_query_backward(const sdfo_grid* g, int32_t mode, const float* d_points, int64_t n,
                         const float* d_dgap, const float* d_dgrad, float* d_dpoints,
                         float* d_dgrid, void* stream);
+
+/* Forward of the differentiable query (no reference counterpart):
+ * sdfo_query on float32 points that also writes, per point, the symmetric
+ * Hessian of the interpolant d_hess6[n*6] = {xx, xy, xz, yy, yz, zz} (zero
+ * where invalid) -- the local linearisation that reverse mode needs, so
+ * that sdfo_query_backward_saved reads 24 bytes per point instead of the
+ * grid stencil.  d_gap, d_grad, d_valid and d_hess6 are required.
+ * Trilinear and Tricubic. */
+int sdfo_query_linearize(const sdfo_grid* g, int32_t mode, const float* d_points, int64_t n,
+                         float* d_gap, float* d_grad, uint8_t* d_valid, float* d_hess6,
+                         void* stream);
+
+/* Backward from the linearisation of sdfo_query_linearize (same grid, mode
+ * and points):
+ *   d_dpoints[n*3] = dgap * grad + H * dgrad     (needs d_grad, d_hess6)
+ *   d_dgrid       += dL/d(stored {phi, n})       (needs d_points, d_valid)
+ * Either output may be NULL; d_dgap / d_dgrad may be NULL (= zero).  The
+ * grid gradient uses only the corner weights at each point, so it is
+ * defined for FP32 and FP16 storage alike (w.r.t. the decoded values). */
+int sdfo_query_backward_saved(const sdfo_grid* g, int32_t mode, const float* d_points, int64_t n,
+                              const float* d_grad, const float* d_hess6, const uint8_t* d_valid,
+                              const float* d_dgap, const float* d_dgrad, float* d_dpoints,
+                              float* d_dgrid, void* stream);
+
+/* ---- batched queries over many grids (no reference counterpart) --------- */
+/* Rigid placement of a grid in the world: x_world = R x_grid + t (R
+ * row-major).  A query point p is looked up at R^T (p - t) (FP64) and its
+ * gradient returned in the world frame, R grad. */
+typedef struct
+{
+    double R[9];
+    double t[3];
+} sdfo_pose;
+
+typedef struct sdfo_query_batch sdfo_query_batch;
+
+/* A fixed layout of queries over n grids: grid g answers h_counts[g]
+ * consecutive points (grids in order).  The grids must outlive the batch
+ * and stay on one device.  Uploads the grid descriptors once, so that
+ * sdfo_query_batch_run allocates nothing and can be captured in a CUDA
+ * graph. */
+int sdfo_query_batch_create(const sdfo_grid* const* grids, int32_t n, const int64_t* h_counts,
+                            sdfo_query_batch** out);
+/* One launch over all grids' queries: d_points (total, 3) float32 world
+ * points; d_poses (n) device array or NULL (identity); outputs d_gap
+ * (total), d_grad (total, 3, world frame, may be NULL), d_valid (total, may
+ * be NULL).  Trilinear or Tricubic; dense and sparse (FP32 / FP16) grids
+ * may be mixed.  Asynchronous on `stream`. */
+int sdfo_query_batch_run(const sdfo_query_batch* b, int32_t mode, const float* d_points,
+                         const sdfo_pose* d_poses, float* d_gap, float* d_grad, uint8_t* d_valid,
+                         void* stream);
+/* Launch shape of sdfo_query_batch_run: threads per CTA, 128, 256 (default)
+ * or 512 -- the knob the autotuner sets. */
+int sdfo_query_batch_set_threads(sdfo_query_batch* b, int32_t threads);
+int sdfo_query_batch_total(const sdfo_query_batch* b, int64_t* total);
+int sdfo_query_batch_destroy(sdfo_query_batch* b);
 
 /* ---- contact (SDFContactEngine.evaluate) --------------------------------- */
 /* Batched SDFContactEngine.evaluate (prototype/src/dynamics/contacts_sdf.py:

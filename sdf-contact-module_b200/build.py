@@ -3,8 +3,8 @@
     python sdf-contact-module_b200/build.py [--force] [--verbose]
 
 Each translation unit is compiled with
-``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``; build.cu (the FP64
-distance / sign path) additionally with ``-fmad=false`` so its FP64
+``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``; build.cu and
+batch.cu (the FP64 distance / sign path) additionally with ``-fmad=false`` so their FP64
 expressions are evaluated exactly in source order.  The static CUDA runtime
 is linked in so the library does not depend on the toolkit's libcudart at
 run time.  Objects go to _build/, the library to lib/.
@@ -28,9 +28,10 @@ INCLUDE = os.path.join(ROOT, "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
           "-ffp-contract=off", "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
-PER_FILE = {"build.cu": ["-fmad=false"]}
-SOURCES = ["grid.cu", "capi.cu", "query.cu", "build.cu", "contact.cu", "static_staging.cu"]
-HEADERS = ["sdfo_internal.cuh", "interp.cuh"]
+PER_FILE = {"build.cu": ["-fmad=false"], "batch.cu": ["-fmad=false"]}
+SOURCES = ["grid.cu", "capi.cu", "query.cu", "build.cu", "batch.cu", "batch_query.cu",
+           "contact.cu", "static_staging.cu"]
+HEADERS = ["sdfo_internal.cuh", "interp.cuh", "build_common.cuh"]
 
 
 def nvcc() -> str:

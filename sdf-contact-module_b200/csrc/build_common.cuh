@@ -1,0 +1,1256 @@
+// Device building blocks of the SDF builders, shared by the single-mesh
+// builders (build.cu) and the batched builder (batch.cu): FP64 triangle
+// primitives in the reference's operation order, the LBVH and the
+// reference-order tree with their traversals, and the fill / Hessian /
+// activation kernels.  Every translation unit that includes this header is
+// compiled with -fmad=false (FP64 expressions evaluated as written), which is
+// what makes the builds bit-identical to the reference's FP64 arithmetic.
+#pragma once
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "sdfo_internal.cuh"
+
+namespace sdfo {
+
+namespace {
+
+constexpr int kStackDepth = 64;
+constexpr int kStatusStackOverflow = 1;
+
+// ---------------------------------------------------------------------------
+// FP64 triangle primitives, in the reference's operation order
+// ---------------------------------------------------------------------------
+struct d3
+{
+    double x, y, z;
+};
+__device__ __forceinline__ d3 mk(double x, double y, double z) { return {x, y, z}; }
+__device__ __forceinline__ d3 sub(const d3& a, const d3& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ double dot(const d3& a, const d3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ d3 cross(const d3& a, const d3& b)
+{
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// closestPointOnTriangle (KdTree.h:26-74): Ericson's Voronoi-region method.
+__device__ d3 closest_point(const d3& p, const d3& a, const d3& b, const d3& c)
+{
+    const d3 ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
+    const double d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.0 && d2 <= 0.0) return a;
+    const d3 bp = sub(p, b);
+    const double d3_ = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3_ >= 0.0 && d4 <= d3_) return b;
+    const double vc = d1 * d4 - d3_ * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3_ <= 0.0)
+    {
+        const double v = d1 / (d1 - d3_);
+        return mk(a.x + v * ab.x, a.y + v * ab.y, a.z + v * ab.z);
+    }
+    const d3 cp = sub(p, c);
+    const double d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0.0 && d5 <= d6) return c;
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0)
+    {
+        const double w = d2 / (d2 - d6);
+        return mk(a.x + w * ac.x, a.y + w * ac.y, a.z + w * ac.z);
+    }
+    const double va = d3_ * d6 - d5 * d4;
+    if (va <= 0.0 && (d4 - d3_) >= 0.0 && (d5 - d6) >= 0.0)
+    {
+        const double w = (d4 - d3_) / ((d4 - d3_) + (d5 - d6));
+        return mk(b.x + w * (c.x - b.x), b.y + w * (c.y - b.y), b.z + w * (c.z - b.z));
+    }
+    const double denom = 1.0 / (va + vb + vc);
+    const double v = vb * denom, w = vc * denom;
+    return mk(a.x + ab.x * v + ac.x * w, a.y + ab.y * v + ac.y * w, a.z + ab.z * v + ac.z * w);
+}
+
+// Face normal kept with the nearest triangle (KdTree.h:310-314).
+__device__ d3 face_normal(const d3& a, const d3& b, const d3& c)
+{
+    const d3 n = cross(sub(b, a), sub(c, a));
+    const double len = sqrt(dot(n, n));
+    if (len > 1.0e-15) return mk(n.x / len, n.y / len, n.z / len);
+    return mk(0.0, 0.0, 1.0);
+}
+
+// rayIntersectsTriangle (KdTree.h:362-396): Moller-Trumbore, eps 1e-12.
+__device__ bool ray_hits(const d3& o, const d3& dir, const d3& a, const d3& b, const d3& c)
+{
+    const double eps = 1.0e-12;
+    const d3 e1 = sub(b, a), e2 = sub(c, a);
+    const d3 h = cross(dir, e2);
+    const double det = dot(e1, h);
+    if (fabs(det) < eps) return false;
+    const double invDet = 1.0 / det;
+    const d3 s = sub(o, a);
+    const double u = invDet * dot(s, h);
+    if (u < -eps || u > 1.0 + eps) return false;
+    const d3 q = cross(s, e1);
+    const double v = invDet * dot(dir, q);
+    if (v < -eps || u + v > 1.0 + eps) return false;
+    const double t = invDet * dot(e2, q);
+    return t > eps;
+}
+
+// ---------------------------------------------------------------------------
+// LBVH
+// ---------------------------------------------------------------------------
+struct LbvhView
+{
+    const float4* nodes;  // 4 float4 per internal node
+    const double* tri9;   // leaf order, 9 doubles per triangle
+    const int32_t* tri_id; // leaf order -> original triangle index
+    int n;                 // triangles
+    double dir[3];         // parity ray direction (FP64)
+    float inv_dir[3];
+};
+
+template <class Tree>
+__device__ __forceinline__ d3 tri_vertex(const Tree& b, int slot, int v)
+{
+    const double* t = b.tri9 + 9 * (int64_t)slot + 3 * v;
+    return mk(__ldg(t), __ldg(t + 1), __ldg(t + 2));
+}
+
+__device__ __forceinline__ uint64_t spread21(uint64_t x)
+{
+    x &= 0x1fffffULL;
+    x = (x | x << 32) & 0x1f00000000ffffULL;
+    x = (x | x << 16) & 0x1f0000ff0000ffULL;
+    x = (x | x << 8) & 0x100f00f00f00f00fULL;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ULL;
+    x = (x | x << 2) & 0x1249249249249249ULL;
+    return x;
+}
+
+__global__ void k_morton(const double* __restrict__ verts, const int32_t* __restrict__ tris, int n,
+                         double3 lo, double3 inv_ext, uint64_t* __restrict__ keys,
+                         int32_t* __restrict__ ids)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    double c[3] = {0, 0, 0};
+    for (int v = 0; v < 3; ++v)
+    {
+        const int vi = tris[3 * t + v];
+        for (int a = 0; a < 3; ++a) c[a] += verts[3 * vi + a];
+    }
+    const double l[3] = {lo.x, lo.y, lo.z}, ie[3] = {inv_ext.x, inv_ext.y, inv_ext.z};
+    uint64_t m = 0;
+    for (int a = 0; a < 3; ++a)
+    {
+        double f = (c[a] / 3.0 - l[a]) * ie[a];
+        f = f < 0.0 ? 0.0 : (f > 1.0 ? 1.0 : f);
+        const uint64_t q = (uint64_t)(f * 2097151.0);
+        m |= spread21(q) << (2 - a);
+    }
+    keys[t] = m;
+    ids[t] = t;
+}
+
+__global__ void k_gather_tris(const double* __restrict__ verts, const int32_t* __restrict__ tris,
+                              const int32_t* __restrict__ sorted_ids, int n,
+                              double* __restrict__ tri9, double* __restrict__ box64)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int t = sorted_ids[s];
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int v = 0; v < 3; ++v)
+    {
+        const int vi = tris[3 * t + v];
+        for (int a = 0; a < 3; ++a)
+        {
+            const double x = verts[3 * vi + a];
+            tri9[9 * (int64_t)s + 3 * v + a] = x;
+            lo[a] = fmin(lo[a], x);
+            hi[a] = fmax(hi[a], x);
+        }
+    }
+    // leaves occupy unified indices n-1 .. 2n-2
+    double* b = box64 + 6 * (int64_t)(n - 1 + s);
+    for (int a = 0; a < 3; ++a)
+    {
+        b[a] = lo[a];
+        b[3 + a] = hi[a];
+    }
+}
+
+__device__ __forceinline__ int delta(const uint64_t* keys, int n, int i, int j)
+{
+    if (j < 0 || j >= n) return -1;
+    const uint64_t a = keys[i], b = keys[j];
+    if (a == b) return 64 + __clz(i ^ j);
+    return __clzll(a ^ b);
+}
+
+// Karras 2012, Algorithm 2: one thread per internal node.  Unified node
+// indices: internal 0..n-2, leaf s at n-1+s.
+__global__ void k_karras(const uint64_t* __restrict__ keys, int n, int2* __restrict__ children,
+                         int32_t* __restrict__ parent)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = delta(keys, n, i, j);
+    int s = 0;
+    int t = l;
+    do
+    {
+        t = (t + 1) / 2;
+        if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    const int gamma = i + s * d + (d < 0 ? d : 0);
+    const int left = (min(i, j) == gamma) ? (n - 1 + gamma) : gamma;
+    const int right = (max(i, j) == gamma + 1) ? (n - 1 + gamma + 1) : gamma + 1;
+    children[i] = make_int2(left, right);
+    parent[left] = i;
+    parent[right] = i;
+}
+
+// Bottom-up box refit: each leaf walks to the root; the second thread to
+// arrive at a node unions its children.  No waiting: the first arrival exits.
+__global__ void k_refit(int n, const int2* __restrict__ children, const int32_t* __restrict__ parent,
+                        int* __restrict__ arrivals, double* box64)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int node = parent[n - 1 + s];
+    while (node >= 0)
+    {
+        __threadfence();
+        if (atomicAdd(&arrivals[node], 1) == 0) return;
+        __threadfence();
+        const int2 c = children[node];
+        double lo[3], hi[3];
+        for (int a = 0; a < 3; ++a)
+        {
+            lo[a] = fmin(__ldcg(box64 + 6 * (int64_t)c.x + a), __ldcg(box64 + 6 * (int64_t)c.y + a));
+            hi[a] = fmax(__ldcg(box64 + 6 * (int64_t)c.x + 3 + a), __ldcg(box64 + 6 * (int64_t)c.y + 3 + a));
+        }
+        for (int a = 0; a < 3; ++a)
+        {
+            __stcg(box64 + 6 * (int64_t)node + a, lo[a]);
+            __stcg(box64 + 6 * (int64_t)node + 3 + a, hi[a]);
+        }
+        node = node == 0 ? -1 : parent[node];
+    }
+}
+
+// Pack internal nodes: {L.lo, L.hi, R.lo, R.hi} in FP32 rounded outward and
+// widened by `margin`; children as node index (internal) or ~slot (leaf).
+__global__ void k_pack(int n, const int2* __restrict__ children, const double* __restrict__ box64,
+                       double margin, float4* __restrict__ nodes)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int2 c = children[i];
+    float f[12];
+    const int ch[2] = {c.x, c.y};
+    for (int k = 0; k < 2; ++k)
+        for (int a = 0; a < 3; ++a)
+        {
+            f[6 * k + a] = __double2float_rd(box64[6 * (int64_t)ch[k] + a] - margin);
+            f[6 * k + 3 + a] = __double2float_ru(box64[6 * (int64_t)ch[k] + 3 + a] + margin);
+        }
+    const int enc[2] = {c.x >= n - 1 ? ~(c.x - (n - 1)) : c.x, c.y >= n - 1 ? ~(c.y - (n - 1)) : c.y};
+    float4* o = nodes + 4 * (int64_t)i;
+    o[0] = make_float4(f[0], f[1], f[2], f[3]);
+    o[1] = make_float4(f[4], f[5], f[6], f[7]);
+    o[2] = make_float4(f[8], f[9], f[10], f[11]);
+    o[3] = make_float4(__int_as_float(enc[0]), __int_as_float(enc[1]), 0.f, 0.f);
+}
+
+// ---------------------------------------------------------------------------
+// traversal
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float box_dist2(const float p[3], float lx, float ly, float lz, float hx,
+                                           float hy, float hz)
+{
+    const float dx = fmaxf(fmaxf(lx - p[0], p[0] - hx), 0.f);
+    const float dy = fmaxf(fmaxf(ly - p[1], p[1] - hy), 0.f);
+    const float dz = fmaxf(fmaxf(lz - p[2], p[2] - hz), 0.f);
+    return dx * dx + dy * dy + dz * dz;
+}
+
+struct Nearest
+{
+    double sq;
+    int slot;
+    int id;
+    d3 cp;
+};
+
+__device__ __forceinline__ void test_triangle(const LbvhView& b, const d3& p, int slot, Nearest& best)
+{
+    const d3 a = tri_vertex(b, slot, 0), bb = tri_vertex(b, slot, 1), c = tri_vertex(b, slot, 2);
+    const d3 cp = closest_point(p, a, bb, c);
+    const d3 d = sub(p, cp);
+    const double sq = dot(d, d);
+    const int id = __ldg(b.tri_id + slot);
+    if (sq < best.sq || (sq == best.sq && id < best.id))
+    {
+        best.sq = sq;
+        best.slot = slot;
+        best.id = id;
+        best.cp = cp;
+    }
+}
+
+// Upper bound used for FP32 culling: bestSq rounded up, plus a relative slack
+// covering FP32 rounding of the box distance.
+__device__ __forceinline__ float cull_limit(double sq)
+{
+    return sq >= 3.0e38 ? INFINITY : __double2float_ru(sq) * 1.000002f;
+}
+
+__device__ Nearest tree_nearest(const LbvhView& b, const d3& p, int* status)
+{
+    Nearest best;
+    best.sq = 1.0e308 * 10.0; // +inf
+    best.slot = -1;
+    best.id = 0x7fffffff;
+    best.cp = p;
+    if (b.n == 1)
+    {
+        test_triangle(b, p, 0, best);
+        return best;
+    }
+    const float pf[3] = {(float)p.x, (float)p.y, (float)p.z};
+    int stack[kStackDepth];
+    float sdist[kStackDepth];
+    int sp = 0;
+    int node = 0;
+    while (true)
+    {
+        if (node < 0)
+        {
+            test_triangle(b, p, ~node, best);
+        }
+        else
+        {
+            const float4 n0 = __ldg(b.nodes + 4 * (int64_t)node);
+            const float4 n1 = __ldg(b.nodes + 4 * (int64_t)node + 1);
+            const float4 n2 = __ldg(b.nodes + 4 * (int64_t)node + 2);
+            const float4 n3 = __ldg(b.nodes + 4 * (int64_t)node + 3);
+            const float dl = box_dist2(pf, n0.x, n0.y, n0.z, n0.w, n1.x, n1.y);
+            const float dr = box_dist2(pf, n1.z, n1.w, n2.x, n2.y, n2.z, n2.w);
+            const int cl = __float_as_int(n3.x), cr = __float_as_int(n3.y);
+            const float lim = cull_limit(best.sq);
+            const bool hl = dl <= lim, hr = dr <= lim;
+            if (hl && hr)
+            {
+                const bool lfirst = dl <= dr;
+                if (sp < kStackDepth)
+                {
+                    stack[sp] = lfirst ? cr : cl;
+                    sdist[sp] = lfirst ? dr : dl;
+                    ++sp;
+                }
+                else
+                {
+                    atomicOr(status, kStatusStackOverflow);
+                }
+                node = lfirst ? cl : cr;
+                continue;
+            }
+            if (hl)
+            {
+                node = cl;
+                continue;
+            }
+            if (hr)
+            {
+                node = cr;
+                continue;
+            }
+        }
+        // pop the next subtree that can still hold a closer triangle
+        bool found = false;
+        while (sp > 0)
+        {
+            --sp;
+            if (sdist[sp] <= cull_limit(best.sq))
+            {
+                node = stack[sp];
+                found = true;
+                break;
+            }
+        }
+        if (!found) break;
+    }
+    return best;
+}
+
+__device__ __forceinline__ bool ray_box(const float o[3], const float inv[3], float lx, float ly,
+                                        float lz, float hx, float hy, float hz)
+{
+    float t0 = (lx - o[0]) * inv[0], t1 = (hx - o[0]) * inv[0];
+    float tmin = fminf(t0, t1), tmax = fmaxf(t0, t1);
+    t0 = (ly - o[1]) * inv[1];
+    t1 = (hy - o[1]) * inv[1];
+    tmin = fmaxf(tmin, fminf(t0, t1));
+    tmax = fminf(tmax, fmaxf(t0, t1));
+    t0 = (lz - o[2]) * inv[2];
+    t1 = (hz - o[2]) * inv[2];
+    tmin = fmaxf(tmin, fminf(t0, t1));
+    tmax = fminf(tmax, fmaxf(t0, t1));
+    tmin = fmaxf(tmin, 0.f);
+    return tmax >= tmin;
+}
+
+// countRayIntersections (KdTree.h:398-441): number of triangles the fixed
+// ray hits (exact FP64 test on every triangle whose widened box it crosses).
+__device__ int tree_ray_count(const LbvhView& b, const d3& p, int* status)
+{
+    const d3 dir = mk(b.dir[0], b.dir[1], b.dir[2]);
+    if (b.n == 1)
+        return ray_hits(p, dir, tri_vertex(b, 0, 0), tri_vertex(b, 0, 1), tri_vertex(b, 0, 2)) ? 1 : 0;
+    const float o[3] = {(float)p.x, (float)p.y, (float)p.z};
+    int stack[kStackDepth];
+    int sp = 0;
+    int node = 0;
+    int hits = 0;
+    while (true)
+    {
+        if (node < 0)
+        {
+            const int s = ~node;
+            hits += ray_hits(p, dir, tri_vertex(b, s, 0), tri_vertex(b, s, 1), tri_vertex(b, s, 2)) ? 1 : 0;
+        }
+        else
+        {
+            const float4 n0 = __ldg(b.nodes + 4 * (int64_t)node);
+            const float4 n1 = __ldg(b.nodes + 4 * (int64_t)node + 1);
+            const float4 n2 = __ldg(b.nodes + 4 * (int64_t)node + 2);
+            const float4 n3 = __ldg(b.nodes + 4 * (int64_t)node + 3);
+            const bool hl = ray_box(o, b.inv_dir, n0.x, n0.y, n0.z, n0.w, n1.x, n1.y);
+            const bool hr = ray_box(o, b.inv_dir, n1.z, n1.w, n2.x, n2.y, n2.z, n2.w);
+            const int cl = __float_as_int(n3.x), cr = __float_as_int(n3.y);
+            if (hl && hr)
+            {
+                if (sp < kStackDepth)
+                    stack[sp++] = cr;
+                else
+                    atomicOr(status, kStatusStackOverflow);
+                node = cl;
+                continue;
+            }
+            if (hl)
+            {
+                node = cl;
+                continue;
+            }
+            if (hr)
+            {
+                node = cr;
+                continue;
+            }
+        }
+        if (sp == 0) break;
+        node = stack[--sp];
+    }
+    return hits;
+}
+
+// ---------------------------------------------------------------------------
+// reference-order tree: the reference's median-split BVH, traversed on the
+// device in the reference's order with FP64 boxes
+// ---------------------------------------------------------------------------
+struct RefNode
+{
+    double lo[3];
+    double hi[3];
+    int left, right; // internal: children (node ids)
+    int start, count; // leaf: range of slots (count > 0)
+};
+static_assert(sizeof(RefNode) == 64, "RefNode is one 64-byte record");
+
+struct RefTreeView
+{
+    const RefNode* nodes;
+    const double* tri9;    // slot order (m_indices), 9 doubles per triangle
+    const int32_t* tri_id; // slot -> original triangle index
+    int n;
+    int nnodes;
+    double dir[3];
+};
+
+__device__ __forceinline__ void load_box(const RefNode* nd, double lo[3], double hi[3])
+{
+    const double2* q = reinterpret_cast<const double2*>(nd);
+    const double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    lo[0] = a.x;
+    lo[1] = a.y;
+    lo[2] = b.x;
+    hi[0] = b.y;
+    hi[1] = c.x;
+    hi[2] = c.y;
+}
+
+// squaredDistanceToAabb (KdTree.h:244-264), same branches and order.
+__device__ __forceinline__ double box_dist_sq(const d3& p, const double lo[3], const double hi[3])
+{
+    const double pp[3] = {p.x, p.y, p.z};
+    double sq = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        if (pp[a] < lo[a])
+        {
+            const double d = lo[a] - pp[a];
+            sq += d * d;
+        }
+        else if (pp[a] > hi[a])
+        {
+            const double d = pp[a] - hi[a];
+            sq += d * d;
+        }
+    }
+    return sq;
+}
+
+// searchNearest (KdTree.h:266-328) without recursion: the explicit stack pops
+// subtrees in the same near-first depth-first order and applies the same
+// "box distance > best" cut when a subtree is entered, and triangles replace
+// the best only on a strictly smaller squared distance -- so the triangle
+// found is the reference's, ties included.
+__device__ Nearest tree_nearest(const RefTreeView& b, const d3& p, int* status)
+{
+    Nearest best;
+    best.sq = DBL_MAX;
+    best.slot = -1;
+    best.id = -1;
+    best.cp = mk(0.0, 0.0, 0.0);
+    if (b.nnodes == 0) return best;
+    int stack[kStackDepth];
+    double sdist[kStackDepth];
+    int sp = 0;
+    {
+        double lo[3], hi[3];
+        load_box(b.nodes, lo, hi);
+        stack[0] = 0;
+        sdist[0] = box_dist_sq(p, lo, hi);
+        sp = 1;
+    }
+    while (sp > 0)
+    {
+        --sp;
+        const int node = stack[sp];
+        if (sdist[sp] > best.sq) continue;
+        const RefNode* nd = b.nodes + node;
+        const int4 meta = __ldg(reinterpret_cast<const int4*>(nd) + 3);
+        if (meta.w > 0)
+        {
+            for (int s = meta.z; s < meta.z + meta.w; ++s)
+            {
+                const d3 a = tri_vertex(b, s, 0), bb = tri_vertex(b, s, 1), c = tri_vertex(b, s, 2);
+                const d3 cp = closest_point(p, a, bb, c);
+                const d3 d = sub(p, cp);
+                const double sq = dot(d, d);
+                if (sq < best.sq)
+                {
+                    best.sq = sq;
+                    best.slot = s;
+                    best.cp = cp;
+                }
+            }
+            continue;
+        }
+        double llo[3], lhi[3], rlo[3], rhi[3];
+        load_box(b.nodes + meta.x, llo, lhi);
+        load_box(b.nodes + meta.y, rlo, rhi);
+        const double dl = box_dist_sq(p, llo, lhi);
+        const double dr = box_dist_sq(p, rlo, rhi);
+        int first = meta.x, second = meta.y;
+        double df = dl, ds = dr;
+        if (dr < dl)
+        {
+            first = meta.y;
+            second = meta.x;
+            df = dr;
+            ds = dl;
+        }
+        if (sp + 2 > kStackDepth)
+        {
+            atomicOr(status, kStatusStackOverflow);
+            break;
+        }
+        stack[sp] = second;
+        sdist[sp] = ds;
+        ++sp;
+        stack[sp] = first;
+        sdist[sp] = df;
+        ++sp;
+    }
+    if (best.slot >= 0) best.id = __ldg(b.tri_id + best.slot);
+    return best;
+}
+
+// rayIntersectsAabb (KdTree.h:335-360), same arithmetic.
+__device__ __forceinline__ bool ray_box_ref(const d3& o, const double dir[3], const double lo[3],
+                                            const double hi[3])
+{
+    const double oo[3] = {o.x, o.y, o.z};
+    double tmin = 0.0, tmax = DBL_MAX;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        const double invD = 1.0 / dir[a];
+        double t0 = (lo[a] - oo[a]) * invD;
+        double t1 = (hi[a] - oo[a]) * invD;
+        if (t0 > t1)
+        {
+            const double t = t0;
+            t0 = t1;
+            t1 = t;
+        }
+        tmin = tmin < t0 ? t0 : tmin;
+        tmax = t1 < tmax ? t1 : tmax;
+        if (tmax < tmin) return false;
+    }
+    return true;
+}
+
+// countRayIntersectionsRecursive (KdTree.h:398-441) over the same tree.
+__device__ int tree_ray_count(const RefTreeView& b, const d3& p, int* status)
+{
+    if (b.nnodes == 0) return 0;
+    const d3 dir = mk(b.dir[0], b.dir[1], b.dir[2]);
+    int stack[kStackDepth];
+    int sp = 0;
+    stack[sp++] = 0;
+    int hits = 0;
+    while (sp > 0)
+    {
+        const int node = stack[--sp];
+        const RefNode* nd = b.nodes + node;
+        double lo[3], hi[3];
+        load_box(nd, lo, hi);
+        if (!ray_box_ref(p, b.dir, lo, hi)) continue;
+        const int4 meta = __ldg(reinterpret_cast<const int4*>(nd) + 3);
+        if (meta.w > 0)
+        {
+            for (int s = meta.z; s < meta.z + meta.w; ++s)
+                hits += ray_hits(p, dir, tri_vertex(b, s, 0), tri_vertex(b, s, 1), tri_vertex(b, s, 2)) ? 1 : 0;
+            continue;
+        }
+        if (sp + 2 > kStackDepth)
+        {
+            atomicOr(status, kStatusStackOverflow);
+            break;
+        }
+        stack[sp++] = meta.y;
+        stack[sp++] = meta.x;
+    }
+    return hits;
+}
+
+struct SignedResult
+{
+    double sd;
+    d3 cp;
+    d3 fn;
+};
+
+// findSignedNearest (KdTree.h:143-165).
+template <class Tree>
+__device__ SignedResult signed_nearest(const Tree& b, const d3& p, int* status)
+{
+    const Nearest best = tree_nearest(b, p, status);
+    SignedResult r;
+    const double dist = sqrt(best.sq);
+    r.cp = best.cp;
+    r.fn = best.slot >= 0 ? face_normal(tri_vertex(b, best.slot, 0), tri_vertex(b, best.slot, 1),
+                                        tri_vertex(b, best.slot, 2))
+                          : mk(0.0, 0.0, 1.0);
+    const int hits = tree_ray_count(b, p, status);
+    if (hits > 0)
+        r.sd = (hits % 2) == 1 ? -dist : dist;
+    else
+        r.sd = dot(sub(p, r.cp), r.fn) >= 0.0 ? dist : -dist;
+    return r;
+}
+
+// SdfBuilder.cpp:1070-1085 normal: sign * (c - cp) / |c - cp|, or the signed
+// face normal within 1e-12 of the surface.
+__device__ __forceinline__ d3 voxel_normal(const d3& c, const SignedResult& r)
+{
+    const d3 diff = sub(c, r.cp);
+    const double dist = sqrt(dot(diff, diff));
+    const double sign = r.sd >= 0.0 ? 1.0 : -1.0;
+    if (dist > 1e-12) return mk(sign * diff.x / dist, sign * diff.y / dist, sign * diff.z / dist);
+    return mk(sign * r.fn.x, sign * r.fn.y, sign * r.fn.z);
+}
+
+struct SpecD
+{
+    double bmin[3];
+    double voxel[3];
+    int n[3];
+};
+
+__device__ __forceinline__ d3 voxel_center(const SpecD& s, int i, int j, int k)
+{
+    // GridSpec::centerFromIndex (GridSpec.h:29-33)
+    return mk(s.bmin[0] + s.voxel[0] * (i + 0.5), s.bmin[1] + s.voxel[1] * (j + 0.5),
+              s.bmin[2] + s.voxel[2] * (k + 0.5));
+}
+
+// Dense fill: CTA = 8x8x4 voxel tile (coherent traversals), thread = voxel.
+template <class Tree>
+__global__ void __launch_bounds__(256) k_dense_fill(Tree b, SpecD s, double* __restrict__ phi64,
+                                                    double* __restrict__ n64, double* __restrict__ w64,
+                                                    float4* __restrict__ phin, int* status)
+{
+    const int tx = threadIdx.x;
+    const int i = blockIdx.x * 8 + (tx & 7);
+    const int j = blockIdx.y * 8 + ((tx >> 3) & 7);
+    const int k = blockIdx.z * 4 + (tx >> 6);
+    if (i >= s.n[0] || j >= s.n[1] || k >= s.n[2]) return;
+    const int64_t idx = i + (int64_t)s.n[0] * (j + (int64_t)s.n[1] * k);
+    const d3 c = voxel_center(s, i, j, k);
+    const SignedResult r = signed_nearest(b, c, status);
+    const d3 g = voxel_normal(c, r);
+    phi64[idx] = r.sd;
+    n64[3 * idx + 0] = g.x;
+    n64[3 * idx + 1] = g.y;
+    n64[3 * idx + 2] = g.z;
+    if (w64)
+    {
+        w64[3 * idx + 0] = r.cp.x;
+        w64[3 * idx + 1] = r.cp.y;
+        w64[3 * idx + 2] = r.cp.z;
+    }
+    phin[idx] = make_float4((float)r.sd, (float)g.x, (float)g.y, (float)g.z);
+}
+
+// Symmetrised central-difference Hessian of the normal field
+// (SdfBuilder.cpp:1105-1152): H[:,a] = (n(+a) - n(-a)) / (2 h_a), clamped at
+// the boundary, H = (H + H^T) / 2; stored xx, xy, xz, yy, yz, zz.
+__device__ __forceinline__ void sym_hessian(const double dn[3][3], double h6[6])
+{
+    h6[0] = 0.5 * (dn[0][0] + dn[0][0]);
+    h6[1] = 0.5 * (dn[1][0] + dn[0][1]);
+    h6[2] = 0.5 * (dn[2][0] + dn[0][2]);
+    h6[3] = 0.5 * (dn[1][1] + dn[1][1]);
+    h6[4] = 0.5 * (dn[2][1] + dn[1][2]);
+    h6[5] = 0.5 * (dn[2][2] + dn[2][2]);
+}
+
+__global__ void k_dense_hessian(SpecD s, const double* __restrict__ n64, double* __restrict__ h64,
+                                float* __restrict__ hess6)
+{
+    const int64_t total = (int64_t)s.n[0] * s.n[1] * s.n[2];
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int nx = s.n[0], ny = s.n[1], nz = s.n[2];
+    const int i = (int)(idx % nx), j = (int)((idx / nx) % ny), k = (int)(idx / ((int64_t)nx * ny));
+    const int ip = min(i + 1, nx - 1), im = max(i - 1, 0);
+    const int jp = min(j + 1, ny - 1), jm = max(j - 1, 0);
+    const int kp = min(k + 1, nz - 1), km = max(k - 1, 0);
+    const int64_t pi[3] = {ip + (int64_t)nx * (j + (int64_t)ny * k), i + (int64_t)nx * (jp + (int64_t)ny * k),
+                           i + (int64_t)nx * (j + (int64_t)ny * kp)};
+    const int64_t mi[3] = {im + (int64_t)nx * (j + (int64_t)ny * k), i + (int64_t)nx * (jm + (int64_t)ny * k),
+                           i + (int64_t)nx * (j + (int64_t)ny * km)};
+    double dn[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int r = 0; r < 3; ++r)
+            dn[a][r] = (__ldg(n64 + 3 * pi[a] + r) - __ldg(n64 + 3 * mi[a] + r)) / (2.0 * s.voxel[a]);
+    double h6[6];
+    sym_hessian(dn, h6);
+    for (int q = 0; q < 6; ++q)
+    {
+        h64[6 * idx + q] = h6[q];
+        hess6[6 * idx + q] = (float)h6[q];
+    }
+}
+
+// Sparse block activation (SdfBuilder.cpp:869-890): distance from the block's
+// geometric centre to the mesh against band + halo*h + (sqrt(3)/2)*bd*h.
+template <class Tree>
+__device__ __forceinline__ int32_t block_active(const Tree& b, const SpecD& s, int bd, int nbx,
+                                                int nby, int bl, double activation, int* status)
+{
+    const int bi = bl % nbx, bj = (bl / nbx) % nby, bk = bl / (nbx * nby);
+    const int i0 = bi * bd, j0 = bj * bd, k0 = bk * bd;
+    const int i1 = min(i0 + bd, s.n[0]), j1 = min(j0 + bd, s.n[1]), k1 = min(k0 + bd, s.n[2]);
+    const d3 c = mk(s.bmin[0] + s.voxel[0] * (0.5 * (double)(i0 + i1)),
+                    s.bmin[1] + s.voxel[1] * (0.5 * (double)(j0 + j1)),
+                    s.bmin[2] + s.voxel[2] * (0.5 * (double)(k0 + k1)));
+    const Nearest best = tree_nearest(b, c, status);
+    const double dist = sqrt(best.sq);
+    return fabs(dist) <= activation ? 1 : 0;
+}
+
+template <class Tree>
+__global__ void k_sparse_activate(Tree b, SpecD s, int bd, int nbx, int nby, int nbz,
+                                  double activation, int32_t* __restrict__ flags, int* status)
+{
+    const int bl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bl >= nbx * nby * nbz) return;
+    flags[bl] = block_active(b, s, bd, nbx, nby, bl, activation, status);
+}
+
+__global__ void k_sparse_table(int total, int nbx, int nby, const int32_t* __restrict__ flags,
+                               const int32_t* __restrict__ slots, int32_t* __restrict__ table,
+                               int32_t* __restrict__ ijk)
+{
+    const int bl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bl >= total) return;
+    if (flags[bl])
+    {
+        const int slot = slots[bl];
+        table[bl] = slot;
+        ijk[3 * slot + 0] = bl % nbx;
+        ijk[3 * slot + 1] = (bl / nbx) % nby;
+        ijk[3 * slot + 2] = bl / (nbx * nby);
+    }
+    else
+    {
+        table[bl] = -1;
+    }
+}
+
+// One voxel of a stored brick (SdfBuilder.cpp:925-965); voxels outside the
+// grid get phi 0, n (1,0,0).
+template <class Tree>
+__device__ __forceinline__ float4 brick_voxel(const Tree& b, const SpecD& s, int bd, int bi,
+                                              int bj, int bk, int local, int* status)
+{
+    const int lx = local % bd, ly = (local / bd) % bd, lz = local / (bd * bd);
+    const int i = bi * bd + lx, j = bj * bd + ly, k = bk * bd + lz;
+    if (i >= s.n[0] || j >= s.n[1] || k >= s.n[2]) return make_float4(0.f, 1.f, 0.f, 0.f);
+    const d3 c = voxel_center(s, i, j, k);
+    const SignedResult r = signed_nearest(b, c, status);
+    const d3 g = voxel_normal(c, r);
+    return make_float4((float)r.sd, (float)g.x, (float)g.y, (float)g.z);
+}
+
+// Brick fill: one CTA per stored block.
+template <class Tree>
+__global__ void __launch_bounds__(256) k_sparse_fill(Tree b, SpecD s, int bd,
+                                                     const int32_t* __restrict__ ijk,
+                                                     float4* __restrict__ phin, int* status)
+{
+    const int blk = blockIdx.x;
+    const int V = bd * bd * bd;
+    const int bi = ijk[3 * blk], bj = ijk[3 * blk + 1], bk = ijk[3 * blk + 2];
+    for (int local = threadIdx.x; local < V; local += blockDim.x)
+        phin[(int64_t)blk * V + local] = brick_voxel(b, s, bd, bi, bj, bk, local, status);
+}
+
+// estimateSparseHessian (SdfBuilder.cpp:1154-1225) for stored voxel `local`
+// of brick `blk` of one grid: neighbours through the block table, a missing
+// neighbour (other block absent, or outside the grid) replaced by the voxel's
+// own normal; FP64 arithmetic on the FP32 normals.
+__device__ __forceinline__ void sparse_hessian_voxel(const SpecD& s, int bd, int nbx, int nby,
+                                                     const int32_t* __restrict__ ijk,
+                                                     const int32_t* __restrict__ table,
+                                                     const float4* __restrict__ phin, int blk,
+                                                     int local, float* __restrict__ out)
+{
+    const int V = bd * bd * bd;
+    const int lx = local % bd, ly = (local / bd) % bd, lz = local / (bd * bd);
+    const int i = ijk[3 * blk] * bd + lx, j = ijk[3 * blk + 1] * bd + ly, k = ijk[3 * blk + 2] * bd + lz;
+    if (i >= s.n[0] || j >= s.n[1] || k >= s.n[2])
+    {
+        for (int q = 0; q < 6; ++q) out[q] = 0.f;
+        return;
+    }
+    const float4 cur = phin[(int64_t)blk * V + local];
+    const double curd[3] = {(double)cur.y, (double)cur.z, (double)cur.w};
+    auto sample = [&](int ii, int jj, int kk, double n[3]) {
+        if (ii < 0 || jj < 0 || kk < 0 || ii >= s.n[0] || jj >= s.n[1] || kk >= s.n[2])
+        {
+            n[0] = curd[0];
+            n[1] = curd[1];
+            n[2] = curd[2];
+            return;
+        }
+        const int b2 = table[ii / bd + nbx * (jj / bd + nby * (kk / bd))];
+        if (b2 < 0)
+        {
+            n[0] = curd[0];
+            n[1] = curd[1];
+            n[2] = curd[2];
+            return;
+        }
+        const int l2 = (ii % bd) + bd * ((jj % bd) + bd * (kk % bd));
+        const float4 c = phin[(int64_t)b2 * V + l2];
+        n[0] = (double)c.y;
+        n[1] = (double)c.z;
+        n[2] = (double)c.w;
+    };
+    double dn[3][3];
+    const int off[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int a = 0; a < 3; ++a)
+    {
+        double pn[3], mn[3];
+        sample(i + off[a][0], j + off[a][1], k + off[a][2], pn);
+        sample(i - off[a][0], j - off[a][1], k - off[a][2], mn);
+        for (int r = 0; r < 3; ++r) dn[a][r] = (pn[r] - mn[r]) / (2.0 * s.voxel[a]);
+    }
+    double h6[6];
+    sym_hessian(dn, h6);
+    for (int q = 0; q < 6; ++q) out[q] = (float)h6[q];
+}
+
+__global__ void k_sparse_hessian(SpecD s, int bd, int nbx, int nby, int64_t stored,
+                                 const int32_t* __restrict__ ijk, const int32_t* __restrict__ table,
+                                 const float4* __restrict__ phin, float* __restrict__ hess6)
+{
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= stored) return;
+    const int V = bd * bd * bd;
+    sparse_hessian_voxel(s, bd, nbx, nby, ijk, table, phin, (int)(v / V), (int)(v % V),
+                         hess6 + 6 * v);
+}
+
+// ---------------------------------------------------------------------------
+// host orchestration
+// ---------------------------------------------------------------------------
+struct Timer
+{
+    cudaEvent_t e0, e1;
+    cudaStream_t s;
+    explicit Timer(cudaStream_t st) : s(st)
+    {
+        SDFO_CUDA(cudaEventCreate(&e0));
+        SDFO_CUDA(cudaEventCreate(&e1));
+        SDFO_CUDA(cudaEventRecord(e0, s));
+    }
+    ~Timer()
+    {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    double lap()
+    {
+        SDFO_CUDA(cudaEventRecord(e1, s));
+        SDFO_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        SDFO_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        SDFO_CUDA(cudaEventRecord(e0, s));
+        return ms;
+    }
+};
+
+// KdTree::rayDirection (KdTree.h:330-333): the fixed vector normalised.
+void parity_ray(double dir[3])
+{
+    const double r[3] = {1.0, 0.3713906763541037, 0.52999894000318};
+    volatile double n2 = r[0] * r[0];
+    n2 = n2 + r[1] * r[1];
+    n2 = n2 + r[2] * r[2];
+    const double len = std::sqrt((double)n2);
+    for (int a = 0; a < 3; ++a) dir[a] = r[a] / len;
+}
+
+// Device-side LBVH with its storage.
+struct DeviceLbvh
+{
+    DeviceBuffer<float4> nodes;
+    DeviceBuffer<double> tri9;
+    DeviceBuffer<int32_t> tri_id;
+    int n = 0;
+    LbvhView view() const
+    {
+        LbvhView v{};
+        v.nodes = nodes.get();
+        v.tri9 = tri9.get();
+        v.tri_id = tri_id.get();
+        v.n = n;
+        parity_ray(v.dir);
+        for (int a = 0; a < 3; ++a) v.inv_dir[a] = (float)(1.0 / v.dir[a]);
+        return v;
+    }
+};
+
+// Host build of the reference's tree (KdTree::build / buildRecursive,
+// KdTree.h:91-121, 188-242): median split of the centroids on the longest
+// centroid-extent axis with std::nth_element, leaves of <= 8 triangles, nodes
+// numbered in creation (pre-)order.  Restated because tie resolution of the
+// nearest search (and with it the face-normal sign fallback) depends on this
+// exact tree.
+struct HostRefTree
+{
+    std::vector<RefNode> nodes;
+    std::vector<int32_t> order;
+    std::vector<double> lo, hi, cen;
+
+    int build(int lo_i, int hi_i)
+    {
+        const int id = (int)nodes.size();
+        nodes.emplace_back();
+        double bmin[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, bmax[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+        double cmin[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, cmax[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+        for (int i = lo_i; i < hi_i; ++i)
+        {
+            const int t = order[(size_t)i];
+            for (int a = 0; a < 3; ++a)
+            {
+                const double l = lo[3 * (size_t)t + a], h = hi[3 * (size_t)t + a],
+                             c = cen[3 * (size_t)t + a];
+                bmin[a] = l < bmin[a] ? l : bmin[a];
+                bmax[a] = bmax[a] < h ? h : bmax[a];
+                cmin[a] = c < cmin[a] ? c : cmin[a];
+                cmax[a] = cmax[a] < c ? c : cmax[a];
+            }
+        }
+        RefNode n{};
+        for (int a = 0; a < 3; ++a)
+        {
+            n.lo[a] = bmin[a];
+            n.hi[a] = bmax[a];
+        }
+        n.left = n.right = -1;
+        n.start = -1;
+        n.count = 0;
+        const int count = hi_i - lo_i;
+        if (count <= 8)
+        {
+            n.start = lo_i;
+            n.count = count;
+            nodes[(size_t)id] = n;
+            return id;
+        }
+        const double ext[3] = {cmax[0] - cmin[0], cmax[1] - cmin[1], cmax[2] - cmin[2]};
+        int axis = 0;
+        if (ext[1] > ext[0]) axis = 1;
+        if (ext[2] > ext[axis]) axis = 2;
+        const int mid = lo_i + count / 2;
+        const double* c = cen.data();
+        std::nth_element(order.begin() + lo_i, order.begin() + mid, order.begin() + hi_i,
+                         [c, axis](int x, int y) { return c[3 * x + axis] < c[3 * y + axis]; });
+        nodes[(size_t)id] = n;
+        const int l = build(lo_i, mid);
+        const int r = build(mid, hi_i);
+        nodes[(size_t)id].left = l;
+        nodes[(size_t)id].right = r;
+        return id;
+    }
+};
+
+struct DeviceRefTree
+{
+    DeviceBuffer<RefNode> nodes;
+    DeviceBuffer<double> tri9;
+    DeviceBuffer<int32_t> tri_id;
+    int n = 0;
+    int nnodes = 0;
+    RefTreeView view() const
+    {
+        RefTreeView v{};
+        v.nodes = nodes.get();
+        v.tri9 = tri9.get();
+        v.tri_id = tri_id.get();
+        v.n = n;
+        v.nnodes = nnodes;
+        parity_ray(v.dir);
+        return v;
+    }
+};
+
+// The reference tree of one mesh on the host: nodes, triangles in slot order
+// (9 doubles each) and slot -> triangle index.
+struct HostTreeData
+{
+    std::vector<RefNode> nodes;
+    std::vector<double> tri9;
+    std::vector<int32_t> tri_id;
+};
+
+void host_ref_tree(HostTreeData& out, const double* verts, const int32_t* tris, int64_t nt)
+{
+    HostRefTree h;
+    const size_t n = (size_t)nt;
+    h.lo.resize(3 * n);
+    h.hi.resize(3 * n);
+    h.cen.resize(3 * n);
+    h.order.resize(n);
+    for (size_t i = 0; i < n; ++i)
+    {
+        const double* a = verts + 3 * (size_t)tris[3 * i];
+        const double* b = verts + 3 * (size_t)tris[3 * i + 1];
+        const double* c = verts + 3 * (size_t)tris[3 * i + 2];
+        for (int q = 0; q < 3; ++q)
+        {
+            // a.cwiseMin(b).cwiseMin(c), a.cwiseMax(b).cwiseMax(c), (a + b + c) / 3.0
+            double mn = b[q] < a[q] ? b[q] : a[q];
+            mn = c[q] < mn ? c[q] : mn;
+            double mx = a[q] < b[q] ? b[q] : a[q];
+            mx = mx < c[q] ? c[q] : mx;
+            h.lo[3 * i + q] = mn;
+            h.hi[3 * i + q] = mx;
+            volatile double sum = a[q] + b[q];
+            sum = sum + c[q];
+            h.cen[3 * i + q] = sum / 3.0;
+        }
+        h.order[i] = (int32_t)i;
+    }
+    h.nodes.reserve(2 * n);
+    h.build(0, (int)nt);
+    out.tri9.resize(9 * n);
+    for (size_t sl = 0; sl < n; ++sl)
+    {
+        const int32_t ti = h.order[sl];
+        for (int v = 0; v < 3; ++v)
+            for (int q = 0; q < 3; ++q)
+                out.tri9[9 * sl + 3 * v + q] = verts[3 * (size_t)tris[3 * (size_t)ti + v] + q];
+    }
+    out.nodes = std::move(h.nodes);
+    out.tri_id = std::move(h.order);
+}
+
+void build_ref_tree(DeviceRefTree& t, const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
+                    cudaStream_t s)
+{
+    (void)nv;
+    HostTreeData h;
+    host_ref_tree(h, verts, tris, nt);
+    const size_t n = (size_t)nt;
+    t.n = (int)nt;
+    t.nnodes = (int)h.nodes.size();
+    t.nodes.reset(h.nodes.size());
+    t.tri9.reset(9 * n);
+    t.tri_id.reset(n);
+    SDFO_CUDA(cudaMemcpyAsync(t.nodes.get(), h.nodes.data(), sizeof(RefNode) * h.nodes.size(),
+                              cudaMemcpyHostToDevice, s));
+    SDFO_CUDA(cudaMemcpyAsync(t.tri9.get(), h.tri9.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, s));
+    SDFO_CUDA(cudaMemcpyAsync(t.tri_id.get(), h.tri_id.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    // the host vectors above are freed on return: finish the copies first
+    SDFO_CUDA(cudaStreamSynchronize(s));
+}
+
+void build_lbvh(DeviceLbvh& bvh, const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
+               double extent, cudaStream_t s)
+{
+    const int n = (int)nt;
+    bvh.n = n;
+    DeviceBuffer<double> verts((size_t)nv * 3);
+    DeviceBuffer<int32_t> tris((size_t)nt * 3);
+    SDFO_CUDA(cudaMemcpyAsync(verts.get(), h_verts, sizeof(double) * 3 * nv, cudaMemcpyHostToDevice, s));
+    SDFO_CUDA(cudaMemcpyAsync(tris.get(), h_tris, sizeof(int32_t) * 3 * nt, cudaMemcpyHostToDevice, s));
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int64_t i = 0; i < nv; ++i)
+        for (int a = 0; a < 3; ++a)
+        {
+            lo[a] = std::min(lo[a], h_verts[3 * i + a]);
+            hi[a] = std::max(hi[a], h_verts[3 * i + a]);
+        }
+    double ie[3];
+    for (int a = 0; a < 3; ++a) ie[a] = hi[a] > lo[a] ? 1.0 / (hi[a] - lo[a]) : 0.0;
+    DeviceBuffer<uint64_t> keys(nt), keys_sorted(nt);
+    DeviceBuffer<int32_t> ids(nt);
+    bvh.tri_id.reset(nt);
+    const int T = 256;
+    k_morton<<<(n + T - 1) / T, T, 0, s>>>(verts.get(), tris.get(), n, make_double3(lo[0], lo[1], lo[2]),
+                                           make_double3(ie[0], ie[1], ie[2]), keys.get(), ids.get());
+    SDFO_CHECK_LAUNCH();
+    size_t temp = 0;
+    SDFO_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, keys.get(), keys_sorted.get(), ids.get(),
+                                              bvh.tri_id.get(), n, 0, 63, s));
+    DeviceBuffer<unsigned char> tmp(temp);
+    SDFO_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), temp, keys.get(), keys_sorted.get(), ids.get(),
+                                              bvh.tri_id.get(), n, 0, 63, s));
+    bvh.tri9.reset((size_t)nt * 9);
+    DeviceBuffer<double> box64((size_t)(2 * n - 1) * 6);
+    k_gather_tris<<<(n + T - 1) / T, T, 0, s>>>(verts.get(), tris.get(), bvh.tri_id.get(), n,
+                                                bvh.tri9.get(), box64.get());
+    SDFO_CHECK_LAUNCH();
+    if (n == 1) return;
+    DeviceBuffer<int2> children((size_t)(n - 1));
+    DeviceBuffer<int32_t> parent((size_t)(2 * n - 1));
+    DeviceBuffer<int> arrivals((size_t)(n - 1));
+    SDFO_CUDA(cudaMemsetAsync(arrivals.get(), 0, sizeof(int) * (n - 1), s));
+    SDFO_CUDA(cudaMemsetAsync(parent.get(), 0xff, sizeof(int32_t) * (2 * n - 1), s));
+    k_karras<<<(n - 1 + T - 1) / T, T, 0, s>>>(keys_sorted.get(), n, children.get(), parent.get());
+    SDFO_CHECK_LAUNCH();
+    k_refit<<<(n + T - 1) / T, T, 0, s>>>(n, children.get(), parent.get(), arrivals.get(), box64.get());
+    SDFO_CHECK_LAUNCH();
+    bvh.nodes.reset((size_t)(n - 1) * 4);
+    const double margin = 4.0e-6 * extent;
+    k_pack<<<(n - 1 + T - 1) / T, T, 0, s>>>(n, children.get(), box64.get(), margin, bvh.nodes.get());
+    SDFO_CHECK_LAUNCH();
+}
+
+// The acceleration structure selected by sdfo_set_bvh_mode.
+struct AnyTree
+{
+    int mode;
+    DeviceRefTree ref;
+    DeviceLbvh lbvh;
+    void build(const double* verts, int64_t nv, const int32_t* tris, int64_t nt, double extent,
+               cudaStream_t s)
+    {
+        if (mode == SDFO_BVH_LBVH)
+            build_lbvh(lbvh, verts, nv, tris, nt, extent, s);
+        else
+            build_ref_tree(ref, verts, nv, tris, nt, s);
+    }
+    int node_count(int64_t nt) const
+    {
+        return mode == SDFO_BVH_LBVH ? (int)(nt > 1 ? nt - 1 : 0) : ref.nnodes;
+    }
+    template <class F>
+    void visit(F&& f) const
+    {
+        if (mode == SDFO_BVH_LBVH)
+            f(lbvh.view());
+        else
+            f(ref.view());
+    }
+};
+
+double scene_extent(const double* verts, int64_t nv, const sdfo_grid_info& info)
+{
+    double e = 0.0;
+    for (int64_t i = 0; i < 3 * nv; ++i) e = std::max(e, std::fabs(verts[i]));
+    for (int a = 0; a < 3; ++a) e = std::max({e, std::fabs(info.bmin[a]), std::fabs(info.bmax[a])});
+    return e > 0.0 ? e : 1.0;
+}
+
+SpecD spec_of(const sdfo_grid_info& info)
+{
+    SpecD s{};
+    for (int a = 0; a < 3; ++a)
+    {
+        s.bmin[a] = info.bmin[a];
+        s.voxel[a] = info.voxel[a];
+        s.n[a] = info.shape[a];
+    }
+    return s;
+}
+
+void check_status(const DeviceBuffer<int>& status, cudaStream_t s)
+{
+    int h = 0;
+    SDFO_CUDA(cudaMemcpyAsync(&h, status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    SDFO_CUDA(cudaStreamSynchronize(s));
+    if (h & kStatusStackOverflow)
+        throw Error(SDFO_ERR_DEVICE_STATUS, "BVH traversal stack overflow (tree deeper than 64)");
+}
+
+} // namespace
+
+} // namespace sdfo

@@ -124,6 +124,36 @@ int sdfo_grid_build_sparse(const double* h_verts, int64_t nv, const int32_t* h_t
     });
 }
 
+int sdfo_grid_build_sparse_batched(const sdfo_mesh_desc* meshes, int32_t n, void* stream,
+                                   sdfo_grid** out)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(out != nullptr && meshes != nullptr, SDFO_ERR_INVALID_ARGUMENT, "NULL argument");
+        SDFO_REQUIRE(n > 0, SDFO_ERR_INVALID_ARGUMENT, "batched build needs at least one mesh");
+        for (int32_t m = 0; m < n; ++m) out[m] = nullptr;
+        for (int32_t m = 0; m < n; ++m)
+        {
+            const sdfo_mesh_desc& d = meshes[m];
+            check_mesh(d.h_verts, d.nv, d.h_tris, d.nt);
+            check_build_params(&d.params.base);
+            SDFO_REQUIRE(d.params.block_dim > 0, SDFO_ERR_INVALID_ARGUMENT,
+                         "Sparse SDF blockDim must be positive");
+            SDFO_REQUIRE(d.params.block_dim <= 16, SDFO_ERR_UNSUPPORTED,
+                         "blockDim above 16 is not provided");
+        }
+        const std::vector<sdfo_grid*> grids = build_sparse_batched(meshes, n, as_stream(stream));
+        for (int32_t m = 0; m < n; ++m) out[m] = grids[(size_t)m];
+    });
+}
+
+int sdfo_set_fill_ctas_per_sm(int32_t ctas)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(ctas >= 0 && ctas <= 64, SDFO_ERR_INVALID_ARGUMENT, "CTAs per SM out of range");
+        set_fill_ctas_per_sm(ctas);
+    });
+}
+
 int sdfo_set_bvh_mode(int32_t mode)
 {
     return guarded([&] {
@@ -215,12 +245,53 @@ int sdfo_query_backward(const sdfo_grid* g, int32_t mode, const float* d_points,
         SDFO_REQUIRE(d_points != nullptr, SDFO_ERR_INVALID_ARGUMENT, "points are required");
         SDFO_REQUIRE(mode == SDFO_TRILINEAR || mode == SDFO_TRICUBIC, SDFO_ERR_UNSUPPORTED,
                      "query backward supports Trilinear and Tricubic");
-        SDFO_REQUIRE(d_dgrid == nullptr || g->info.storage == SDFO_STORAGE_FP32, SDFO_ERR_UNSUPPORTED,
-                     "grid gradients need FP32 storage");
         SDFO_REQUIRE((reinterpret_cast<uintptr_t>(d_dgrid) & 15) == 0, SDFO_ERR_INVALID_ARGUMENT,
                      "grid gradient buffer must be 16-byte aligned");
         launch_query_backward(make_view(g), mode, d_points, n, d_dgap, d_dgrad, d_dpoints, d_dgrid,
                               as_stream(stream));
+    });
+}
+
+int sdfo_query_linearize(const sdfo_grid* g, int32_t mode, const float* d_points, int64_t n,
+                         float* d_gap, float* d_grad, uint8_t* d_valid, float* d_hess6,
+                         void* stream)
+{
+    return guarded([&] {
+        check_grid(g);
+        SDFO_REQUIRE(n >= 0, SDFO_ERR_INVALID_ARGUMENT, "negative query count");
+        if (n == 0) return;
+        SDFO_REQUIRE(mode == SDFO_TRILINEAR || mode == SDFO_TRICUBIC, SDFO_ERR_UNSUPPORTED,
+                     "query linearisation supports Trilinear and Tricubic");
+        SDFO_REQUIRE(d_points && d_gap && d_grad && d_valid && d_hess6, SDFO_ERR_INVALID_ARGUMENT,
+                     "points, gap, grad, valid and hess6 are required");
+        SDFO_REQUIRE(n <= (int64_t)65535 * 256 * 4096, SDFO_ERR_INVALID_ARGUMENT, "too many queries");
+        QueryOutputs o{d_gap, d_grad, nullptr, nullptr, d_valid, nullptr};
+        o.hess6 = d_hess6;
+        launch_query(make_view(g), mode, d_points, false, n, o, as_stream(stream));
+    });
+}
+
+int sdfo_query_backward_saved(const sdfo_grid* g, int32_t mode, const float* d_points, int64_t n,
+                              const float* d_grad, const float* d_hess6, const uint8_t* d_valid,
+                              const float* d_dgap, const float* d_dgrad, float* d_dpoints,
+                              float* d_dgrid, void* stream)
+{
+    return guarded([&] {
+        check_grid(g);
+        SDFO_REQUIRE(n >= 0, SDFO_ERR_INVALID_ARGUMENT, "negative query count");
+        if (n == 0) return;
+        SDFO_REQUIRE(mode == SDFO_TRILINEAR || mode == SDFO_TRICUBIC, SDFO_ERR_UNSUPPORTED,
+                     "query backward supports Trilinear and Tricubic");
+        SDFO_REQUIRE(d_dpoints == nullptr || (d_grad && d_hess6), SDFO_ERR_INVALID_ARGUMENT,
+                     "point gradients need the saved grad and hess6");
+        SDFO_REQUIRE(d_dgrid == nullptr || (d_points && d_valid), SDFO_ERR_INVALID_ARGUMENT,
+                     "grid gradients need the points and the saved valid flags");
+        SDFO_REQUIRE((reinterpret_cast<uintptr_t>(d_dgrid) & 15) == 0, SDFO_ERR_INVALID_ARGUMENT,
+                     "grid gradient buffer must be 16-byte aligned");
+        SDFO_REQUIRE(n <= (int64_t)65535 * 256 * 4096, SDFO_ERR_INVALID_ARGUMENT, "too many queries");
+        const SavedBackward b{d_points, n, d_grad, d_hess6, d_valid, d_dgap, d_dgrad, d_dpoints,
+                              d_dgrid};
+        launch_backward_saved(make_view(g), mode, b, as_stream(stream));
     });
 }
 

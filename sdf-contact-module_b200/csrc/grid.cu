@@ -598,6 +598,7 @@ int sdfo_grid_create_view(const sdfo_grid* g, void* d_phin, sdfo_grid** out)
         v->d.phi64 = v->d.n64 = v->d.w64 = v->d.h64 = nullptr; // export reads the live payload
         v->d.xpair = v->d.cell8 = nullptr; // stencil copies would go stale: read the payload
         v->borrowed = true;
+        v->arena = g->arena;
         *out = v.release();
     });
 }

@@ -326,4 +326,133 @@ __device__ __forceinline__ Interp trilinear(const float c[8], float u, float v, 
     return r;
 }
 
+// ---------------------------------------------------------------------------
+// one query of any mode (SdfOracle::queryFast and the per-mode queries,
+// SdfOracle.cpp:226-432, 448-851, 932-1092)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void unit_of(const float g[3], float u[3])
+{
+    const float len = sqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+    if (len > 1e-15f)
+    {
+        const float inv = 1.f / len;
+        u[0] = g[0] * inv;
+        u[1] = g[1] * inv;
+        u[2] = g[2] * inv;
+    }
+    else
+    {
+        u[0] = 1.f;
+        u[1] = 0.f;
+        u[2] = 0.f;
+    }
+}
+
+template <int MODE, bool SPARSE, int BD, bool HESS>
+__device__ __forceinline__ bool evaluate(const GridView& g, const double p[3], Interp& r,
+                                         float unit[3])
+{
+    const float h[3] = {(float)g.voxel[0], (float)g.voxel[1], (float)g.voxel[2]};
+    if (MODE == SDFO_TRILINEAR || MODE == SDFO_TRICUBIC)
+    {
+        const Cell c = cell_of(g, p);
+        if (!c.ok) return false;
+        if (!SPARSE && MODE == SDFO_TRILINEAR && g.cell8 != nullptr)
+        {
+            // one 32-byte load: the 8 corner phi of the cell
+            float4 a, b;
+            ld256(g.cell8 + 2 * dense_index(g, c.i0, c.j0, c.k0), a, b);
+            const float phi[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+            r = trilinear<HESS>(phi, c.u, c.v, c.w, h);
+            unit_of(r.g, unit);
+            return true;
+        }
+        float4 cs[8];
+        if (!SPARSE && MODE == SDFO_TRICUBIC && g.xpair != nullptr)
+        {
+            // four 32-byte loads: the x-pairs of the 4 (dj, dk) corner rows
+            const int64_t base = dense_index(g, c.i0, c.j0, c.k0);
+            const int64_t sy = g.nx, sz = (int64_t)g.nx * g.ny;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                const int64_t v = base + ((q & 1) ? sy : 0) + ((q & 2) ? sz : 0);
+                ld256(g.xpair + 2 * v, cs[2 * q], cs[2 * q + 1]);
+            }
+        }
+        else
+        {
+            int64_t idx[8];
+            if (!gather_corners<SPARSE, BD>(g, c, cs, idx)) return false;
+        }
+        if (MODE == SDFO_TRICUBIC)
+        {
+            r = tricubic<HESS>(cs, c.u, c.v, c.w, h);
+        }
+        else
+        {
+            float phi[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) phi[q] = cs[q].x;
+            r = trilinear<HESS>(phi, c.u, c.v, c.w, h);
+        }
+        unit_of(r.g, unit);
+        return true;
+    }
+    // FirstOrder / SecondOrder at the nearest voxel (SdfOracle.cpp:448-520,
+    // 600-654).
+    int ijk[3];
+    float dx[3];
+    if (!nearest_voxel(g, p, ijk, dx)) return false;
+    int64_t idx;
+    if (SPARSE)
+    {
+        idx = sparse_index<BD>(g, ijk[0], ijk[1], ijk[2]);
+        if (idx < 0) return false;
+    }
+    else
+    {
+        idx = dense_index(g, ijk[0], ijk[1], ijk[2]);
+    }
+    const float4 c = load_stored<BD>(g, idx);
+    const float n0[3] = {c.y, c.z, c.w};
+    const float first = n0[0] * dx[0] + n0[1] * dx[1] + n0[2] * dx[2];
+    if (MODE == SDFO_SECOND_ORDER && g.has_hessian && g.hess6 != nullptr)
+    {
+        float H[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) H[q] = __ldg(g.hess6 + 6 * idx + q);
+        const float Hd[3] = {H[0] * dx[0] + H[1] * dx[1] + H[2] * dx[2],
+                             H[1] * dx[0] + H[3] * dx[1] + H[4] * dx[2],
+                             H[2] * dx[0] + H[4] * dx[1] + H[5] * dx[2]};
+        r.gap = c.x + first + 0.5f * (dx[0] * Hd[0] + dx[1] * Hd[1] + dx[2] * Hd[2]);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) r.g[a] = n0[a] + Hd[a];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) r.H[q] = H[q];
+        const float len = sqrtf(r.g[0] * r.g[0] + r.g[1] * r.g[1] + r.g[2] * r.g[2]);
+        if (len > 1e-15f)
+        {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) unit[a] = r.g[a] / len;
+        }
+        else
+        {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) unit[a] = n0[a];
+        }
+        return true;
+    }
+    r.gap = c.x + first;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        r.g[a] = n0[a];
+        unit[a] = n0[a];
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) r.H[q] = 0.f;
+    return true;
+}
+
 } // namespace sdfo

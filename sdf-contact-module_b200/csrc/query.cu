@@ -26,157 +26,135 @@ __device__ __forceinline__ void load_point(const PT* pts, int64_t q, double p[3]
     p[2] = (double)__ldcs(pts + 3 * q + 2);
 }
 
-__device__ __forceinline__ void unit_of(const float g[3], float u[3])
+// Block-cooperative I/O of K-float records (points in; gradient, unit,
+// witness, Hessian out): the block's 256 records are one contiguous range,
+// moved with 16-byte accesses through shared memory instead of K 4-byte
+// accesses per thread at a 4K-byte stride.  Used when the pointers are
+// 16-byte aligned (the host checks); `src`/`dst` point at the block's first
+// record and `cnt` = records of this block.
+template <int K>
+__device__ __forceinline__ void stage_in(float* sbuf, const float* src, int cnt)
 {
-    const float len = sqrtf(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
-    if (len > 1e-15f)
-    {
-        const float inv = 1.f / len;
-        u[0] = g[0] * inv;
-        u[1] = g[1] * inv;
-        u[2] = g[2] * inv;
-    }
-    else
-    {
-        u[0] = 1.f;
-        u[1] = 0.f;
-        u[2] = 0.f;
-    }
-}
-
-template <int MODE, bool SPARSE, int BD, bool HESS>
-__device__ __forceinline__ bool evaluate(const GridView& g, const double p[3], Interp& r,
-                                         float unit[3])
-{
-    const float h[3] = {(float)g.voxel[0], (float)g.voxel[1], (float)g.voxel[2]};
-    if (MODE == SDFO_TRILINEAR || MODE == SDFO_TRICUBIC)
-    {
-        const Cell c = cell_of(g, p);
-        if (!c.ok) return false;
-        if (!SPARSE && MODE == SDFO_TRILINEAR && g.cell8 != nullptr)
-        {
-            // one 32-byte load: the 8 corner phi of the cell
-            float4 a, b;
-            ld256(g.cell8 + 2 * dense_index(g, c.i0, c.j0, c.k0), a, b);
-            const float phi[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-            r = trilinear<HESS>(phi, c.u, c.v, c.w, h);
-            unit_of(r.g, unit);
-            return true;
-        }
-        float4 cs[8];
-        if (!SPARSE && MODE == SDFO_TRICUBIC && g.xpair != nullptr)
-        {
-            // four 32-byte loads: the x-pairs of the 4 (dj, dk) corner rows
-            const int64_t base = dense_index(g, c.i0, c.j0, c.k0);
-            const int64_t sy = g.nx, sz = (int64_t)g.nx * g.ny;
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-            {
-                const int64_t v = base + ((q & 1) ? sy : 0) + ((q & 2) ? sz : 0);
-                ld256(g.xpair + 2 * v, cs[2 * q], cs[2 * q + 1]);
-            }
-        }
-        else
-        {
-            int64_t idx[8];
-            if (!gather_corners<SPARSE, BD>(g, c, cs, idx)) return false;
-        }
-        if (MODE == SDFO_TRICUBIC)
-        {
-            r = tricubic<HESS>(cs, c.u, c.v, c.w, h);
-        }
-        else
-        {
-            float phi[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) phi[q] = cs[q].x;
-            r = trilinear<HESS>(phi, c.u, c.v, c.w, h);
-        }
-        unit_of(r.g, unit);
-        return true;
-    }
-    // FirstOrder / SecondOrder at the nearest voxel (SdfOracle.cpp:448-520,
-    // 600-654).
-    int ijk[3];
-    float dx[3];
-    if (!nearest_voxel(g, p, ijk, dx)) return false;
-    int64_t idx;
-    if (SPARSE)
-    {
-        idx = sparse_index<BD>(g, ijk[0], ijk[1], ijk[2]);
-        if (idx < 0) return false;
-    }
-    else
-    {
-        idx = dense_index(g, ijk[0], ijk[1], ijk[2]);
-    }
-    const float4 c = load_stored<BD>(g, idx);
-    const float n0[3] = {c.y, c.z, c.w};
-    const float first = n0[0] * dx[0] + n0[1] * dx[1] + n0[2] * dx[2];
-    if (MODE == SDFO_SECOND_ORDER && g.has_hessian && g.hess6 != nullptr)
-    {
-        float H[6];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) H[q] = __ldg(g.hess6 + 6 * idx + q);
-        const float Hd[3] = {H[0] * dx[0] + H[1] * dx[1] + H[2] * dx[2],
-                             H[1] * dx[0] + H[3] * dx[1] + H[4] * dx[2],
-                             H[2] * dx[0] + H[4] * dx[1] + H[5] * dx[2]};
-        r.gap = c.x + first + 0.5f * (dx[0] * Hd[0] + dx[1] * Hd[1] + dx[2] * Hd[2]);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) r.g[a] = n0[a] + Hd[a];
-#pragma unroll
-        for (int q = 0; q < 6; ++q) r.H[q] = H[q];
-        const float len = sqrtf(r.g[0] * r.g[0] + r.g[1] * r.g[1] + r.g[2] * r.g[2]);
-        if (len > 1e-15f)
-        {
-#pragma unroll
-            for (int a = 0; a < 3; ++a) unit[a] = r.g[a] / len;
-        }
-        else
-        {
-#pragma unroll
-            for (int a = 0; a < 3; ++a) unit[a] = n0[a];
-        }
-        return true;
-    }
-    r.gap = c.x + first;
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-    {
-        r.g[a] = n0[a];
-        unit[a] = n0[a];
-    }
-#pragma unroll
-    for (int q = 0; q < 6; ++q) r.H[q] = 0.f;
-    return true;
-}
-
-// Block-cooperative I/O of 3-float records (points in, gradient / unit /
-// witness out): the block's 256 records are one contiguous 3 KB range, moved
-// with 16-byte accesses through shared memory instead of three 4-byte
-// accesses per thread at a 12-byte stride.  Used when the pointers are
-// 16-byte aligned (the host checks); `cnt` = records of this block.
-__device__ __forceinline__ void stage_in3(float* sbuf, const float* src, int cnt)
-{
-    const int nf = 3 * cnt, nv = nf >> 2;
+    const int nf = K * cnt, nv = nf >> 2;
     for (int t = threadIdx.x; t < nv; t += kThreads)
         reinterpret_cast<float4*>(sbuf)[t] = __ldcs(reinterpret_cast<const float4*>(src) + t);
     for (int t = 4 * nv + threadIdx.x; t < nf; t += kThreads) sbuf[t] = __ldcs(src + t);
 }
 
-__device__ __forceinline__ void stage_out3(float* sbuf, float* dst, int cnt)
+template <int K>
+__device__ __forceinline__ void stage_out(const float* sbuf, float* dst, int cnt)
 {
-    const int nf = 3 * cnt, nv = nf >> 2;
+    const int nf = K * cnt, nv = nf >> 2;
     for (int t = threadIdx.x; t < nv; t += kThreads)
         __stcs(reinterpret_cast<float4*>(dst) + t, reinterpret_cast<const float4*>(sbuf)[t]);
     for (int t = 4 * nv + threadIdx.x; t < nf; t += kThreads) __stcs(dst + t, sbuf[t]);
+}
+
+// This thread's K-float record of a block-uniform array (staged or direct).
+template <int K, bool STAGED>
+__device__ __forceinline__ void read_rec(float* sbuf, const float* base, int64_t q0, int cnt,
+                                         bool active, float r[K])
+{
+    if (STAGED)
+    {
+        __syncthreads();
+        stage_in<K>(sbuf, base + K * q0, cnt);
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < K; ++a) r[a] = active ? sbuf[K * threadIdx.x + a] : 0.f;
+    }
+    else
+    {
+#pragma unroll
+        for (int a = 0; a < K; ++a) r[a] = active ? __ldcs(base + K * (q0 + threadIdx.x) + a) : 0.f;
+    }
+}
+
+template <int K, bool STAGED>
+__device__ __forceinline__ void write_rec(float* sbuf, float* base, int64_t q0, int cnt,
+                                          bool active, const float r[K])
+{
+    if (STAGED)
+    {
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < K; ++a) sbuf[K * threadIdx.x + a] = r[a];
+        __syncthreads();
+        stage_out<K>(sbuf, base + K * q0, cnt);
+    }
+    else if (active)
+    {
+#pragma unroll
+        for (int a = 0; a < K; ++a) __stcs(base + K * (q0 + threadIdx.x) + a, r[a]);
+    }
+}
+
+// dL/d(stored payload) of one valid query: the interpolant is linear in
+// the corner values, so the scatter weights are the basis functions (and
+// their derivatives / h for the gradient outputs) at the point.  float4
+// atomics {d phi, d n} per corner.  A corner whose brick is not stored
+// (possible only when the caller's valid flags belong to other points or
+// another grid) is skipped.
+template <int MODE, bool SPARSE, int BD>
+__device__ __forceinline__ void scatter_grid_gradient(const GridView& g, const Cell& c, float dG,
+                                                      const float dg[3], float* dgrid)
+{
+    const float h[3] = {(float)g.voxel[0], (float)g.voxel[1], (float)g.voxel[2]};
+    const float ig[3] = {dg[0] / h[0], dg[1] / h[1], dg[2] / h[2]};
+    float4* out = reinterpret_cast<float4*>(dgrid);
+    auto index = [&](int k) -> int64_t {
+        const int i = c.i0 + (k & 1), j = c.j0 + ((k >> 1) & 1), kk = c.k0 + (k >> 2);
+        return SPARSE ? sparse_index<BD>(g, i, j, kk) : dense_index(g, i, j, kk);
+    };
+    if (MODE == SDFO_TRICUBIC)
+    {
+        float bx[4], dx[4], by[4], dy[4], bz[4], dz[4];
+        hermite(c.u, bx, dx);
+        hermite(c.v, by, dy);
+        hermite(c.w, bz, dz);
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+        {
+            const int di = k & 1, dj = (k >> 1) & 1, dk = k >> 2;
+            const float P0 = bx[2 * di], P1 = bx[2 * di + 1], dP0 = dx[2 * di], dP1 = dx[2 * di + 1];
+            const float Q0 = by[2 * dj], Q1 = by[2 * dj + 1], dQ0 = dy[2 * dj], dQ1 = dy[2 * dj + 1];
+            const float R0 = bz[2 * dk], R1 = bz[2 * dk + 1], dR0 = dz[2 * dk], dR1 = dz[2 * dk + 1];
+            // d/d phi_k
+            const float wphi = dG * (P0 * Q0 * R0) + ig[0] * (dP0 * Q0 * R0) +
+                               ig[1] * (P0 * dQ0 * R0) + ig[2] * (P0 * Q0 * dR0);
+            // d/d (n h) components, chained through the slope n * h
+            const float wgx = dG * (P1 * Q0 * R0) + ig[0] * (dP1 * Q0 * R0) +
+                              ig[1] * (P1 * dQ0 * R0) + ig[2] * (P1 * Q0 * dR0);
+            const float wgy = dG * (P0 * Q1 * R0) + ig[0] * (dP0 * Q1 * R0) +
+                              ig[1] * (P0 * dQ1 * R0) + ig[2] * (P0 * Q1 * dR0);
+            const float wgz = dG * (P0 * Q0 * R1) + ig[0] * (dP0 * Q0 * R1) +
+                              ig[1] * (P0 * dQ0 * R1) + ig[2] * (P0 * Q0 * dR1);
+            const int64_t ix = index(k);
+            if (ix >= 0) atomicAdd(out + ix, make_float4(wphi, wgx * h[0], wgy * h[1], wgz * h[2]));
+        }
+    }
+    else
+    {
+        const float u = c.u, v = c.v, w = c.w;
+        const float bu[2] = {1.f - u, u}, bv[2] = {1.f - v, v}, bw[2] = {1.f - w, w};
+        const float du[2] = {-1.f, 1.f};
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+        {
+            const int di = k & 1, dj = (k >> 1) & 1, dk = k >> 2;
+            const float wphi = dG * (bu[di] * bv[dj] * bw[dk]) + ig[0] * (du[di] * bv[dj] * bw[dk]) +
+                               ig[1] * (bu[di] * du[dj] * bw[dk]) + ig[2] * (bu[di] * bv[dj] * du[dk]);
+            const int64_t ix = index(k);
+            if (ix >= 0) atomicAdd(&out[ix].x, wphi);
+        }
+    }
 }
 
 template <int MODE, bool SPARSE, int BD, typename PT, bool HESS, bool STAGED>
 __global__ void __launch_bounds__(kThreads) k_query(GridView g, const PT* __restrict__ pts,
                                                   int64_t n, QueryOutputs o)
 {
-    __shared__ __align__(16) float sbuf[STAGED ? 3 * kThreads : 1];
+    __shared__ __align__(16) float sbuf[STAGED ? (HESS ? 6 : 3) * kThreads : 1];
     const int64_t q0 = (int64_t)blockIdx.x * kThreads;
     const int64_t q = q0 + threadIdx.x;
     const bool active = q < n;
@@ -184,14 +162,11 @@ __global__ void __launch_bounds__(kThreads) k_query(GridView g, const PT* __rest
     double p[3] = {0.0, 0.0, 0.0};
     if (STAGED)
     {
-        stage_in3(sbuf, reinterpret_cast<const float*>(pts) + 3 * q0, cnt);
-        __syncthreads();
-        if (active)
-        {
-            p[0] = sbuf[3 * threadIdx.x];
-            p[1] = sbuf[3 * threadIdx.x + 1];
-            p[2] = sbuf[3 * threadIdx.x + 2];
-        }
+        float pf[3];
+        read_rec<3, true>(sbuf, reinterpret_cast<const float*>(pts), q0, cnt, active, pf);
+        p[0] = pf[0];
+        p[1] = pf[1];
+        p[2] = pf[2];
     }
     else if (active)
     {
@@ -217,36 +192,12 @@ __global__ void __launch_bounds__(kThreads) k_query(GridView g, const PT* __rest
     float w[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) w[a] = valid ? (float)(p[a] - (double)r.gap * unit[a]) : 0.f;
-    if (STAGED)
-    {
-        // o.grad / o.unit / o.witness are uniform over the block
-        const float* outs[3] = {r.g, unit, w};
-        float* dsts[3] = {o.grad, o.unit, o.witness};
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-        {
-            if (dsts[k] == nullptr) continue;
-            __syncthreads();
-            sbuf[3 * threadIdx.x] = outs[k][0];
-            sbuf[3 * threadIdx.x + 1] = outs[k][1];
-            sbuf[3 * threadIdx.x + 2] = outs[k][2];
-            __syncthreads();
-            stage_out3(sbuf, dsts[k] + 3 * q0, cnt);
-        }
-    }
-    else if (active)
-    {
-        if (o.grad)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) __stcs(o.grad + 3 * q + a, r.g[a]);
-        if (o.unit)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) __stcs(o.unit + 3 * q + a, unit[a]);
-        if (o.witness)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) __stcs(o.witness + 3 * q + a, w[a]);
-    }
-    if (HESS && active)
+    // the output pointers are uniform over the block
+    if (o.grad) write_rec<3, STAGED>(sbuf, o.grad, q0, cnt, active, r.g);
+    if (o.unit) write_rec<3, STAGED>(sbuf, o.unit, q0, cnt, active, unit);
+    if (o.witness) write_rec<3, STAGED>(sbuf, o.witness, q0, cnt, active, w);
+    if (HESS && o.hess6) write_rec<6, STAGED>(sbuf, o.hess6, q0, cnt, active, r.H);
+    if (HESS && o.hess && active)
     {
         const float H9[9] = {r.H[0], r.H[1], r.H[2], r.H[1], r.H[3], r.H[4], r.H[2], r.H[4], r.H[5]};
 #pragma unroll
@@ -254,8 +205,50 @@ __global__ void __launch_bounds__(kThreads) k_query(GridView g, const PT* __rest
     }
 }
 
-// Backward: dL/dp = dgap * grad + H dgrad, and the scatter of dL/d(payload)
-// onto the 8 corners (float4 atomics: d phi, d n).
+// Reverse mode from the linearisation the forward saved (grad, symmetric
+// Hessian, valid flag): dL/dp = dgap * grad + H dgrad is elementwise, and the
+// grid gradient needs only the corner weights, which depend on the point
+// but not on the grid values, so nothing of the grid is read again.
+template <int MODE, bool SPARSE, int BD, bool STAGED, bool DPTS, bool DGRID>
+__global__ void __launch_bounds__(kThreads)
+    k_backward_saved(GridView g, const float* __restrict__ pts, int64_t n,
+                     const float* __restrict__ grad, const float* __restrict__ hess6,
+                     const uint8_t* __restrict__ valid, const float* __restrict__ dgap,
+                     const float* __restrict__ dgrad, float* __restrict__ dpts,
+                     float* __restrict__ dgrid)
+{
+    __shared__ __align__(16) float sbuf[STAGED ? 6 * kThreads : 1];
+    const int64_t q0 = (int64_t)blockIdx.x * kThreads;
+    const int64_t q = q0 + threadIdx.x;
+    const bool active = q < n;
+    const int cnt = (int)(n - q0 < kThreads ? n - q0 : kThreads);
+    const float dG = (dgap && active) ? __ldcs(dgap + q) : 0.f;
+    float dg[3] = {0.f, 0.f, 0.f};
+    if (dgrad) read_rec<3, STAGED>(sbuf, dgrad, q0, cnt, active, dg);
+    if (DPTS)
+    {
+        float gr[3], H[6];
+        read_rec<3, STAGED>(sbuf, grad, q0, cnt, active, gr);
+        read_rec<6, STAGED>(sbuf, hess6, q0, cnt, active, H);
+        const float out[3] = {dG * gr[0] + H[0] * dg[0] + H[1] * dg[1] + H[2] * dg[2],
+                              dG * gr[1] + H[1] * dg[0] + H[3] * dg[1] + H[4] * dg[2],
+                              dG * gr[2] + H[2] * dg[0] + H[4] * dg[1] + H[5] * dg[2]};
+        write_rec<3, STAGED>(sbuf, dpts, q0, cnt, active, out);
+    }
+    if (DGRID)
+    {
+        float pf[3];
+        read_rec<3, STAGED>(sbuf, pts, q0, cnt, active, pf);
+        if (!active || !valid[q]) return;
+        const double p[3] = {pf[0], pf[1], pf[2]};
+        const Cell c = cell_of(g, p);
+        if (!c.ok) return;
+        scatter_grid_gradient<MODE, SPARSE, BD>(g, c, dG, dg, dgrid);
+    }
+}
+
+// Backward with the stencil gathered again (no saved state): dL/dp =
+// dgap * grad + H dgrad, and the grid gradient scatter.
 template <int MODE, bool SPARSE, int BD>
 __global__ void __launch_bounds__(kThreads)
     k_query_backward(GridView g, const float* __restrict__ pts, int64_t n,
@@ -274,85 +267,23 @@ __global__ void __launch_bounds__(kThreads)
         dg[1] = __ldcs(dgrad + 3 * q + 1);
         dg[2] = __ldcs(dgrad + 3 * q + 2);
     }
-    const float h[3] = {(float)g.voxel[0], (float)g.voxel[1], (float)g.voxel[2]};
-    const Cell c = cell_of(g, p);
-    float4 cs[8];
-    int64_t idx[8];
-    const bool ok = c.ok && gather_corners<SPARSE, BD>(g, c, cs, idx);
-    if (!ok)
-    {
-        if (dpts)
-        {
-            dpts[3 * q + 0] = 0.f;
-            dpts[3 * q + 1] = 0.f;
-            dpts[3 * q + 2] = 0.f;
-        }
-        return;
-    }
     Interp r;
-    if (MODE == SDFO_TRICUBIC)
-    {
-        r = tricubic<true>(cs, c.u, c.v, c.w, h);
-    }
-    else
-    {
-        float phi[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) phi[k] = cs[k].x;
-        r = trilinear<true>(phi, c.u, c.v, c.w, h);
-    }
+    float unit[3];
+    const bool ok = evaluate<MODE, SPARSE, BD, true>(g, p, r, unit);
     if (dpts)
     {
-        const float H[9] = {r.H[0], r.H[1], r.H[2], r.H[1], r.H[3], r.H[4], r.H[2], r.H[4], r.H[5]};
+        const float* H = r.H;
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
-            dpts[3 * q + a] = dG * r.g[a] + H[3 * a + 0] * dg[0] + H[3 * a + 1] * dg[1] +
-                              H[3 * a + 2] * dg[2];
-    }
-    if (!dgrid) return;
-    // Per-corner weights of gap and of grad (= d/du etc. / h).
-    const float ig[3] = {dg[0] / h[0], dg[1] / h[1], dg[2] / h[2]};
-    if (MODE == SDFO_TRICUBIC)
-    {
-        float bx[4], dx[4], by[4], dy[4], bz[4], dz[4];
-        hermite(c.u, bx, dx);
-        hermite(c.v, by, dy);
-        hermite(c.w, bz, dz);
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
+        for (int a = 0; a < 3; ++a) dpts[3 * q + a] = 0.f;
+        if (ok)
         {
-            const int di = k & 1, dj = (k >> 1) & 1, dk = k >> 2;
-            const float P0 = bx[2 * di], P1 = bx[2 * di + 1], dP0 = dx[2 * di], dP1 = dx[2 * di + 1];
-            const float Q0 = by[2 * dj], Q1 = by[2 * dj + 1], dQ0 = dy[2 * dj], dQ1 = dy[2 * dj + 1];
-            const float R0 = bz[2 * dk], R1 = bz[2 * dk + 1], dR0 = dz[2 * dk], dR1 = dz[2 * dk + 1];
-            // d/d phi_k
-            const float wphi = dG * (P0 * Q0 * R0) + ig[0] * (dP0 * Q0 * R0) +
-                               ig[1] * (P0 * dQ0 * R0) + ig[2] * (P0 * Q0 * dR0);
-            // d/d gx_k, gy_k, gz_k, then chain through g = n * h
-            const float wgx = dG * (P1 * Q0 * R0) + ig[0] * (dP1 * Q0 * R0) +
-                              ig[1] * (P1 * dQ0 * R0) + ig[2] * (P1 * Q0 * dR0);
-            const float wgy = dG * (P0 * Q1 * R0) + ig[0] * (dP0 * Q1 * R0) +
-                              ig[1] * (P0 * dQ1 * R0) + ig[2] * (P0 * Q1 * dR0);
-            const float wgz = dG * (P0 * Q0 * R1) + ig[0] * (dP0 * Q0 * R1) +
-                              ig[1] * (P0 * dQ0 * R1) + ig[2] * (P0 * Q0 * dR1);
-            atomicAdd(reinterpret_cast<float4*>(dgrid) + idx[k],
-                      make_float4(wphi, wgx * h[0], wgy * h[1], wgz * h[2]));
+            dpts[3 * q + 0] = dG * r.g[0] + H[0] * dg[0] + H[1] * dg[1] + H[2] * dg[2];
+            dpts[3 * q + 1] = dG * r.g[1] + H[1] * dg[0] + H[3] * dg[1] + H[4] * dg[2];
+            dpts[3 * q + 2] = dG * r.g[2] + H[2] * dg[0] + H[4] * dg[1] + H[5] * dg[2];
         }
     }
-    else
-    {
-        const float u = c.u, v = c.v, w = c.w;
-        const float bu[2] = {1.f - u, u}, bv[2] = {1.f - v, v}, bw[2] = {1.f - w, w};
-        const float du[2] = {-1.f, 1.f};
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-        {
-            const int di = k & 1, dj = (k >> 1) & 1, dk = k >> 2;
-            const float wphi = dG * (bu[di] * bv[dj] * bw[dk]) + ig[0] * (du[di] * bv[dj] * bw[dk]) +
-                               ig[1] * (bu[di] * du[dj] * bw[dk]) + ig[2] * (bu[di] * bv[dj] * du[dk]);
-            atomicAdd(reinterpret_cast<float4*>(dgrid) + idx[k], make_float4(wphi, 0.f, 0.f, 0.f));
-        }
-    }
+    if (!dgrid || !ok) return;
+    scatter_grid_gradient<MODE, SPARSE, BD>(g, cell_of(g, p), dG, dg, dgrid);
 }
 
 template <int MODE, bool SPARSE, int BD, bool HESS>
@@ -378,8 +309,8 @@ void launch_pt(const GridView& v, const void* pts, bool f64, int64_t n, const Qu
                cudaStream_t s)
 {
     const bool staged = !f64 && aligned16(pts) && aligned16(o.grad) && aligned16(o.unit) &&
-                        aligned16(o.witness);
-    if (o.hess)
+                        aligned16(o.witness) && aligned16(o.hess6);
+    if (o.hess || o.hess6)
         launch_pt2<MODE, SPARSE, BD, true>(v, pts, f64, staged, n, o, s);
     else
         launch_pt2<MODE, SPARSE, BD, false>(v, pts, f64, staged, n, o, s);
@@ -410,6 +341,41 @@ void launch_bwd_mode(const GridView& v, const float* pts, int64_t n, const float
         k_query_backward<MODE, true, 0><<<blocks, kThreads, 0, s>>>(v, pts, n, dgap, dgrad, dpts, dgrid);
 }
 
+template <int MODE, bool SPARSE, int BD, bool STAGED>
+void launch_saved3(const GridView& v, const SavedBackward& b, cudaStream_t s)
+{
+    const unsigned blocks = (unsigned)((b.n + kThreads - 1) / kThreads);
+#define SDFO_LAUNCH_SAVED(DP, DG)                                                          \
+    k_backward_saved<MODE, SPARSE, BD, STAGED, DP, DG><<<blocks, kThreads, 0, s>>>(        \
+        v, b.pts, b.n, b.grad, b.hess6, b.valid, b.dgap, b.dgrad, b.dpts, b.dgrid)
+    if (b.dpts && b.dgrid) SDFO_LAUNCH_SAVED(true, true);
+    else if (b.dpts) SDFO_LAUNCH_SAVED(true, false);
+    else if (b.dgrid) SDFO_LAUNCH_SAVED(false, true);
+#undef SDFO_LAUNCH_SAVED
+}
+
+template <int MODE, bool SPARSE, int BD>
+void launch_saved2(const GridView& v, const SavedBackward& b, cudaStream_t s)
+{
+    const bool staged = aligned16(b.pts) && aligned16(b.grad) && aligned16(b.hess6) &&
+                        aligned16(b.dgrad) && aligned16(b.dpts);
+    if (staged)
+        launch_saved3<MODE, SPARSE, BD, true>(v, b, s);
+    else
+        launch_saved3<MODE, SPARSE, BD, false>(v, b, s);
+}
+
+template <int MODE>
+void launch_saved_mode(const GridView& v, const SavedBackward& b, cudaStream_t s)
+{
+    if (v.layout == SDFO_LAYOUT_DENSE)
+        launch_saved2<MODE, false, 0>(v, b, s);
+    else if (v.bd == 8)
+        launch_saved2<MODE, true, 8>(v, b, s);
+    else
+        launch_saved2<MODE, true, 0>(v, b, s);
+}
+
 } // namespace
 
 void launch_query(const GridView& v, int mode, const void* pts, bool f64, int64_t n,
@@ -437,6 +403,22 @@ void launch_query_backward(const GridView& v, int mode, const float* pts, int64_
         launch_bwd_mode<SDFO_TRICUBIC>(v, pts, n, dgap, dgrad, dpts, dgrid, s);
     else if (mode == SDFO_TRILINEAR)
         launch_bwd_mode<SDFO_TRILINEAR>(v, pts, n, dgap, dgrad, dpts, dgrid, s);
+    else
+        throw Error(SDFO_ERR_UNSUPPORTED, "query backward supports Trilinear and Tricubic");
+    SDFO_CHECK_LAUNCH();
+}
+
+} // namespace sdfo
+
+namespace sdfo {
+
+void launch_backward_saved(const GridView& v, int mode, const SavedBackward& b, cudaStream_t s)
+{
+    if (b.n <= 0 || (!b.dpts && !b.dgrid)) return;
+    if (mode == SDFO_TRICUBIC)
+        launch_saved_mode<SDFO_TRICUBIC>(v, b, s);
+    else if (mode == SDFO_TRILINEAR)
+        launch_saved_mode<SDFO_TRILINEAR>(v, b, s);
     else
         throw Error(SDFO_ERR_UNSUPPORTED, "query backward supports Trilinear and Tricubic");
     SDFO_CHECK_LAUNCH();

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -136,6 +137,9 @@ struct sdfo_grid
     int64_t stored_voxels = 0;
     int32_t nb[3] = {0, 0, 0};
     bool borrowed = false; // a view: storage belongs to another handle / caller
+    // Storage shared by the grids of one batched build (released with the
+    // last of them); empty otherwise.
+    std::shared_ptr<void> arena;
     // Device staging for the host-buffer query path, grown on demand and
     // reused across calls; calls on one handle serialise on the mutex.
     mutable std::mutex ws_mutex;
@@ -145,6 +149,23 @@ struct sdfo_grid
 };
 
 namespace sdfo {
+
+// Largest m in [0, n) with offs[m] <= x (offs non-decreasing, offs[0] = 0):
+// the segment of a concatenation that holds element x, skipping empty
+// segments.
+__device__ __forceinline__ int find_segment(const int64_t* __restrict__ offs, int n, int64_t x)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(offs + mid) <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
 
 // Kernel-side view of a grid (passed by value).
 struct GridView
@@ -181,7 +202,8 @@ struct QueryOutputs
     float* unit;
     float* witness;
     uint8_t* valid;
-    float* hess;
+    float* hess;            // 9 per query (full 3x3), or NULL
+    float* hess6 = nullptr; // 6 per query (xx, xy, xz, yy, yz, zz), or NULL
 };
 void launch_query(const GridView& v, int mode, const void* pts, bool f64, int64_t n,
                   const QueryOutputs& o, cudaStream_t s);
@@ -189,12 +211,30 @@ void launch_query_backward(const GridView& v, int mode, const float* pts, int64_
                            const float* dgap, const float* dgrad, float* dpts, float* dgrid,
                            cudaStream_t s);
 
+// Reverse mode from a saved linearisation (query.cu).
+struct SavedBackward
+{
+    const float* pts;
+    int64_t n;
+    const float* grad;
+    const float* hess6;
+    const uint8_t* valid;
+    const float* dgap;
+    const float* dgrad;
+    float* dpts;
+    float* dgrid;
+};
+void launch_backward_saved(const GridView& v, int mode, const SavedBackward& b, cudaStream_t s);
+
 // Builders (build.cu).
 sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
                        const sdfo_build_params& p, cudaStream_t s);
 sdfo_grid* build_sparse(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
                         const sdfo_sparse_build_params& p, cudaStream_t s);
 sdfo_grid_info setup_grid(const double* verts, int64_t nv, const sdfo_build_params& p);
+// Batched sparse build (batch.cu): one grid per mesh, storage in one arena.
+std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n, cudaStream_t s);
+void set_fill_ctas_per_sm(int k);
 int bvh_mode();
 void set_bvh_mode(int m);
 

@@ -47,6 +47,15 @@ class SparseBuildParams(ctypes.Structure):
                 ("band_voxels", _I32), ("store_hessian", _I32), ("band_distance", _D)]
 
 
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("h_verts", _P), ("nv", _I64), ("h_tris", _P), ("nt", _I64),
+                ("params", SparseBuildParams)]
+
+
+class Pose(ctypes.Structure):
+    _fields_ = [("R", _D * 9), ("t", _D * 3)]
+
+
 class BodyState(ctypes.Structure):
     _fields_ = [("r", _D * 3), ("R", _D * 9), ("v", _D * 3), ("w", _D * 3)]
 
@@ -80,6 +89,9 @@ SIGNATURES = [
      [_P, _I64, _P, _I64, ctypes.POINTER(BuildParams), _P, ctypes.POINTER(_P)]),
     ("sdfo_grid_build_sparse", ctypes.c_int,
      [_P, _I64, _P, _I64, ctypes.POINTER(SparseBuildParams), _P, ctypes.POINTER(_P)]),
+    ("sdfo_grid_build_sparse_batched", ctypes.c_int,
+     [ctypes.POINTER(MeshDesc), _I32, _P, ctypes.POINTER(_P)]),
+    ("sdfo_set_fill_ctas_per_sm", ctypes.c_int, [_I32]),
     ("sdfo_grid_build_stats", ctypes.c_int, [_P, ctypes.POINTER(BuildStats)]),
     ("sdfo_set_bvh_mode", ctypes.c_int, [_I32]),
     ("sdfo_get_bvh_mode", ctypes.c_int, []),
@@ -99,6 +111,14 @@ SIGNATURES = [
     ("sdfo_query_host", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P, _P, _P]),
     ("sdfo_query_host_static", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P]),
     ("sdfo_query_backward", ctypes.c_int, [_P, _I32, _P, _I64, _P, _P, _P, _P, _P]),
+    ("sdfo_query_linearize", ctypes.c_int, [_P, _I32, _P, _I64, _P, _P, _P, _P, _P]),
+    ("sdfo_query_backward_saved", ctypes.c_int,
+     [_P, _I32, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P]),
+    ("sdfo_query_batch_create", ctypes.c_int, [_P, _I32, _P, ctypes.POINTER(_P)]),
+    ("sdfo_query_batch_run", ctypes.c_int, [_P, _I32, _P, _P, _P, _P, _P, _P]),
+    ("sdfo_query_batch_set_threads", ctypes.c_int, [_P, _I32]),
+    ("sdfo_query_batch_total", ctypes.c_int, [_P, ctypes.POINTER(_I64)]),
+    ("sdfo_query_batch_destroy", ctypes.c_int, [_P]),
     ("sdfo_contact_eval", ctypes.c_int,
      [_P, _I32, _P, _P, _I64, _P, _I64, _P, ctypes.POINTER(ContactParams), _P, _P, _P]),
 ]

@@ -133,6 +133,29 @@ class SdfGrid:
                                            ctypes.byref(out)))
         return cls(out.value, mode)
 
+    @classmethod
+    def build_sparse_batched(cls, meshes, mode=N.TRILINEAR, stream=None) -> list:
+        """Many SdfBuilder::buildSparse calls in one batched build
+        (sdfo_grid_build_sparse_batched): ``meshes`` is a list of dicts with
+        ``verts``, ``tris`` and the build_sparse keyword arguments (same
+        block_dim for all).  Returns one SdfGrid per mesh; the grids share one
+        device allocation."""
+        lib = N.load()
+        keep = []
+        descs = (N.MeshDesc * len(meshes))()
+        for i, m in enumerate(meshes):
+            v, t = cls._mesh(m["verts"], m["tris"])
+            keep.append((v, t))
+            p = N.SparseBuildParams(
+                N.BuildParams(m.get("padding", 0.1), m.get("voxel_size", 0.0),
+                              m.get("target_resolution", 128), m.get("max_resolution", 512)),
+                m.get("block_dim", 8), m.get("halo_voxels", 2), m.get("band_voxels", 8),
+                1 if m.get("store_hessian", True) else 0, m.get("band_distance", 0.0))
+            descs[i] = N.MeshDesc(_np_ptr(v), len(v), _np_ptr(t), len(t), p)
+        out = (ctypes.c_void_p * len(meshes))()
+        N.check(lib.sdfo_grid_build_sparse_batched(descs, len(meshes), _stream_ptr(stream), out))
+        return [cls(out[i], mode) for i in range(len(meshes))]
+
     def build_stats(self) -> dict:
         s = N.BuildStats()
         N.check(self._lib.sdfo_grid_build_stats(self.handle, ctypes.byref(s)))
@@ -325,6 +348,46 @@ class SdfGrid:
         m = self.mode if mode is None else N.mode_id(mode)
         N.check(self._lib.sdfo_query_backward(
             self.handle, m, _t_ptr(pts), n,
+            _t_ptr(None if dgap is None else dgap.contiguous()),
+            _t_ptr(None if dgrad is None else dgrad.contiguous()),
+            _t_ptr(dpts), _t_ptr(dgrid), _stream_ptr(stream)))
+        return dpts
+
+    def query_linearize(self, points, mode=None, stream=None):
+        """Forward that also keeps the local linearisation for reverse mode:
+        dict gap (N,), grad (N,3), valid (N,) uint8 and hess6 (N,6) = the
+        interpolant's symmetric Hessian {xx, xy, xz, yy, yz, zz}."""
+        torch = _torch()
+        pts = points.contiguous().reshape(-1, 3)
+        if pts.dtype != torch.float32:
+            raise ValueError("query_linearize takes float32 points")
+        n = pts.shape[0]
+        dev = pts.device
+        out = dict(gap=torch.empty(n, dtype=torch.float32, device=dev),
+                   grad=torch.empty((n, 3), dtype=torch.float32, device=dev),
+                   valid=torch.empty(n, dtype=torch.uint8, device=dev),
+                   hess6=torch.empty((n, 6), dtype=torch.float32, device=dev))
+        m = self.mode if mode is None else N.mode_id(mode)
+        N.check(self._lib.sdfo_query_linearize(
+            self.handle, m, _t_ptr(pts), n, _t_ptr(out["gap"]), _t_ptr(out["grad"]),
+            _t_ptr(out["valid"]), _t_ptr(out["hess6"]), _stream_ptr(stream)))
+        return out
+
+    def query_backward_saved(self, points, saved, dgap=None, dgrad=None, mode=None, dgrid=None,
+                             want_points=True, stream=None):
+        """Backward from ``saved`` = query_linearize(points) (or a dict with at
+        least ``valid`` when only ``dgrid`` is wanted): returns dL/dpoints
+        (N,3) or None, and accumulates dL/dpayload into ``dgrid``."""
+        torch = _torch()
+        pts = points.contiguous().reshape(-1, 3)
+        if pts.dtype != torch.float32:
+            raise ValueError("backward takes float32 points")
+        n = pts.shape[0]
+        dpts = torch.empty((n, 3), dtype=torch.float32, device=pts.device) if want_points else None
+        m = self.mode if mode is None else N.mode_id(mode)
+        N.check(self._lib.sdfo_query_backward_saved(
+            self.handle, m, _t_ptr(pts), n, _t_ptr(saved.get("grad")),
+            _t_ptr(saved.get("hess6")), _t_ptr(saved.get("valid")),
             _t_ptr(None if dgap is None else dgap.contiguous()),
             _t_ptr(None if dgrad is None else dgrad.contiguous()),
             _t_ptr(dpts), _t_ptr(dgrid), _stream_ptr(stream)))

@@ -110,6 +110,28 @@ def c5_icosphere(subdivisions=8, seed=4):
                             band_voxels=3, halo_voxels=2))
 
 
+def c5_points(verts, tris, voxel, n=16_000_000, seed=4, chunk=2_000_000):
+    """C5 queries: surface points (triangle by area, uniform barycentric)
+    offset along the face normal by U(-4h, 4h), drawn in chunks of ``chunk``
+    from one generator; float32 (n, 3)."""
+    rng = np.random.default_rng(seed)
+    nrm, area = M.face_normals(verts, tris)
+    cdf = np.cumsum(area)
+    cdf /= cdf[-1]
+    out = np.empty((n, 3), np.float32)
+    for a in range(0, n, chunk):
+        m = min(n, a + chunk) - a
+        idx = np.minimum(np.searchsorted(cdf, rng.random(m), side="right"), len(tris) - 1)
+        s = np.sqrt(rng.random(m))
+        r2 = rng.random(m)
+        t = tris[idx]
+        x = ((1.0 - s)[:, None] * verts[t[:, 0]] + (s * (1.0 - r2))[:, None] * verts[t[:, 1]] +
+             (s * r2)[:, None] * verts[t[:, 2]])
+        off = rng.uniform(-4.0 * voxel, 4.0 * voxel, m)
+        out[a:a + m] = x + off[:, None] * nrm[idx]
+    return out
+
+
 def near_surface_points(verts, tris, voxel, n, seed, band_voxels=4.0):
     """Surface points offset along the normal by U(-band*h, band*h)."""
     rng = np.random.default_rng(seed)

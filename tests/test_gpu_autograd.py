@@ -65,13 +65,14 @@ def test_point_gradient_vs_oracle(cuda, port, layout, mode):
     assert np.all(dp[~v] == 0)
 
 
+@pytest.mark.parametrize("layout", ["dense", "sparse"])
 @pytest.mark.parametrize("mode", [2, 3])
-def test_payload_gradient_vs_central_differences(cuda, port, mode):
+def test_payload_gradient_vs_central_differences(cuda, port, layout, mode):
     import torch
 
     from sdfo.autograd import sdf_query
 
-    grid, _, g = _grid_and_ref(port, "dense")
+    grid, _, g = _grid_and_ref(port, layout)
     pts = g["pts"][:600].astype(np.float32)
     x = torch.tensor(pts, device="cuda")
     payload = grid.payload().clone().requires_grad_(True)
@@ -101,3 +102,43 @@ def _loss(grid, x, payload, mode):
 
     gap, grad = sdf_query(grid, x, payload=payload.contiguous(), mode=mode)
     return float((gap.double().sum() + 0.5 * grad[:, 0].double().sum() - 0.25 * grad[:, 2].double().sum()).item())
+
+
+@pytest.mark.parametrize("storage", ["dense", "sparse", "sparse_fp16"])
+@pytest.mark.parametrize("mode", [2, 3])
+def test_saved_and_regathered_backward_agree(cuda, port, storage, mode):
+    """sdfo_query_backward_saved (elementwise from the forward's saved grad
+    and Hessian, weights-only grid scatter) against sdfo_query_backward (the
+    stencil gathered again): the same interpolant, so agreement to rounding."""
+    import torch
+
+    grid, _, g = _grid_and_ref(port, "dense" if storage == "dense" else "sparse")
+    if storage == "sparse_fp16":
+        grid = grid.to_fp16()
+    pts = torch.tensor(g["pts"].astype(np.float32), device="cuda")
+    n = pts.shape[0]
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    dgap = torch.randn(n, device="cuda", generator=gen)
+    dgrad = torch.randn((n, 3), device="cuda", generator=gen)
+    saved = grid.query_linearize(pts, mode=mode)
+    plain = grid.query_tensors(pts, mode=mode, valid=True)
+    assert torch.equal(saved["valid"], plain["valid"])
+    h = float(g["voxel"][0])
+    assert float((saved["gap"] - plain["gap"]).abs().max()) <= 1e-6 * h
+    assert float((saved["grad"] - plain["grad"]).abs().max()) <= 1e-6
+    G1 = torch.zeros((grid.stored_voxels, 4), device="cuda")
+    G2 = torch.zeros_like(G1)
+    d1 = grid.query_backward_saved(pts, saved, dgap, dgrad, mode=mode, dgrid=G1)
+    d2 = grid.query_backward(pts, dgap, dgrad, mode=mode, dgrid=G2)
+    scale = float(d2.abs().max())
+    assert float((d1 - d2).abs().max()) <= 1e-6 * scale
+    assert float((G1 - G2).abs().max()) <= 1e-5 * max(float(G2.abs().max()), 1.0)
+    v = saved["valid"].bool()
+    assert torch.all(d1[~v] == 0)
+    # each output alone
+    d3 = grid.query_backward_saved(pts, saved, dgap, None, mode=mode)
+    assert torch.allclose(d3, dgap[:, None] * saved["grad"], rtol=0, atol=1e-6 * scale)
+    G3 = torch.zeros_like(G1)
+    assert grid.query_backward_saved(pts, {"valid": saved["valid"]}, dgap, dgrad, mode=mode,
+                                     dgrid=G3, want_points=False) is None
+    assert float((G3 - G1).abs().max()) <= 1e-5 * max(float(G1.abs().max()), 1.0)
