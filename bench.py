@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--kernels-once", choices=["c2", "c5"], default=None,
+                    help="one launch of each query kernel on the workload (for ncu), then exit")
     ap.add_argument("--skip-c4", action="store_true",
                     help="leave out the 256-gear batched build / query section")
     ap.add_argument("--skip-c5", action="store_true",
@@ -742,6 +744,61 @@ def run_ours(args, rank, world, local_rank):
     del sdfo
 
 
+def kernels_once(which):
+    """Setup of a workload, then ONE launch of each query kernel (forward,
+    FP16 forward where sparse, linearising forward, saved backward, the
+    regathering backward) with a 64 MB buffer written before each -- the
+    program an ncu capture (-k regex:"k_query|k_backward") runs."""
+    import ctypes
+
+    import torch
+
+    from sdfo import SdfGrid
+    from sdfo import _native as N
+    from sdfo import workloads as W
+
+    lib = N.load()
+    if which == "c2":
+        c = W.c2_cylinder()
+        grids = [SdfGrid.build_dense(c["verts"], c["tris"], mode=TRICUBIC, **c["dense"])]
+        pts = torch.tensor(points_for(c, float(grids[0].voxel[0])), device="cuda")
+    else:
+        c = W.c5_icosphere()
+        g = SdfGrid.build_sparse(c["verts"], c["tris"], mode=TRICUBIC, **c["sparse"])
+        grids = [g, g.to_fp16()]
+        pts = torch.tensor(W.c5_points(c["verts"], c["tris"], float(g.voxel[0]), n=4_000_000),
+                           device="cuda")
+    n = pts.shape[0]
+
+    def P(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    f32 = dict(device="cuda", dtype=torch.float32)
+    gap, grad, h6 = torch.empty(n, **f32), torch.empty((n, 3), **f32), torch.empty((n, 6), **f32)
+    valid = torch.empty(n, dtype=torch.uint8, device="cuda")
+    dgap, dgrad, dp = torch.randn(n, **f32), torch.randn((n, 3), **f32), torch.empty((n, 3), **f32)
+    dgrid = torch.zeros((grids[0].stored_voxels, 4), **f32)
+    buf = torch.empty(16 << 20, **f32)
+    g = grids[0]
+    for gg in grids:
+        buf.zero_()
+        N.check(lib.sdfo_query(gg.handle, TRICUBIC, P(pts), 0, n, P(gap), P(grad), None, None,
+                               P(valid), None, s))
+    buf.zero_()
+    N.check(lib.sdfo_query_linearize(g.handle, TRICUBIC, P(pts), n, P(gap), P(grad), P(valid),
+                                     P(h6), s))
+    buf.zero_()
+    N.check(lib.sdfo_query_backward_saved(g.handle, TRICUBIC, P(pts), n, P(grad), P(h6), P(valid),
+                                          P(dgap), P(dgrad), P(dp),
+                                          P(dgrid) if which == "c5" else None, s))
+    buf.zero_()
+    N.check(lib.sdfo_query_backward(g.handle, TRICUBIC, P(pts), n, P(dgap), P(dgrad), P(dp), None,
+                                    s))
+    torch.cuda.synchronize()
+    print(json.dumps({"kernels_once": which, "queries": n}))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -749,6 +806,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.kernels_once:
+        kernels_once(args.kernels_once)
         return
     import torch
 

@@ -59,13 +59,14 @@ __device__ __forceinline__ bool sample(const GridView& g, const double Y[3], flo
     const Cell c = cell_of(g, Y);
     if (!c.ok) return false;
     const float h[3] = {(float)g.voxel[0], (float)g.voxel[1], (float)g.voxel[2]};
+    const float ih[3] = {g.ih[0], g.ih[1], g.ih[2]};
     Interp r;
     if (!SPARSE && MODE == SDFO_TRILINEAR && g.cell8 != nullptr)
     {
         float4 a, b;
         ld256(g.cell8 + 2 * dense_index(g, c.i0, c.j0, c.k0), a, b);
         const float phi[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-        r = trilinear<JAC>(phi, c.u, c.v, c.w, h);
+        r = trilinear<JAC>(phi, c.u, c.v, c.w, ih);
     }
     else
     {
@@ -86,14 +87,14 @@ __device__ __forceinline__ bool sample(const GridView& g, const double Y[3], flo
         }
         if (MODE == SDFO_TRICUBIC)
         {
-            r = tricubic<JAC>(cs, c.u, c.v, c.w, h);
+            r = tricubic<JAC>(cs, c.u, c.v, c.w, h, ih);
         }
         else
         {
             float phi[8];
 #pragma unroll
             for (int q = 0; q < 8; ++q) phi[q] = cs[q].x;
-            r = trilinear<JAC>(phi, c.u, c.v, c.w, h);
+            r = trilinear<JAC>(phi, c.u, c.v, c.w, ih);
         }
     }
     gap = r.gap;
@@ -119,8 +120,129 @@ struct PointState
     bool damp, fric;
 };
 
+// Pose-level quantities shared by all points of a CTA.
+struct PoseFrame
+{
+    v3 rA, rB, vA, wA, vB, wB, tl;
+};
+
+// The SDFContactEngine.evaluate force law of quadrature point i
+// (contacts_sdf.py:256-385); returns whether the point is active (valid and
+// k max(-g,0)^n > 1e-30).  HESS also records the interpolant's Hessian for
+// the Jacobian.
+template <int MODE, bool SPARSE, int BD, bool HESS>
+__device__ __forceinline__ bool point_state(const GridView& g, const float* __restrict__ qx,
+                                            const float* __restrict__ qw, int i,
+                                            const sdfo_body_state& sA, const sdfo_body_state& sB,
+                                            const PoseFrame& f, const sdfo_contact_params& prm,
+                                            PointState& st)
+{
+    const v3 X = V(__ldg(qx + 3 * i), __ldg(qx + 3 * i + 1), __ldg(qx + 3 * i + 2));
+    st.off = mul(sA.R, X);                   // x_w - r_A
+    const v3 Yv = mulT(sB.R, st.off) + f.tl; // body-B local point
+    const double Y[3] = {Yv.x, Yv.y, Yv.z};
+    float gapf;
+    if (!sample<MODE, SPARSE, BD, HESS>(g, Y, gapf, st.gl, st.Hl)) return false;
+    const double gap = gapf;
+    const double delta = gap < 0.0 ? -gap : 0.0;
+    const double dpow = prm.order == 2.0 ? delta * delta : prm.order == 1.0 ? delta : pow(delta, prm.order);
+    st.p = prm.stiffness * dpow;
+    if (!(st.p > 1e-30)) return false;
+    st.wq = (double)__ldg(qw + i);
+    const v3 xw = f.rA + st.off;
+    st.rg = mul(sB.R, st.gl);
+    st.gn = sqrt(dot(st.gl, st.gl));
+    st.fq = st.p * st.rg;
+    const v3 uA = f.vA + cross(f.wA, st.off);
+    const v3 uB = f.vB + cross(f.wB, xw - f.rB);
+    st.u = uA - uB;
+    st.damp = prm.damping > 0.0 && gap < 0.0;
+    st.vn = dot(st.u, st.rg);
+    if (st.damp) st.fq = st.fq + (prm.damping * (-st.vn)) * st.rg;
+    const double gsafe = st.gn > 1e-30 ? st.gn : 1e-30;
+    st.un = (1.0 / gsafe) * st.rg;
+    st.udn = dot(st.u, st.un);
+    st.ut = st.u - st.udn * st.un;
+    st.den = sqrt(dot(st.ut, st.ut) + prm.regularizer * prm.regularizer);
+    st.phat = st.p * st.gn;
+    st.fric = prm.friction * st.phat > 0.0;
+    if (st.fric) st.fq = st.fq + (-prm.friction * st.phat / st.den) * st.ut;
+    st.dgdd = -prm.stiffness * (prm.order == 2.0 ? 2.0 * delta
+                                : prm.order == 1.0 ? 1.0
+                                                   : prm.order * pow(delta, prm.order - 1.0));
+    return true;
+}
+
+// Column j of the point's d(f, x f)/d(dx, dtheta), weighted by w.
+__device__ __forceinline__ void jacobian_column(const PointState& st, const sdfo_body_state& sB,
+                                                const PoseFrame& f, const sdfo_contact_params& prm,
+                                                int j, double col[6])
+{
+    const double Hm[9] = {st.Hl[0], st.Hl[1], st.Hl[2], st.Hl[1], st.Hl[3],
+                          st.Hl[4], st.Hl[2], st.Hl[4], st.Hl[5]};
+    v3 dxw, doff;
+    if (j < 3)
+    {
+        dxw = V(j == 0, j == 1, j == 2);
+        doff = V(0.0, 0.0, 0.0);
+    }
+    else
+    {
+        doff = cross(V(j == 3, j == 4, j == 5), st.off);
+        dxw = doff;
+    }
+    const v3 dYl = mulT(sB.R, dxw);
+    const v3 dgl = V(Hm[0] * dYl.x + Hm[1] * dYl.y + Hm[2] * dYl.z,
+                     Hm[3] * dYl.x + Hm[4] * dYl.y + Hm[5] * dYl.z,
+                     Hm[6] * dYl.x + Hm[7] * dYl.y + Hm[8] * dYl.z);
+    const double dg = dot(st.gl, dYl);
+    const v3 drg = mul(sB.R, dgl);
+    const double dp = st.dgdd * dg; // p = k delta^n, delta = -g
+    v3 dfq = dp * st.rg + st.p * drg;
+    const v3 du = cross(f.wA, doff) - cross(f.wB, dxw);
+    if (st.damp)
+    {
+        const double dvn = dot(du, st.rg) + dot(st.u, drg);
+        dfq = dfq + (-prm.damping) * (dvn * st.rg + st.vn * drg);
+    }
+    if (st.fric)
+    {
+        const double gsafe = st.gn > 1e-30 ? st.gn : 1e-30;
+        const double dgn = st.gn > 1e-30 ? dot(st.gl, dgl) / st.gn : 0.0;
+        const double dphat = dp * st.gn + st.p * dgn;
+        const v3 dun = (1.0 / gsafe) * (st.gn > 1e-30 ? drg - dot(st.un, drg) * st.un : drg);
+        const double dudn = dot(du, st.un) + dot(st.u, dun);
+        const v3 dut = du - dudn * st.un - st.udn * dun;
+        const double dden = dot(st.ut, dut) / st.den;
+        dfq = dfq + (-prm.friction) * ((dphat / st.den) * st.ut + (st.phat / st.den) * dut -
+                                       (st.phat * dden / (st.den * st.den)) * st.ut);
+    }
+    const v3 dtq = cross(doff, st.fq) + cross(st.off, dfq);
+    col[0] = st.wq * dfq.x;
+    col[1] = st.wq * dfq.y;
+    col[2] = st.wq * dfq.z;
+    col[3] = st.wq * dtq.x;
+    col[4] = st.wq * dtq.y;
+    col[5] = st.wq * dtq.z;
+}
+
+// One CTA per pose.  Per chunk of 256 quadrature points: every thread
+// evaluates its point (no Hessian) and accumulates F, tau; with JAC the
+// chunk's active points (typically a small fraction) are then compacted in
+// point order into the first threads, which re-evaluate them with the
+// interpolant's Hessian and form the six Jacobian columns -- so only
+// ceil(active / 32) warps run the FP64 derivative code, with full lanes.
+// Resident CTAs per SM asked of the register allocator (256 threads each).
+#ifndef SDFO_CONTACT_MIN_BLOCKS
+#define SDFO_CONTACT_MIN_BLOCKS 3
+#endif
+#ifndef SDFO_CONTACT_JAC_MIN_BLOCKS
+#define SDFO_CONTACT_JAC_MIN_BLOCKS 2
+#endif
+
 template <int MODE, bool SPARSE, int BD, bool JAC>
-__global__ void __launch_bounds__(kContactThreads)
+__global__ void __launch_bounds__(kContactThreads,
+                                  JAC ? SDFO_CONTACT_JAC_MIN_BLOCKS : SDFO_CONTACT_MIN_BLOCKS)
     k_contact(GridView g, const float* __restrict__ qx, const float* __restrict__ qw, int nq,
               const sdfo_body_state* __restrict__ poses, const sdfo_body_state* __restrict__ body_b,
               sdfo_contact_params prm, double* __restrict__ ft, double* __restrict__ jac)
@@ -130,6 +252,8 @@ __global__ void __launch_bounds__(kContactThreads)
     __shared__ sdfo_body_state sA, sB;
     __shared__ double red[kWarps][6];
     __shared__ double sjac[JAC ? kWarps : 1][JAC ? 36 : 1];
+    __shared__ int s_list[JAC ? kContactThreads : 1];
+    __shared__ int s_wcnt[kWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0)
     {
@@ -139,132 +263,71 @@ __global__ void __launch_bounds__(kContactThreads)
     if (JAC)
         for (int t = lane; t < 36; t += 32) sjac[warp][t] = 0.0;
     __syncthreads();
-    const v3 rA = V(sA.r[0], sA.r[1], sA.r[2]), rB = V(sB.r[0], sB.r[1], sB.r[2]);
-    const v3 vA = V(sA.v[0], sA.v[1], sA.v[2]), wA = V(sA.w[0], sA.w[1], sA.w[2]);
-    const v3 vB = V(sB.v[0], sB.v[1], sB.v[2]), wB = V(sB.w[0], sB.w[1], sB.w[2]);
-    const v3 tl = mulT(sB.R, rA - rB); // R_B^T (r_A - r_B)
+    PoseFrame f;
+    f.rA = V(sA.r[0], sA.r[1], sA.r[2]);
+    f.rB = V(sB.r[0], sB.r[1], sB.r[2]);
+    f.vA = V(sA.v[0], sA.v[1], sA.v[2]);
+    f.wA = V(sA.w[0], sA.w[1], sA.w[2]);
+    f.vB = V(sB.v[0], sB.v[1], sB.v[2]);
+    f.wB = V(sB.w[0], sB.w[1], sB.w[2]);
+    f.tl = mulT(sB.R, f.rA - f.rB); // R_B^T (r_A - r_B)
     double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 
-    // block-uniform trip count so whole warps stay converged for the
-    // warp-level Jacobian reduction below
+    // block-uniform trip count: the barriers and warp reductions below see
+    // every thread
     for (int i0 = 0; i0 < nq; i0 += kContactThreads)
     {
         const int i = i0 + threadIdx.x;
-        PointState st;
         bool act = false;
         if (i < nq)
         {
-            const v3 X = V(__ldg(qx + 3 * i), __ldg(qx + 3 * i + 1), __ldg(qx + 3 * i + 2));
-            st.off = mul(sA.R, X);               // x_w - r_A
-            const v3 Yv = mulT(sB.R, st.off) + tl; // body-B local point
-            const double Y[3] = {Yv.x, Yv.y, Yv.z};
-            float gapf;
-            if (sample<MODE, SPARSE, BD, JAC>(g, Y, gapf, st.gl, st.Hl))
-            {
-                const double gap = gapf;
-                const double delta = gap < 0.0 ? -gap : 0.0;
-                const double dpow = prm.order == 2.0 ? delta * delta
-                                  : prm.order == 1.0 ? delta
-                                                     : pow(delta, prm.order);
-                st.p = prm.stiffness * dpow;
-                act = st.p > 1e-30;
-                if (act)
-                {
-                    st.wq = (double)__ldg(qw + i);
-                    const v3 xw = rA + st.off;
-                    st.rg = mul(sB.R, st.gl);
-                    st.gn = sqrt(dot(st.gl, st.gl));
-                    st.fq = st.p * st.rg;
-                    const v3 uA = vA + cross(wA, st.off);
-                    const v3 uB = vB + cross(wB, xw - rB);
-                    st.u = uA - uB;
-                    st.damp = prm.damping > 0.0 && gap < 0.0;
-                    st.vn = dot(st.u, st.rg);
-                    if (st.damp) st.fq = st.fq + (prm.damping * (-st.vn)) * st.rg;
-                    const double gsafe = st.gn > 1e-30 ? st.gn : 1e-30;
-                    st.un = (1.0 / gsafe) * st.rg;
-                    st.udn = dot(st.u, st.un);
-                    st.ut = st.u - st.udn * st.un;
-                    st.den = sqrt(dot(st.ut, st.ut) + prm.regularizer * prm.regularizer);
-                    st.phat = st.p * st.gn;
-                    st.fric = prm.friction * st.phat > 0.0;
-                    if (st.fric) st.fq = st.fq + (-prm.friction * st.phat / st.den) * st.ut;
-                    const v3 tq = cross(st.off, st.fq);
-                    acc[0] += st.wq * st.fq.x;
-                    acc[1] += st.wq * st.fq.y;
-                    acc[2] += st.wq * st.fq.z;
-                    acc[3] += st.wq * tq.x;
-                    acc[4] += st.wq * tq.y;
-                    acc[5] += st.wq * tq.z;
-                    st.dgdd = -prm.stiffness * (prm.order == 2.0 ? 2.0 * delta
-                                                : prm.order == 1.0 ? 1.0
-                                                                   : prm.order * pow(delta, prm.order - 1.0));
-                }
-            }
-        }
-        if (!JAC || !__any_sync(0xffffffffu, act)) continue;
-        // Forward-mode derivatives of this point's force / torque w.r.t. the 6
-        // pose parameters, one column at a time, summed over the warp.
-        const double Hm[9] = {st.Hl[0], st.Hl[1], st.Hl[2], st.Hl[1], st.Hl[3],
-                              st.Hl[4], st.Hl[2], st.Hl[4], st.Hl[5]};
-#pragma unroll 1
-        for (int j = 0; j < 6; ++j)
-        {
-            double col[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            PointState st;
+            act = point_state<MODE, SPARSE, BD, false>(g, qx, qw, i, sA, sB, f, prm, st);
             if (act)
             {
-                v3 dxw, doff;
-                if (j < 3)
-                {
-                    dxw = V(j == 0, j == 1, j == 2);
-                    doff = V(0.0, 0.0, 0.0);
-                }
-                else
-                {
-                    doff = cross(V(j == 3, j == 4, j == 5), st.off);
-                    dxw = doff;
-                }
-                const v3 dYl = mulT(sB.R, dxw);
-                const v3 dgl = V(Hm[0] * dYl.x + Hm[1] * dYl.y + Hm[2] * dYl.z,
-                                 Hm[3] * dYl.x + Hm[4] * dYl.y + Hm[5] * dYl.z,
-                                 Hm[6] * dYl.x + Hm[7] * dYl.y + Hm[8] * dYl.z);
-                const double dg = dot(st.gl, dYl);
-                const v3 drg = mul(sB.R, dgl);
-                const double dp = st.dgdd * dg; // p = k delta^n, delta = -g
-                v3 dfq = dp * st.rg + st.p * drg;
-                const v3 du = cross(wA, doff) - cross(wB, dxw);
-                if (st.damp)
-                {
-                    const double dvn = dot(du, st.rg) + dot(st.u, drg);
-                    dfq = dfq + (-prm.damping) * (dvn * st.rg + st.vn * drg);
-                }
-                if (st.fric)
-                {
-                    const double gsafe = st.gn > 1e-30 ? st.gn : 1e-30;
-                    const double dgn = st.gn > 1e-30 ? dot(st.gl, dgl) / st.gn : 0.0;
-                    const double dphat = dp * st.gn + st.p * dgn;
-                    const v3 dun = (1.0 / gsafe) * (st.gn > 1e-30 ? drg - dot(st.un, drg) * st.un : drg);
-                    const double dudn = dot(du, st.un) + dot(st.u, dun);
-                    const v3 dut = du - dudn * st.un - st.udn * dun;
-                    const double dden = dot(st.ut, dut) / st.den;
-                    dfq = dfq + (-prm.friction) * ((dphat / st.den) * st.ut + (st.phat / st.den) * dut -
-                                                   (st.phat * dden / (st.den * st.den)) * st.ut);
-                }
-                const v3 dtq = cross(doff, st.fq) + cross(st.off, dfq);
-                col[0] = st.wq * dfq.x;
-                col[1] = st.wq * dfq.y;
-                col[2] = st.wq * dfq.z;
-                col[3] = st.wq * dtq.x;
-                col[4] = st.wq * dtq.y;
-                col[5] = st.wq * dtq.z;
-            }
-#pragma unroll
-            for (int r = 0; r < 6; ++r)
-            {
-                const double sum = warp_sum(col[r]);
-                if (lane == 0) sjac[warp][6 * r + j] += sum;
+                const v3 tq = cross(st.off, st.fq);
+                acc[0] += st.wq * st.fq.x;
+                acc[1] += st.wq * st.fq.y;
+                acc[2] += st.wq * st.fq.z;
+                acc[3] += st.wq * tq.x;
+                acc[4] += st.wq * tq.y;
+                acc[5] += st.wq * tq.z;
             }
         }
+        if (!JAC) continue;
+        const unsigned m = __ballot_sync(0xffffffffu, act);
+        if (lane == 0) s_wcnt[warp] = __popc(m);
+        __syncthreads();
+        int off = 0, total = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w)
+        {
+            const int c = s_wcnt[w];
+            off += w < warp ? c : 0;
+            total += c;
+        }
+        if (act) s_list[off + __popc(m & ((1u << lane) - 1u))] = i;
+        __syncthreads();
+        if (warp * 32 < total)
+        {
+            PointState st;
+            const bool mine = threadIdx.x < total &&
+                              point_state<MODE, SPARSE, BD, true>(g, qx, qw, s_list[threadIdx.x], sA,
+                                                                  sB, f, prm, st);
+#pragma unroll 1
+            for (int j = 0; j < 6; ++j)
+            {
+                double col[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                if (mine) jacobian_column(st, sB, f, prm, j, col);
+#pragma unroll
+                for (int r = 0; r < 6; ++r)
+                {
+                    const double sum = warp_sum(col[r]);
+                    if (lane == 0) sjac[warp][6 * r + j] += sum;
+                }
+            }
+        }
+        __syncthreads(); // s_list and s_wcnt are rewritten by the next chunk
     }
 #pragma unroll
     for (int q = 0; q < 6; ++q)

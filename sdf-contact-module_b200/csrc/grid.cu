@@ -53,6 +53,8 @@ GridView make_view(const sdfo_grid* g)
     {
         v.bmin[a] = g->info.bmin[a];
         v.voxel[a] = g->info.voxel[a];
+        v.ivoxel[a] = 1.0 / g->info.voxel[a];
+        v.ih[a] = (float)(1.0 / g->info.voxel[a]);
     }
     v.nx = g->info.shape[0];
     v.ny = g->info.shape[1];

@@ -22,11 +22,23 @@ struct Cell
     bool ok;         // inside the index domain
 };
 
-// Fractional grid coordinate as in GridSpec/trilinearQuery:
-// f = (p - bmin).cwiseQuotient(voxel) - 0.5.
-__device__ __forceinline__ double frac_coord(double p, double bmin, double voxel)
+// Fractional grid coordinate as in GridSpec/trilinearQuery,
+// f = (p - bmin).cwiseQuotient(voxel) - 0.5, without the FP64 division where that cannot change
+// the cell where it cannot change the result: (p - bmin) * (1/voxel) is within 2^-39 of the quotient for
+// |f| < 2^12, so when it lies more than 2^-30 from the decision points
+// (integers for the cell index, half-integers for the nearest voxel) both
+// select the same cell, and the fraction differs by < 2^-39 (below FP32
+// resolution); near a decision point the reference's division is used.
+template <bool NEAREST>
+__device__ __forceinline__ double frac_coord_fast(double p, double bmin, double voxel,
+                                                  double ivoxel)
 {
-    return (p - bmin) / voxel - 0.5;
+    const double d = p - bmin;
+    const double f = d * ivoxel - 0.5;
+    const double t = NEAREST ? f + 0.5 : f;
+    const double fr = t - floor(t);
+    if (fr > 0x1p-30 && fr < 1.0 - 0x1p-30 && fabs(f) < 4096.0) return f;
+    return d / voxel - 0.5;
 }
 
 // Lower-corner cell of p; ok iff i0 >= 0 and i0 + 1 < n on every axis.
@@ -41,7 +53,7 @@ __device__ __forceinline__ Cell cell_of(const GridView& g, const double p[3])
 #pragma unroll
     for (int a = 0; a < 3; ++a)
     {
-        f[a] = frac_coord(p[a], g.bmin[a], g.voxel[a]);
+        f[a] = frac_coord_fast<false>(p[a], g.bmin[a], g.voxel[a], g.ivoxel[a]);
         // NaN / huge coordinates are outside the domain.
         if (!(f[a] >= -1.0 && f[a] < (double)n[a]))
         {
@@ -75,7 +87,7 @@ __device__ __forceinline__ bool nearest_voxel(const GridView& g, const double p[
 #pragma unroll
     for (int a = 0; a < 3; ++a)
     {
-        const double f = frac_coord(p[a], g.bmin[a], g.voxel[a]);
+        const double f = frac_coord_fast<true>(p[a], g.bmin[a], g.voxel[a], g.ivoxel[a]);
         if (!(f > -1.0 && f < (double)n[a] + 1.0))
         {
             ok = false;
@@ -160,12 +172,29 @@ __device__ __forceinline__ bool gather_corners(const GridView& g, const Cell& c,
         }
         return true;
     }
+    const int bd = BD > 0 ? BD : g.bd;
+    const int bi = c.i0 / bd, bj = c.j0 / bd, bk = c.k0 / bd;
+    const int li = c.i0 - bi * bd, lj = c.j0 - bj * bd, lk = c.k0 - bk * bd;
     bool ok = true;
-#pragma unroll
-    for (int q = 0; q < 8; ++q)
+    if (li < bd - 1 && lj < bd - 1 && lk < bd - 1)
     {
-        idx[q] = sparse_index<BD>(g, c.i0 + (q & 1), c.j0 + ((q >> 1) & 1), c.k0 + (q >> 2));
-        ok = ok && idx[q] >= 0;
+        // the whole cell lies in one brick (343 of 512 cells for 8^3):
+        // one table lookup
+        const int slot = __ldg(g.table + bi + g.nbx * (bj + g.nby * bk));
+        if (slot < 0) return false;
+        const int64_t i0 = (int64_t)slot * (bd * bd * bd) + li + bd * (lj + bd * lk);
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            idx[q] = i0 + ((q & 1) ? 1 : 0) + ((q & 2) ? bd : 0) + ((q & 4) ? bd * bd : 0);
+    }
+    else
+    {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+        {
+            idx[q] = sparse_index<BD>(g, c.i0 + (q & 1), c.j0 + ((q >> 1) & 1), c.k0 + (q >> 2));
+            ok = ok && idx[q] >= 0;
+        }
     }
     if (!ok) return false;
 #pragma unroll
@@ -248,7 +277,7 @@ struct Interp
 // derivative sums then carry errors of order ulp(h), not ulp(|phi|).
 template <bool HESS>
 __device__ __forceinline__ Interp tricubic(const float4 c[8], float u, float v, float w,
-                                           const float h[3])
+                                           const float h[3], const float ih[3])
 {
     float phi[8], gx[8], gy[8], gz[8];
     const float phi0 = c[0].x;
@@ -268,9 +297,9 @@ __device__ __forceinline__ Interp tricubic(const float4 c[8], float u, float v, 
     const XColl xd = collapse_x(dx, phi, gx, gy, gz);
     Interp r;
     r.gap = collapse_yz(xa, by, bz) + phi0;
-    r.g[0] = collapse_yz(xd, by, bz) / h[0];
-    r.g[1] = collapse_yz(xa, dy, bz) / h[1];
-    r.g[2] = collapse_yz(xa, by, dz) / h[2];
+    r.g[0] = collapse_yz(xd, by, bz) * ih[0];
+    r.g[1] = collapse_yz(xa, dy, bz) * ih[1];
+    r.g[2] = collapse_yz(xa, by, dz) * ih[2];
     if (HESS)
     {
         float sx[4], sy[4], sz[4];
@@ -278,12 +307,12 @@ __device__ __forceinline__ Interp tricubic(const float4 c[8], float u, float v, 
         hermite2(v, sy);
         hermite2(w, sz);
         const XColl xs = collapse_x(sx, phi, gx, gy, gz);
-        r.H[0] = collapse_yz(xs, by, bz) / (h[0] * h[0]);
-        r.H[1] = collapse_yz(xd, dy, bz) / (h[0] * h[1]);
-        r.H[2] = collapse_yz(xd, by, dz) / (h[0] * h[2]);
-        r.H[3] = collapse_yz(xa, sy, bz) / (h[1] * h[1]);
-        r.H[4] = collapse_yz(xa, dy, dz) / (h[1] * h[2]);
-        r.H[5] = collapse_yz(xa, by, sz) / (h[2] * h[2]);
+        r.H[0] = collapse_yz(xs, by, bz) * (ih[0] * ih[0]);
+        r.H[1] = collapse_yz(xd, dy, bz) * (ih[0] * ih[1]);
+        r.H[2] = collapse_yz(xd, by, dz) * (ih[0] * ih[2]);
+        r.H[3] = collapse_yz(xa, sy, bz) * (ih[1] * ih[1]);
+        r.H[4] = collapse_yz(xa, dy, dz) * (ih[1] * ih[2]);
+        r.H[5] = collapse_yz(xa, by, sz) * (ih[2] * ih[2]);
     }
     else
     {
@@ -299,7 +328,7 @@ __device__ __forceinline__ float lerpf(float a, float b, float t) { return fmaf(
 // derivatives (the diagonal ones are zero).
 template <bool HESS>
 __device__ __forceinline__ Interp trilinear(const float c[8], float u, float v, float w,
-                                            const float h[3])
+                                            const float ih[3])
 {
     Interp r;
     const float c00 = lerpf(c[0], c[1], u), c10 = lerpf(c[2], c[3], u);
@@ -309,15 +338,15 @@ __device__ __forceinline__ Interp trilinear(const float c[8], float u, float v, 
     const float dx00 = c[1] - c[0], dx10 = c[3] - c[2], dx01 = c[5] - c[4], dx11 = c[7] - c[6];
     const float dy00 = c[2] - c[0], dy10 = c[3] - c[1], dy01 = c[6] - c[4], dy11 = c[7] - c[5];
     const float dz00 = c[4] - c[0], dz10 = c[5] - c[1], dz01 = c[6] - c[2], dz11 = c[7] - c[3];
-    r.g[0] = lerpf(lerpf(dx00, dx10, v), lerpf(dx01, dx11, v), w) / h[0];
-    r.g[1] = lerpf(lerpf(dy00, dy10, u), lerpf(dy01, dy11, u), w) / h[1];
-    r.g[2] = lerpf(lerpf(dz00, dz10, u), lerpf(dz01, dz11, u), v) / h[2];
+    r.g[0] = lerpf(lerpf(dx00, dx10, v), lerpf(dx01, dx11, v), w) * ih[0];
+    r.g[1] = lerpf(lerpf(dy00, dy10, u), lerpf(dy01, dy11, u), w) * ih[1];
+    r.g[2] = lerpf(lerpf(dz00, dz10, u), lerpf(dz01, dz11, u), v) * ih[2];
     r.H[0] = r.H[3] = r.H[5] = 0.f;
     if (HESS)
     {
-        r.H[1] = lerpf(dx10 - dx00, dx11 - dx01, w) / (h[0] * h[1]);
-        r.H[2] = lerpf(dx01 - dx00, dx11 - dx10, v) / (h[0] * h[2]);
-        r.H[4] = lerpf(dy01 - dy00, dy11 - dy10, u) / (h[1] * h[2]);
+        r.H[1] = lerpf(dx10 - dx00, dx11 - dx01, w) * (ih[0] * ih[1]);
+        r.H[2] = lerpf(dx01 - dx00, dx11 - dx10, v) * (ih[0] * ih[2]);
+        r.H[4] = lerpf(dy01 - dy00, dy11 - dy10, u) * (ih[1] * ih[2]);
     }
     else
     {
@@ -348,11 +377,14 @@ __device__ __forceinline__ void unit_of(const float g[3], float u[3])
     }
 }
 
+// unit (the normalised gradient) is computed only when want_unit is set;
+// otherwise it is left unset for Trilinear / Tricubic.
 template <int MODE, bool SPARSE, int BD, bool HESS>
 __device__ __forceinline__ bool evaluate(const GridView& g, const double p[3], Interp& r,
-                                         float unit[3])
+                                         float unit[3], bool want_unit = true)
 {
     const float h[3] = {(float)g.voxel[0], (float)g.voxel[1], (float)g.voxel[2]};
+    const float ih[3] = {g.ih[0], g.ih[1], g.ih[2]};
     if (MODE == SDFO_TRILINEAR || MODE == SDFO_TRICUBIC)
     {
         const Cell c = cell_of(g, p);
@@ -363,8 +395,8 @@ __device__ __forceinline__ bool evaluate(const GridView& g, const double p[3], I
             float4 a, b;
             ld256(g.cell8 + 2 * dense_index(g, c.i0, c.j0, c.k0), a, b);
             const float phi[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-            r = trilinear<HESS>(phi, c.u, c.v, c.w, h);
-            unit_of(r.g, unit);
+            r = trilinear<HESS>(phi, c.u, c.v, c.w, ih);
+            if (want_unit) unit_of(r.g, unit);
             return true;
         }
         float4 cs[8];
@@ -387,16 +419,16 @@ __device__ __forceinline__ bool evaluate(const GridView& g, const double p[3], I
         }
         if (MODE == SDFO_TRICUBIC)
         {
-            r = tricubic<HESS>(cs, c.u, c.v, c.w, h);
+            r = tricubic<HESS>(cs, c.u, c.v, c.w, h, ih);
         }
         else
         {
             float phi[8];
 #pragma unroll
             for (int q = 0; q < 8; ++q) phi[q] = cs[q].x;
-            r = trilinear<HESS>(phi, c.u, c.v, c.w, h);
+            r = trilinear<HESS>(phi, c.u, c.v, c.w, ih);
         }
-        unit_of(r.g, unit);
+        if (want_unit) unit_of(r.g, unit);
         return true;
     }
     // FirstOrder / SecondOrder at the nearest voxel (SdfOracle.cpp:448-520,

@@ -100,7 +100,7 @@ __device__ __forceinline__ void scatter_grid_gradient(const GridView& g, const C
                                                       const float dg[3], float* dgrid)
 {
     const float h[3] = {(float)g.voxel[0], (float)g.voxel[1], (float)g.voxel[2]};
-    const float ig[3] = {dg[0] / h[0], dg[1] / h[1], dg[2] / h[2]};
+    const float ig[3] = {dg[0] * g.ih[0], dg[1] * g.ih[1], dg[2] * g.ih[2]};
     float4* out = reinterpret_cast<float4*>(dgrid);
     auto index = [&](int k) -> int64_t {
         const int i = c.i0 + (k & 1), j = c.j0 + ((k >> 1) & 1), kk = c.k0 + (k >> 2);
@@ -150,9 +150,20 @@ __device__ __forceinline__ void scatter_grid_gradient(const GridView& g, const C
     }
 }
 
+// Minimum resident CTAs per SM requested from the register allocator for
+// the plain query and for the query with the Hessian.
+#ifndef SDFO_QUERY_MIN_BLOCKS
+#define SDFO_QUERY_MIN_BLOCKS 5
+#endif
+#ifndef SDFO_QUERY_HESS_MIN_BLOCKS
+#define SDFO_QUERY_HESS_MIN_BLOCKS 4
+#endif
+template <bool HESS>
+constexpr int query_min_blocks() { return HESS ? SDFO_QUERY_HESS_MIN_BLOCKS : SDFO_QUERY_MIN_BLOCKS; }
+
 template <int MODE, bool SPARSE, int BD, typename PT, bool HESS, bool STAGED>
-__global__ void __launch_bounds__(kThreads) k_query(GridView g, const PT* __restrict__ pts,
-                                                  int64_t n, QueryOutputs o)
+__global__ void __launch_bounds__(kThreads, query_min_blocks<HESS>())
+    k_query(GridView g, const PT* __restrict__ pts, int64_t n, QueryOutputs o)
 {
     __shared__ __align__(16) float sbuf[STAGED ? (HESS ? 6 : 3) * kThreads : 1];
     const int64_t q0 = (int64_t)blockIdx.x * kThreads;
@@ -173,8 +184,9 @@ __global__ void __launch_bounds__(kThreads) k_query(GridView g, const PT* __rest
         load_point(pts, q, p);
     }
     Interp r;
-    float unit[3];
-    const bool valid = active && evaluate<MODE, SPARSE, BD, HESS>(g, p, r, unit);
+    float unit[3] = {1.f, 0.f, 0.f};
+    const bool want_unit = o.unit != nullptr || o.witness != nullptr;
+    const bool valid = active && evaluate<MODE, SPARSE, BD, HESS>(g, p, r, unit, want_unit);
     if (!valid)
     {
         r.gap = 0.f;
@@ -189,13 +201,16 @@ __global__ void __launch_bounds__(kThreads) k_query(GridView g, const PT* __rest
         __stcs(o.gap + q, r.gap);
         if (o.valid) o.valid[q] = valid ? 1 : 0;
     }
-    float w[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) w[a] = valid ? (float)(p[a] - (double)r.gap * unit[a]) : 0.f;
     // the output pointers are uniform over the block
     if (o.grad) write_rec<3, STAGED>(sbuf, o.grad, q0, cnt, active, r.g);
     if (o.unit) write_rec<3, STAGED>(sbuf, o.unit, q0, cnt, active, unit);
-    if (o.witness) write_rec<3, STAGED>(sbuf, o.witness, q0, cnt, active, w);
+    if (o.witness)
+    {
+        float w[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) w[a] = valid ? (float)(p[a] - (double)r.gap * unit[a]) : 0.f;
+        write_rec<3, STAGED>(sbuf, o.witness, q0, cnt, active, w);
+    }
     if (HESS && o.hess6) write_rec<6, STAGED>(sbuf, o.hess6, q0, cnt, active, r.H);
     if (HESS && o.hess && active)
     {
@@ -217,23 +232,54 @@ __global__ void __launch_bounds__(kThreads)
                      const float* __restrict__ dgrad, float* __restrict__ dpts,
                      float* __restrict__ dgrid)
 {
-    __shared__ __align__(16) float sbuf[STAGED ? 6 * kThreads : 1];
+    // staged inputs, all loaded before one barrier: dgrad | grad | hess6
+    __shared__ __align__(16) float sbuf[STAGED ? 12 * kThreads : 1];
     const int64_t q0 = (int64_t)blockIdx.x * kThreads;
     const int64_t q = q0 + threadIdx.x;
     const bool active = q < n;
     const int cnt = (int)(n - q0 < kThreads ? n - q0 : kThreads);
     const float dG = (dgap && active) ? __ldcs(dgap + q) : 0.f;
     float dg[3] = {0.f, 0.f, 0.f};
-    if (dgrad) read_rec<3, STAGED>(sbuf, dgrad, q0, cnt, active, dg);
     if (DPTS)
     {
-        float gr[3], H[6];
-        read_rec<3, STAGED>(sbuf, grad, q0, cnt, active, gr);
-        read_rec<6, STAGED>(sbuf, hess6, q0, cnt, active, H);
+        float gr[3] = {0.f, 0.f, 0.f}, H[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (STAGED)
+        {
+            if (dgrad) stage_in<3>(sbuf, dgrad + 3 * q0, cnt);
+            stage_in<3>(sbuf + 3 * kThreads, grad + 3 * q0, cnt);
+            stage_in<6>(sbuf + 6 * kThreads, hess6 + 6 * q0, cnt);
+            __syncthreads();
+            if (active)
+            {
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                {
+                    if (dgrad) dg[a] = sbuf[3 * threadIdx.x + a];
+                    gr[a] = sbuf[3 * kThreads + 3 * threadIdx.x + a];
+                }
+#pragma unroll
+                for (int a = 0; a < 6; ++a) H[a] = sbuf[6 * kThreads + 6 * threadIdx.x + a];
+            }
+        }
+        else if (active)
+        {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+            {
+                if (dgrad) dg[a] = __ldcs(dgrad + 3 * q + a);
+                gr[a] = __ldcs(grad + 3 * q + a);
+            }
+#pragma unroll
+            for (int a = 0; a < 6; ++a) H[a] = __ldcs(hess6 + 6 * q + a);
+        }
         const float out[3] = {dG * gr[0] + H[0] * dg[0] + H[1] * dg[1] + H[2] * dg[2],
                               dG * gr[1] + H[1] * dg[0] + H[3] * dg[1] + H[4] * dg[2],
                               dG * gr[2] + H[2] * dg[0] + H[4] * dg[1] + H[5] * dg[2]};
         write_rec<3, STAGED>(sbuf, dpts, q0, cnt, active, out);
+    }
+    else if (dgrad)
+    {
+        read_rec<3, STAGED>(sbuf, dgrad, q0, cnt, active, dg);
     }
     if (DGRID)
     {

@@ -172,6 +172,8 @@ struct GridView
 {
     double bmin[3];
     double voxel[3];
+    double ivoxel[3]; // 1 / voxel (FP64)
+    float ih[3];      // 1 / voxel (FP32)
     int nx, ny, nz;
     int layout;  // SDFO_LAYOUT_*
     int storage; // SDFO_STORAGE_*
