@@ -59,6 +59,17 @@ def lib():
         L.port_query_sparse.argtypes = [ctypes.POINTER(_Spec), _I, _I, _P, _P, _P, _P, _I, _P,
                                         _L, _P, _P, _P, _P, _P, _P]
         L.port_set_threads.argtypes = [_I]
+        L.port_ca_prepare.restype = _P
+        L.port_ca_prepare.argtypes = [_P, _I, _P, _I, _P, ctypes.POINTER(_Spec), _I, _I, _D]
+        L.port_ca_free.argtypes = [_P]
+        L.port_ca_dense.argtypes = [_P, _I, _D, _D, _P, _P, _P, _P, _P, _P, _P]
+        L.port_ca_sparse_activate.restype = _I
+        L.port_ca_sparse_activate.argtypes = [_P, _I, _D, _P]
+        L.port_ca_sparse_fill.argtypes = [_P, _I, _I, _P, _I, _D, _D, _P, _P, _P, _P, _P, _P]
+        L.port_ca_query_dense.argtypes = [ctypes.POINTER(_Spec), _I, _P, _P, _P, _P, _P, _L, _P,
+                                          _P, _P, _P, _P, _P, _P, _P, _P]
+        L.port_ca_query_sparse.argtypes = [ctypes.POINTER(_Spec), _I, _I, _P, _I, _P, _P, _P, _P,
+                                           _P, _L, _P, _P, _P, _P, _P, _P, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -232,3 +243,116 @@ def query_sparse(spec: GridSpec, block_dim, ijk, phi, normal, hessian, mode: int
                             _ptr(nrm), _ptr(hes), int(mode), _ptr(p), n, _ptr(gap), _ptr(grad),
                             _ptr(unit), _ptr(wit), _ptr(valid), _ptr(hs))
     return dict(gap=gap, grad=grad, unit=unit, witness=wit, valid=valid.astype(bool), hess=hs)
+
+
+# ---------------------------------------------------------------------------
+# contact-aware builds and queries (SdfBuilder.cpp:27-359, 416-821;
+# SdfOracle.cpp:269-431)
+# ---------------------------------------------------------------------------
+def build_contact_aware(verts, tris, corner_normals, padding=0.1, voxel_size=0.0,
+                        target_resolution=128, max_resolution=512, max_candidates=4,
+                        feature_distance_tolerance=0.0, normal_merge_angle_degrees=5.0,
+                        tile_dim=8, use_tile_acceleration=True, store_hessian=True, sparse=False,
+                        block_dim=8, halo_voxels=2, band_voxels=8, band_distance=0.0):
+    """SdfBuilder::buildContactAware / buildSparseContactAware restated.
+    Dense: phi, normal, witness (primary candidate), hessian, count (N,),
+    cphi (N,s), cnormal (N,s,3), cbranch (N,s).  Sparse: ijk, phi (B,V),
+    normal (B,V,3), hessian (B,V,6), count (B,V), cphi (B,V,s), cnormal
+    (B,V,s,3), cbranch (B,V,s) -- FP32."""
+    v = np.ascontiguousarray(verts, np.float64).reshape(-1, 3)
+    t = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+    cn = np.ascontiguousarray(corner_normals, np.float64).reshape(-1, 3, 3)
+    spec = setup_grid(v, padding, voxel_size, target_resolution, max_resolution)
+    h = float(np.max(spec["voxel"]))
+    tol = feature_distance_tolerance if feature_distance_tolerance > 0.0 else 1.5 * h
+    cos_merge = float(np.cos(normal_merge_angle_degrees * np.arccos(-1.0) / 180.0))
+    stride = max(0, min(max_candidates, 8))
+    s = spec.to_c()
+    if not sparse:
+        influence = tol + 2.0 * h
+    else:
+        band = band_distance if band_distance > 0.0 else float(band_voxels) * h
+        activation = band + float(halo_voxels) * h
+        influence = max(activation, tol + 2.0 * h)
+    ctx = lib().port_ca_prepare(_ptr(v), len(v), _ptr(t), len(t), _ptr(cn), ctypes.byref(s),
+                                tile_dim, 1 if use_tile_acceleration else 0, influence)
+    try:
+        if not sparse:
+            n = int(np.prod(spec["shape"]))
+            out = dict(spec=spec, stride=stride, count=np.zeros(n, np.uint8),
+                       cphi=np.zeros((n, stride)), cnormal=np.zeros((n, stride, 3)),
+                       cbranch=np.zeros((n, stride), np.int32), phi=np.zeros(n),
+                       normal=np.zeros((n, 3)), witness=np.zeros((n, 3)))
+            lib().port_ca_dense(ctx, stride, tol, cos_merge, _ptr(out["count"]), _ptr(out["cphi"]),
+                                _ptr(out["cnormal"]), _ptr(out["cbranch"]), _ptr(out["phi"]),
+                                _ptr(out["normal"]), _ptr(out["witness"]))
+            out["hessian"] = dense_hessian(spec, out["normal"]) if store_hessian else None
+            return out
+        nb = [(spec["shape"][a] + block_dim - 1) // block_dim for a in range(3)]
+        active = np.zeros(nb[0] * nb[1] * nb[2], np.uint8)
+        lib().port_ca_sparse_activate(ctx, block_dim, activation, _ptr(active))
+        lin = np.nonzero(active)[0]
+        ijk = np.ascontiguousarray(
+            np.stack([lin % nb[0], (lin // nb[0]) % nb[1], lin // (nb[0] * nb[1])], -1), np.int32)
+        B, V = len(ijk), block_dim ** 3
+        out = dict(spec=spec, stride=stride, block_dim=block_dim, halo=halo_voxels, band=band,
+                   ijk=ijk, phi=np.zeros((B, V), np.float32), normal=np.zeros((B, V, 3), np.float32),
+                   count=np.zeros((B, V), np.uint8), cphi=np.zeros((B, V, stride), np.float32),
+                   cnormal=np.zeros((B, V, stride, 3), np.float32),
+                   cbranch=np.zeros((B, V, stride), np.int32))
+        lib().port_ca_sparse_fill(ctx, block_dim, B, _ptr(ijk), stride, tol, cos_merge,
+                                  _ptr(out["phi"]), _ptr(out["normal"]), _ptr(out["count"]),
+                                  _ptr(out["cphi"]), _ptr(out["cnormal"]), _ptr(out["cbranch"]))
+        out["hessian"] = (sparse_hessian(spec, block_dim, ijk, out["normal"])
+                          if store_hessian else None)
+        return out
+    finally:
+        lib().port_ca_free(ctx)
+
+
+def query_contact_aware(g: dict, pts):
+    """queryFast(ContactAware) on a build_contact_aware result: gap, normal
+    (gapNormal), witness, valid, ncand, and the candidates kgap (n,8),
+    knormal (n,8,3), kwitness (n,8,3), kbranch (n,8).  Voxels without
+    candidates take the FirstOrder query (SdfOracle.cpp:329, 385), as in the
+    reference, with a single candidate of branch 0."""
+    p = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+    n = len(p)
+    out = dict(gap=np.zeros(n), normal=np.zeros((n, 3)), witness=np.zeros((n, 3)),
+               valid=np.zeros(n, np.uint8), ncand=np.zeros(n, np.int32),
+               kgap=np.zeros((n, 8)), knormal=np.zeros((n, 8, 3)), kwitness=np.zeros((n, 8, 3)),
+               kbranch=np.full((n, 8), -1, np.int32))
+    s = g["spec"].to_c()
+    cnt = np.ascontiguousarray(g["count"], np.uint8)
+    br = np.ascontiguousarray(g["cbranch"], np.int32)
+    if "ijk" in g:
+        ijk = np.ascontiguousarray(g["ijk"], np.int32)
+        lib().port_ca_query_sparse(ctypes.byref(s), g["block_dim"], len(ijk), _ptr(ijk), g["stride"],
+                                   _ptr(cnt), _ptr(np.ascontiguousarray(g["cphi"], np.float32)),
+                                   _ptr(np.ascontiguousarray(g["cnormal"], np.float32)), _ptr(br),
+                                   _ptr(p), n, _ptr(out["valid"]), _ptr(out["gap"]),
+                                   _ptr(out["normal"]), _ptr(out["witness"]), _ptr(out["ncand"]),
+                                   _ptr(out["kgap"]), _ptr(out["knormal"]), _ptr(out["kwitness"]),
+                                   _ptr(out["kbranch"]))
+        first = query_sparse(g["spec"], g["block_dim"], ijk, g["phi"], g["normal"], None,
+                             FIRST_ORDER, p)
+    else:
+        lib().port_ca_query_dense(ctypes.byref(s), g["stride"], _ptr(cnt),
+                                  _ptr(np.ascontiguousarray(g["cphi"], np.float64)),
+                                  _ptr(np.ascontiguousarray(g["cnormal"], np.float64)), _ptr(br),
+                                  _ptr(p), n, _ptr(out["valid"]), _ptr(out["gap"]),
+                                  _ptr(out["normal"]), _ptr(out["witness"]), _ptr(out["ncand"]),
+                                  _ptr(out["kgap"]), _ptr(out["knormal"]), _ptr(out["kwitness"]),
+                                  _ptr(out["kbranch"]))
+        first = query_dense(g["spec"], g["phi"], g["normal"], None, FIRST_ORDER, p)
+    out["valid"] = out["valid"].astype(bool)
+    fo = out["valid"] & (out["ncand"] == 0)
+    out["gap"][fo] = first["gap"][fo]
+    out["normal"][fo] = first["unit"][fo]
+    out["witness"][fo] = first["witness"][fo]
+    out["ncand"][fo] = 1
+    out["kgap"][fo, 0] = first["gap"][fo]
+    out["knormal"][fo, 0] = first["unit"][fo]
+    out["kwitness"][fo, 0] = first["witness"][fo]
+    out["kbranch"][fo, 0] = 0
+    return out

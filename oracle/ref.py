@@ -55,6 +55,19 @@ def lib():
         L.ref_signed_nearest.argtypes = [_P, _I, _P, _I, _P, _L, _P, _P, _P, _P]
         L.ref_load_obj.restype = _I
         L.ref_load_obj.argtypes = [ctypes.c_char_p, _P, _P, _P, _P]
+        L.ref_build_contact_aware.restype = _P
+        L.ref_build_contact_aware.argtypes = [_P, _I, _P, _I, _P, _D, _D, _I, _I, _I, _D, _D, _I,
+                                              _I, _I, _I, _I, _I, _I, _D, _P]
+        L.ref_ca_stride.restype = _I
+        L.ref_ca_stride.argtypes = [_P]
+        L.ref_ca_export_dense.restype = _I
+        L.ref_ca_export_dense.argtypes = [_P, _P, _P, _P, _P]
+        L.ref_ca_export_sparse.restype = _I
+        L.ref_ca_export_sparse.argtypes = [_P, _P, _P, _P, _P]
+        L.ref_query_candidates.restype = _I
+        L.ref_query_candidates.argtypes = [_P, _I, _P, _L, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.ref_load_ca_surface.restype = _I
+        L.ref_load_ca_surface.argtypes = [ctypes.c_char_p, _P, _P, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -210,3 +223,74 @@ def load_obj(path: str):
     t = np.zeros((int(nt[0]), 3), np.int32)
     lib().ref_load_obj(path.encode(), _ptr(v), _ptr(nv), _ptr(t), _ptr(nt))
     return v, t
+
+
+def build_contact_aware(verts, tris, corner_normals, padding=0.1, voxel_size=0.0,
+                        target_resolution=128, max_resolution=512, max_candidates=4,
+                        feature_distance_tolerance=0.0, normal_merge_angle_degrees=5.0,
+                        tile_dim=8, use_tile_acceleration=True, store_hessian=True, sparse=False,
+                        block_dim=8, halo_voxels=2, band_voxels=8, band_distance=0.0) -> "RefGrid":
+    """SdfBuilder::buildContactAware / buildSparseContactAware
+    (SdfBuilder.cpp:416-821) with ContactAwareBuilderParams' defaults."""
+    v, t = _mesh(verts, tris)
+    cn = np.ascontiguousarray(corner_normals, np.float64).reshape(-1, 3, 3)
+    sec = np.zeros(1)
+    h = lib().ref_build_contact_aware(
+        _ptr(v), len(v), _ptr(t), len(t), _ptr(cn), padding, voxel_size, target_resolution,
+        max_resolution, max_candidates, feature_distance_tolerance, normal_merge_angle_degrees,
+        tile_dim, 1 if use_tile_acceleration else 0, 1 if store_hessian else 0,
+        1 if sparse else 0, block_dim, halo_voxels, band_voxels, band_distance, _ptr(sec))
+    if not h:
+        raise RuntimeError(_err())
+    return RefGrid(h, float(sec[0]))
+
+
+def ca_arrays(g: "RefGrid"):
+    """Candidate arrays of a contact-aware grid: stride, count, phi, normal,
+    branch (dense: (N, s[, 3]) FP64; sparse: (B, V, s[, 3]) FP32)."""
+    s = lib().ref_ca_stride(g.handle)
+    info = g.info()
+    if info["sparse"]:
+        B, V = info["blocks"], info["block_dim"] ** 3
+        cnt = np.zeros((B, V), np.uint8)
+        phi = np.zeros((B, V, s), np.float32)
+        nrm = np.zeros((B, V, s, 3), np.float32)
+        br = np.zeros((B, V, s), np.int32)
+        lib().ref_ca_export_sparse(g.handle, _ptr(cnt), _ptr(phi), _ptr(nrm), _ptr(br))
+    else:
+        N = int(np.prod(info["shape"]))
+        cnt = np.zeros(N, np.uint8)
+        phi = np.zeros((N, s))
+        nrm = np.zeros((N, s, 3))
+        br = np.zeros((N, s), np.int32)
+        lib().ref_ca_export_dense(g.handle, _ptr(cnt), _ptr(phi), _ptr(nrm), _ptr(br))
+    return dict(stride=s, count=cnt, phi=phi, normal=nrm, branch=br)
+
+
+def query_candidates(g: "RefGrid", mode: int, pts):
+    """queryFast with the candidate list (SdfFastQueryResult, SdfCommon.h:29-37)."""
+    p = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+    n = len(p)
+    out = dict(gap=np.zeros(n), normal=np.zeros((n, 3)), witness=np.zeros((n, 3)),
+               valid=np.zeros(n, np.uint8), ncand=np.zeros(n, np.int32),
+               kgap=np.zeros((n, 8)), knormal=np.zeros((n, 8, 3)), kwitness=np.zeros((n, 8, 3)),
+               kbranch=np.zeros((n, 8), np.int32))
+    lib().ref_query_candidates(g.handle, int(mode), _ptr(p), n, _ptr(out["gap"]),
+                               _ptr(out["normal"]), _ptr(out["witness"]), _ptr(out["valid"]),
+                               _ptr(out["ncand"]), _ptr(out["kgap"]), _ptr(out["knormal"]),
+                               _ptr(out["kwitness"]), _ptr(out["kbranch"]))
+    out["valid"] = out["valid"].astype(bool)
+    return out
+
+
+def load_ca_surface(path: str):
+    """loadContactAwareSurfaceFile: verts (nv,3), tris (nt,3), corner normals (nt,3,3)."""
+    nv = np.zeros(1, np.int32)
+    nt = np.zeros(1, np.int32)
+    if lib().ref_load_ca_surface(path.encode(), None, _ptr(nv), None, _ptr(nt), None) != 0:
+        raise RuntimeError(_err())
+    v = np.zeros((int(nv[0]), 3))
+    t = np.zeros((int(nt[0]), 3), np.int32)
+    cn = np.zeros((int(nt[0]), 3, 3))
+    lib().ref_load_ca_surface(path.encode(), _ptr(v), _ptr(nv), _ptr(t), _ptr(nt), _ptr(cn))
+    return v, t, cn

@@ -8,6 +8,8 @@
 //
 // Wrapped reference entry points:
 //   SdfBuilder::build / buildSparse           (src/SdfBuilder.cpp:364, 823)
+//   SdfBuilder::buildContactAware / buildSparseContactAware (src/SdfBuilder.cpp:416, 551)
+//   loadContactAwareSurfaceFile               (src/SdfSurfaceMesh.cpp:157)
 //   SdfOracle::queryFast                      (src/SdfOracle.cpp:226)
 //   saveSdf / loadSdf / saveSparseSdf / ...   (src/SdfIO.cpp:93-552)
 //   KdTree::findSignedNearest                 (include/SdfOracle/KdTree.h:143)
@@ -331,6 +333,172 @@ int ref_load_obj(const char* path, double* verts, int* nv, int* tris, int* nt)
                 for (int a = 0; a < 3; ++a) tris[3 * i + static_cast<size_t>(a)] = m.triangles[i][static_cast<size_t>(a)];
         *nv = static_cast<int>(m.vertices.size());
         *nt = static_cast<int>(m.triangles.size());
+        return 0;
+    }
+    catch (const std::exception& e)
+    {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+
+// SdfBuilder::buildContactAware / buildSparseContactAware (sparse != 0) on a
+// mesh with corner normals (nt, 3, 3).
+void* ref_build_contact_aware(const double* verts, int nv, const int* tris, int nt,
+                              const double* cornerNormals, double padding, double voxelSize,
+                              int targetResolution, int maxResolution, int maxCandidates,
+                              double featureDistanceTolerance, double normalMergeAngleDegrees,
+                              int tileDim, int useTileAcceleration, int storeHessian, int sparse,
+                              int blockDim, int haloVoxels, int bandVoxels, double bandDistance,
+                              double* seconds)
+{
+    try
+    {
+        sdf::ContactAwareBuilderParams p;
+        p.padding = padding;
+        p.voxelSize = voxelSize;
+        p.targetResolution = targetResolution;
+        p.maxResolution = maxResolution;
+        p.maxCandidates = maxCandidates;
+        p.featureDistanceTolerance = featureDistanceTolerance;
+        p.normalMergeAngleDegrees = normalMergeAngleDegrees;
+        p.tileDim = tileDim;
+        p.useTileAcceleration = useTileAcceleration != 0;
+        p.storeHessian = storeHessian != 0;
+        p.sparse = sparse != 0;
+        p.blockDim = blockDim;
+        p.haloVoxels = haloVoxels;
+        p.bandVoxels = bandVoxels;
+        p.bandDistance = bandDistance;
+        p.logCallback = quietLog;
+        sdf::CornerNormalTriangleMesh mesh;
+        mesh.vertices = toVerts(verts, nv);
+        mesh.triangles = toTris(tris, nt);
+        mesh.cornerNormals.resize(static_cast<size_t>(nt));
+        for (int t = 0; t < nt; ++t)
+            for (int v = 0; v < 3; ++v)
+                mesh.cornerNormals[static_cast<size_t>(t)][static_cast<size_t>(v)] =
+                    Eigen::Vector3d(cornerNormals[9 * t + 3 * v], cornerNormals[9 * t + 3 * v + 1],
+                                    cornerNormals[9 * t + 3 * v + 2]);
+        const auto t0 = std::chrono::steady_clock::now();
+        RefHandle* h = nullptr;
+        if (sparse)
+            h = new RefHandle{sdf::SdfOracle(sdf::SdfBuilder::buildSparseContactAware(mesh, p))};
+        else
+            h = new RefHandle{sdf::SdfOracle(sdf::SdfBuilder::buildContactAware(mesh, p))};
+        const auto t1 = std::chrono::steady_clock::now();
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+        return h;
+    }
+    catch (const std::exception& e)
+    {
+        g_error = e.what();
+        return nullptr;
+    }
+}
+
+// Candidate stride of a contact-aware grid (0 = none).
+int ref_ca_stride(void* hp)
+{
+    auto* h = static_cast<RefHandle*>(hp);
+    return h->oracle.isSparse() ? h->oracle.sparseData().contactCandidateStride
+                                : h->oracle.data().contactCandidateStride;
+}
+
+// Dense candidates: count[N], phi[N*s], normal[N*s*3], branch[N*s].
+int ref_ca_export_dense(void* hp, unsigned char* count, double* phi, double* normal, int* branch)
+{
+    auto* h = static_cast<RefHandle*>(hp);
+    if (h->oracle.isSparse()) return -1;
+    const sdf::SdfData& d = h->oracle.data();
+    const size_t N = d.contactCandidateCount.size(), M = d.contactCandidatePhi0.size();
+    std::memcpy(count, d.contactCandidateCount.data(), N);
+    std::memcpy(phi, d.contactCandidatePhi0.data(), M * sizeof(double));
+    for (size_t i = 0; i < M; ++i)
+        for (int a = 0; a < 3; ++a) normal[3 * i + a] = d.contactCandidateNormal0[i](a);
+    std::memcpy(branch, d.contactCandidateBranchId.data(), M * sizeof(int));
+    return 0;
+}
+
+// Sparse candidates per block in stored order: count[B*V], phi[B*V*s],
+// normal[B*V*s*3], branch[B*V*s].
+int ref_ca_export_sparse(void* hp, unsigned char* count, float* phi, float* normal, int* branch)
+{
+    auto* h = static_cast<RefHandle*>(hp);
+    if (!h->oracle.isSparse()) return -1;
+    const sdf::SparseSdfData& sp = h->oracle.sparseData();
+    const int V = sp.blockDim * sp.blockDim * sp.blockDim;
+    const int s = sp.contactCandidateStride;
+    for (size_t b = 0; b < sp.blocks.size(); ++b)
+    {
+        const auto& blk = sp.blocks[b];
+        std::memcpy(count + b * V, blk.contactCandidateCount.data(), (size_t)V);
+        std::memcpy(phi + b * V * s, blk.contactCandidatePhi0.data(), (size_t)V * s * sizeof(float));
+        std::memcpy(normal + b * V * s * 3, blk.contactCandidateNormal0.data(),
+                    (size_t)V * s * 3 * sizeof(float));
+        std::memcpy(branch + b * V * s, blk.contactCandidateBranchId.data(), (size_t)V * s * sizeof(int));
+    }
+    return 0;
+}
+
+// queryFast with its candidate list: ncand[n], kgap[n*8], knormal[n*24],
+// kwitness[n*24], kbranch[n*8] (plus gap/normal/witness/valid as ref_query).
+int ref_query_candidates(void* hp, int mode, const double* pts, int64_t n, double* gap,
+                         double* normal, double* witness, unsigned char* valid, int* ncand,
+                         double* kgap, double* knormal, double* kwitness, int* kbranch)
+{
+    auto* h = static_cast<RefHandle*>(hp);
+    const auto m = static_cast<sdf::QueryMode>(mode);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i)
+    {
+        const Eigen::Vector3d p(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+        const sdf::SdfFastQueryResult r = h->oracle.queryFast(p, m);
+        gap[i] = r.gap;
+        valid[i] = r.valid ? 1 : 0;
+        ncand[i] = r.candidateCount;
+        for (int a = 0; a < 3; ++a)
+        {
+            normal[3 * i + a] = r.gapNormal(a);
+            witness[3 * i + a] = r.witnessPoint(a);
+        }
+        for (int c = 0; c < 8; ++c)
+        {
+            const sdf::SdfQueryCandidate& k = r.candidates[static_cast<size_t>(c)];
+            kgap[8 * i + c] = k.gap;
+            kbranch[8 * i + c] = k.branchId;
+            for (int a = 0; a < 3; ++a)
+            {
+                knormal[24 * i + 3 * c + a] = k.gapNormal(a);
+                kwitness[24 * i + 3 * c + a] = k.witnessPoint(a);
+            }
+        }
+    }
+    return 0;
+}
+
+// loadContactAwareSurfaceFile: call with NULL arrays for the counts, then
+// with arrays of those sizes (verts (nv,3), tris (nt,3), normals (nt,3,3)).
+int ref_load_ca_surface(const char* path, double* verts, int* nv, int* tris, int* nt,
+                        double* normals)
+{
+    try
+    {
+        const sdf::CornerNormalTriangleMesh m = sdf::loadContactAwareSurfaceFile(path);
+        *nv = static_cast<int>(m.vertices.size());
+        *nt = static_cast<int>(m.triangles.size());
+        if (verts)
+            for (size_t i = 0; i < m.vertices.size(); ++i)
+                for (int a = 0; a < 3; ++a) verts[3 * i + a] = m.vertices[i](a);
+        if (tris)
+            for (size_t i = 0; i < m.triangles.size(); ++i)
+                for (int a = 0; a < 3; ++a) tris[3 * i + a] = m.triangles[i][static_cast<size_t>(a)];
+        if (normals)
+            for (size_t i = 0; i < m.cornerNormals.size(); ++i)
+                for (int v = 0; v < 3; ++v)
+                    for (int a = 0; a < 3; ++a)
+                        normals[9 * i + 3 * v + a] = m.cornerNormals[i][static_cast<size_t>(v)](a);
         return 0;
     }
     catch (const std::exception& e)

@@ -1137,3 +1137,530 @@ void port_query_sparse(const port_grid_spec* s, int blockDim, int nblocks, const
                   hess ? hess + 9 * q : NULL);
     free(ctx.x.table);
 }
+
+/* ======================================================================== */
+/* contact-aware build and query (SdfBuilder.cpp:27-359, 416-821;            */
+/* SdfOracle.cpp:269-431)                                                    */
+/* ======================================================================== */
+
+namespace {
+
+struct ca_tri
+{
+    double a[3], b[3], c[3];
+    double cn[3][3]; /* corner normals */
+    double fn[3];    /* face normal */
+    double lo[3], hi[3];
+};
+
+struct ca_cand
+{
+    double phi, dist;
+    double n[3], w[3];
+    int branch;
+};
+
+/* normalizedOrDefault (SdfBuilder.cpp:27-43) */
+void normalized_or(const double* v, const double* fallback, double* out)
+{
+    const double nrm = norm3(v);
+    if (nrm <= 1.0e-15)
+    {
+        const double fnrm = norm3(fallback);
+        if (fnrm > 1.0e-15)
+        {
+            for (int a = 0; a < 3; ++a) out[a] = fallback[a] / fnrm;
+            return;
+        }
+        out[0] = 1.0;
+        out[1] = 0.0;
+        out[2] = 0.0;
+        return;
+    }
+    for (int a = 0; a < 3; ++a) out[a] = v[a] / nrm;
+}
+
+const double kUnitX[3] = {1.0, 0.0, 0.0};
+
+/* barycentricOnTriangle (SdfBuilder.cpp:45-67) */
+void barycentric(const double* p, const double* a, const double* b, const double* c, double* out)
+{
+    double v0[3], v1[3], v2[3];
+    sub3(b, a, v0);
+    sub3(c, a, v1);
+    sub3(p, a, v2);
+    const double d00 = dot3(v0, v0), d01 = dot3(v0, v1), d11 = dot3(v1, v1);
+    const double d20 = dot3(v2, v0), d21 = dot3(v2, v1);
+    const double denom = d00 * d11 - d01 * d01;
+    if (fabs(denom) <= 1.0e-15)
+    {
+        out[0] = out[1] = out[2] = 1.0 / 3.0;
+        return;
+    }
+    const double v = (d11 * d20 - d01 * d21) / denom;
+    const double w = (d00 * d21 - d01 * d20) / denom;
+    out[0] = 1.0 - v - w;
+    out[1] = v;
+    out[2] = w;
+}
+
+/* branchIdFromNormal (SdfBuilder.cpp:114-134): FNV-1a of the normal
+ * quantised to 1/4095. */
+int branch_id(const double* raw)
+{
+    double n[3];
+    normalized_or(raw, kUnitX, n);
+    uint32_t hash = 2166136261u;
+    for (int a = 0; a < 3; ++a)
+    {
+        double v = n[a];
+        v = std::max(-1.0, std::min(1.0, v));
+        const int32_t q = (int32_t)lround(v * 4095.0);
+        hash ^= (uint32_t)q;
+        hash *= 16777619u;
+    }
+    return (int)(1u + (hash & 0x3fffffffu));
+}
+
+/* makeContactCandidate (SdfBuilder.cpp:245-266) */
+void make_candidate(const double* p, const ca_tri& t, ca_cand& out)
+{
+    double cp[3], bary[3], raw[3], d[3];
+    closest_point_on_triangle(p, t.a, t.b, t.c, cp);
+    barycentric(cp, t.a, t.b, t.c, bary);
+    for (int a = 0; a < 3; ++a)
+        raw[a] = bary[0] * t.cn[0][a] + bary[1] * t.cn[1][a] + bary[2] * t.cn[2][a];
+    normalized_or(raw, t.fn, out.n);
+    sub3(p, cp, d);
+    out.phi = dot3(d, out.n);
+    out.dist = norm3(d);
+    memcpy(out.w, cp, sizeof(cp));
+    out.branch = branch_id(out.n);
+}
+
+/* mergeContactCandidate (SdfBuilder.cpp:136-153) */
+void merge_candidate(std::vector<ca_cand>& list, const ca_cand& in, double cosMerge)
+{
+    for (ca_cand& e : list)
+    {
+        if (dot3(e.n, in.n) >= cosMerge)
+        {
+            if (fabs(in.phi) < fabs(e.phi)) e = in;
+            return;
+        }
+    }
+    list.push_back(in);
+}
+
+} // namespace
+
+struct port_ca
+{
+    port_grid_spec spec;
+    std::vector<ca_tri> tris;
+    port_bvh* tree = nullptr;
+    int tileDim = 8, tnx = 1, tny = 1, tnz = 1;
+    bool useTiles = true;
+    std::vector<std::vector<int>> tiles;
+    std::vector<int> all;
+    ~port_ca() { port_bvh_free(tree); }
+};
+
+/* makeContactTriangleInfos (SdfBuilder.cpp:155-184) and
+ * buildContactTileIndex (SdfBuilder.cpp:202-243). */
+port_ca* port_ca_prepare(const double* verts, int nv, const int* tris, int nt,
+                         const double* cornerNormals, const port_grid_spec* spec, int tileDim,
+                         int useTiles, double influenceRadius)
+{
+    port_ca* c = new port_ca();
+    c->spec = *spec;
+    c->tree = port_bvh_build(verts, nv, tris, nt);
+    c->tris.resize((size_t)nt);
+    for (int t = 0; t < nt; ++t)
+    {
+        ca_tri& T = c->tris[(size_t)t];
+        for (int a = 0; a < 3; ++a)
+        {
+            T.a[a] = verts[3 * tris[3 * t] + a];
+            T.b[a] = verts[3 * tris[3 * t + 1] + a];
+            T.c[a] = verts[3 * tris[3 * t + 2] + a];
+        }
+        for (int v = 0; v < 3; ++v)
+            for (int a = 0; a < 3; ++a) T.cn[v][a] = cornerNormals[9 * t + 3 * v + a];
+        double e0[3], e1[3], cr[3];
+        sub3(T.b, T.a, e0);
+        sub3(T.c, T.a, e1);
+        cross3(e0, e1, cr);
+        normalized_or(cr, kUnitX, T.fn);
+        for (int a = 0; a < 3; ++a)
+        {
+            double mn = T.b[a] < T.a[a] ? T.b[a] : T.a[a];
+            mn = T.c[a] < mn ? T.c[a] : mn;
+            double mx = T.a[a] < T.b[a] ? T.b[a] : T.a[a];
+            mx = mx < T.c[a] ? T.c[a] : mx;
+            T.lo[a] = mn;
+            T.hi[a] = mx;
+        }
+    }
+    c->all.resize((size_t)nt);
+    for (int t = 0; t < nt; ++t) c->all[(size_t)t] = t;
+    c->useTiles = useTiles != 0;
+    if (!c->useTiles) return c;
+    c->tileDim = std::max(1, tileDim);
+    c->tnx = (spec->shape[0] + c->tileDim - 1) / c->tileDim;
+    c->tny = (spec->shape[1] + c->tileDim - 1) / c->tileDim;
+    c->tnz = (spec->shape[2] + c->tileDim - 1) / c->tileDim;
+    c->tiles.assign((size_t)c->tnx * c->tny * c->tnz, std::vector<int>());
+    const double h = std::max(spec->voxel[0], std::max(spec->voxel[1], spec->voxel[2]));
+    const double tileRadius = 0.5 * sqrt(3.0) * (double)c->tileDim * h;
+    const double expansion = std::max(0.0, influenceRadius) + tileRadius + h;
+    for (int t = 0; t < nt; ++t)
+    {
+        const ca_tri& T = c->tris[(size_t)t];
+        int lo[3], hi[3];
+        for (int a = 0; a < 3; ++a)
+        {
+            const double l = T.lo[a] - expansion, u = T.hi[a] + expansion;
+            int i0 = (int)floor((l - spec->bmin[a]) / spec->voxel[a] - 0.5);
+            int i1 = (int)ceil((u - spec->bmin[a]) / spec->voxel[a] - 0.5);
+            i0 = std::max(0, std::min(spec->shape[a] - 1, i0));
+            i1 = std::max(0, std::min(spec->shape[a] - 1, i1));
+            lo[a] = i0 / c->tileDim;
+            hi[a] = i1 / c->tileDim;
+        }
+        for (int tk = lo[2]; tk <= hi[2]; ++tk)
+            for (int tj = lo[1]; tj <= hi[1]; ++tj)
+                for (int ti = lo[0]; ti <= hi[0]; ++ti)
+                    c->tiles[(size_t)(ti + c->tnx * (tj + c->tny * tk))].push_back(t);
+    }
+    return c;
+}
+
+void port_ca_free(port_ca* c) { delete c; }
+
+static const std::vector<int>& ca_list(const port_ca* c, int i, int j, int k)
+{
+    if (!c->useTiles) return c->all;
+    static const std::vector<int> empty;
+    if (c->tiles.empty()) return empty;
+    const int ti = std::max(0, std::min(c->tnx - 1, i / c->tileDim));
+    const int tj = std::max(0, std::min(c->tny - 1, j / c->tileDim));
+    const int tk = std::max(0, std::min(c->tnz - 1, k / c->tileDim));
+    return c->tiles[(size_t)(ti + c->tnx * (tj + c->tny * tk))];
+}
+
+/* buildContactCandidatesForPoint (SdfBuilder.cpp:268-343) */
+static void ca_point(const port_ca* c, const double* p, const std::vector<int>& ids, double tol,
+                     double cosMerge, int maxCand, std::vector<ca_cand>& merged)
+{
+    const int nt = (int)c->tris.size();
+    double minDistance = DBL_MAX;
+    for (int t : ids)
+    {
+        if (t < 0 || t >= nt) continue;
+        ca_cand cc;
+        make_candidate(p, c->tris[(size_t)t], cc);
+        minDistance = std::min(minDistance, cc.dist);
+    }
+    int fallback = -1;
+    if (!std::isfinite(minDistance))
+    {
+        nearest_t nb;
+        nearest(c->tree, p, &nb);
+        fallback = nb.tri;
+        minDistance = nb.tri >= 0 ? sqrt(nb.sq) : DBL_MAX;
+    }
+    merged.clear();
+    const double allowed = minDistance + tol;
+    auto tryTri = [&](int t) {
+        if (t < 0 || t >= nt) return;
+        ca_cand cc;
+        make_candidate(p, c->tris[(size_t)t], cc);
+        if (cc.dist <= allowed) merge_candidate(merged, cc, cosMerge);
+    };
+    if (ids.empty())
+        tryTri(fallback);
+    else
+        for (int t : ids) tryTri(t);
+    if (merged.empty())
+    {
+        if (fallback < 0)
+        {
+            nearest_t nb;
+            nearest(c->tree, p, &nb);
+            fallback = nb.tri;
+        }
+        tryTri(fallback);
+    }
+    std::sort(merged.begin(), merged.end(),
+              [](const ca_cand& a, const ca_cand& b) { return fabs(a.phi) < fabs(b.phi); });
+    if ((int)merged.size() > maxCand) merged.resize((size_t)maxCand);
+}
+
+/* Dense contact-aware fill (SdfBuilder.cpp:472-528): per voxel x-fastest,
+ * count[N], cphi[N*s], cnormal[N*s*3], cbranch[N*s] (s = stride), and the
+ * primary candidate as phi0[N], n0[N*3], w0[N*3] (left at 0 / UnitX / 0
+ * where the voxel has none). */
+void port_ca_dense(const port_ca* c, int stride, double tol, double cosMerge, uint8_t* count,
+                   double* cphi, double* cn, int* cbr, double* phi0, double* n0, double* w0)
+{
+    const port_grid_spec* s = &c->spec;
+    const int64_t N = (int64_t)s->shape[0] * s->shape[1] * s->shape[2];
+#pragma omp parallel for schedule(dynamic, 128)
+    for (int64_t idx = 0; idx < N; ++idx)
+    {
+        const int i = (int)(idx % s->shape[0]);
+        const int j = (int)((idx / s->shape[0]) % s->shape[1]);
+        const int k = (int)(idx / ((int64_t)s->shape[0] * s->shape[1]));
+        double ctr[3];
+        center_from_index(s, i, j, k, ctr);
+        std::vector<ca_cand> m;
+        ca_point(c, ctr, ca_list(c, i, j, k), tol, cosMerge, stride, m);
+        const int cnt = std::min((int)m.size(), stride);
+        count[idx] = (uint8_t)cnt;
+        phi0[idx] = 0.0;
+        n0[3 * idx] = 1.0;
+        n0[3 * idx + 1] = n0[3 * idx + 2] = 0.0;
+        w0[3 * idx] = w0[3 * idx + 1] = w0[3 * idx + 2] = 0.0;
+        if (cnt > 0)
+        {
+            phi0[idx] = m[0].phi;
+            memcpy(n0 + 3 * idx, m[0].n, 3 * sizeof(double));
+            memcpy(w0 + 3 * idx, m[0].w, 3 * sizeof(double));
+        }
+        for (int q = 0; q < stride; ++q)
+        {
+            const int64_t o = idx * stride + q;
+            if (q < cnt)
+            {
+                cphi[o] = m[(size_t)q].phi;
+                memcpy(cn + 3 * o, m[(size_t)q].n, 3 * sizeof(double));
+                cbr[o] = m[(size_t)q].branch;
+            }
+            else
+            {
+                cphi[o] = 0.0;
+                cn[3 * o] = 1.0;
+                cn[3 * o + 1] = cn[3 * o + 2] = 0.0;
+                cbr[o] = -1;
+            }
+        }
+    }
+}
+
+/* Sparse contact-aware block selection (SdfBuilder.cpp:593-646): with tiles,
+ * a block is active iff a tile it overlaps lists a triangle; without, the
+ * nearest-triangle distance from the block centre against activation +
+ * block radius.  active[] over all blocks (bi fastest); returns the count. */
+int port_ca_sparse_activate(const port_ca* c, int bd, double activation, uint8_t* active)
+{
+    const port_grid_spec* s = &c->spec;
+    const int nbx = (s->shape[0] + bd - 1) / bd, nby = (s->shape[1] + bd - 1) / bd,
+              nbz = (s->shape[2] + bd - 1) / bd;
+    const int total = nbx * nby * nbz;
+    const double h = std::max(s->voxel[0], std::max(s->voxel[1], s->voxel[2]));
+    int count = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : count)
+    for (int bl = 0; bl < total; ++bl)
+    {
+        const int bi = bl % nbx, bj = (bl / nbx) % nby, bk = bl / (nbx * nby);
+        bool act = false;
+        if (c->useTiles && !c->tiles.empty())
+        {
+            const int i0 = bi * bd, j0 = bj * bd, k0 = bk * bd;
+            const int i1 = std::min(i0 + bd - 1, s->shape[0] - 1);
+            const int j1 = std::min(j0 + bd - 1, s->shape[1] - 1);
+            const int k1 = std::min(k0 + bd - 1, s->shape[2] - 1);
+            for (int tk = k0 / c->tileDim; tk <= k1 / c->tileDim && !act; ++tk)
+                for (int tj = j0 / c->tileDim; tj <= j1 / c->tileDim && !act; ++tj)
+                    for (int ti = i0 / c->tileDim; ti <= i1 / c->tileDim; ++ti)
+                        if (!c->tiles[(size_t)(ti + c->tnx * (tj + c->tny * tk))].empty())
+                        {
+                            act = true;
+                            break;
+                        }
+        }
+        else
+        {
+            const int i0 = bi * bd, j0 = bj * bd, k0 = bk * bd;
+            const int i1 = std::min(i0 + bd, s->shape[0]), j1 = std::min(j0 + bd, s->shape[1]),
+                      k1 = std::min(k0 + bd, s->shape[2]);
+            const double ctr[3] = {s->bmin[0] + s->voxel[0] * (0.5 * (double)(i0 + i1)),
+                                   s->bmin[1] + s->voxel[1] * (0.5 * (double)(j0 + j1)),
+                                   s->bmin[2] + s->voxel[2] * (0.5 * (double)(k0 + k1))};
+            nearest_t nb;
+            nearest(c->tree, ctr, &nb);
+            const double dist = nb.tri >= 0 ? sqrt(nb.sq) : DBL_MAX;
+            const double blockRadius = 0.5 * sqrt(3.0) * (double)bd * h;
+            act = dist <= activation + blockRadius;
+        }
+        active[bl] = act ? 1 : 0;
+        count += act ? 1 : 0;
+    }
+    return count;
+}
+
+/* Sparse contact-aware brick fill (SdfBuilder.cpp:680-770), FP32 storage:
+ * phi (B,V), normal (B,V,3), count (B,V), cphi (B,V,s), cn (B,V,s,3),
+ * cbr (B,V,s). */
+void port_ca_sparse_fill(const port_ca* c, int bd, int nblocks, const int* ijk, int stride,
+                         double tol, double cosMerge, float* phi, float* normal, uint8_t* count,
+                         float* cphi, float* cn, int* cbr)
+{
+    const port_grid_spec* s = &c->spec;
+    const int V = bd * bd * bd;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int b = 0; b < nblocks; ++b)
+    {
+        std::vector<ca_cand> m;
+        for (int local = 0; local < V; ++local)
+        {
+            const int lx = local % bd, ly = (local / bd) % bd, lz = local / (bd * bd);
+            const int i = ijk[3 * b] * bd + lx, j = ijk[3 * b + 1] * bd + ly, k = ijk[3 * b + 2] * bd + lz;
+            const int64_t v = (int64_t)b * V + local;
+            for (int q = 0; q < stride; ++q)
+            {
+                cphi[v * stride + q] = 0.f;
+                cn[3 * (v * stride + q)] = cn[3 * (v * stride + q) + 1] = cn[3 * (v * stride + q) + 2] = 0.f;
+                cbr[v * stride + q] = -1;
+            }
+            phi[v] = 0.f;
+            normal[3 * v] = 1.f;
+            normal[3 * v + 1] = normal[3 * v + 2] = 0.f;
+            count[v] = 0;
+            if (!in_bounds(s, i, j, k)) continue;
+            double ctr[3];
+            center_from_index(s, i, j, k, ctr);
+            ca_point(c, ctr, ca_list(c, i, j, k), tol, cosMerge, stride, m);
+            const int cnt = std::min((int)m.size(), stride);
+            count[v] = (uint8_t)cnt;
+            if (cnt > 0)
+            {
+                phi[v] = (float)m[0].phi;
+                for (int a = 0; a < 3; ++a) normal[3 * v + a] = (float)m[0].n[a];
+            }
+            for (int q = 0; q < cnt; ++q)
+            {
+                const int64_t o = v * stride + q;
+                cphi[o] = (float)m[(size_t)q].phi;
+                for (int a = 0; a < 3; ++a) cn[3 * o + a] = (float)m[(size_t)q].n[a];
+                cbr[o] = m[(size_t)q].branch;
+            }
+        }
+    }
+}
+
+/* queryFast ContactAware branch (SdfOracle.cpp:296-423) for one point given
+ * its voxel's candidates (count > 0): gap, normal, witness of the candidate
+ * with the smallest |gap| (first on ties), and every candidate's (gap,
+ * normal, witness, branch). */
+static void ca_eval(const double* p, const double* ctr, int cnt, const double* cphi,
+                    const double* cn, const int* cbr, double* gap, double* nrm, double* wit,
+                    double* kgap, double* kn, double* kw, int* kb)
+{
+    double dx[3];
+    sub3(p, ctr, dx);
+    int sel = 0;
+    double best = DBL_MAX;
+    for (int q = 0; q < cnt; ++q)
+    {
+        double n[3] = {cn[3 * q], cn[3 * q + 1], cn[3 * q + 2]};
+        const double l = norm3(n);
+        if (l > 1.0e-15)
+            for (int a = 0; a < 3; ++a) n[a] /= l;
+        else
+        {
+            n[0] = 1.0;
+            n[1] = n[2] = 0.0;
+        }
+        const double g = cphi[q] + dot3(n, dx);
+        kgap[q] = g;
+        for (int a = 0; a < 3; ++a)
+        {
+            kn[3 * q + a] = n[a];
+            kw[3 * q + a] = p[a] - g * n[a];
+        }
+        kb[q] = cbr[q];
+        if (fabs(g) < best)
+        {
+            best = fabs(g);
+            sel = q;
+        }
+    }
+    *gap = kgap[sel];
+    for (int a = 0; a < 3; ++a)
+    {
+        nrm[a] = kn[3 * sel + a];
+        wit[a] = kw[3 * sel + a];
+    }
+}
+
+/* Dense ContactAware queries.  Per point: valid, gap, normal[3], witness[3],
+ * ncand (0 where the voxel has no candidate: the point then takes the
+ * FirstOrder query, done by the caller), and up to 8 candidates
+ * (kgap[n*8], kn[n*24], kw[n*24], kb[n*8]). */
+void port_ca_query_dense(const port_grid_spec* s, int stride, const uint8_t* count,
+                         const double* cphi, const double* cn, const int* cbr, const double* pts,
+                         int64_t n, uint8_t* valid, double* gap, double* nrm, double* wit,
+                         int* ncand, double* kgap, double* kn, double* kw, int* kb)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t q = 0; q < n; ++q)
+    {
+        const double* p = pts + 3 * q;
+        int ijk[3];
+        for (int a = 0; a < 3; ++a) ijk[a] = (int)round((p[a] - s->bmin[a]) / s->voxel[a] - 0.5);
+        valid[q] = 0;
+        ncand[q] = 0;
+        if (!in_bounds(s, ijk[0], ijk[1], ijk[2])) continue;
+        const int64_t v = ijk[0] + (int64_t)s->shape[0] * (ijk[1] + (int64_t)s->shape[1] * ijk[2]);
+        const int cnt = std::min((int)count[v], stride);
+        valid[q] = 1;
+        if (cnt <= 0) continue;
+        const int kc = std::min(cnt, 8);
+        double ctr[3];
+        center_from_index(s, ijk[0], ijk[1], ijk[2], ctr);
+        ncand[q] = kc;
+        ca_eval(p, ctr, kc, cphi + v * stride, cn + 3 * v * stride, cbr + v * stride, gap + q,
+                nrm + 3 * q, wit + 3 * q, kgap + 8 * q, kn + 24 * q, kw + 24 * q, kb + 8 * q);
+    }
+}
+
+/* Sparse ContactAware queries (FP32 candidate storage widened to FP64). */
+void port_ca_query_sparse(const port_grid_spec* s, int bd, int nblocks, const int* ijk,
+                          int stride, const uint8_t* count, const float* cphi, const float* cn,
+                          const int* cbr, const double* pts, int64_t n, uint8_t* valid,
+                          double* gap, double* nrm, double* wit, int* ncand, double* kgap,
+                          double* kn, double* kw, int* kb)
+{
+    sparse_index x;
+    sparse_index_init(&x, s, bd, nblocks, ijk);
+#pragma omp parallel for schedule(static)
+    for (int64_t q = 0; q < n; ++q)
+    {
+        const double* p = pts + 3 * q;
+        int c3[3];
+        for (int a = 0; a < 3; ++a) c3[a] = (int)round((p[a] - s->bmin[a]) / s->voxel[a] - 0.5);
+        valid[q] = 0;
+        ncand[q] = 0;
+        if (!in_bounds(s, c3[0], c3[1], c3[2])) continue;
+        const int64_t v = sparse_voxel(&x, c3[0], c3[1], c3[2]);
+        if (v < 0) continue;
+        const int cnt = std::min((int)count[v], stride);
+        valid[q] = 1;
+        if (cnt <= 0) continue;
+        const int kc = std::min(cnt, 8);
+        double ph[8], nn[24];
+        for (int k = 0; k < kc; ++k)
+        {
+            ph[k] = (double)cphi[v * stride + k];
+            for (int a = 0; a < 3; ++a) nn[3 * k + a] = (double)cn[3 * (v * stride + k) + a];
+        }
+        double ctr[3];
+        center_from_index(s, c3[0], c3[1], c3[2], ctr);
+        ncand[q] = kc;
+        ca_eval(p, ctr, kc, ph, nn, cbr + v * stride, gap + q, nrm + 3 * q, wit + 3 * q,
+                kgap + 8 * q, kn + 24 * q, kw + 24 * q, kb + 8 * q);
+    }
+    free(x.table);
+}

@@ -90,6 +90,33 @@ void port_query_sparse(const port_grid_spec* spec, int blockDim, int nblocks, co
                        const double* pts, int64_t n, double* gap, double* grad, double* unit,
                        double* witness, uint8_t* valid, double* hess);
 
+/* Contact-aware builds (SdfBuilder.cpp:27-359 helpers, 416-821) and the
+ * ContactAware branch of queryFast (SdfOracle.cpp:269-431).  prepare: the
+ * triangle records (corner normals (nt,3,3)), the reference tree for the
+ * nearest-triangle fallback and, with useTiles, the tile index (tileDim^3
+ * voxel tiles, triangles whose bounds grown by influenceRadius + tile radius
+ * + h overlap the tile, in triangle order). */
+typedef struct port_ca port_ca;
+port_ca* port_ca_prepare(const double* verts, int nv, const int* tris, int nt,
+                         const double* cornerNormals, const port_grid_spec* spec, int tileDim,
+                         int useTiles, double influenceRadius);
+void port_ca_free(port_ca* c);
+void port_ca_dense(const port_ca* c, int stride, double tol, double cosMerge, uint8_t* count,
+                   double* cphi, double* cn, int* cbr, double* phi0, double* n0, double* w0);
+int port_ca_sparse_activate(const port_ca* c, int bd, double activation, uint8_t* active);
+void port_ca_sparse_fill(const port_ca* c, int bd, int nblocks, const int* ijk, int stride,
+                         double tol, double cosMerge, float* phi, float* normal, uint8_t* count,
+                         float* cphi, float* cn, int* cbr);
+void port_ca_query_dense(const port_grid_spec* s, int stride, const uint8_t* count,
+                         const double* cphi, const double* cn, const int* cbr, const double* pts,
+                         int64_t n, uint8_t* valid, double* gap, double* nrm, double* wit,
+                         int* ncand, double* kgap, double* kn, double* kw, int* kb);
+void port_ca_query_sparse(const port_grid_spec* s, int bd, int nblocks, const int* ijk,
+                          int stride, const uint8_t* count, const float* cphi, const float* cn,
+                          const int* cbr, const double* pts, int64_t n, uint8_t* valid,
+                          double* gap, double* nrm, double* wit, int* ncand, double* kgap,
+                          double* kn, double* kw, int* kb);
+
 void port_set_threads(int n);
 
 #ifdef __cplusplus

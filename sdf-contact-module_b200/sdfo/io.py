@@ -208,43 +208,67 @@ def load(path: str) -> dict:
     return load_sparse(path) if is_sparse_sdf(path) else load_dense(path)
 
 
-def save_dense(path: str, spec: dict, phi, normal, hessian=None, witness=None) -> bool:
-    """saveSdf (SdfIO.cpp:93-183), plain dense layout."""
+def save_dense(path: str, spec: dict, phi, normal, hessian=None, witness=None, ca=None) -> bool:
+    """saveSdf (SdfIO.cpp:93-183); with ``ca`` (dict stride, count (N,),
+    phi (N*s,), normal (N*s,3), branch (N*s,)) the contact-aware dense
+    layout 3."""
     n = int(np.prod(spec["shape"]))
-    reserved = struct.pack("<I", LAYOUT_DENSE)
+    flags = FLAG_HESSIAN | (FLAG_CONTACT_AWARE if ca is not None else 0)
+    reserved = (struct.pack("<II", LAYOUT_DENSE_CA, int(ca["stride"])) if ca is not None
+                else struct.pack("<I", LAYOUT_DENSE))
     try:
         with open(path, "wb") as f:
-            f.write(_header(spec, FLAG_HESSIAN, reserved))
+            f.write(_header(spec, flags, reserved))
             f.write(np.ascontiguousarray(phi, "<f8").reshape(n).tobytes())
             f.write(np.ascontiguousarray(normal, "<f8").reshape(n, 3).tobytes())
             hs = np.zeros((n, 6)) if hessian is None else hessian
             f.write(np.ascontiguousarray(hs, "<f8").reshape(n, 6).tobytes())
             w = np.zeros((n, 3)) if witness is None else witness
             f.write(np.ascontiguousarray(w, "<f8").reshape(n, 3).tobytes())
+            if ca is not None:
+                s = int(ca["stride"])
+                f.write(np.ascontiguousarray(ca["count"], "<u4").reshape(n).tobytes())
+                f.write(np.ascontiguousarray(ca["phi"], "<f8").reshape(n * s).tobytes())
+                f.write(np.ascontiguousarray(ca["normal"], "<f8").reshape(n * s, 3).tobytes())
+                f.write(np.ascontiguousarray(ca["branch"], "<i4").reshape(n * s).tobytes())
     except OSError:
         return False
     return True
 
 
 def save_sparse(path: str, spec: dict, block_dim: int, halo_voxels: int, band_distance: float,
-                ijk, phi, normal, hessian=None) -> bool:
-    """saveSparseSdf (SdfIO.cpp:185-275), plain sparse layout."""
+                ijk, phi, normal, hessian=None, ca=None) -> bool:
+    """saveSparseSdf (SdfIO.cpp:185-275); with ``ca`` (dict stride, count
+    (B,V), phi (B,V*s), normal (B,V*s,3), branch (B,V*s)) the contact-aware
+    sparse layout 4."""
     if block_dim <= 0:
         return False
     ijk = np.ascontiguousarray(ijk, np.int32).reshape(-1, 3)
     B, V = len(ijk), block_dim ** 3
-    flags = FLAG_SPARSE | (FLAG_HESSIAN if hessian is not None else 0)
-    reserved = struct.pack("<IIII", LAYOUT_SPARSE, block_dim, halo_voxels, B) + struct.pack(
-        "<d", band_distance)
+    flags = (FLAG_SPARSE | (FLAG_HESSIAN if hessian is not None else 0) |
+             (FLAG_CONTACT_AWARE if ca is not None else 0))
+    reserved = struct.pack("<IIII", LAYOUT_SPARSE_CA if ca is not None else LAYOUT_SPARSE,
+                           block_dim, halo_voxels, B) + struct.pack("<d", band_distance)
+    if ca is not None:
+        reserved += struct.pack("<I", int(ca["stride"]))
     fields = [("hdr", "<i4", (4,)), ("phi", "<f4", (V,)), ("normal", "<f4", (V, 3))]
     if hessian is not None:
         fields.append(("hessian", "<f4", (V, 6)))
+    if ca is not None:
+        s = int(ca["stride"])
+        fields += [("ca_count", "u1", (V,)), ("ca_phi", "<f4", (V * s,)),
+                   ("ca_normal", "<f4", (V * s, 3)), ("ca_branch", "<i4", (V * s,))]
     rec = np.zeros(B, dtype=np.dtype(fields))
     rec["hdr"][:, :3] = ijk
     rec["phi"] = np.asarray(phi, np.float32).reshape(B, V)
     rec["normal"] = np.asarray(normal, np.float32).reshape(B, V, 3)
     if hessian is not None:
         rec["hessian"] = np.asarray(hessian, np.float32).reshape(B, V, 6)
+    if ca is not None:
+        rec["ca_count"] = np.asarray(ca["count"], np.uint8).reshape(B, V)
+        rec["ca_phi"] = np.asarray(ca["phi"], np.float32).reshape(B, V * s)
+        rec["ca_normal"] = np.asarray(ca["normal"], np.float32).reshape(B, V * s, 3)
+        rec["ca_branch"] = np.asarray(ca["branch"], np.int32).reshape(B, V * s)
     try:
         with open(path, "wb") as f:
             f.write(_header(spec, flags, reserved))
@@ -252,3 +276,145 @@ def save_sparse(path: str, spec: dict, block_dim: int, halo_voxels: int, band_di
     except OSError:
         return False
     return True
+
+
+def load_contact_aware_surface(path: str):
+    """loadContactAwareSurfaceFile (SdfSurfaceMesh.cpp:157-344): the
+    NEXDYN_CONTACT_AWARE_SURFACE 1 text format -- named surfaces, each with an
+    optional row-major 4x4 transform, ``v <id> x y z`` vertices and
+    ``tri <id> <v0> <v1> <v2>`` + three corner normals per triangle; normals
+    are mapped by the inverse transpose of the transform's linear part and
+    normalised.  Returns verts (nv,3), tris (nt,3) int32, corner normals
+    (nt,3,3); raises RuntimeError with the reference's messages."""
+    def err(line_no, msg):
+        return RuntimeError(f"{path}:{line_no}: {msg}")
+
+    def fresh():
+        return dict(active=False, name="", nv=-1, nt=-1, sv=0, st=0, T=np.eye(4), N=np.eye(3),
+                    ids={})
+
+    def close(line_no, st):
+        if not st["active"]:
+            return fresh()
+        if st["nv"] < 0:
+            raise err(line_no, f"surface '{st['name']}' is missing vertices block")
+        if st["nt"] < 0:
+            raise err(line_no, f"surface '{st['name']}' is missing triangles block")
+        if st["sv"] != st["nv"]:
+            raise err(line_no, f"surface '{st['name']}' vertex count mismatch")
+        if st["st"] != st["nt"]:
+            raise err(line_no, f"surface '{st['name']}' triangle count mismatch")
+        return fresh()
+
+    try:
+        f = open(path, "r")
+    except OSError:
+        raise RuntimeError(f"Cannot open contact-aware surface file: {path}") from None
+    verts, tris, cnorm = [], [], []
+    header = False
+    st = fresh()
+    line_no = 0
+    with f:
+        for raw in f:
+            line_no += 1
+            line = raw.split("#", 1)[0].strip()
+            if not line:
+                continue
+            tok = line.split()
+            key = tok[0]
+            if not header:
+                if key != "NEXDYN_CONTACT_AWARE_SURFACE" or len(tok) < 2 or tok[1] != "1":
+                    raise err(line_no, "expected header 'NEXDYN_CONTACT_AWARE_SURFACE 1'")
+                header = True
+                continue
+            if key == "surface":
+                st = close(line_no, st)
+                st["active"] = True
+                if len(tok) < 2:
+                    raise err(line_no, "surface requires a name")
+                st["name"] = tok[1]
+                continue
+            if key == "end":
+                st = close(line_no, st)
+                continue
+            if not st["active"]:
+                raise err(line_no, "expected surface block")
+            if key == "transform":
+                try:
+                    vals = [float(x) for x in tok[1:17]]
+                except ValueError:
+                    vals = []
+                if len(vals) != 16:
+                    raise err(line_no, "transform requires 16 row-major values")
+                T = np.array(vals).reshape(4, 4)
+                L = T[:3, :3]
+                if abs(np.linalg.det(L)) <= 1.0e-15:
+                    raise err(line_no, "transform linear part must be invertible")
+                st["T"] = T
+                st["N"] = np.linalg.inv(L).T
+                continue
+            if key in ("vertices", "triangles"):
+                try:
+                    cnt = int(tok[1])
+                except (IndexError, ValueError):
+                    cnt = -1
+                if cnt < 0:
+                    raise err(line_no, f"{key} requires a non-negative count")
+                st["nv" if key == "vertices" else "nt"] = cnt
+                continue
+            if key == "v":
+                if st["nv"] < 0:
+                    raise err(line_no, "vertex appears before vertices block")
+                try:
+                    vid = int(tok[1])
+                    p = [float(x) for x in tok[2:5]]
+                except (IndexError, ValueError):
+                    p = []
+                if len(p) != 3:
+                    raise err(line_no, "vertex requires: v <id> <x> <y> <z>")
+                if vid in st["ids"]:
+                    raise err(line_no, "duplicate vertex id in surface")
+                st["ids"][vid] = len(verts)
+                hp = st["T"] @ np.array([p[0], p[1], p[2], 1.0])
+                verts.append(hp[:3] / hp[3] if abs(hp[3]) > 1.0e-15 else hp[:3])
+                st["sv"] += 1
+                continue
+            if key == "tri":
+                if st["nt"] < 0:
+                    raise err(line_no, "triangle appears before triangles block")
+                try:
+                    ids = [int(x) for x in tok[2:5]]
+                    nums = [float(x) for x in tok[5:14]]
+                except (IndexError, ValueError):
+                    ids, nums = [], []
+                if len(ids) != 3 or len(nums) != 9:
+                    raise err(line_no, "triangle requires id, 3 vertex ids, and 3 corner normals")
+                nrm = np.array(nums).reshape(3, 3)
+                tri = []
+                for vid in ids:
+                    if vid not in st["ids"]:
+                        raise err(line_no, "triangle references unknown vertex id")
+                    tri.append(st["ids"][vid])
+                out = np.zeros((3, 3))
+                for c in range(3):
+                    m = st["N"] @ nrm[c]
+                    nn = float(np.sqrt(m @ m))
+                    if not np.all(np.isfinite(m)) or not np.isfinite(nn) or nn <= 1.0e-15:
+                        raise err(line_no, "corner normal must be a finite non-zero vector")
+                    out[c] = m / nn
+                e0 = verts[tri[1]] - verts[tri[0]]
+                e1 = verts[tri[2]] - verts[tri[0]]
+                if np.linalg.norm(np.cross(e0, e1)) <= 1.0e-15:
+                    raise err(line_no, "triangle is degenerate")
+                tris.append(tri)
+                cnorm.append(out)
+                st["st"] += 1
+                continue
+            raise err(line_no, f"unknown token '{key}'")
+    if not header:
+        raise RuntimeError(f"{path}: missing contact-aware surface header")
+    close(line_no, st)
+    if not verts or not tris:
+        raise RuntimeError(f"{path}: contact-aware surface contains no triangles")
+    return (np.array(verts, np.float64), np.array(tris, np.int32),
+            np.array(cnorm, np.float64).reshape(-1, 3, 3))

@@ -265,3 +265,60 @@ def write_obj(path: str, verts: np.ndarray, tris: np.ndarray) -> None:
             f.write(f"v {p[0]:.17g} {p[1]:.17g} {p[2]:.17g}\n")
         for t in tris:
             f.write(f"f {t[0] + 1} {t[1] + 1} {t[2] + 1}\n")
+
+
+def corner_normals(verts: np.ndarray, tris: np.ndarray, kind: str = "face",
+                   crease_degrees: float = 30.0) -> np.ndarray:
+    """Per-triangle corner normals (nt, 3, 3) for contact-aware builds
+    (CornerNormalTriangleMesh, SdfSurfaceMesh.h:16-21):
+      "face"   every corner carries its triangle's unit normal (sharp edges);
+      "smooth" area-weighted vertex normals;
+      "crease" vertex normals averaged only over incident faces within
+               ``crease_degrees`` of the corner's own face (smooth surfaces
+               keep their shading, sharp edges stay sharp)."""
+    v = np.asarray(verts, np.float64)
+    t = np.asarray(tris, np.int64)
+    fn, area = face_normals(v, t)
+    if kind == "face":
+        return np.repeat(fn[:, None, :], 3, axis=1).copy()
+    weighted = fn * area[:, None]
+    if kind == "smooth":
+        acc = np.zeros_like(v)
+        for c in range(3):
+            np.add.at(acc, t[:, c], weighted)
+        vn = acc / np.maximum(np.linalg.norm(acc, axis=1, keepdims=True), 1e-300)
+        return vn[t]
+    if kind != "crease":
+        raise ValueError(f"unknown corner-normal kind {kind!r}")
+    cos_c = np.cos(np.deg2rad(crease_degrees))
+    incident = [[] for _ in range(len(v))]
+    for f in range(len(t)):
+        for c in range(3):
+            incident[int(t[f, c])].append(f)
+    out = np.zeros((len(t), 3, 3))
+    for f in range(len(t)):
+        for c in range(3):
+            acc = np.zeros(3)
+            for g in incident[int(t[f, c])]:
+                if fn[g] @ fn[f] >= cos_c:
+                    acc += weighted[g]
+            out[f, c] = acc / max(np.linalg.norm(acc), 1e-300)
+    return out
+
+
+def write_ca_surface(path: str, verts: np.ndarray, tris: np.ndarray, cnormals: np.ndarray,
+                     name: str = "body") -> None:
+    """A NEXDYN_CONTACT_AWARE_SURFACE 1 file (the format
+    loadContactAwareSurfaceFile reads, SdfSurfaceMesh.cpp:157-344), one
+    surface, identity transform, 1-based ids."""
+    with open(path, "w") as f:
+        f.write("NEXDYN_CONTACT_AWARE_SURFACE 1\n")
+        f.write(f"surface {name}\n")
+        f.write(f"vertices {len(verts)}\n")
+        for i, p in enumerate(verts):
+            f.write(f"v {i + 1} {p[0]:.17g} {p[1]:.17g} {p[2]:.17g}\n")
+        f.write(f"triangles {len(tris)}\n")
+        for i, (tri, cn) in enumerate(zip(tris, cnormals)):
+            nums = " ".join(f"{x:.17g}" for x in np.asarray(cn).reshape(-1))
+            f.write(f"tri {i + 1} {tri[0] + 1} {tri[1] + 1} {tri[2] + 1} {nums}\n")
+        f.write("end\n")

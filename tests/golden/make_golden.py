@@ -81,8 +81,13 @@ def ref_queries(g, pts):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", choices=["all", "contact_aware"], default="all")
     a = ap.parse_args()
     ms = meshes()
+    if a.only == "contact_aware":
+        _contact_aware_fixtures(ms)
+        print("contact-aware fixtures written to", HERE)
+        return
 
     # grid setup (SdfBuilder::setupGrid through a tiny build)
     rows = []
@@ -149,7 +154,58 @@ def main():
                      band_voxels=2).save(os.path.join(HERE, "cube16_sparse.sdf"))
 
     _prototype_fixtures(a.reference, ms)
+    _contact_aware_fixtures(ms)
     print("golden fixtures written to", HERE)
+
+
+CA_CASES = [
+    # (file, mesh, corner-normal kind, SdfBuilder::buildContactAware kwargs)
+    ("ca_dense_cube", "cube", "face", dict(target_resolution=16, max_resolution=16)),
+    ("ca_dense_torus", "torus", "smooth", dict(target_resolution=20, max_resolution=20,
+                                               max_candidates=3)),
+    ("ca_sparse_gear", "gear", "crease", dict(target_resolution=32, max_resolution=32, sparse=True,
+                                              band_voxels=3)),
+    ("ca_sparse_cube_notiles", "cube", "face", dict(target_resolution=16, max_resolution=16,
+                                                    sparse=True, band_voxels=2,
+                                                    use_tile_acceleration=False)),
+]
+
+
+def _contact_aware_fixtures(ms):
+    """SdfBuilder::buildContactAware / buildSparseContactAware, queryFast in
+    ContactAware mode with its candidate lists, contact-aware SDFO files and
+    a NEXDYN_CONTACT_AWARE_SURFACE file parsed by the reference."""
+    for fname, mesh, kind, kw in CA_CASES:
+        v, t = ms[mesh]
+        cn = M.corner_normals(v, t, kind)
+        g = ref.build_contact_aware(v, t, cn, padding=0.1, **kw)
+        info = g.info()
+        ca = ref.ca_arrays(g)
+        prim = g.sparse_arrays() if info["sparse"] else g.dense_arrays()
+        pts = query_points(info, 3000, seed=14)
+        q = ref.query_candidates(g, 4, pts)
+        extra = {} if not info["sparse"] else dict(block_dim=info["block_dim"], halo=info["halo"],
+                                                    band=info["band"])
+        np.savez_compressed(
+            os.path.join(HERE, f"{fname}.npz"), verts=v, tris=t, corner_normals=cn,
+            params=np.array(repr(kw)), shape=np.array(info["shape"]), bmin=info["bmin"],
+            bmax=info["bmax"], voxel=info["voxel"], stride=ca["stride"], count=ca["count"],
+            cphi=ca["phi"], cnormal=ca["normal"], cbranch=ca["branch"], pts=pts,
+            **{f"prim_{k}": val for k, val in prim.items() if val is not None},
+            **{f"q_{k}": val for k, val in q.items()}, **extra)
+    v, t = ms["cube"]
+    cn = M.corner_normals(v, t, "face")
+    ref.build_contact_aware(v, t, cn, padding=0.1, target_resolution=8, max_resolution=8).save(
+        os.path.join(HERE, "ca_cube8_dense.sdf"))
+    ref.build_contact_aware(v, t, cn, padding=0.1, target_resolution=16, max_resolution=16,
+                            sparse=True, band_voxels=2).save(
+        os.path.join(HERE, "ca_cube16_sparse.sdf"))
+    v, t = M.torus(0.05, 0.01, 12, 6)
+    path = os.path.join(HERE, "torus_small.ncas")
+    M.write_ca_surface(path, v, t, M.corner_normals(v, t, "smooth"), name="ring")
+    rv, rt, rcn = ref.load_ca_surface(path)
+    np.savez_compressed(os.path.join(HERE, "torus_small_ncas.npz"), verts=rv, tris=rt,
+                        corner_normals=rcn)
 
 
 def _spec_only(v, t, kw):
