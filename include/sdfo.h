@@ -89,7 +89,7 @@ typedef struct
     int32_t block_dim;      /* sparse */
     int32_t halo_voxels;    /* sparse */
     int32_t block_count;    /* sparse: number of stored blocks */
-    int32_t reserved0;
+    int32_t candidate_stride; /* contact-aware candidate slots per voxel, 0 = none */
     double band_distance;   /* sparse */
 } sdfo_grid_info;
 
@@ -112,6 +112,23 @@ typedef struct
     int32_t store_hessian; /* default 1 */
     double band_distance;  /* 0 = band_voxels * voxel */
 } sdfo_sparse_build_params;
+
+/* ContactAwareBuilderParams (SdfBuilder.h:42-55). */
+typedef struct
+{
+    sdfo_build_params base;
+    int32_t max_candidates;            /* default 4; at most 8 are stored */
+    int32_t tile_dim;                  /* default 8 */
+    int32_t use_tile_acceleration;     /* default 1 */
+    int32_t store_hessian;             /* default 1 */
+    double feature_distance_tolerance; /* 0 = 1.5 * voxel */
+    double normal_merge_angle_degrees; /* default 5 */
+    int32_t sparse;                    /* default 0 */
+    int32_t block_dim;                 /* default 8 */
+    int32_t halo_voxels;               /* default 2 */
+    int32_t band_voxels;               /* default 8 */
+    double band_distance;              /* 0 = band_voxels * voxel */
+} sdfo_contact_aware_params;
 
 /* Body state for contact: position r, rotation R (row-major 3x3, body to
  * world), linear velocity v and angular velocity w (world frame). */
@@ -170,6 +187,7 @@ int sdfo_device_check(int device);
 
 void sdfo_build_params_default(sdfo_build_params* p);
 void sdfo_sparse_build_params_default(sdfo_sparse_build_params* p);
+void sdfo_contact_aware_params_default(sdfo_contact_aware_params* p);
 
 /* Host-only grid setup: SdfBuilder::setupGrid (SdfBuilder.cpp:994-1035) with
  * snapToStandardResolution (GridSpec.h:65-74). */
@@ -187,6 +205,20 @@ int sdfo_grid_build_dense(const double* h_verts, int64_t nv, const int32_t* h_tr
  * narrow-band blocks in (bk, bj, bi) order, FP32 payload.  Synchronous. */
 int sdfo_grid_build_sparse(const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
                            const sdfo_sparse_build_params* p, void* stream, sdfo_grid** out);
+
+/* SdfBuilder::buildContactAware / buildSparseContactAware (p->sparse)
+ * (SdfBuilder.cpp:416-821): per voxel up to min(max_candidates, 8)
+ * surface-feature candidates {phi, normal, FNV branch id} from the
+ * triangles within the nearest distance + tolerance, merged by normal angle
+ * and sorted by |phi|; the first is the voxel's phi / n / witness.
+ * h_corner_normals (nt, 3, 3) float64: the three corner normals of each
+ * triangle (CornerNormalTriangleMesh).  At most 512 merged normal groups per
+ * voxel before truncation to max_candidates (more returns
+ * SDFO_ERR_UNSUPPORTED).  Synchronous. */
+int sdfo_grid_build_contact_aware(const double* h_verts, int64_t nv, const int32_t* h_tris,
+                                  int64_t nt, const double* h_corner_normals,
+                                  const sdfo_contact_aware_params* p, void* stream,
+                                  sdfo_grid** out);
 
 /* One mesh of a batched build: host arrays as for sdfo_grid_build_sparse. */
 typedef struct
@@ -253,6 +285,20 @@ int sdfo_grid_copy_payload(const sdfo_grid* g, void* d_dst, void* stream);
  * payload from caller-owned device memory d_phin (stored_voxels float4, not
  * copied, not freed).  Used to differentiate w.r.t. the payload held in a
  * framework tensor.  Must be destroyed before g and before d_phin is freed. */
+/* Contact-aware candidates of a grid (candidate_stride s > 0), host
+ * arrays in stored-voxel order: h_count (N) u8, h_phi (N*s), h_normal
+ * (N*s*3), h_branch (N*s) -- SdfData::contactCandidate* (SdfData.h:46-50)
+ * and SparseSdfBlock::contactCandidate* (SdfData.h:126-129); sparse values
+ * are the stored FP32 widened.  Any output may be NULL. */
+int sdfo_grid_export_candidates(const sdfo_grid* g, uint8_t* h_count, double* h_phi,
+                                double* h_normal, int32_t* h_branch);
+/* Attaches contact-aware candidates (same layout) to a grid made by
+ * sdfo_grid_create_dense / _sparse, e.g. from a contact-aware SDFO file;
+ * call before the grid is queried.  stride 1..8. */
+int sdfo_grid_attach_candidates(sdfo_grid* g, int32_t stride, const uint8_t* h_count,
+                                const double* h_phi, const double* h_normal,
+                                const int32_t* h_branch);
+
 int sdfo_grid_create_view(const sdfo_grid* g, void* d_phin, sdfo_grid** out);
 
 int sdfo_grid_get_info(const sdfo_grid* g, sdfo_grid_info* out);
@@ -337,6 +383,28 @@ int sdfo_query_backward_saved(const sdfo_grid* g, int32_t mode, const float* d_p
                               const float* d_grad, const float* d_hess6, const uint8_t* d_valid,
                               const float* d_dgap, const float* d_dgrad, float* d_dpoints,
                               float* d_dgrid, void* stream);
+
+/* SdfFastQueryResult's candidate list (SdfCommon.h:29-37) for every point:
+ * d_ncand (n) int32, d_kgap (n*8), d_knormal (n*8*3), d_kwitness (n*8*3)
+ * float32, d_kbranch (n*8) int32 (slots past ncand: gap 0, normal (1,0,0),
+ * witness 0, branch -1).  ContactAware on a grid with candidates: each of
+ * the voxel's candidates extrapolated linearly, gap = phi + n.(p - centre)
+ * (SdfOracle.cpp:296-423); otherwise one candidate, the query's own result
+ * with branch 0 (fastFromQueryResult, SdfOracle.cpp:86-120).  Invalid
+ * points: ncand 0.  The main results go to d_gap / d_normal (gapNormal) /
+ * d_witness / d_valid; every output is required; float32 points. */
+int sdfo_query_candidates(const sdfo_grid* g, int32_t mode, const float* d_points, int64_t n,
+                          float* d_gap, float* d_normal, float* d_witness, uint8_t* d_valid,
+                          int32_t* d_ncand, float* d_kgap, float* d_knormal, float* d_kwitness,
+                          int32_t* d_kbranch, void* stream);
+/* sdfo_query_candidates with host buffers (points float32 or float64 per
+ * points_f64); synchronous.  The C++ SdfOracle::queryFast / query /
+ * queryBatch fill their candidate lists from it. */
+int sdfo_query_candidates_host(const sdfo_grid* g, int32_t mode, const void* h_points,
+                               int32_t points_f64, int64_t n, float* h_gap, float* h_normal,
+                               float* h_witness, uint8_t* h_valid, int32_t* h_ncand,
+                               float* h_kgap, float* h_knormal, float* h_kwitness,
+                               int32_t* h_kbranch, void* stream);
 
 /* ---- batched queries over many grids (no reference counterpart) --------- */
 /* Rigid placement of a grid in the world: x_world = R x_grid + t (R

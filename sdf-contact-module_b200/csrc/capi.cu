@@ -85,6 +85,23 @@ void sdfo_sparse_build_params_default(sdfo_sparse_build_params* p)
     p->band_distance = 0.0;
 }
 
+void sdfo_contact_aware_params_default(sdfo_contact_aware_params* p)
+{
+    if (!p) return;
+    sdfo_build_params_default(&p->base);
+    p->max_candidates = 4;
+    p->tile_dim = 8;
+    p->use_tile_acceleration = 1;
+    p->store_hessian = 1;
+    p->feature_distance_tolerance = 0.0;
+    p->normal_merge_angle_degrees = 5.0;
+    p->sparse = 0;
+    p->block_dim = 8;
+    p->halo_voxels = 2;
+    p->band_voxels = 8;
+    p->band_distance = 0.0;
+}
+
 int sdfo_setup_grid(const double* h_verts, int64_t nv, const sdfo_build_params* p,
                     sdfo_grid_info* out)
 {
@@ -121,6 +138,35 @@ int sdfo_grid_build_sparse(const double* h_verts, int64_t nv, const int32_t* h_t
                      "Sparse SDF blockDim must be positive");
         SDFO_REQUIRE(p->block_dim <= 16, SDFO_ERR_UNSUPPORTED, "blockDim above 16 is not provided");
         *out = build_sparse(h_verts, nv, h_tris, nt, *p, as_stream(stream));
+    });
+}
+
+int sdfo_grid_build_contact_aware(const double* h_verts, int64_t nv, const int32_t* h_tris,
+                                  int64_t nt, const double* h_corner_normals,
+                                  const sdfo_contact_aware_params* p, void* stream,
+                                  sdfo_grid** out)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(out != nullptr, SDFO_ERR_INVALID_ARGUMENT, "out is NULL");
+        *out = nullptr;
+        SDFO_REQUIRE(p != nullptr, SDFO_ERR_INVALID_ARGUMENT, "build params are NULL");
+        // SdfBuilder.cpp:419-425 / 554-562
+        SDFO_REQUIRE(nv > 0 && nt > 0 && h_verts && h_tris, SDFO_ERR_EMPTY_MESH,
+                     p->sparse ? "Empty mesh provided to sparse contact-aware SdfBuilder"
+                               : "Empty mesh provided to contact-aware SdfBuilder");
+        SDFO_REQUIRE(h_corner_normals != nullptr, SDFO_ERR_INVALID_ARGUMENT,
+                     p->sparse ? "Sparse contact-aware SDF requires one corner-normal triplet per triangle"
+                               : "Contact-aware SDF requires one corner-normal triplet per triangle");
+        SDFO_REQUIRE(p->max_candidates > 0, SDFO_ERR_INVALID_ARGUMENT,
+                     p->sparse ? "Sparse contact-aware SDF maxCandidates must be positive"
+                               : "Contact-aware SDF maxCandidates must be positive");
+        SDFO_REQUIRE(!p->sparse || p->block_dim > 0, SDFO_ERR_INVALID_ARGUMENT,
+                     "Sparse contact-aware SDF blockDim must be positive");
+        SDFO_REQUIRE(!p->sparse || p->block_dim <= 16, SDFO_ERR_UNSUPPORTED,
+                     "blockDim above 16 is not provided");
+        check_mesh(h_verts, nv, h_tris, nt);
+        check_build_params(&p->base);
+        *out = build_contact_aware(h_verts, nv, h_tris, nt, h_corner_normals, *p, as_stream(stream));
     });
 }
 
@@ -249,6 +295,103 @@ int sdfo_query_backward(const sdfo_grid* g, int32_t mode, const float* d_points,
                      "grid gradient buffer must be 16-byte aligned");
         launch_query_backward(make_view(g), mode, d_points, n, d_dgap, d_dgrad, d_dpoints, d_dgrid,
                               as_stream(stream));
+    });
+}
+
+int sdfo_query_candidates(const sdfo_grid* g, int32_t mode, const float* d_points, int64_t n,
+                          float* d_gap, float* d_normal, float* d_witness, uint8_t* d_valid,
+                          int32_t* d_ncand, float* d_kgap, float* d_knormal, float* d_kwitness,
+                          int32_t* d_kbranch, void* stream)
+{
+    return guarded([&] {
+        check_grid(g);
+        SDFO_REQUIRE(n >= 0, SDFO_ERR_INVALID_ARGUMENT, "negative query count");
+        if (n == 0) return;
+        SDFO_REQUIRE(d_points && d_gap && d_normal && d_witness && d_valid && d_ncand && d_kgap &&
+                         d_knormal && d_kwitness && d_kbranch,
+                     SDFO_ERR_INVALID_ARGUMENT, "every output of sdfo_query_candidates is required");
+        SDFO_REQUIRE(mode >= SDFO_FIRST_ORDER && mode <= SDFO_CONTACT_AWARE,
+                     SDFO_ERR_INVALID_ARGUMENT, "unknown query mode");
+        SDFO_REQUIRE(n <= (int64_t)65535 * 256 * 4096, SDFO_ERR_INVALID_ARGUMENT, "too many queries");
+        const GridView v = make_view(g);
+        const CandidateOutputs co{d_ncand, d_kgap, d_knormal, d_kwitness, d_kbranch};
+        const QueryOutputs o{d_gap, nullptr, d_normal, d_witness, d_valid, nullptr};
+        cudaStream_t s = as_stream(stream);
+        if (mode == SDFO_CONTACT_AWARE && v.ca_stride > 0)
+        {
+            launch_query_ca(v, d_points, false, n, o, co, s);
+            return;
+        }
+        launch_query(v, mode, d_points, false, n, o, s);
+        launch_single_candidate(n, d_gap, d_normal, d_witness, d_valid, co, s);
+    });
+}
+
+int sdfo_query_candidates_host(const sdfo_grid* g, int32_t mode, const void* h_points,
+                               int32_t points_f64, int64_t n, float* h_gap, float* h_normal,
+                               float* h_witness, uint8_t* h_valid, int32_t* h_ncand,
+                               float* h_kgap, float* h_knormal, float* h_kwitness,
+                               int32_t* h_kbranch, void* stream)
+{
+    return guarded([&] {
+        check_grid(g);
+        SDFO_REQUIRE(n >= 0, SDFO_ERR_INVALID_ARGUMENT, "negative query count");
+        if (n == 0) return;
+        SDFO_REQUIRE(h_points && h_gap && h_normal && h_witness && h_valid && h_ncand && h_kgap &&
+                         h_knormal && h_kwitness && h_kbranch,
+                     SDFO_ERR_INVALID_ARGUMENT, "every output of sdfo_query_candidates_host is required");
+        SDFO_REQUIRE(mode >= SDFO_FIRST_ORDER && mode <= SDFO_CONTACT_AWARE,
+                     SDFO_ERR_INVALID_ARGUMENT, "unknown query mode");
+        SDFO_REQUIRE(n <= (int64_t)65535 * 256 * 4096, SDFO_ERR_INVALID_ARGUMENT, "too many queries");
+        cudaStream_t s = as_stream(stream);
+        auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+        const size_t N = (size_t)n;
+        const size_t pb = N * 3 * (points_f64 ? sizeof(double) : sizeof(float));
+        // points | gap | normal | witness | valid | ncand | kgap | knormal | kwitness | kbranch
+        const size_t sizes[10] = {pb, 4 * N, 12 * N, 12 * N, N, 4 * N, 32 * N, 96 * N, 96 * N, 32 * N};
+        size_t need = 0;
+        for (size_t b : sizes) need += up(b);
+        std::lock_guard<std::mutex> lock(g->ws_mutex);
+        if (g->ws_bytes < need)
+        {
+            SDFO_CUDA(cudaStreamSynchronize(s));
+            device_free(g->ws);
+            g->ws = nullptr;
+            g->ws_bytes = 0;
+            g->ws = device_alloc(need);
+            g->ws_bytes = need;
+        }
+        unsigned char* base = static_cast<unsigned char*>(g->ws);
+        unsigned char* d[10];
+        for (int i = 0; i < 10; ++i)
+        {
+            d[i] = base;
+            base += up(sizes[i]);
+        }
+        SDFO_CUDA(cudaMemcpyAsync(d[0], h_points, pb, cudaMemcpyHostToDevice, s));
+        float* gap = reinterpret_cast<float*>(d[1]);
+        float* nrm = reinterpret_cast<float*>(d[2]);
+        float* wit = reinterpret_cast<float*>(d[3]);
+        uint8_t* valid = d[4];
+        const CandidateOutputs co{reinterpret_cast<int32_t*>(d[5]), reinterpret_cast<float*>(d[6]),
+                                  reinterpret_cast<float*>(d[7]), reinterpret_cast<float*>(d[8]),
+                                  reinterpret_cast<int32_t*>(d[9])};
+        const QueryOutputs o{gap, nullptr, nrm, wit, valid, nullptr};
+        const GridView v = make_view(g);
+        if (mode == SDFO_CONTACT_AWARE && v.ca_stride > 0)
+        {
+            launch_query_ca(v, d[0], points_f64 != 0, n, o, co, s);
+        }
+        else
+        {
+            launch_query(v, mode, d[0], points_f64 != 0, n, o, s);
+            launch_single_candidate(n, gap, nrm, wit, valid, co, s);
+        }
+        void* outs[9] = {h_gap, h_normal, h_witness, h_valid, h_ncand, h_kgap, h_knormal, h_kwitness,
+                         h_kbranch};
+        for (int i = 0; i < 9; ++i)
+            SDFO_CUDA(cudaMemcpyAsync(outs[i], d[i + 1], sizes[i + 1], cudaMemcpyDeviceToHost, s));
+        SDFO_CUDA(cudaStreamSynchronize(s));
     });
 }
 

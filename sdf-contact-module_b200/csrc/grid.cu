@@ -73,6 +73,13 @@ GridView make_view(const sdfo_grid* g)
     v.brick_affine = g->d.brick_affine;
     v.xpair = g->d.xpair;
     v.cell8 = g->d.cell8;
+    v.ca_stride = g->ca_stride;
+    v.ca_count = g->d.ca_count;
+    v.ca_phi64 = g->d.ca_phi64;
+    v.ca_n64 = g->d.ca_n64;
+    v.ca_phi32 = g->d.ca_phi32;
+    v.ca_n32 = g->d.ca_n32;
+    v.ca_branch = g->d.ca_branch;
     return v;
 }
 
@@ -259,6 +266,12 @@ sdfo_grid::~sdfo_grid()
     device_free(d.brick_affine);
     device_free(d.xpair);
     device_free(d.cell8);
+    device_free(d.ca_count);
+    device_free(d.ca_phi64);
+    device_free(d.ca_n64);
+    device_free(d.ca_phi32);
+    device_free(d.ca_n32);
+    device_free(d.ca_branch);
 }
 
 using namespace sdfo;
@@ -287,6 +300,7 @@ int sdfo_grid_create_dense(const sdfo_grid_info* info, const double* h_phi,
         const int64_t N = (int64_t)info->shape[0] * info->shape[1] * info->shape[2];
         std::unique_ptr<sdfo_grid> g(new sdfo_grid());
         g->info = *info;
+        g->info.candidate_stride = 0;
         g->info.layout = SDFO_LAYOUT_DENSE;
         g->info.storage = SDFO_STORAGE_FP32;
         g->info.has_hessian = h_hessian6 != nullptr;
@@ -344,6 +358,7 @@ int sdfo_grid_create_sparse(const sdfo_grid_info* info, const int32_t* h_block_i
         const int V = bd * bd * bd;
         std::unique_ptr<sdfo_grid> g(new sdfo_grid());
         g->info = *info;
+        g->info.candidate_stride = 0;
         g->info.layout = SDFO_LAYOUT_SPARSE;
         g->info.storage = SDFO_STORAGE_FP32;
         g->info.has_hessian = h_hessian6 != nullptr;
@@ -578,6 +593,79 @@ int sdfo_grid_copy_payload(const sdfo_grid* g, void* d_dst, void* stream)
         if (g->stored_voxels > 0)
             SDFO_CUDA(cudaMemcpyAsync(d_dst, g->d.phin, sizeof(float4) * g->stored_voxels,
                                       cudaMemcpyDeviceToDevice, as_stream(stream)));
+    });
+}
+
+int sdfo_grid_export_candidates(const sdfo_grid* g, uint8_t* h_count, double* h_phi,
+                                double* h_normal, int32_t* h_branch)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(g != nullptr, SDFO_ERR_INVALID_ARGUMENT, "grid is NULL");
+        SDFO_REQUIRE(g->ca_stride > 0, SDFO_ERR_INVALID_ARGUMENT, "grid has no contact-aware candidates");
+        const int64_t N = g->stored_voxels;
+        const int64_t M = N * g->ca_stride;
+        if (N == 0) return;
+        if (h_count) SDFO_CUDA(cudaMemcpy(h_count, g->d.ca_count, (size_t)N, cudaMemcpyDeviceToHost));
+        if (h_branch)
+            SDFO_CUDA(cudaMemcpy(h_branch, g->d.ca_branch, sizeof(int32_t) * M, cudaMemcpyDeviceToHost));
+        if (g->d.ca_phi64)
+        {
+            if (h_phi) SDFO_CUDA(cudaMemcpy(h_phi, g->d.ca_phi64, sizeof(double) * M, cudaMemcpyDeviceToHost));
+            if (h_normal)
+                SDFO_CUDA(cudaMemcpy(h_normal, g->d.ca_n64, sizeof(double) * 3 * M, cudaMemcpyDeviceToHost));
+            return;
+        }
+        std::vector<float> tmp((size_t)(3 * M));
+        if (h_phi)
+        {
+            SDFO_CUDA(cudaMemcpy(tmp.data(), g->d.ca_phi32, sizeof(float) * M, cudaMemcpyDeviceToHost));
+            for (int64_t i = 0; i < M; ++i) h_phi[i] = (double)tmp[(size_t)i];
+        }
+        if (h_normal)
+        {
+            SDFO_CUDA(cudaMemcpy(tmp.data(), g->d.ca_n32, sizeof(float) * 3 * M, cudaMemcpyDeviceToHost));
+            for (int64_t i = 0; i < 3 * M; ++i) h_normal[i] = (double)tmp[(size_t)i];
+        }
+    });
+}
+
+int sdfo_grid_attach_candidates(sdfo_grid* g, int32_t stride, const uint8_t* h_count,
+                                const double* h_phi, const double* h_normal,
+                                const int32_t* h_branch)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(g && h_count && h_phi && h_normal && h_branch, SDFO_ERR_INVALID_ARGUMENT,
+                     "NULL argument");
+        SDFO_REQUIRE(stride >= 1 && stride <= 8, SDFO_ERR_INVALID_ARGUMENT,
+                     "candidate stride must be 1..8");
+        SDFO_REQUIRE(!g->borrowed && g->ca_stride == 0, SDFO_ERR_INVALID_ARGUMENT,
+                     "candidates can be attached once, to an owning grid");
+        const int64_t N = g->stored_voxels;
+        const int64_t M = N * stride;
+        if (N == 0) return;
+        g->d.ca_count = dalloc<uint8_t>((size_t)N);
+        g->d.ca_branch = dalloc<int32_t>((size_t)M);
+        SDFO_CUDA(cudaMemcpy(g->d.ca_count, h_count, (size_t)N, cudaMemcpyHostToDevice));
+        SDFO_CUDA(cudaMemcpy(g->d.ca_branch, h_branch, sizeof(int32_t) * M, cudaMemcpyHostToDevice));
+        if (g->info.layout == SDFO_LAYOUT_DENSE)
+        {
+            g->d.ca_phi64 = dalloc<double>((size_t)M);
+            g->d.ca_n64 = dalloc<double>((size_t)M * 3);
+            SDFO_CUDA(cudaMemcpy(g->d.ca_phi64, h_phi, sizeof(double) * M, cudaMemcpyHostToDevice));
+            SDFO_CUDA(cudaMemcpy(g->d.ca_n64, h_normal, sizeof(double) * 3 * M, cudaMemcpyHostToDevice));
+        }
+        else
+        {
+            std::vector<float> f((size_t)(3 * M));
+            for (int64_t i = 0; i < M; ++i) f[(size_t)i] = (float)h_phi[i];
+            g->d.ca_phi32 = dalloc<float>((size_t)M);
+            SDFO_CUDA(cudaMemcpy(g->d.ca_phi32, f.data(), sizeof(float) * M, cudaMemcpyHostToDevice));
+            for (int64_t i = 0; i < 3 * M; ++i) f[(size_t)i] = (float)h_normal[i];
+            g->d.ca_n32 = dalloc<float>((size_t)M * 3);
+            SDFO_CUDA(cudaMemcpy(g->d.ca_n32, f.data(), sizeof(float) * 3 * M, cudaMemcpyHostToDevice));
+        }
+        g->ca_stride = stride;
+        g->info.candidate_stride = stride;
     });
 }
 

@@ -433,8 +433,17 @@ void launch_query(const GridView& v, int mode, const void* pts, bool f64, int64_
     case SDFO_FIRST_ORDER: launch_mode<SDFO_FIRST_ORDER>(v, pts, f64, n, o, s); break;
     case SDFO_SECOND_ORDER: launch_mode<SDFO_SECOND_ORDER>(v, pts, f64, n, o, s); break;
     case SDFO_TRILINEAR: launch_mode<SDFO_TRILINEAR>(v, pts, f64, n, o, s); break;
-    case SDFO_TRICUBIC:
-    case SDFO_CONTACT_AWARE: launch_mode<SDFO_TRICUBIC>(v, pts, f64, n, o, s); break;
+    case SDFO_TRICUBIC: launch_mode<SDFO_TRICUBIC>(v, pts, f64, n, o, s); break;
+    case SDFO_CONTACT_AWARE:
+        // grids without candidates answer ContactAware with Tricubic
+        // (SdfOracle.cpp:187-191, 265-268, 371-374)
+        if (v.ca_stride > 0)
+        {
+            launch_query_ca(v, pts, f64, n, o, CandidateOutputs{}, s);
+            return;
+        }
+        launch_mode<SDFO_TRICUBIC>(v, pts, f64, n, o, s);
+        break;
     default: throw Error(SDFO_ERR_INVALID_ARGUMENT, "unknown query mode");
     }
     SDFO_CHECK_LAUNCH();

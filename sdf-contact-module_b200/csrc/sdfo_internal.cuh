@@ -124,6 +124,15 @@ struct GridStorage
     float2* brick_affine = nullptr;
     float4* xpair = nullptr; // 2 float4 per voxel
     float4* cell8 = nullptr; // 2 float4 per voxel
+    // contact-aware candidates, `stride` slots per stored voxel: count (u8),
+    // phi and normal (FP64 for dense grids, FP32 for sparse ones, as the
+    // reference stores them), branch id
+    uint8_t* ca_count = nullptr;
+    double* ca_phi64 = nullptr;
+    double* ca_n64 = nullptr;
+    float* ca_phi32 = nullptr;
+    float* ca_n32 = nullptr;
+    int32_t* ca_branch = nullptr;
 };
 
 } // namespace sdfo
@@ -136,6 +145,7 @@ struct sdfo_grid
     int device = 0;
     int64_t stored_voxels = 0;
     int32_t nb[3] = {0, 0, 0};
+    int ca_stride = 0;      // contact-aware candidate slots per voxel (0 = none)
     bool borrowed = false; // a view: storage belongs to another handle / caller
     // Storage shared by the grids of one batched build (released with the
     // last of them); empty otherwise.
@@ -190,6 +200,14 @@ struct GridView
     //   cell8[v] = phi of the 8 corners of cell v       Trilinear: 1 load / query
     const float4* xpair;
     const float4* cell8;
+    // contact-aware candidates (ca_stride == 0: none)
+    int ca_stride;
+    const uint8_t* ca_count;
+    const double* ca_phi64;
+    const double* ca_n64;
+    const float* ca_phi32;
+    const float* ca_n32;
+    const int32_t* ca_branch;
 };
 
 GridView make_view(const sdfo_grid* g);
@@ -209,6 +227,20 @@ struct QueryOutputs
 };
 void launch_query(const GridView& v, int mode, const void* pts, bool f64, int64_t n,
                   const QueryOutputs& o, cudaStream_t s);
+// Candidate lists of SdfFastQueryResult (NULL kgap: not written).
+struct CandidateOutputs
+{
+    int32_t* ncand;
+    float* kgap;
+    float* knormal;
+    float* kwitness;
+    int32_t* kbranch;
+};
+// ContactAware on a grid with candidates (ca_query.cu).
+void launch_query_ca(const GridView& v, const void* pts, bool f64, int64_t n, const QueryOutputs& o,
+                     const CandidateOutputs& co, cudaStream_t s);
+void launch_single_candidate(int64_t n, const float* gap, const float* unit, const float* wit,
+                             const uint8_t* valid, const CandidateOutputs& co, cudaStream_t s);
 void launch_query_backward(const GridView& v, int mode, const float* pts, int64_t n,
                            const float* dgap, const float* dgrad, float* dpts, float* dgrid,
                            cudaStream_t s);
@@ -237,6 +269,10 @@ sdfo_grid_info setup_grid(const double* verts, int64_t nv, const sdfo_build_para
 // Batched sparse build (batch.cu): one grid per mesh, storage in one arena.
 std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n, cudaStream_t s);
 void set_fill_ctas_per_sm(int k);
+// Contact-aware build (ca_build.cu).
+sdfo_grid* build_contact_aware(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
+                               const double* cnormals, const sdfo_contact_aware_params& p,
+                               cudaStream_t s);
 int bvh_mode();
 void set_bvh_mode(int m);
 

@@ -4,6 +4,7 @@
 // (plugins/SdfOracle/src/SdfBuilder.cpp:364-407, 823-983).
 #include "SdfOracle/SdfBuilder.h"
 
+#include <algorithm>
 #include <chrono>
 #include <stdexcept>
 #include <string>
@@ -74,6 +75,139 @@ struct GridGuard
     ~GridGuard() { sdfo_grid_destroy(g); }
 };
 
+// The dense grid of a handle as the reference's SdfData (FP64 arrays), with
+// its contact-aware candidates when it has them.
+SdfData toDense(const sdfo_grid* g)
+{
+    sdfo_grid_info info;
+    sdfo_grid_get_info(g, &info);
+    SdfData data;
+    data.resize(toSpec(info));
+    const size_t N = static_cast<size_t>(data.spec.totalVoxels());
+    std::vector<double> nrm(3 * N), hes(6 * N), wit(3 * N);
+    if (sdfo_grid_export_dense(g, data.phi0.data(), nrm.data(), hes.data(), wit.data()) != SDFO_OK)
+        throw std::runtime_error(lastError());
+    for (size_t i = 0; i < N; ++i)
+    {
+        data.n0[i] = Eigen::Vector3d(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]);
+        data.witness0[i] = Eigen::Vector3d(wit[3 * i], wit[3 * i + 1], wit[3 * i + 2]);
+        const double* h = &hes[6 * i];
+        Eigen::Matrix3d& H = data.H0[i];
+        H(0, 0) = h[0];
+        H(0, 1) = H(1, 0) = h[1];
+        H(0, 2) = H(2, 0) = h[2];
+        H(1, 1) = h[3];
+        H(1, 2) = H(2, 1) = h[4];
+        H(2, 2) = h[5];
+    }
+    if (info.candidate_stride > 0)
+    {
+        data.resizeContactCandidates(info.candidate_stride);
+        const size_t M = N * static_cast<size_t>(info.candidate_stride);
+        std::vector<double> cn(3 * M);
+        if (sdfo_grid_export_candidates(g, data.contactCandidateCount.data(),
+                                        data.contactCandidatePhi0.data(), cn.data(),
+                                        data.contactCandidateBranchId.data()) != SDFO_OK)
+            throw std::runtime_error(lastError());
+        for (size_t i = 0; i < M; ++i)
+            data.contactCandidateNormal0[i] = Eigen::Vector3d(cn[3 * i], cn[3 * i + 1], cn[3 * i + 2]);
+    }
+    return data;
+}
+
+// The sparse grid of a handle as the reference's SparseSdfData (FP32
+// blocks in stored order), with its contact-aware candidates.
+SparseSdfData toSparse(const sdfo_grid* g)
+{
+    sdfo_grid_info info;
+    sdfo_grid_get_info(g, &info);
+    SparseSdfData s;
+    s.spec = toSpec(info);
+    s.blockDim = info.block_dim;
+    s.haloVoxels = info.halo_voxels;
+    s.bandDistance = info.band_distance;
+    s.hasHessian = info.has_hessian != 0;
+    const size_t B = static_cast<size_t>(info.block_count), V = static_cast<size_t>(s.blockVoxelCount());
+    std::vector<int32_t> ijk(3 * B);
+    std::vector<float> phi(B * V), nrm(3 * B * V), hes(s.hasHessian ? 6 * B * V : 0);
+    if (B > 0 && sdfo_grid_export_sparse(g, ijk.data(), phi.data(), nrm.data(),
+                                         s.hasHessian ? hes.data() : nullptr) != SDFO_OK)
+        throw std::runtime_error(lastError());
+    const size_t S = static_cast<size_t>(std::max(0, info.candidate_stride));
+    std::vector<uint8_t> ccount(S ? B * V : 0);
+    std::vector<double> cphi(S * B * V), cn(3 * S * B * V);
+    std::vector<int32_t> cbr(S * B * V);
+    if (S && B > 0 &&
+        sdfo_grid_export_candidates(g, ccount.data(), cphi.data(), cn.data(), cbr.data()) != SDFO_OK)
+        throw std::runtime_error(lastError());
+    s.contactCandidateStride = static_cast<int>(S);
+    s.blocks.resize(B);
+    for (size_t b = 0; b < B; ++b)
+    {
+        SparseSdfBlock& blk = s.blocks[b];
+        blk.index = {ijk[3 * b], ijk[3 * b + 1], ijk[3 * b + 2]};
+        blk.phi0.assign(phi.begin() + static_cast<long>(b * V), phi.begin() + static_cast<long>((b + 1) * V));
+        blk.normal0.assign(nrm.begin() + static_cast<long>(3 * b * V),
+                           nrm.begin() + static_cast<long>(3 * (b + 1) * V));
+        if (s.hasHessian)
+            blk.hessian0.assign(hes.begin() + static_cast<long>(6 * b * V),
+                                hes.begin() + static_cast<long>(6 * (b + 1) * V));
+        if (S)
+        {
+            blk.contactCandidateCount.assign(ccount.begin() + static_cast<long>(b * V),
+                                             ccount.begin() + static_cast<long>((b + 1) * V));
+            blk.contactCandidatePhi0.resize(V * S);
+            blk.contactCandidateNormal0.resize(3 * V * S);
+            blk.contactCandidateBranchId.resize(V * S);
+            for (size_t i = 0; i < V * S; ++i)
+            {
+                blk.contactCandidatePhi0[i] = static_cast<float>(cphi[b * V * S + i]);
+                blk.contactCandidateBranchId[i] = cbr[b * V * S + i];
+                for (int a = 0; a < 3; ++a)
+                    blk.contactCandidateNormal0[3 * i + static_cast<size_t>(a)] =
+                        static_cast<float>(cn[3 * (b * V * S + i) + static_cast<size_t>(a)]);
+            }
+        }
+    }
+    s.rebuildIndex();
+    return s;
+}
+
+struct CaMesh
+{
+    HostMesh m;
+    std::vector<double> cn;
+};
+
+CaMesh flattenCa(const CornerNormalTriangleMesh& mesh)
+{
+    CaMesh c{flatten(mesh.vertices, mesh.triangles), {}};
+    c.cn.resize(9 * mesh.cornerNormals.size());
+    for (size_t t = 0; t < mesh.cornerNormals.size(); ++t)
+        for (size_t v = 0; v < 3; ++v)
+            for (int a = 0; a < 3; ++a) c.cn[9 * t + 3 * v + static_cast<size_t>(a)] = mesh.cornerNormals[t][v](a);
+    return c;
+}
+
+sdfo_contact_aware_params toCaParams(const ContactAwareBuilderParams& p, bool sparse)
+{
+    sdfo_contact_aware_params q;
+    sdfo_contact_aware_params_default(&q);
+    q.base = toParams(p);
+    q.max_candidates = p.maxCandidates;
+    q.tile_dim = p.tileDim;
+    q.use_tile_acceleration = p.useTileAcceleration ? 1 : 0;
+    q.store_hessian = p.storeHessian ? 1 : 0;
+    q.feature_distance_tolerance = p.featureDistanceTolerance;
+    q.normal_merge_angle_degrees = p.normalMergeAngleDegrees;
+    q.sparse = sparse ? 1 : 0;
+    q.block_dim = p.blockDim;
+    q.halo_voxels = p.haloVoxels;
+    q.band_voxels = p.bandVoxels;
+    q.band_distance = p.bandDistance;
+    return q;
+}
+
 } // namespace
 
 SdfData SdfBuilder::build(const std::vector<Eigen::Vector3d>& vertices,
@@ -91,25 +225,8 @@ SdfData SdfBuilder::build(const std::vector<Eigen::Vector3d>& vertices,
         throw std::runtime_error(lastError());
     sdfo_grid_info info;
     sdfo_grid_get_info(g.g, &info);
-    SdfData data;
-    data.resize(toSpec(info));
+    SdfData data = toDense(g.g);
     const size_t N = static_cast<size_t>(data.spec.totalVoxels());
-    std::vector<double> nrm(3 * N), hes(6 * N), wit(3 * N);
-    if (sdfo_grid_export_dense(g.g, data.phi0.data(), nrm.data(), hes.data(), wit.data()) != SDFO_OK)
-        throw std::runtime_error(lastError());
-    for (size_t i = 0; i < N; ++i)
-    {
-        data.n0[i] = Eigen::Vector3d(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]);
-        data.witness0[i] = Eigen::Vector3d(wit[3 * i], wit[3 * i + 1], wit[3 * i + 2]);
-        const double* h = &hes[6 * i];
-        Eigen::Matrix3d& H = data.H0[i];
-        H(0, 0) = h[0];
-        H(0, 1) = H(1, 0) = h[1];
-        H(0, 2) = H(2, 0) = h[2];
-        H(1, 1) = h[3];
-        H(1, 2) = H(2, 1) = h[4];
-        H(2, 2) = h[5];
-    }
     log(params, "[SdfBuilder] Grid: " + std::to_string(info.shape[0]) + " x " +
                     std::to_string(info.shape[1]) + " x " + std::to_string(info.shape[2]) + " = " +
                     std::to_string(N) + " voxels (GPU, " +
@@ -144,33 +261,8 @@ SparseSdfData SdfBuilder::buildSparse(const std::vector<Eigen::Vector3d>& vertic
     if (sdfo_grid_build_sparse(m.v.data(), static_cast<int64_t>(vertices.size()), m.t.data(),
                                static_cast<int64_t>(triangles.size()), &p, nullptr, &g.g) != SDFO_OK)
         throw std::runtime_error(lastError());
-    sdfo_grid_info info;
-    sdfo_grid_get_info(g.g, &info);
-    SparseSdfData s;
-    s.spec = toSpec(info);
-    s.blockDim = info.block_dim;
-    s.haloVoxels = info.halo_voxels;
-    s.bandDistance = info.band_distance;
-    s.hasHessian = info.has_hessian != 0;
-    const size_t B = static_cast<size_t>(info.block_count), V = static_cast<size_t>(s.blockVoxelCount());
-    std::vector<int32_t> ijk(3 * B);
-    std::vector<float> phi(B * V), nrm(3 * B * V), hes(s.hasHessian ? 6 * B * V : 0);
-    if (sdfo_grid_export_sparse(g.g, ijk.data(), phi.data(), nrm.data(),
-                                s.hasHessian ? hes.data() : nullptr) != SDFO_OK)
-        throw std::runtime_error(lastError());
-    s.blocks.resize(B);
-    for (size_t b = 0; b < B; ++b)
-    {
-        SparseSdfBlock& blk = s.blocks[b];
-        blk.index = {ijk[3 * b], ijk[3 * b + 1], ijk[3 * b + 2]};
-        blk.phi0.assign(phi.begin() + static_cast<long>(b * V), phi.begin() + static_cast<long>((b + 1) * V));
-        blk.normal0.assign(nrm.begin() + static_cast<long>(3 * b * V),
-                           nrm.begin() + static_cast<long>(3 * (b + 1) * V));
-        if (s.hasHessian)
-            blk.hessian0.assign(hes.begin() + static_cast<long>(6 * b * V),
-                                hes.begin() + static_cast<long>(6 * (b + 1) * V));
-    }
-    s.rebuildIndex();
+    SparseSdfData s = toSparse(g.g);
+    const size_t B = s.blocks.size();
     log(params, "[SdfBuilder] Sparse SDF blocks: " + std::to_string(B));
     return s;
 }
@@ -189,7 +281,16 @@ SdfData SdfBuilder::buildContactAware(const CornerNormalTriangleMesh& mesh,
         throw std::runtime_error("Contact-aware SDF requires one corner-normal triplet per triangle");
     if (params.maxCandidates <= 0)
         throw std::runtime_error("Contact-aware SDF maxCandidates must be positive");
-    throw std::runtime_error("Contact-aware SDF builds are not provided by the GPU backend");
+    const CaMesh m = flattenCa(mesh);
+    const sdfo_contact_aware_params p = toCaParams(params, false);
+    GridGuard g;
+    if (sdfo_grid_build_contact_aware(m.m.v.data(), static_cast<int64_t>(mesh.vertices.size()),
+                                      m.m.t.data(), static_cast<int64_t>(mesh.triangles.size()),
+                                      m.cn.data(), &p, nullptr, &g.g) != SDFO_OK)
+        throw std::runtime_error(lastError());
+    SdfData data = toDense(g.g);
+    log(params, "[SdfBuilder] Contact-aware grid built on the GPU");
+    return data;
 }
 
 SparseSdfData SdfBuilder::buildSparseContactAware(const CornerNormalTriangleMesh& mesh,
@@ -204,7 +305,16 @@ SparseSdfData SdfBuilder::buildSparseContactAware(const CornerNormalTriangleMesh
         throw std::runtime_error("Sparse contact-aware SDF maxCandidates must be positive");
     if (params.blockDim <= 0)
         throw std::runtime_error("Sparse contact-aware SDF blockDim must be positive");
-    throw std::runtime_error("Contact-aware SDF builds are not provided by the GPU backend");
+    const CaMesh m = flattenCa(mesh);
+    const sdfo_contact_aware_params p = toCaParams(params, true);
+    GridGuard g;
+    if (sdfo_grid_build_contact_aware(m.m.v.data(), static_cast<int64_t>(mesh.vertices.size()),
+                                      m.m.t.data(), static_cast<int64_t>(mesh.triangles.size()),
+                                      m.cn.data(), &p, nullptr, &g.g) != SDFO_OK)
+        throw std::runtime_error(lastError());
+    SparseSdfData s = toSparse(g.g);
+    log(params, "[SdfBuilder] Sparse contact-aware SDF blocks: " + std::to_string(s.blocks.size()));
+    return s;
 }
 
 } // namespace sdf

@@ -2,9 +2,11 @@
 // for the behaviour kept): the oracle owns its host data; its device copy is
 // created on the first query and shared by copies of the oracle.  Every
 // query mode runs on the GPU; results match the reference's queryFast to the
-// FP32 storage / arithmetic tolerance (1e-5 relative).
+// FP32 storage / arithmetic tolerance (1e-5 relative); ContactAware queries
+// on grids with candidates return the reference's candidate lists.
 #include "SdfOracle/SdfOracle.h"
 
+#include <algorithm>
 #include <stdexcept>
 #include <vector>
 
@@ -121,6 +123,43 @@ const sdfo_grid* SdfOracle::deviceGrid() const
                                      s.hasHessian ? hes.data() : nullptr, nullptr, &g);
     }
     if (rc != SDFO_OK) throw std::runtime_error(lastError());
+    // contact-aware candidates travel with the grid
+    if (!m_sparse && m_data.hasContactCandidates())
+    {
+        const SdfData& d = m_data;
+        std::vector<double> cn(3 * d.contactCandidateNormal0.size());
+        for (size_t i = 0; i < d.contactCandidateNormal0.size(); ++i)
+            for (int a = 0; a < 3; ++a) cn[3 * i + static_cast<size_t>(a)] = d.contactCandidateNormal0[i](a);
+        rc = sdfo_grid_attach_candidates(g, d.contactCandidateStride, d.contactCandidateCount.data(),
+                                         d.contactCandidatePhi0.data(), cn.data(),
+                                         d.contactCandidateBranchId.data());
+    }
+    else if (m_sparse && m_sparseData.hasContactCandidates())
+    {
+        const SparseSdfData& sp = m_sparseData;
+        const size_t V = static_cast<size_t>(sp.blockVoxelCount());
+        const size_t S = static_cast<size_t>(sp.contactCandidateStride);
+        std::vector<uint8_t> cnt;
+        std::vector<double> ph, cn;
+        std::vector<int32_t> br;
+        for (const SparseSdfBlock& blk : sp.blocks)
+        {
+            cnt.insert(cnt.end(), blk.contactCandidateCount.begin(), blk.contactCandidateCount.begin() + static_cast<long>(V));
+            for (size_t i = 0; i < V * S; ++i)
+            {
+                ph.push_back(blk.contactCandidatePhi0[i]);
+                br.push_back(blk.contactCandidateBranchId[i]);
+                for (int a = 0; a < 3; ++a) cn.push_back(blk.contactCandidateNormal0[3 * i + static_cast<size_t>(a)]);
+            }
+        }
+        rc = sdfo_grid_attach_candidates(g, static_cast<int32_t>(S), cnt.data(), ph.data(), cn.data(), br.data());
+    }
+    if (rc != SDFO_OK)
+    {
+        const std::string err = lastError();
+        sdfo_grid_destroy(g);
+        throw std::runtime_error(err);
+    }
     m_device->g = g;
     return g;
 }
@@ -128,30 +167,61 @@ const sdfo_grid* SdfOracle::deviceGrid() const
 void SdfOracle::runQueries(const double* points, size_t n, QueryMode mode, float* gap,
                            float* normal, float* witness, unsigned char* valid) const
 {
-    const bool ca = m_sparse ? m_sparseData.hasContactCandidates() : m_data.hasContactCandidates();
-    if (mode == QueryMode::ContactAware && ca)
-        throw std::runtime_error("contact-aware candidate queries are not provided by the GPU backend");
     const sdfo_grid* g = deviceGrid();
     if (sdfo_query_host(g, modeId(mode), points, SDFO_POINTS_F64, static_cast<int64_t>(n), gap, nullptr,
                         normal, witness, valid, nullptr) != SDFO_OK)
         throw std::runtime_error(lastError());
 }
 
+namespace {
+
+// Per-point results with the candidate lists of SdfFastQueryResult.
+struct CandidateBatch
+{
+    std::vector<float> gap, nrm, wit, kgap, kn, kw;
+    std::vector<unsigned char> valid;
+    std::vector<int32_t> ncand, kb;
+    explicit CandidateBatch(size_t n)
+        : gap(n), nrm(3 * n), wit(3 * n), kgap(8 * n), kn(24 * n), kw(24 * n), valid(n), ncand(n), kb(8 * n)
+    {
+    }
+    SdfFastQueryResult at(size_t i) const
+    {
+        SdfFastQueryResult r;
+        r.valid = valid[i] != 0;
+        if (!r.valid) return r;
+        r.gap = gap[i];
+        r.gapNormal = Eigen::Vector3d(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]);
+        r.witnessPoint = Eigen::Vector3d(wit[3 * i], wit[3 * i + 1], wit[3 * i + 2]);
+        r.candidateCount = std::min(ncand[i], kMaxSdfQueryCandidates);
+        for (int c = 0; c < r.candidateCount; ++c)
+        {
+            const size_t k = 8 * i + static_cast<size_t>(c);
+            r.candidates[static_cast<size_t>(c)] = SdfQueryCandidate{
+                kgap[k], Eigen::Vector3d(kn[3 * k], kn[3 * k + 1], kn[3 * k + 2]),
+                Eigen::Vector3d(kw[3 * k], kw[3 * k + 1], kw[3 * k + 2]), kb[k]};
+        }
+        return r;
+    }
+};
+
+void queryCandidates(const sdfo_grid* g, QueryMode mode, const double* pts, size_t n, CandidateBatch& b)
+{
+    if (sdfo_query_candidates_host(g, modeId(mode), pts, SDFO_POINTS_F64, static_cast<int64_t>(n),
+                                   b.gap.data(), b.nrm.data(), b.wit.data(), b.valid.data(),
+                                   b.ncand.data(), b.kgap.data(), b.kn.data(), b.kw.data(), b.kb.data(),
+                                   nullptr) != SDFO_OK)
+        throw std::runtime_error(lastError());
+}
+
+} // namespace
+
 SdfFastQueryResult SdfOracle::queryFast(const Eigen::Vector3d& point, QueryMode mode) const
 {
-    SdfFastQueryResult r;
-    if (!isValid()) return r;
-    float gap = 0.f, nrm[3], wit[3];
-    unsigned char valid = 0;
-    runQueries(point.data(), 1, mode, &gap, nrm, wit, &valid);
-    r.valid = valid != 0;
-    if (!r.valid) return r;
-    r.gap = gap;
-    r.gapNormal = Eigen::Vector3d(nrm[0], nrm[1], nrm[2]);
-    r.witnessPoint = Eigen::Vector3d(wit[0], wit[1], wit[2]);
-    r.candidateCount = 1;
-    r.candidates[0] = SdfQueryCandidate{r.gap, r.gapNormal, r.witnessPoint, 0};
-    return r;
+    if (!isValid()) return SdfFastQueryResult{};
+    CandidateBatch b(1);
+    queryCandidates(deviceGrid(), mode, point.data(), 1, b);
+    return b.at(0);
 }
 
 SdfQueryResult SdfOracle::query(const Eigen::Vector3d& point, QueryMode mode) const
@@ -162,7 +232,7 @@ SdfQueryResult SdfOracle::query(const Eigen::Vector3d& point, QueryMode mode) co
     r.gapNormal = f.gapNormal;
     r.witnessPoint = f.witnessPoint;
     r.valid = f.valid;
-    if (f.valid) r.candidates.push_back(f.candidates[0]);
+    for (int c = 0; c < f.candidateCount; ++c) r.candidates.push_back(f.candidates[static_cast<size_t>(c)]);
     return r;
 }
 
@@ -175,18 +245,18 @@ std::vector<SdfQueryResult> SdfOracle::queryBatch(const std::vector<Eigen::Vecto
     std::vector<double> p(3 * n);
     for (size_t i = 0; i < n; ++i)
         for (int a = 0; a < 3; ++a) p[3 * i + static_cast<size_t>(a)] = points[i](a);
-    std::vector<float> gap(n), nrm(3 * n), wit(3 * n);
-    std::vector<unsigned char> valid(n);
-    runQueries(p.data(), n, mode, gap.data(), nrm.data(), wit.data(), valid.data());
+    CandidateBatch b(n);
+    queryCandidates(deviceGrid(), mode, p.data(), n, b);
     for (size_t i = 0; i < n; ++i)
     {
+        const SdfFastQueryResult f = b.at(i);
         SdfQueryResult& r = out[i];
-        r.valid = valid[i] != 0;
+        r.valid = f.valid;
         if (!r.valid) continue;
-        r.gap = gap[i];
-        r.gapNormal = Eigen::Vector3d(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]);
-        r.witnessPoint = Eigen::Vector3d(wit[3 * i], wit[3 * i + 1], wit[3 * i + 2]);
-        r.candidates.push_back(SdfQueryCandidate{r.gap, r.gapNormal, r.witnessPoint, 0});
+        r.gap = f.gap;
+        r.gapNormal = f.gapNormal;
+        r.witnessPoint = f.witnessPoint;
+        for (int c = 0; c < f.candidateCount; ++c) r.candidates.push_back(f.candidates[static_cast<size_t>(c)]);
     }
     return out;
 }

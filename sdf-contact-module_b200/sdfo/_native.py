@@ -33,7 +33,7 @@ _D = ctypes.c_double
 class GridInfo(ctypes.Structure):
     _fields_ = [("bmin", _D * 3), ("bmax", _D * 3), ("voxel", _D * 3), ("shape", _I32 * 3),
                 ("layout", _I32), ("storage", _I32), ("has_hessian", _I32), ("block_dim", _I32),
-                ("halo_voxels", _I32), ("block_count", _I32), ("reserved0", _I32),
+                ("halo_voxels", _I32), ("block_count", _I32), ("candidate_stride", _I32),
                 ("band_distance", _D)]
 
 
@@ -45,6 +45,14 @@ class BuildParams(ctypes.Structure):
 class SparseBuildParams(ctypes.Structure):
     _fields_ = [("base", BuildParams), ("block_dim", _I32), ("halo_voxels", _I32),
                 ("band_voxels", _I32), ("store_hessian", _I32), ("band_distance", _D)]
+
+
+class ContactAwareParams(ctypes.Structure):
+    _fields_ = [("base", BuildParams), ("max_candidates", _I32), ("tile_dim", _I32),
+                ("use_tile_acceleration", _I32), ("store_hessian", _I32),
+                ("feature_distance_tolerance", _D), ("normal_merge_angle_degrees", _D),
+                ("sparse", _I32), ("block_dim", _I32), ("halo_voxels", _I32),
+                ("band_voxels", _I32), ("band_distance", _D)]
 
 
 class MeshDesc(ctypes.Structure):
@@ -84,11 +92,14 @@ SIGNATURES = [
     ("sdfo_device_check", ctypes.c_int, [ctypes.c_int]),
     ("sdfo_build_params_default", None, [ctypes.POINTER(BuildParams)]),
     ("sdfo_sparse_build_params_default", None, [ctypes.POINTER(SparseBuildParams)]),
+    ("sdfo_contact_aware_params_default", None, [ctypes.POINTER(ContactAwareParams)]),
     ("sdfo_setup_grid", ctypes.c_int, [_P, _I64, ctypes.POINTER(BuildParams), ctypes.POINTER(GridInfo)]),
     ("sdfo_grid_build_dense", ctypes.c_int,
      [_P, _I64, _P, _I64, ctypes.POINTER(BuildParams), _P, ctypes.POINTER(_P)]),
     ("sdfo_grid_build_sparse", ctypes.c_int,
      [_P, _I64, _P, _I64, ctypes.POINTER(SparseBuildParams), _P, ctypes.POINTER(_P)]),
+    ("sdfo_grid_build_contact_aware", ctypes.c_int,
+     [_P, _I64, _P, _I64, _P, ctypes.POINTER(ContactAwareParams), _P, ctypes.POINTER(_P)]),
     ("sdfo_grid_build_sparse_batched", ctypes.c_int,
      [ctypes.POINTER(MeshDesc), _I32, _P, ctypes.POINTER(_P)]),
     ("sdfo_set_fill_ctas_per_sm", ctypes.c_int, [_I32]),
@@ -103,6 +114,8 @@ SIGNATURES = [
     ("sdfo_grid_export_dense", ctypes.c_int, [_P, _P, _P, _P, _P]),
     ("sdfo_grid_export_sparse", ctypes.c_int, [_P, _P, _P, _P, _P]),
     ("sdfo_grid_copy_payload", ctypes.c_int, [_P, _P, _P]),
+    ("sdfo_grid_export_candidates", ctypes.c_int, [_P, _P, _P, _P, _P]),
+    ("sdfo_grid_attach_candidates", ctypes.c_int, [_P, _I32, _P, _P, _P, _P]),
     ("sdfo_grid_create_view", ctypes.c_int, [_P, _P, ctypes.POINTER(_P)]),
     ("sdfo_grid_get_info", ctypes.c_int, [_P, ctypes.POINTER(GridInfo)]),
     ("sdfo_grid_device_views", ctypes.c_int, [_P, ctypes.POINTER(DeviceViews)]),
@@ -111,6 +124,10 @@ SIGNATURES = [
     ("sdfo_query_host", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P, _P, _P]),
     ("sdfo_query_host_static", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P]),
     ("sdfo_query_backward", ctypes.c_int, [_P, _I32, _P, _I64, _P, _P, _P, _P, _P]),
+    ("sdfo_query_candidates", ctypes.c_int,
+     [_P, _I32, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    ("sdfo_query_candidates_host", ctypes.c_int,
+     [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     ("sdfo_query_linearize", ctypes.c_int, [_P, _I32, _P, _I64, _P, _P, _P, _P, _P]),
     ("sdfo_query_backward_saved", ctypes.c_int,
      [_P, _I32, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P]),

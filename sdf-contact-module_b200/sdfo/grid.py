@@ -88,6 +88,7 @@ class SdfGrid:
         self.block_count = int(info.block_count)
         self.band_distance = float(info.band_distance)
         self.storage = int(info.storage)
+        self.candidate_stride = int(info.candidate_stride)
         views = N.DeviceViews()
         N.check(self._lib.sdfo_grid_device_views(self._h, ctypes.byref(views)))
         self.stored_voxels = int(views.stored_voxels)
@@ -132,6 +133,92 @@ class SdfGrid:
                                            ctypes.byref(p), _stream_ptr(stream),
                                            ctypes.byref(out)))
         return cls(out.value, mode)
+
+    @classmethod
+    def build_contact_aware(cls, verts, tris, corner_normals, padding=0.1, voxel_size=0.0,
+                            target_resolution=128, max_resolution=512, max_candidates=4,
+                            feature_distance_tolerance=0.0, normal_merge_angle_degrees=5.0,
+                            tile_dim=8, use_tile_acceleration=True, store_hessian=True,
+                            sparse=False, block_dim=8, halo_voxels=2, band_voxels=8,
+                            band_distance=0.0, mode=N.CONTACT_AWARE, stream=None) -> "SdfGrid":
+        """SdfBuilder::buildContactAware / buildSparseContactAware
+        (SdfBuilder.cpp:416-821) on the GPU; corner_normals (nt, 3, 3)."""
+        v, t = cls._mesh(verts, tris)
+        cn = np.ascontiguousarray(corner_normals, np.float64).reshape(-1, 3, 3)
+        if len(cn) != len(t):
+            raise ValueError("one corner-normal triplet per triangle is required")
+        lib = N.load()
+        p = N.ContactAwareParams()
+        lib.sdfo_contact_aware_params_default(ctypes.byref(p))
+        p.base = N.BuildParams(padding, voxel_size, target_resolution, max_resolution)
+        p.max_candidates = max_candidates
+        p.tile_dim = tile_dim
+        p.use_tile_acceleration = 1 if use_tile_acceleration else 0
+        p.store_hessian = 1 if store_hessian else 0
+        p.feature_distance_tolerance = feature_distance_tolerance
+        p.normal_merge_angle_degrees = normal_merge_angle_degrees
+        p.sparse = 1 if sparse else 0
+        p.block_dim = block_dim
+        p.halo_voxels = halo_voxels
+        p.band_voxels = band_voxels
+        p.band_distance = band_distance
+        out = ctypes.c_void_p()
+        N.check(lib.sdfo_grid_build_contact_aware(_np_ptr(v), len(v), _np_ptr(t), len(t),
+                                                  _np_ptr(cn), ctypes.byref(p), _stream_ptr(stream),
+                                                  ctypes.byref(out)))
+        return cls(out.value, mode)
+
+    def export_candidates(self) -> dict:
+        """Contact-aware candidates in stored-voxel order: stride, count (N,),
+        phi (N,s), normal (N,s,3), branch (N,s) (sparse: FP32 values)."""
+        s = self.candidate_stride
+        if s <= 0:
+            raise ValueError("grid has no contact-aware candidates")
+        n = self.stored_voxels
+        out = dict(stride=s, count=np.zeros(n, np.uint8), phi=np.zeros((n, s)),
+                   normal=np.zeros((n, s, 3)), branch=np.zeros((n, s), np.int32))
+        _torch().cuda.synchronize()
+        N.check(self._lib.sdfo_grid_export_candidates(self.handle, _np_ptr(out["count"]),
+                                                      _np_ptr(out["phi"]), _np_ptr(out["normal"]),
+                                                      _np_ptr(out["branch"])))
+        return out
+
+    def attach_candidates(self, stride, count, phi, normal, branch) -> None:
+        """Contact-aware candidates for a grid made from host data (e.g. a
+        contact-aware SDFO file); stored-voxel order as export_candidates."""
+        n = self.stored_voxels
+        cnt = np.ascontiguousarray(count, np.uint8).reshape(n)
+        ph = np.ascontiguousarray(phi, np.float64).reshape(n * stride)
+        nr = np.ascontiguousarray(normal, np.float64).reshape(n * stride * 3)
+        br = np.ascontiguousarray(branch, np.int32).reshape(n * stride)
+        N.check(self._lib.sdfo_grid_attach_candidates(self.handle, int(stride), _np_ptr(cnt),
+                                                      _np_ptr(ph), _np_ptr(nr), _np_ptr(br)))
+        self._refresh_info()
+
+    def query_candidates(self, points, mode=None, stream=None) -> dict:
+        """queryFast with its candidate list (SdfFastQueryResult): dict of CUDA
+        tensors gap (N,), normal (N,3), witness (N,3), valid (N,), ncand (N,),
+        kgap (N,8), knormal (N,8,3), kwitness (N,8,3), kbranch (N,8)."""
+        torch = _torch()
+        pts = points.contiguous().reshape(-1, 3)
+        if pts.dtype != torch.float32 or not pts.is_cuda:
+            raise ValueError("points must be a CUDA float32 tensor")
+        n = pts.shape[0]
+        d = pts.device
+        f = dict(dtype=torch.float32, device=d)
+        out = dict(gap=torch.empty(n, **f), normal=torch.empty((n, 3), **f),
+                   witness=torch.empty((n, 3), **f),
+                   valid=torch.empty(n, dtype=torch.uint8, device=d),
+                   ncand=torch.empty(n, dtype=torch.int32, device=d), kgap=torch.empty((n, 8), **f),
+                   knormal=torch.empty((n, 8, 3), **f), kwitness=torch.empty((n, 8, 3), **f),
+                   kbranch=torch.empty((n, 8), dtype=torch.int32, device=d))
+        m = self.mode if mode is None else N.mode_id(mode)
+        N.check(self._lib.sdfo_query_candidates(
+            self.handle, m, _t_ptr(pts), n, _t_ptr(out["gap"]), _t_ptr(out["normal"]),
+            _t_ptr(out["witness"]), _t_ptr(out["valid"]), _t_ptr(out["ncand"]), _t_ptr(out["kgap"]),
+            _t_ptr(out["knormal"]), _t_ptr(out["kwitness"]), _t_ptr(out["kbranch"]),
+            _stream_ptr(stream)))
+        return out
 
     @classmethod
     def build_sparse_batched(cls, meshes, mode=N.TRILINEAR, stream=None) -> list:
@@ -401,19 +488,38 @@ class SdfGrid:
 
         d = sio.load(path)
         if d["layout"] == "sparse":
-            return cls.from_sparse(d["spec"], d["block_dim"], d["ijk"], d["phi"], d["normal"],
-                                   d["hessian"], d["halo_voxels"], d["band_distance"], mode)
-        return cls.from_dense(d["spec"], d["phi"], d["normal"], d["hessian"], d["witness"], mode)
+            g = cls.from_sparse(d["spec"], d["block_dim"], d["ijk"], d["phi"], d["normal"],
+                                d["hessian"], d["halo_voxels"], d["band_distance"], mode)
+        else:
+            g = cls.from_dense(d["spec"], d["phi"], d["normal"], d["hessian"], d["witness"], mode)
+        if "ca" in d:
+            ca = d["ca"]
+            g.attach_candidates(ca["stride"], ca["count"], ca["phi"], ca["normal"], ca["branch"])
+        return g
 
     def save(self, path: str) -> bool:
         """saveSdf / saveSparseSdf (SdfIO.cpp:93-275) of the device grid."""
         from . import io as sio
 
+        ca = None
+        if self.candidate_stride > 0:
+            c = self.export_candidates()
+            s = c["stride"]
+            if self.is_sparse:
+                V = self.block_dim ** 3
+                B = self.block_count
+                ca = dict(stride=s, count=c["count"].reshape(B, V),
+                          phi=c["phi"].reshape(B, V * s).astype(np.float32),
+                          normal=c["normal"].reshape(B, V * s, 3).astype(np.float32),
+                          branch=c["branch"].reshape(B, V * s))
+            else:
+                ca = dict(stride=s, count=c["count"], phi=c["phi"].reshape(-1),
+                          normal=c["normal"].reshape(-1, 3), branch=c["branch"].reshape(-1))
         if self.is_sparse:
             d = self.export_sparse()
             return sio.save_sparse(path, self.spec(), self.block_dim, self.halo_voxels,
                                    self.band_distance, d["ijk"], d["phi"], d["normal"],
-                                   d["hessian"])
+                                   d["hessian"], ca=ca)
         d = self.export_dense()
         return sio.save_dense(path, self.spec(), d["phi"], d["normal"], d["hessian"],
-                              d["witness"])
+                              d["witness"], ca=ca)

@@ -21,7 +21,8 @@ def check_bin():
     return CHECK
 
 
-@pytest.mark.parametrize("name", ["cube8_dense.sdf", "cube16_sparse.sdf"])
+@pytest.mark.parametrize("name", ["cube8_dense.sdf", "cube16_sparse.sdf", "ca_cube8_dense.sdf",
+                                  "ca_cube16_sparse.sdf"])
 def test_cpp_io_round_trip_is_byte_exact(check_bin, tmp_path, name):
     src = os.path.join(GOLDEN, name)
     dst = str(tmp_path / name)
@@ -124,3 +125,58 @@ def test_cpp_build_and_query_batch(cuda, port, check_bin, tmp_path):
             assert np.array_equal(valid, ref["valid"])
             assert np.all(np.abs(out[valid, 0] - ref["gap"][valid]) <=
                           1e-5 * np.maximum(np.abs(ref["gap"][valid]), h))
+
+
+def test_cpp_contact_aware_surface_loader(check_bin, tmp_path):
+    """loadContactAwareSurfaceFile of the C++ API against the reference's
+    parse of the same file."""
+    from conftest import golden
+
+    out = str(tmp_path / "surf.bin")
+    subprocess.run([check_bin, "surface", os.path.join(GOLDEN, "torus_small.ncas"), out], check=True)
+    raw = np.fromfile(out)
+    nv, nt = int(raw[0]), int(raw[1])
+    g = golden("torus_small_ncas.npz")
+    v = raw[2:2 + 3 * nv].reshape(nv, 3)
+    t = raw[2 + 3 * nv:2 + 3 * nv + 3 * nt].reshape(nt, 3).astype(np.int32)
+    cn = raw[2 + 3 * nv + 3 * nt:].reshape(nt, 3, 3)
+    assert np.array_equal(v, g["verts"]) and np.array_equal(t, g["tris"])
+    assert np.allclose(cn, g["corner_normals"], rtol=0, atol=1e-15)
+
+
+@pytest.mark.gpu
+def test_cpp_contact_aware_build_and_queries(cuda, ref, check_bin, tmp_path):
+    """SdfBuilder::buildContactAware / buildSparseContactAware of the C++ API
+    (GPU) save the reference's bytes; SdfOracle::queryBatch(ContactAware)
+    returns the reference's candidate lists."""
+    from sdfo import io as sio
+
+    surf = os.path.join(GOLDEN, "torus_small.ncas")
+    v, t, cn = ref.load_ca_surface(surf)
+    R = ref.build_contact_aware(v, t, cn, target_resolution=24, max_resolution=24)
+    Rs = ref.build_contact_aware(v, t, cn, target_resolution=24, max_resolution=24, sparse=True,
+                                 band_voxels=3)
+    info = R.info()
+    rng = np.random.default_rng(4)
+    pts = rng.uniform(info["bmin"], info["bmax"], (2000, 3))
+    pts.tofile(str(tmp_path / "pts.bin"))
+    pre = str(tmp_path / "out")
+    r = subprocess.run([check_bin, "ca", surf, "24", pre, str(tmp_path / "pts.bin")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    R.save(str(tmp_path / "ref_dense.sdf"))
+    Rs.save(str(tmp_path / "ref_sparse.sdf"))
+    assert open(pre + ".ca_dense.sdf", "rb").read() == open(tmp_path / "ref_dense.sdf", "rb").read()
+    assert open(pre + ".ca_sparse.sdf", "rb").read() == open(tmp_path / "ref_sparse.sdf", "rb").read()
+    h = float(info["voxel"][0])
+    for layout, g in (("dense", R), ("sparse", Rs)):
+        out = np.fromfile(f"{pre}.ca.{layout}.bin").reshape(-1, 9 + 64)
+        q = ref.query_candidates(g, 4, pts)
+        v = q["valid"]
+        assert np.array_equal(out[:, 7] > 0, v)
+        assert np.array_equal(out[v, 8].astype(int), q["ncand"][v])
+        assert np.all(np.abs(out[v, 0] - q["gap"][v]) <= 1e-6 * np.maximum(np.abs(q["gap"][v]), h))
+        k = out[:, 9:].reshape(-1, 8, 8)
+        m = np.arange(8)[None, :] < q["ncand"][:, None]
+        assert np.array_equal(k[..., 7][m].astype(np.int64), q["kbranch"][m])
+        assert np.all(np.abs(k[..., 0][m] - q["kgap"][m]) <= 1e-6 * np.maximum(np.abs(q["kgap"][m]), h))
