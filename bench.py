@@ -57,8 +57,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--kernels-once", choices=["c2", "c5"], default=None,
+    ap.add_argument("--kernels-once", choices=["c2", "c5", "ca"], default=None,
                     help="one launch of each query kernel on the workload (for ncu), then exit")
+    ap.add_argument("--skip-ca", action="store_true",
+                    help="leave out the contact-aware build / query section")
+    ap.add_argument("--skip-io", action="store_true",
+                    help="leave out the SDFO file load / save section")
     ap.add_argument("--skip-c4", action="store_true",
                     help="leave out the 256-gear batched build / query section")
     ap.add_argument("--skip-c5", action="store_true",
@@ -406,6 +410,126 @@ def c5_section(torch, lib, N, dev, stream, flush, steps, warmup, peak):
     return out
 
 
+def contact_aware_section(torch, lib, N, dev, stream, flush, steps, warmup, cpu_ok):
+    """Contact-aware grids (SdfBuilder::buildContactAware): the hollow
+    cylinder with per-face corner normals (sharp rims), dense at the headline
+    resolution (128 along the longest axis) and sparse band 3, up to 4
+    candidates per voxel; the headline query points in ContactAware mode.
+    CPU reference: the reference's contact-aware build of the same mesh at
+    resolution 64 (bounded sample)."""
+    import ctypes
+
+    from sdfo import SdfGrid
+    from sdfo import meshes as M
+
+    c = workload()
+    cn = M.corner_normals(c["verts"], c["tris"], "face")
+    SdfGrid.build_contact_aware(c["verts"], c["tris"], cn, target_resolution=32,
+                                max_resolution=32).close()  # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g = SdfGrid.build_contact_aware(c["verts"], c["tris"], cn, **c["dense"])
+    t_dense = time.perf_counter() - t0
+    st = g.build_stats()
+    t0 = time.perf_counter()
+    gs = SdfGrid.build_contact_aware(c["verts"], c["tris"], cn, sparse=True, band_voxels=3,
+                                     **c["dense"])
+    t_sparse = time.perf_counter() - t0
+    n_vox = int(np.prod(g.shape))
+    pts = torch.tensor(points_for(c, float(g.voxel[0])), device=dev)
+    n = pts.shape[0]
+    gap = torch.empty(n, device=dev)
+    grad = torch.empty((n, 3), device=dev)
+    valid = torch.empty(n, dtype=torch.uint8, device=dev)
+
+    def P(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def q(grid):
+        N.check(lib.sdfo_query(grid.handle, 4, P(pts), 0, n, P(gap), P(grad), None, None,
+                               P(valid), None, ctypes.c_void_p(stream.cuda_stream)))
+
+    q_ms = timed(torch, lambda: q(g), steps, warmup, flush, stream) / steps
+    qs_ms = timed(torch, lambda: q(gs), steps, warmup, flush, stream) / steps
+    counts = g.export_candidates()["count"]
+    out = {
+        "workload": "hollow_cylinder_face_normals_ca_dense128x128x64_and_sparse_band3_1M_queries",
+        "dense_build_ms": 1e3 * t_dense, "dense_fill_ms": st["fill_ms"],
+        "dense_voxels_per_s": n_vox / t_dense,
+        "sparse_build_ms": 1e3 * t_sparse, "sparse_stored_voxels_per_s": gs.stored_voxels / t_sparse,
+        "mean_candidates": float(counts.mean()), "max_candidates": int(counts.max()),
+        "dense_queries_per_s": n / (q_ms * 1e-3), "sparse_queries_per_s": n / (qs_ms * 1e-3),
+        "cpu_reference_dense_voxels_per_s": None,
+    }
+    if cpu_ok:
+        from oracle import ref
+
+        if ref.available():
+            R = ref.build_contact_aware(c["verts"], c["tris"], cn, target_resolution=64,
+                                        max_resolution=64)
+            out["cpu_reference_dense_voxels_per_s"] = (
+                float(np.prod(R.info()["shape"])) / R.build_seconds)
+            out["cpu_reference_sample"] = "buildContactAware of the same mesh at 64^3, OpenMP"
+    g.close()
+    gs.close()
+    return out
+
+
+def io_section(torch, cpu_ok, repeats=3):
+    """SDFO 0.1.0 files straight to and from the device (sdfo_grid_save_file /
+    sdfo_grid_load_file) for the headline dense grid (FP64 phi, n, H, witness:
+    104 B/voxel) and its sparse band-3 counterpart; wall time of whole calls,
+    file in the page cache, median of ``repeats``.  CPU reference: loadSdf /
+    saveSdf and loadSparseSdf / saveSparseSdf of the same files."""
+    import shutil
+    import tempfile
+
+    from sdfo import SdfGrid
+
+    c = workload()
+    tmp = tempfile.mkdtemp(prefix="sdfo_io_")
+    try:
+        out = {"workload": "hollow_cylinder dense 128x128x64 and sparse band 3, SDFO 0.1.0"}
+        grids = {"dense": SdfGrid.build_dense(c["verts"], c["tris"], **c["dense"]),
+                 "sparse": SdfGrid.build_sparse(c["verts"], c["tris"], **c["sparse"])}
+        for name, g in grids.items():
+            path = os.path.join(tmp, f"{name}.sdf")
+            g.save(path)  # warm: pinned staging, page cache
+            SdfGrid.load(path).close()
+            save_s, load_s = [], []
+            for _ in range(repeats):
+                t0 = time.perf_counter()
+                assert g.save(path)
+                save_s.append(time.perf_counter() - t0)
+                t0 = time.perf_counter()
+                h = SdfGrid.load(path)
+                torch.cuda.synchronize()
+                load_s.append(time.perf_counter() - t0)
+                h.close()
+            size = os.path.getsize(path)
+            out[name] = {"file_bytes": size, "save_ms": 1e3 * statistics.median(save_s),
+                         "load_ms": 1e3 * statistics.median(load_s),
+                         "save_gbs": size / statistics.median(save_s) / 1e9,
+                         "load_gbs": size / statistics.median(load_s) / 1e9}
+            if cpu_ok:
+                from oracle import ref
+
+                if ref.available():
+                    rl, rs = [], []
+                    for _ in range(repeats):
+                        R = ref.load_kind(path, name)
+                        rl.append(R.build_seconds)
+                        ok, sec = ref.save_timed(R, os.path.join(tmp, f"{name}_ref.sdf"))
+                        rs.append(sec)
+                        del R
+                    out[name]["cpu_reference_load_ms"] = 1e3 * statistics.median(rl)
+                    out[name]["cpu_reference_save_ms"] = 1e3 * statistics.median(rs)
+            g.close()
+        return out
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def c4_section(torch, lib, N, dev, stream, flush, steps, warmup):
     """Config 4: 256 gear prisms (2k-60k tris, sparse 64^3..256^3, band 3):
     one batched build against 256 single builds, then 256 x 65,536 Tricubic
@@ -663,6 +787,13 @@ def run_ours(args, rank, world, local_rank):
     ct_ad3 = timed(torch, lambda: batch3.evaluate(poses, body_b, jacobian=True), csteps,
                    args.warmup, flush, stream) / csteps
     peak, peak_src = measured_peaks()
+    ca = None
+    if not args.skip_ca:
+        ca = contact_aware_section(torch, lib, N, dev, stream, flush, max(3, args.steps // 10),
+                                   args.warmup, rank == 0 and world == 1)
+    sdfo_io = None
+    if not args.skip_io:
+        sdfo_io = io_section(torch, rank == 0 and world == 1)
     c4 = None
     if not args.skip_c4:
         c4 = c4_section(torch, lib, N, dev, stream, flush, max(3, args.steps // 20), args.warmup)
@@ -736,6 +867,8 @@ def run_ours(args, rank, world, local_rank):
             "ad_vs_fd_speedup": ct_fd / ct_ad,
             "tricubic_fwd_jac_poses_per_s": 4096 / (ct_ad3 * 1e-3),
         },
+        "contact_aware": ca,
+        "sdfo_io": sdfo_io,
         "c4": c4,
         "c5": c5,
     }
@@ -748,7 +881,9 @@ def kernels_once(which):
     """Setup of a workload, then ONE launch of each query kernel (forward,
     FP16 forward where sparse, linearising forward, saved backward, the
     regathering backward) with a 64 MB buffer written before each -- the
-    program an ncu capture (-k regex:"k_query|k_backward") runs."""
+    program an ncu capture (-k regex:"k_query|k_backward") runs.  "ca": one
+    contact-aware build of the cylinder (its fill kernels) and one
+    ContactAware query launch."""
     import ctypes
 
     import torch
@@ -758,6 +893,24 @@ def kernels_once(which):
     from sdfo import workloads as W
 
     lib = N.load()
+    if which == "ca":
+        from sdfo import meshes as M
+
+        c = W.c2_cylinder()
+        cn = M.corner_normals(c["verts"], c["tris"], "face")
+        g = SdfGrid.build_contact_aware(c["verts"], c["tris"], cn, **c["dense"])
+        pts = torch.tensor(points_for(c, float(g.voxel[0])), device="cuda")
+        n = pts.shape[0]
+        out = torch.empty(n, device="cuda")
+        valid = torch.empty(n, dtype=torch.uint8, device="cuda")
+        torch.empty(16 << 20, device="cuda").zero_()
+        N.check(lib.sdfo_query(g.handle, 4, ctypes.c_void_p(pts.data_ptr()), 0, n,
+                               ctypes.c_void_p(out.data_ptr()), None, None, None,
+                               ctypes.c_void_p(valid.data_ptr()), None,
+                               ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        torch.cuda.synchronize()
+        print(json.dumps({"kernels_once": which, "queries": n}))
+        return
     if which == "c2":
         c = W.c2_cylinder()
         grids = [SdfGrid.build_dense(c["verts"], c["tris"], mode=TRICUBIC, **c["dense"])]

@@ -42,6 +42,8 @@ extern "C" {
 #define SDFO_ERR_DEVICE_STATUS (-5)    /* a kernel reported a failure (see message) */
 #define SDFO_ERR_UNSUPPORTED (-6)      /* mode/layout combination not provided */
 #define SDFO_ERR_NO_DEVICE (-7)        /* no CUDA device / not an sm_100 device */
+#define SDFO_ERR_IO (-8)               /* a file cannot be opened, read or written, or
+                                          is not an SDFO 0.1.0 file of the asked layout */
 
 /* ---- enums --------------------------------------------------------------- */
 /* QueryMode (SdfOracle.h:11-18). */
@@ -305,6 +307,32 @@ int sdfo_grid_get_info(const sdfo_grid* g, sdfo_grid_info* out);
 int sdfo_grid_device_views(const sdfo_grid* g, sdfo_device_views* out);
 int sdfo_grid_destroy(sdfo_grid* g);
 
+/* ---- SDFO 0.1.0 files, device-direct (SdfIO.cpp:93-552) ------------------ */
+#define SDFO_FILE_ANY 0    /* SdfOracle::loadFromFile (SdfOracle.cpp:165-172):
+                              sparse when isSparseSdf, else dense */
+#define SDFO_FILE_DENSE 1  /* loadSdf */
+#define SDFO_FILE_SPARSE 2 /* loadSparseSdf */
+
+/* isValidSdf / isSparseSdf (SdfIO.cpp:527-550): reads the 128-byte header
+ * only (no device work); a missing or short file gives 0 / 0. */
+int sdfo_file_probe(const char* path, int32_t* is_valid, int32_t* is_sparse);
+
+/* loadSdf / loadSparseSdf straight into a device grid: the header is checked
+ * with the reference's messages (SDFO_ERR_IO, sdfo_last_error), the payload
+ * is read by up to 4 threads through pinned staging and decoded on the device
+ * (dense: FP64 arrays kept for exact export plus the FP32 query payload;
+ * sparse: FP32 bricks, Hessians if stored, block table; contact-aware
+ * candidates when the file has them).  The 64 MiB of pinned staging is
+ * allocated on first use and held until the process exits; calls serialise.
+ * Synchronous. */
+int sdfo_grid_load_file(const char* path, int32_t expect, void* stream, sdfo_grid** out);
+
+/* saveSdf / saveSparseSdf of a device grid: byte-identical to the reference
+ * writing the same data (dense files always carry Hessians, zero when the
+ * grid has none; FP16 grids are written decoded to FP32).  SDFO_ERR_IO when
+ * the file cannot be opened or written.  Synchronous. */
+int sdfo_grid_save_file(const sdfo_grid* g, const char* path, void* stream);
+
 /* ---- queries (SdfOracle::queryFast / queryBatch) ------------------------- */
 /* SdfOracle::queryFast + queryBatch (SdfOracle.cpp:226-444) for n points.
  * d_points: (n,3) float32 or float64 (points_f64).  Outputs (device, any may
@@ -319,8 +347,11 @@ int sdfo_grid_destroy(sdfo_grid* g);
  *   d_hess[n*9]       d grad / d p of the interpolant (row-major), the
  *                     forward-mode Jacobian of (gap, grad) w.r.t. p
  * Invalid queries write gap 0, grad 0, unit (1,0,0), witness 0, hess 0.
- * ContactAware on grids without candidates behaves as Tricubic, as the
- * reference does (SdfOracle.cpp:209-212). */
+ * ContactAware on a grid with surface-feature candidates (built by
+ * sdfo_grid_build_contact_aware, loaded, or attached) answers with the
+ * candidate of smallest |gap| at the nearest voxel (SdfOracle.cpp:296-423);
+ * on grids without candidates it behaves as Tricubic, as the reference does
+ * (SdfOracle.cpp:209-212). */
 int sdfo_query(const sdfo_grid* g, int32_t mode, const void* d_points, int32_t points_f64,
                int64_t n, float* d_gap, float* d_grad, float* d_unit, float* d_witness,
                uint8_t* d_valid, float* d_hess, void* stream);
