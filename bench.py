@@ -505,12 +505,16 @@ def io_section(torch, cpu_ok, repeats=3):
                 h = SdfGrid.load(path)
                 torch.cuda.synchronize()
                 load_s.append(time.perf_counter() - t0)
+                st = h.build_stats()
                 h.close()
             size = os.path.getsize(path)
             out[name] = {"file_bytes": size, "save_ms": 1e3 * statistics.median(save_s),
                          "load_ms": 1e3 * statistics.median(load_s),
                          "save_gbs": size / statistics.median(save_s) / 1e9,
-                         "load_gbs": size / statistics.median(load_s) / 1e9}
+                         "load_gbs": size / statistics.median(load_s) / 1e9,
+                         "last_load_phases_ms": {"allocate": st["setup_ms"],
+                                                 "read_and_transfer": st["fill_ms"],
+                                                 "decode": st["hessian_ms"]}}
             if cpu_ok:
                 from oracle import ref
 

@@ -324,7 +324,9 @@ int sdfo_file_probe(const char* path, int32_t* is_valid, int32_t* is_sparse);
  * sparse: FP32 bricks, Hessians if stored, block table; contact-aware
  * candidates when the file has them).  The 64 MiB of pinned staging is
  * allocated on first use and held until the process exits; calls serialise.
- * Synchronous. */
+ * sdfo_grid_build_stats of the new grid reports the load's phases: setup_ms
+ * (allocation), fill_ms (file read and transfer), hessian_ms (decoding on the
+ * device), total_ms.  Synchronous. */
 int sdfo_grid_load_file(const char* path, int32_t expect, void* stream, sdfo_grid** out);
 
 /* saveSdf / saveSparseSdf of a device grid: byte-identical to the reference

@@ -44,6 +44,10 @@ def lib():
         L.ref_load.argtypes = [ctypes.c_char_p]
         L.ref_save.restype = _I
         L.ref_save.argtypes = [_P, ctypes.c_char_p]
+        L.ref_load_kind.restype = _P
+        L.ref_load_kind.argtypes = [ctypes.c_char_p, _I, _P]
+        L.ref_save_timed.restype = _I
+        L.ref_save_timed.argtypes = [_P, ctypes.c_char_p, _P]
         L.ref_free.argtypes = [_P]
         L.ref_grid_info.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P]
         L.ref_dense_export.argtypes = [_P, _P, _P, _P, _P]
@@ -197,6 +201,24 @@ def load(path: str) -> RefGrid:
     if not h:
         raise RuntimeError(_err())
     return RefGrid(h)
+
+
+def load_kind(path: str, kind: str = "any") -> RefGrid:
+    """SdfOracle::loadFromFile ("any"), loadSdf ("dense") or loadSparseSdf
+    ("sparse") (SdfIO.cpp:277-523); RuntimeError with the reference's message
+    on failure; ``build_seconds`` holds the load's wall time."""
+    sec = np.zeros(1)
+    h = lib().ref_load_kind(path.encode(), {"any": 0, "dense": 1, "sparse": 2}[kind], _ptr(sec))
+    if not h:
+        raise RuntimeError(_err())
+    return RefGrid(h, float(sec[0]))
+
+
+def save_timed(g: "RefGrid", path: str):
+    """saveSdf / saveSparseSdf: (ok, seconds)."""
+    sec = np.zeros(1)
+    rc = lib().ref_save_timed(g.handle, path.encode(), _ptr(sec))
+    return rc == 0, float(sec[0])
 
 
 def signed_nearest(verts, tris, pts):

@@ -153,6 +153,41 @@ int ref_save(void* hp, const char* path)
     return sdf::saveSdf(h->oracle.data(), path) ? 0 : -1;
 }
 
+// kind 0: SdfOracle::loadFromFile; 1: loadSdf; 2: loadSparseSdf
+// (SdfIO.cpp:277-523); *seconds = wall time of the load.
+void* ref_load_kind(const char* path, int kind, double* seconds)
+{
+    try
+    {
+        const auto t0 = std::chrono::steady_clock::now();
+        RefHandle* h = nullptr;
+        if (kind == 1)
+            h = new RefHandle{sdf::SdfOracle(sdf::loadSdf(path))};
+        else if (kind == 2)
+            h = new RefHandle{sdf::SdfOracle(sdf::loadSparseSdf(path))};
+        else
+            h = new RefHandle{sdf::SdfOracle::loadFromFile(path)};
+        if (seconds)
+            *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return h;
+    }
+    catch (const std::exception& e)
+    {
+        g_error = e.what();
+        return nullptr;
+    }
+}
+
+// saveSdf / saveSparseSdf with the wall time of the write.
+int ref_save_timed(void* hp, const char* path, double* seconds)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = ref_save(hp, path);
+    if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+
 void ref_free(void* hp) { delete static_cast<RefHandle*>(hp); }
 
 // shape[3], bmin[3], bmax[3], voxel[3]; sparse: info[0]=blocks, info[1]=blockDim,

@@ -32,7 +32,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 PER_FILE = {"build.cu": ["-fmad=false"], "batch.cu": ["-fmad=false"], "ca_build.cu": ["-fmad=false"],
             "ca_query.cu": ["-fmad=false"]}
 SOURCES = ["grid.cu", "capi.cu", "query.cu", "build.cu", "batch.cu", "batch_query.cu",
-           "ca_build.cu", "ca_query.cu", "contact.cu", "static_staging.cu"]
+           "ca_build.cu", "ca_query.cu", "contact.cu", "static_staging.cu", "sdfo_file.cu"]
 HEADERS = ["sdfo_internal.cuh", "interp.cuh", "build_common.cuh"]
 
 

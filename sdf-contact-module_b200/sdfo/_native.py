@@ -14,6 +14,8 @@ PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG_DIR, "lib", "libsdfo_cuda.so")
 
 SDFO_OK = 0
+SDFO_ERR_IO = -8
+FILE_ANY, FILE_DENSE, FILE_SPARSE = 0, 1, 2
 FIRST_ORDER, SECOND_ORDER, TRILINEAR, TRICUBIC, CONTACT_AWARE = 0, 1, 2, 3, 4
 LAYOUT_DENSE, LAYOUT_SPARSE = 1, 2
 STORAGE_FP32, STORAGE_FP16 = 0, 1
@@ -120,6 +122,9 @@ SIGNATURES = [
     ("sdfo_grid_get_info", ctypes.c_int, [_P, ctypes.POINTER(GridInfo)]),
     ("sdfo_grid_device_views", ctypes.c_int, [_P, ctypes.POINTER(DeviceViews)]),
     ("sdfo_grid_destroy", ctypes.c_int, [_P]),
+    ("sdfo_file_probe", ctypes.c_int, [ctypes.c_char_p, _P, _P]),
+    ("sdfo_grid_load_file", ctypes.c_int, [ctypes.c_char_p, _I32, _P, _P]),
+    ("sdfo_grid_save_file", ctypes.c_int, [_P, ctypes.c_char_p, _P]),
     ("sdfo_query", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P, _P, _P, _P]),
     ("sdfo_query_host", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P, _P, _P]),
     ("sdfo_query_host_static", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P]),

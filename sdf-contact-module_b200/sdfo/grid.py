@@ -16,6 +16,7 @@ Everything runs on the GPU; there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -482,44 +483,25 @@ class SdfGrid:
 
     # ----------------------------------------------------------------- io
     @classmethod
-    def load(cls, path: str, mode=N.TRILINEAR) -> "SdfGrid":
-        """SdfOracle::loadFromFile (SdfOracle.cpp:165-172) onto the device."""
-        from . import io as sio
+    def load(cls, path: str, mode=N.TRILINEAR, expect: str = "any", stream=None) -> "SdfGrid":
+        """SdfOracle::loadFromFile (SdfOracle.cpp:165-172) straight onto the
+        device; ``expect`` "dense" / "sparse" give loadSdf / loadSparseSdf
+        (SdfIO.cpp:277-523) and their errors (SdfoError with the reference's
+        message)."""
+        kinds = {"any": N.FILE_ANY, "dense": N.FILE_DENSE, "sparse": N.FILE_SPARSE}
+        if expect not in kinds:
+            raise ValueError(f"expect must be one of {sorted(kinds)}")
+        lib = N.load()
+        out = ctypes.c_void_p()
+        N.check(lib.sdfo_grid_load_file(os.fsencode(path), kinds[expect], _stream_ptr(stream),
+                                        ctypes.byref(out)))
+        return cls(out.value, mode)
 
-        d = sio.load(path)
-        if d["layout"] == "sparse":
-            g = cls.from_sparse(d["spec"], d["block_dim"], d["ijk"], d["phi"], d["normal"],
-                                d["hessian"], d["halo_voxels"], d["band_distance"], mode)
-        else:
-            g = cls.from_dense(d["spec"], d["phi"], d["normal"], d["hessian"], d["witness"], mode)
-        if "ca" in d:
-            ca = d["ca"]
-            g.attach_candidates(ca["stride"], ca["count"], ca["phi"], ca["normal"], ca["branch"])
-        return g
-
-    def save(self, path: str) -> bool:
-        """saveSdf / saveSparseSdf (SdfIO.cpp:93-275) of the device grid."""
-        from . import io as sio
-
-        ca = None
-        if self.candidate_stride > 0:
-            c = self.export_candidates()
-            s = c["stride"]
-            if self.is_sparse:
-                V = self.block_dim ** 3
-                B = self.block_count
-                ca = dict(stride=s, count=c["count"].reshape(B, V),
-                          phi=c["phi"].reshape(B, V * s).astype(np.float32),
-                          normal=c["normal"].reshape(B, V * s, 3).astype(np.float32),
-                          branch=c["branch"].reshape(B, V * s))
-            else:
-                ca = dict(stride=s, count=c["count"], phi=c["phi"].reshape(-1),
-                          normal=c["normal"].reshape(-1, 3), branch=c["branch"].reshape(-1))
-        if self.is_sparse:
-            d = self.export_sparse()
-            return sio.save_sparse(path, self.spec(), self.block_dim, self.halo_voxels,
-                                   self.band_distance, d["ijk"], d["phi"], d["normal"],
-                                   d["hessian"], ca=ca)
-        d = self.export_dense()
-        return sio.save_dense(path, self.spec(), d["phi"], d["normal"], d["hessian"],
-                              d["witness"], ca=ca)
+    def save(self, path: str, stream=None) -> bool:
+        """saveSdf / saveSparseSdf (SdfIO.cpp:93-275) of the device grid:
+        False when the file cannot be opened or written, as the reference."""
+        rc = self._lib.sdfo_grid_save_file(self.handle, os.fsencode(path), _stream_ptr(stream))
+        if rc == N.SDFO_ERR_IO:
+            return False
+        N.check(rc)
+        return True
