@@ -154,6 +154,23 @@ typedef struct
     double activation_distance; /* read but unused by the reference law */
 } sdfo_contact_params;
 
+/* ContactMeasure (contacts_sdf.py:8-17) of one pose, from measure_pair
+ * (contacts_sdf.py:171-214): the minimum gap over the in-grid quadrature
+ * points the broad phase keeps (+inf when there is none), its penetration
+ * max(0, -gap), the normal relative velocity at that point, the point's
+ * index in the broad phase's point list (-1 when none), and the counts of
+ * in-grid points with gap < 0 and of in-grid points. */
+typedef struct
+{
+    double gap;
+    double penetration;
+    double normal_velocity;
+    int32_t min_point_index;
+    int32_t active_count;
+    int32_t valid_count;
+    int32_t reserved0;
+} sdfo_contact_measure;
+
 /* Build statistics of the last build on a handle. */
 typedef struct
 {
@@ -489,6 +506,119 @@ int sdfo_contact_eval(const sdfo_grid* g, int32_t mode, const float* d_quad_x,
                       int64_t np, const sdfo_body_state* d_body_b,
                       const sdfo_contact_params* h_params, double* d_ft, double* d_jac,
                       void* stream);
+
+/* ---- contact pairs with the engine's culling ---------------------------- */
+typedef struct sdfo_contact_pair sdfo_contact_pair;
+
+/* SDFContactEngine.register_pair (contacts_sdf.py:52-62): quadrature points
+ * (nq,3) FP64 in body A's frame and their weights (normalised to sum 1 when
+ * normalize_weights != 0), bound to grid g (which must outlive the pair),
+ * with the AABB_BVH point hierarchy (geometry/bvh.py:16-60, leaf_size 16 in
+ * the reference).  narrow_margin >= 0 enables the engine's culling with that
+ * narrow margin (0.01 in the reference): the BVH cull with box margin
+ * max(narrow_margin, 0.05) and evaluate's |Y_z| < narrow_margin filter;
+ * narrow_margin < 0 evaluates every point.  At most 32768 BVH leaves when
+ * culling is enabled (SDFO_ERR_UNSUPPORTED beyond).  g == NULL builds the
+ * hierarchy only, on the host (for sdfo_contact_pair_export_bvh). */
+int sdfo_contact_pair_create(const sdfo_grid* g, const double* h_quad_x, const double* h_quad_w,
+                             int64_t nq, int32_t normalize_weights, double narrow_margin,
+                             int32_t leaf_size, sdfo_contact_pair** out);
+
+/* The pair's point hierarchy: leaf count, the original point indices in
+ * stored order (nq), leaf offsets into that order (nleaves + 1) and leaf
+ * boxes (nleaves x 6: min xyz, max xyz).  Leaves are in the order the
+ * reference's query visits them.  Any output may be NULL. */
+int sdfo_contact_pair_export_bvh(const sdfo_contact_pair* p, int32_t* h_nleaves,
+                                 int32_t* h_point_order, int32_t* h_leaf_start,
+                                 double* h_leaf_box);
+
+/* evaluate (contacts_sdf.py:225-385) and/or measure_pair
+ * (contacts_sdf.py:171-214) for np poses of body A against body B: d_ft
+ * (np x 6: F_A, tau_A), d_jac (np x 36, as sdfo_contact_eval; needs d_ft) and
+ * d_measure (np) -- any of them may be NULL, not all. */
+int sdfo_contact_pair_eval(const sdfo_contact_pair* p, int32_t mode,
+                           const sdfo_body_state* d_pose_a, int64_t np,
+                           const sdfo_body_state* d_body_b, const sdfo_contact_params* h_params,
+                           double* d_ft, double* d_jac, sdfo_contact_measure* d_measure,
+                           void* stream);
+
+int sdfo_contact_pair_destroy(sdfo_contact_pair* p);
+
+/* ---- Backward-Euler contact steps ---------------------------------------- */
+/* BackwardEulerIntegrator parameters (implicit_be.py:60-107 defaults via
+ * sdfo_be_params_default). */
+typedef struct
+{
+    int32_t max_iter;            /* 20 */
+    int32_t line_search;         /* 1 */
+    int32_t max_toi_bisect_iter; /* 60 */
+    int32_t stable_steps;        /* contact_stable_steps, 5 */
+    int32_t release_steps;       /* contact_release_steps, 3 */
+    int32_t reserved0;
+    double tol;                  /* 1e-8 */
+    double pen_max;              /* contact_penetration_tol, 1e-6 */
+    double dt_min;               /* contact_dt_min, 1e-8 */
+    double dt_impact;            /* contact_dt_impact, 1e-7 */
+    double dt_contact;           /* contact_dt_active, 1e-5 */
+    double dt_max_contact;       /* contact_dt_max, 1e-4 */
+    double dt_normal;            /* contact_dt_normal, 1e-3 */
+    double dt_growth;            /* contact_dt_growth, 1.5 */
+} sdfo_be_params;
+
+/* RigidBody mass properties (ir/body.py): mass, body-frame inertia
+ * (row-major 3x3), and the model's gravity. */
+typedef struct
+{
+    double mass;
+    double inertia[9];
+    double gravity[3];
+} sdfo_rigid_body;
+
+/* One scene: the state of body A and its contact region
+ * (ContactRegionState, implicit_be.py:22-39; phase numbered as ContactPhase:
+ * 0 INACTIVE, 2 IMPACTING, 3 ACTIVE, 4 STABLE, 5 LEAVING). */
+typedef struct
+{
+    sdfo_body_state body;
+    double t;
+    double dt_current;
+    double last_gap;
+    double last_penetration;
+    double last_normal_velocity;
+    double last_toi;
+    int32_t phase;
+    int32_t stable_count;
+    int32_t release_count;
+    int32_t min_dt_hits;
+} sdfo_be_scene;
+
+typedef struct sdfo_be_stepper sdfo_be_stepper;
+
+void sdfo_be_params_default(sdfo_be_params* p);
+/* A scene at rest in the state machine: INACTIVE, dt_current = dt_normal,
+ * last_gap and last_toi +inf (ContactRegionState defaults). */
+void sdfo_be_scene_init(sdfo_be_scene* s, const sdfo_body_state* body, double t,
+                        const sdfo_be_params* p);
+
+/* BackwardEulerIntegrator.step (implicit_be.py:131-181) for batches of
+ * scenes: body A (free, mass properties body_a) carries the pair's
+ * quadrature set; body B (fixed, state body_b) carries the pair's grid,
+ * which must be dense with FP64 values.  The engine's culling follows the
+ * pair's narrow margin, its linearisation cache is used as the reference
+ * uses it.  Holds scratch for max_scenes scenes (40 B per scene and
+ * quadrature point). */
+int sdfo_be_stepper_create(const sdfo_contact_pair* pair, const sdfo_contact_params* contact,
+                           const sdfo_rigid_body* body_a, const sdfo_body_state* body_b,
+                           const sdfo_be_params* params, int64_t max_scenes,
+                           sdfo_be_stepper** out);
+
+/* One step of every scene: d_scenes (n, device) advanced in place, d_dt (n)
+ * the requested step (<= 0: the scene is left as it is), d_h (n, may be NULL)
+ * the step taken (the time of impact when contact begins).  Asynchronous. */
+int sdfo_be_stepper_step(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n,
+                         const double* d_dt, double* d_h, void* stream);
+
+int sdfo_be_stepper_destroy(sdfo_be_stepper* st);
 
 #ifdef __cplusplus
 }

@@ -4,8 +4,8 @@
 
 Each translation unit is compiled with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3``; build.cu and
-batch.cu, ca_build.cu and ca_query.cu (the FP64 distance / sign / candidate
-paths) additionally with ``-fmad=false`` so their FP64
+batch.cu, ca_build.cu, ca_query.cu and be_step.cu (the FP64 distance / sign /
+candidate / integrator paths) additionally with ``-fmad=false`` so their FP64
 expressions are evaluated exactly in source order.  The static CUDA runtime
 is linked in so the library does not depend on the toolkit's libcudart at
 run time.  Objects go to _build/, the library to lib/.
@@ -30,9 +30,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
           "-ffp-contract=off", "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
 PER_FILE = {"build.cu": ["-fmad=false"], "batch.cu": ["-fmad=false"], "ca_build.cu": ["-fmad=false"],
-            "ca_query.cu": ["-fmad=false"]}
+            "ca_query.cu": ["-fmad=false"], "be_step.cu": ["-fmad=false"]}
 SOURCES = ["grid.cu", "capi.cu", "query.cu", "build.cu", "batch.cu", "batch_query.cu",
-           "ca_build.cu", "ca_query.cu", "contact.cu", "static_staging.cu", "sdfo_file.cu"]
+           "ca_build.cu", "ca_query.cu", "contact.cu", "static_staging.cu", "sdfo_file.cu",
+           "contact_pair.cu", "be_step.cu"]
 HEADERS = ["sdfo_internal.cuh", "interp.cuh", "build_common.cuh"]
 
 

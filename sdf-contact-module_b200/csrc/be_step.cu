@@ -1,0 +1,1066 @@
+// Backward-Euler contact steps on the GPU: BackwardEulerIntegrator.step
+// (prototype/src/integrators/implicit_be.py:131-181) for batches of
+// independent scenes.  Each scene is one free rigid body A carrying the
+// quadrature set of a contact pair, against the fixed body B whose dense grid
+// the pair is bound to (one movable body, one contact pair, no joints or
+// drives).  One CTA runs one scene's whole adaptive step:
+//   * measure_pair of the start state; a region found penetrating becomes
+//     IMPACTING (_activate_initially_penetrating_regions, :223-233);
+//   * h_cap = min(dt, the region's dt_current when active, else dt_normal);
+//   * for an inactive region, a trial BE step over h_cap without contact
+//     forces and, when it crosses into contact, the bisection of
+//     _bisect_toi_pair (:336-394) with a BE trial step per halving;
+//   * the real BE step (to the TOI, or over h_cap with contact forces when
+//     the region is active) and the phase state machine
+//     (_refresh_contact_states, :248-295).
+// A BE step (_step_be, :468-505) is Newton on V = (v, w): residual
+// M (V - V0)/h + C - Q (:536-604), the reference's diagonal tangent
+// (_contact_tangent / _tangent, :606-687), exact solve of its two blocks,
+// backtracking line search over 1, 1/2, .. 1/16 (:689-697).  Contact forces
+// follow SDFContactEngine.evaluate with its culling and linearisation cache
+// (contacts_sdf.py:225-385): the first evaluation of a step queries the
+// narrow-filtered points and stores (g, grad, valid) by position together
+// with the SDF-frame translation; later evaluations with the same number of
+// narrow-filtered points use g + grad . (t - t_ref).
+//
+// Grid samples are FP64 trilinear on the grid's FP64 values, written as the
+// prototype's TrilinearSDFGrid.query_batch (prototype/src/sdf_grid.py:
+// 138-204); this translation unit is compiled with -fmad=false so that every
+// FP64 expression is evaluated in source order, as NumPy does.
+//
+// Control flow: every thread runs the same loops and branches; decisions and
+// all scalar state live in shared memory, written by thread 0 between
+// barriers; the contact passes use all threads.
+#include <cfloat>
+#include <climits>
+#include <cstring>
+
+#include "sdfo_internal.cuh"
+
+namespace sdfo {
+namespace {
+
+constexpr int kT = 256;
+constexpr int kWarps = kT / 32;
+
+enum : int
+{
+    kInactive = 0,
+    kImpacting = 2,
+    kActive = 3,
+    kStable = 4,
+    kLeaving = 5
+};
+
+struct Body
+{
+    double r[3], R[9], v[3], w[3], t;
+};
+
+struct BeView
+{
+    GridView g;
+    const double* phi64;
+    int nq, nleaves, cull;
+    const double* px;         // stored (leaf) order
+    const double* pw;
+    const int32_t* pleaf;
+    const double* ox;         // original order
+    const double* ow;
+    const double* leaf_box;
+    double root[6], bmin[3], bmax[3], box_margin, narrow;
+    double rB[3], RB[9], vB[3], wB[3];
+    double mass, Ib[9], gravity[3], area;
+    sdfo_contact_params c;
+    sdfo_be_params p;
+    double* cg;               // cache scratch, nq per scene
+    double* cgrad;            // 3 nq per scene
+    unsigned char* cvalid;    // nq per scene
+};
+
+struct MinRec
+{
+    double gap;
+    int key; // position in the kept list
+    int i;   // index into the point arrays
+};
+
+struct Shared
+{
+    Body q, q0, tr, cur;
+    double dt_current, last_gap, last_pen, last_vn, last_toi;
+    int phase, stable_count, release_count, min_dt_hits;
+    double z[6], dz[6], zt[6], res[6], err, r0, Iw[9];
+    double F[3], tau[3];
+    double m_gap, m_pen, m_vn;
+    int m_active, m_valid;
+    int c_enabled, c_cleared, c_len;
+    double c_tref[3];
+    unsigned mask[kMaxCullLeaves / 32];
+    int full;
+    double box[6];
+    double red[kWarps][6];
+    MinRec mins[kWarps];
+    int cnt[kWarps][2];
+    int scan[kWarps];
+    int flag, count, mi;
+    double lo, hi, hm_pen, toi; // bisection bracket, its measure, the step
+    int hit, event;
+    double alpha;               // line search
+    int found;
+};
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ void matvec(const double R[9], const double x[3], double y[3])
+{
+    for (int i = 0; i < 3; ++i) y[i] = R[3 * i] * x[0] + R[3 * i + 1] * x[1] + R[3 * i + 2] * x[2];
+}
+
+__device__ __forceinline__ void matTvec(const double R[9], const double x[3], double y[3])
+{
+    for (int i = 0; i < 3; ++i) y[i] = R[i] * x[0] + R[3 + i] * x[1] + R[6 + i] * x[2];
+}
+
+__device__ __forceinline__ void cross3(const double a[3], const double b[3], double c[3])
+{
+    c[0] = a[1] * b[2] - a[2] * b[1];
+    c[1] = a[2] * b[0] - a[0] * b[2];
+    c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+__device__ __forceinline__ double dot3(const double a[3], const double b[3])
+{
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+__device__ __forceinline__ double warp_dsum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int warp_isum(int v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// TrilinearSDFGrid.query_batch for one point (sdf_grid.py:138-204).
+__device__ bool sample64(const BeView& b, const double Y[3], double& g, double grad[3])
+{
+    const int n[3] = {b.g.nx, b.g.ny, b.g.nz};
+    int c[3];
+    double f[3];
+    for (int a = 0; a < 3; ++a)
+    {
+        f[a] = (Y[a] - b.g.bmin[a]) / b.g.voxel[a] - 0.5;
+        if (!(f[a] >= 0.0 && f[a] < (double)(n[a] - 1))) return false;
+        c[a] = (int)floor(f[a]);
+        if (c[a] < 0 || c[a] + 1 >= n[a]) return false;
+    }
+    const double uv = f[0] - c[0], vv = f[1] - c[1], wv = f[2] - c[2];
+    const int64_t sy = n[0], sz = (int64_t)n[0] * n[1];
+    const int64_t i0 = c[0] + sy * c[1] + sz * c[2];
+    const double* phi = b.phi64;
+    const double p000 = phi[i0], p100 = phi[i0 + 1], p010 = phi[i0 + sy], p110 = phi[i0 + 1 + sy];
+    const double p001 = phi[i0 + sz], p101 = phi[i0 + 1 + sz], p011 = phi[i0 + sy + sz],
+                 p111 = phi[i0 + 1 + sy + sz];
+    const double one_u = 1.0 - uv, one_v = 1.0 - vv, one_w = 1.0 - wv;
+    g = p000 * one_u * one_v * one_w + p100 * uv * one_v * one_w + p010 * one_u * vv * one_w +
+        p110 * uv * vv * one_w + p001 * one_u * one_v * wv + p101 * uv * one_v * wv +
+        p011 * one_u * vv * wv + p111 * uv * vv * wv;
+    const double ihx = 1.0 / b.g.voxel[0], ihy = 1.0 / b.g.voxel[1], ihz = 1.0 / b.g.voxel[2];
+    grad[0] = ((p100 - p000) * one_v * one_w + (p110 - p010) * vv * one_w + (p101 - p001) * one_v * wv +
+               (p111 - p011) * vv * wv) * ihx;
+    grad[1] = ((p010 - p000) * one_u * one_w + (p110 - p100) * uv * one_w + (p011 - p001) * one_u * wv +
+               (p111 - p101) * uv * wv) * ihy;
+    grad[2] = ((p001 - p000) * one_u * one_v + (p101 - p100) * uv * one_v + (p011 - p010) * one_u * vv +
+               (p111 - p110) * uv * vv) * ihz;
+    return true;
+}
+
+// Y = R_B^T R_A X + R_B^T (r_A - r_B) (contacts_sdf.py:275-286).
+__device__ __forceinline__ void to_sdf(const BeView& b, const Body& s, const double X[3], double Y[3])
+{
+    double Rs[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            Rs[3 * i + j] = b.RB[i] * s.R[j] + b.RB[3 + i] * s.R[3 + j] + b.RB[6 + i] * s.R[6 + j];
+    double d[3] = {s.r[0] - b.rB[0], s.r[1] - b.rB[1], s.r[2] - b.rB[2]};
+    double t[3];
+    matTvec(b.RB, d, t);
+    matvec(Rs, X, Y);
+    for (int a = 0; a < 3; ++a) Y[a] = Y[a] + t[a];
+}
+
+// The broad phase of evaluate / measure_pair for the pose in s.cur
+// (contacts_sdf.py:244-269, bvh.py:62-80): leaf mask and the `full` flag.
+__device__ void broad_phase(const BeView& b, Shared& s)
+{
+    if (!b.cull)
+    {
+        if (threadIdx.x == 0) s.full = 1;
+        __syncthreads();
+        return;
+    }
+    if (threadIdx.x == 0)
+    {
+        double lo[3], hi[3], d[3];
+        for (int a = 0; a < 3; ++a) d[a] = b.bmin[a] - s.cur.r[a];
+        matTvec(s.cur.R, d, lo);
+        for (int a = 0; a < 3; ++a) d[a] = b.bmax[a] - s.cur.r[a];
+        matTvec(s.cur.R, d, hi);
+        bool enc = true;
+        for (int a = 0; a < 3; ++a)
+        {
+            s.box[a] = lo[a] - b.box_margin;
+            s.box[3 + a] = hi[a] + b.box_margin;
+            enc = enc && s.box[a] <= b.root[a] && s.box[3 + a] >= b.root[3 + a];
+        }
+        s.full = enc ? 1 : 0;
+    }
+    for (int w = threadIdx.x; w < (b.nleaves + 31) / 32; w += kT) s.mask[w] = 0u;
+    __syncthreads();
+    if (s.full) return;
+    bool any = false;
+    for (int l = threadIdx.x; l < b.nleaves; l += kT)
+    {
+        const double* x = b.leaf_box + 6 * (int64_t)l;
+        const bool skip = x[3] < s.box[0] || x[4] < s.box[1] || x[5] < s.box[2] || x[0] > s.box[3] ||
+                          x[1] > s.box[4] || x[2] > s.box[5];
+        if (!skip)
+        {
+            atomicOr(&s.mask[l >> 5], 1u << (l & 31));
+            any = true;
+        }
+    }
+    const int none = __syncthreads_or(any) == 0;
+    if (threadIdx.x == 0 && none) s.full = 1;
+    __syncthreads();
+}
+
+// Point i of the kept list in the reference's order (original order when
+// every point is kept, else the stored leaf order restricted to kept
+// leaves); returns whether it is kept and its coordinates / weight.
+__device__ __forceinline__ bool point_at(const BeView& b, const Shared& s, int i, double X[3], double& w)
+{
+    if (i >= b.nq) return false;
+    if (s.full)
+    {
+        X[0] = b.ox[3 * i];
+        X[1] = b.ox[3 * i + 1];
+        X[2] = b.ox[3 * i + 2];
+        w = b.ow[i];
+        return true;
+    }
+    const int l = b.pleaf[i];
+    if (!((s.mask[l >> 5] >> (l & 31)) & 1u)) return false;
+    X[0] = b.px[3 * i];
+    X[1] = b.px[3 * i + 1];
+    X[2] = b.px[3 * i + 2];
+    w = b.pw[i];
+    return true;
+}
+
+// Block-wide exclusive position of `flag` within the chunk; *total = count.
+__device__ __forceinline__ int chunk_scan(Shared& s, bool flag, int& total)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned bal = __ballot_sync(0xffffffffu, flag);
+    if (lane == 0) s.scan[warp] = __popc(bal);
+    __syncthreads();
+    int off = 0;
+    total = 0;
+    for (int w = 0; w < kWarps; ++w)
+    {
+        off += w < warp ? s.scan[w] : 0;
+        total += s.scan[w];
+    }
+    __syncthreads();
+    return off + __popc(bal & ((1u << lane) - 1u));
+}
+
+// SDFContactEngine.evaluate for s.cur with the cache (F, tau into shared).
+__device__ void eval_pass(const BeView& b, Shared& s)
+{
+    broad_phase(b, s);
+    const double narrow = b.cull ? b.narrow : INFINITY;
+    // the number of narrow-filtered points decides whether the cache is used
+    int L = 0;
+    for (int c0 = 0; c0 < b.nq; c0 += kT)
+    {
+        double X[3], w, Y[3];
+        bool f = false;
+        if (point_at(b, s, c0 + threadIdx.x, X, w))
+        {
+            to_sdf(b, s.cur, X, Y);
+            f = fabs(Y[2]) < narrow;
+        }
+        L += __syncthreads_count(f);
+    }
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (L > 0)
+    {
+        const bool use = s.c_enabled && !s.c_cleared && s.c_len >= 0 && L == s.c_len;
+        const bool store = !use && s.c_enabled;
+        double tsdf[3], d[3] = {s.cur.r[0] - b.rB[0], s.cur.r[1] - b.rB[1], s.cur.r[2] - b.rB[2]};
+        matTvec(b.RB, d, tsdf);
+        const int64_t base_c = (int64_t)blockIdx.x * b.nq;
+        int base = 0;
+        for (int c0 = 0; c0 < b.nq; c0 += kT)
+        {
+            double X[3], w = 0.0, Y[3];
+            bool f = false;
+            if (point_at(b, s, c0 + threadIdx.x, X, w))
+            {
+                to_sdf(b, s.cur, X, Y);
+                f = fabs(Y[2]) < narrow;
+            }
+            int total;
+            const int pos = base + chunk_scan(s, f, total);
+            base += total;
+            if (!f) continue;
+            double g, gr[3];
+            bool valid;
+            const int64_t ci = base_c + pos;
+            if (use)
+            {
+                const double dt3[3] = {tsdf[0] - s.c_tref[0], tsdf[1] - s.c_tref[1], tsdf[2] - s.c_tref[2]};
+                gr[0] = b.cgrad[3 * ci];
+                gr[1] = b.cgrad[3 * ci + 1];
+                gr[2] = b.cgrad[3 * ci + 2];
+                g = b.cg[ci] + (gr[0] * dt3[0] + gr[1] * dt3[1] + gr[2] * dt3[2]);
+                valid = b.cvalid[ci] != 0;
+            }
+            else
+            {
+                valid = sample64(b, Y, g, gr);
+                if (!valid)
+                {
+                    g = 0.0;
+                    gr[0] = gr[1] = gr[2] = 0.0;
+                }
+                if (store)
+                {
+                    b.cg[ci] = g;
+                    b.cgrad[3 * ci] = gr[0];
+                    b.cgrad[3 * ci + 1] = gr[1];
+                    b.cgrad[3 * ci + 2] = gr[2];
+                    b.cvalid[ci] = valid ? 1 : 0;
+                }
+            }
+            const double delta = -g > 0.0 ? -g : 0.0;
+            const double p = b.c.stiffness *
+                             (b.c.order == 2.0 ? delta * delta : b.c.order == 1.0 ? delta : pow(delta, b.c.order));
+            if (!(valid && p > 1e-30)) continue;
+            // force law (contacts_sdf.py:329-385)
+            double rg[3], off[3], xw[3], uA[3], uB[3], u[3], t3[3];
+            matvec(b.RB, gr, rg);
+            const double gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+            matvec(s.cur.R, X, off);
+            for (int a = 0; a < 3; ++a) xw[a] = s.cur.r[a] + off[a];
+            double fq[3] = {p * rg[0], p * rg[1], p * rg[2]};
+            const double phat = p * gn;
+            cross3(s.cur.w, off, t3);
+            for (int a = 0; a < 3; ++a) uA[a] = s.cur.v[a] + t3[a];
+            double offB[3] = {xw[0] - b.rB[0], xw[1] - b.rB[1], xw[2] - b.rB[2]};
+            cross3(b.wB, offB, t3);
+            for (int a = 0; a < 3; ++a) uB[a] = b.vB[a] + t3[a];
+            for (int a = 0; a < 3; ++a) u[a] = uA[a] - uB[a];
+            if (b.c.damping > 0.0 && g < 0.0)
+            {
+                const double vn = u[0] * rg[0] + u[1] * rg[1] + u[2] * rg[2];
+                for (int a = 0; a < 3; ++a) fq[a] = fq[a] + b.c.damping * (-vn) * rg[a];
+            }
+            const double gs = gn > 1e-30 ? gn : 1e-30;
+            double un[3] = {rg[0] / gs, rg[1] / gs, rg[2] / gs};
+            const double udn = u[0] * un[0] + u[1] * un[1] + u[2] * un[2];
+            double ut[3] = {u[0] - udn * un[0], u[1] - udn * un[1], u[2] - udn * un[2]};
+            const double utn = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
+            const double den = sqrt(utn * utn + b.c.regularizer * b.c.regularizer);
+            if (b.c.friction * phat > 0.0)
+                for (int a = 0; a < 3; ++a) fq[a] = fq[a] + -b.c.friction * phat * ut[a] / den;
+            double tq[3];
+            cross3(off, fq, tq);
+            for (int a = 0; a < 3; ++a)
+            {
+                acc[a] += w * fq[a];
+                acc[3 + a] += w * tq[a];
+            }
+        }
+        if (threadIdx.x == 0 && store)
+        {
+            for (int a = 0; a < 3; ++a) s.c_tref[a] = tsdf[a];
+            s.c_len = L;
+            s.c_cleared = 0;
+        }
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int q = 0; q < 6; ++q)
+    {
+        const double v = warp_dsum(acc[q]);
+        if (lane == 0) s.red[warp][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        for (int q = 0; q < 6; ++q)
+        {
+            double v = 0.0;
+            for (int w = 0; w < kWarps; ++w) v += s.red[w][q];
+            if (q < 3)
+                s.F[q] = v;
+            else
+                s.tau[q - 3] = v;
+        }
+    }
+    __syncthreads();
+}
+
+// measure_pair for s.cur (contacts_sdf.py:171-214): m_gap, m_pen, m_vn,
+// m_active, m_valid.
+__device__ void measure_pass(const BeView& b, Shared& s)
+{
+    broad_phase(b, s);
+    MinRec best{INFINITY, INT_MAX, -1};
+    int nv = 0, na = 0;
+    int base = 0;
+    for (int c0 = 0; c0 < b.nq; c0 += kT)
+    {
+        double X[3], w, Y[3];
+        const bool kept = point_at(b, s, c0 + threadIdx.x, X, w);
+        int total;
+        const int pos = base + chunk_scan(s, kept, total);
+        base += total;
+        if (!kept) continue;
+        to_sdf(b, s.cur, X, Y);
+        double g, gr[3];
+        if (!sample64(b, Y, g, gr)) continue;
+        ++nv;
+        if (g < 0.0) ++na;
+        if (g < best.gap || (g == best.gap && pos < best.key)) best = MinRec{g, pos, c0 + (int)threadIdx.x};
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        MinRec q;
+        q.gap = __shfl_down_sync(0xffffffffu, best.gap, o);
+        q.key = __shfl_down_sync(0xffffffffu, best.key, o);
+        q.i = __shfl_down_sync(0xffffffffu, best.i, o);
+        if (q.gap < best.gap || (q.gap == best.gap && q.key < best.key)) best = q;
+    }
+    nv = warp_isum(nv);
+    na = warp_isum(na);
+    if (lane == 0)
+    {
+        s.mins[warp] = best;
+        s.cnt[warp][0] = nv;
+        s.cnt[warp][1] = na;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        MinRec m = s.mins[0];
+        int v = s.cnt[0][0], a = s.cnt[0][1];
+        for (int k = 1; k < kWarps; ++k)
+        {
+            if (s.mins[k].gap < m.gap || (s.mins[k].gap == m.gap && s.mins[k].key < m.key)) m = s.mins[k];
+            v += s.cnt[k][0];
+            a += s.cnt[k][1];
+        }
+        s.m_valid = v;
+        s.m_active = a;
+        s.m_gap = v ? m.gap : INFINITY;
+        s.m_pen = v && m.gap < 0.0 ? -m.gap : 0.0;
+        s.m_vn = 0.0;
+        s.count = v ? m.key : -1;
+        s.mi = v ? m.i : -1;
+    }
+    __syncthreads();
+    // normal relative velocity at the minimum point (contacts_sdf.py:199-211)
+    if (threadIdx.x == 0 && s.mi >= 0)
+    {
+        double X[3], w, Y[3], g, gr[3];
+        point_at(b, s, s.mi, X, w);
+        to_sdf(b, s.cur, X, Y);
+        sample64(b, Y, g, gr);
+        const double gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+        double un[3] = {0.0, 0.0, 1.0};
+        if (gn > 1e-30)
+            for (int a = 0; a < 3; ++a) un[a] = gr[a] / gn;
+        double n[3];
+        matvec(b.RB, un, n);
+        const double nn = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (nn > 1e-30)
+            for (int a = 0; a < 3; ++a) n[a] = n[a] / nn;
+        double off[3], xw[3], t3[3], uA[3], uB[3];
+        matvec(s.cur.R, X, off);
+        for (int a = 0; a < 3; ++a) xw[a] = s.cur.r[a] + off[a];
+        cross3(s.cur.w, off, t3);
+        for (int a = 0; a < 3; ++a) uA[a] = s.cur.v[a] + t3[a];
+        double offB[3] = {xw[0] - b.rB[0], xw[1] - b.rB[1], xw[2] - b.rB[2]};
+        cross3(b.wB, offB, t3);
+        for (int a = 0; a < 3; ++a) uB[a] = b.vB[a] + t3[a];
+        double du[3] = {uA[0] - uB[0], uA[1] - uB[1], uA[2] - uB[2]};
+        s.m_vn = dot3(du, n);
+    }
+    __syncthreads();
+}
+
+// _kinematic_update (implicit_be.py:507-534), thread 0.
+__device__ void kinematic(const Body& q0, const double V[6], double dt, Body& out)
+{
+    for (int a = 0; a < 3; ++a)
+    {
+        out.v[a] = V[a];
+        out.w[a] = V[3 + a];
+        out.r[a] = q0.r[a] + dt * V[a];
+    }
+    const double th[3] = {dt * V[3], dt * V[4], dt * V[5]};
+    const double n = sqrt(th[0] * th[0] + th[1] * th[1] + th[2] * th[2]);
+    if (n > 1e-30)
+    {
+        const double ax[3] = {th[0] / n, th[1] / n, th[2] / n};
+        const double c = cos(n), sn = sin(n);
+        const double K[9] = {0.0, -ax[2], ax[1], ax[2], 0.0, -ax[0], -ax[1], ax[0], 0.0};
+        double dR[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                dR[3 * i + j] = (i == j ? c : 0.0) + sn * K[3 * i + j] + (1.0 - c) * (ax[i] * ax[j]);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                out.R[3 * i + j] = dR[3 * i] * q0.R[j] + dR[3 * i + 1] * q0.R[3 + j] + dR[3 * i + 2] * q0.R[6 + j];
+    }
+    else
+    {
+        for (int k = 0; k < 9; ++k) out.R[k] = q0.R[k];
+    }
+    out.t = q0.t;
+}
+
+// _residual at V = z (implicit_be.py:536-604): s.res, s.err, s.Iw, s.cur.
+__device__ void residual(const BeView& b, Shared& s, const double* z, double dt, bool allowed)
+{
+    if (threadIdx.x == 0) kinematic(s.q0, z, dt, s.cur);
+    __syncthreads();
+    if (allowed) eval_pass(b, s);
+    if (threadIdx.x == 0)
+    {
+        double RI[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                RI[3 * i + j] = s.cur.R[3 * i] * b.Ib[j] + s.cur.R[3 * i + 1] * b.Ib[3 + j] + s.cur.R[3 * i + 2] * b.Ib[6 + j];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                s.Iw[3 * i + j] = RI[3 * i] * s.cur.R[3 * j] + RI[3 * i + 1] * s.cur.R[3 * j + 1] +
+                                  RI[3 * i + 2] * s.cur.R[3 * j + 2];
+        double dV[6];
+        dV[0] = z[0] - s.q0.v[0];
+        dV[1] = z[1] - s.q0.v[1];
+        dV[2] = z[2] - s.q0.v[2];
+        dV[3] = z[3] - s.q0.w[0];
+        dV[4] = z[4] - s.q0.w[1];
+        dV[5] = z[5] - s.q0.w[2];
+        double Iww[3], C[3];
+        matvec(s.Iw, s.cur.w, Iww);
+        cross3(s.cur.w, Iww, C);
+        double err = 0.0;
+        for (int a = 0; a < 3; ++a)
+        {
+            double Q = b.mass * b.gravity[a];
+            if (allowed) Q = Q + s.F[a];
+            s.res[a] = b.mass * dV[a] / dt + 0.0 - Q;
+        }
+        for (int a = 0; a < 3; ++a)
+        {
+            const double MdV = s.Iw[3 * a] * dV[3] + s.Iw[3 * a + 1] * dV[4] + s.Iw[3 * a + 2] * dV[5];
+            double Q = 0.0;
+            if (allowed) Q = Q + s.tau[a];
+            s.res[3 + a] = MdV / dt + C[a] - Q;
+        }
+        for (int a = 0; a < 6; ++a) err = fmax(err, fabs(s.res[a]));
+        s.err = err;
+    }
+    __syncthreads();
+}
+
+// _step_be (implicit_be.py:468-505): src -> dst (thread-0 copies), contact
+// forces of the pair when `allowed`.
+__device__ void step_be(const BeView& b, Shared& s, const Body* src, Body* dst, double dt, bool allowed)
+{
+    if (threadIdx.x == 0)
+    {
+        s.q0 = *src;
+        for (int a = 0; a < 3; ++a)
+        {
+            s.z[a] = src->v[a];
+            s.z[3 + a] = src->w[a];
+        }
+        s.c_enabled = allowed ? 1 : 0;
+        s.c_cleared = 1;
+    }
+    __syncthreads();
+    residual(b, s, s.z, dt, allowed);
+    for (int it = 0; it < b.p.max_iter; ++it)
+    {
+        if (s.err < b.p.tol) break;
+        if (threadIdx.x == 0)
+        {
+            // tangent (_tangent / _contact_tangent): M/h + diag(Kc) on the
+            // translational rows; the two diagonal blocks solved exactly
+            double ktt = b.mass / dt;
+            double kd[3] = {ktt, ktt, ktt};
+            if (allowed)
+            {
+                const double vel = sqrt(s.cur.v[0] * s.cur.v[0] + s.cur.v[1] * s.cur.v[1] + s.cur.v[2] * s.cur.v[2]);
+                const double de = fmax(vel * dt, 1e-10);
+                double stiff;
+                if (b.c.order == 1.0)
+                    stiff = b.c.stiffness * dt;
+                else
+                    stiff = b.c.stiffness * b.c.order * pow(de, b.c.order - 1.0) * dt + 5e2;
+                const double tot = stiff + b.c.damping * b.area;
+                for (int a = 0; a < 3; ++a) kd[a] = kd[a] + tot;
+            }
+            for (int a = 0; a < 3; ++a) s.dz[a] = -s.res[a] / kd[a];
+            // (Iw/h) x = -res_w by Cholesky
+            double A[9];
+            for (int k = 0; k < 9; ++k) A[k] = s.Iw[k] / dt;
+            const double l00 = sqrt(A[0]);
+            const double l10 = A[3] / l00, l20 = A[6] / l00;
+            const double l11 = sqrt(A[4] - l10 * l10);
+            const double l21 = (A[7] - l20 * l10) / l11;
+            const double l22 = sqrt(A[8] - l20 * l20 - l21 * l21);
+            const double r0 = -s.res[3], r1 = -s.res[4], r2 = -s.res[5];
+            const double y0 = r0 / l00, y1 = (r1 - l10 * y0) / l11, y2 = (r2 - l20 * y0 - l21 * y1) / l22;
+            const double x2 = y2 / l22, x1 = (y1 - l21 * x2) / l11, x0 = (y0 - l10 * x1 - l20 * x2) / l00;
+            s.dz[3] = x0;
+            s.dz[4] = x1;
+            s.dz[5] = x2;
+            double nr = 0.0;
+            for (int a = 0; a < 6; ++a) nr += s.res[a] * s.res[a];
+            s.r0 = sqrt(nr);
+            s.found = 0;
+            s.alpha = 1.0;
+        }
+        __syncthreads();
+        if (b.p.line_search)
+        {
+            const double alphas[5] = {1.0, 0.5, 0.25, 0.125, 0.0625};
+            for (int k = 0; k < 5; ++k)
+            {
+                if (threadIdx.x < 6) s.zt[threadIdx.x] = s.z[threadIdx.x] + alphas[k] * s.dz[threadIdx.x];
+                __syncthreads();
+                residual(b, s, s.zt, dt, allowed);
+                if (threadIdx.x == 0)
+                {
+                    double nr = 0.0;
+                    for (int a = 0; a < 6; ++a) nr += s.res[a] * s.res[a];
+                    if (sqrt(nr) < s.r0)
+                    {
+                        s.alpha = alphas[k];
+                        s.found = 1;
+                    }
+                }
+                __syncthreads();
+                if (s.found) break;
+            }
+        }
+        if (threadIdx.x == 0)
+        {
+            const double alpha = s.found ? s.alpha : 1.0;
+            for (int a = 0; a < 6; ++a) s.z[a] = s.z[a] + alpha * s.dz[a];
+        }
+        __syncthreads();
+        residual(b, s, s.z, dt, allowed);
+    }
+    if (threadIdx.x == 0)
+    {
+        Body out;
+        kinematic(s.q0, s.z, dt, out);
+        out.t = s.q0.t + dt;
+        *dst = out;
+        s.c_enabled = 0;
+        s.c_cleared = 1;
+    }
+    __syncthreads();
+}
+
+__device__ void measure_body(const BeView& b, Shared& s, const Body& body)
+{
+    if (threadIdx.x == 0) s.cur = body;
+    __syncthreads();
+    measure_pass(b, s);
+}
+
+__device__ __forceinline__ bool region_active(int ph)
+{
+    return ph == kImpacting || ph == kActive || ph == kStable || ph == kLeaving;
+}
+
+// _refresh_contact_states (implicit_be.py:248-295), thread 0, after a
+// measure of the new state.
+__device__ void refresh(const BeView& b, Shared& s)
+{
+    const sdfo_be_params& p = b.p;
+    const double old = s.last_pen;
+    s.last_gap = s.m_gap;
+    s.last_pen = s.m_pen;
+    s.last_vn = s.m_vn;
+    if (s.phase == kInactive) return;
+    const double release_gap = fmax(5.0 * p.pen_max, 1e-9);
+    if (s.m_gap > release_gap && s.m_vn >= -1e-5)
+    {
+        s.release_count += 1;
+        s.phase = kLeaving;
+        s.dt_current = fmin(p.dt_normal, fmax(s.dt_current * p.dt_growth, p.dt_contact));
+        if (s.release_count >= p.release_steps)
+        {
+            s.phase = kInactive;
+            s.dt_current = p.dt_normal;
+            s.stable_count = s.release_count = s.min_dt_hits = 0;
+            s.last_toi = INFINITY;
+        }
+        return;
+    }
+    s.release_count = 0;
+    if (s.phase == kImpacting)
+    {
+        s.phase = kActive;
+        s.dt_current = fmax(p.dt_contact, p.dt_min);
+        return;
+    }
+    const double change = fabs(s.m_pen - old);
+    const double base = fmax(fabs(old), p.pen_max);
+    const bool stable_pen = change <= p.pen_max || change / base <= 5e-2;
+    const bool stable_vn = fabs(s.m_vn) <= 1e-5;
+    if (s.m_active > 0 && stable_pen && stable_vn)
+        s.stable_count += 1;
+    else
+        s.stable_count = 0;
+    if (s.stable_count >= p.stable_steps)
+    {
+        s.phase = kStable;
+        s.dt_current = fmin(fmin(p.dt_max_contact, p.dt_normal), fmax(s.dt_current * p.dt_growth, p.dt_contact));
+    }
+    else
+    {
+        s.phase = kActive;
+        s.dt_current = fmax(p.dt_contact, p.dt_min);
+    }
+}
+
+__global__ void __launch_bounds__(kT) k_be_step(BeView b, sdfo_be_scene* __restrict__ scenes, int n,
+                                                const double* __restrict__ dt_req, double* __restrict__ h_out)
+{
+    __shared__ Shared s;
+    const int sc = blockIdx.x;
+    const sdfo_be_params& p = b.p;
+    if (threadIdx.x == 0)
+    {
+        const sdfo_be_scene& in = scenes[sc];
+        for (int a = 0; a < 3; ++a)
+        {
+            s.q.r[a] = in.body.r[a];
+            s.q.v[a] = in.body.v[a];
+            s.q.w[a] = in.body.w[a];
+        }
+        for (int k = 0; k < 9; ++k) s.q.R[k] = in.body.R[k];
+        s.q.t = in.t;
+        s.dt_current = in.dt_current;
+        s.last_gap = in.last_gap;
+        s.last_pen = in.last_penetration;
+        s.last_vn = in.last_normal_velocity;
+        s.last_toi = in.last_toi;
+        s.phase = in.phase;
+        s.stable_count = in.stable_count;
+        s.release_count = in.release_count;
+        s.min_dt_hits = in.min_dt_hits;
+        s.c_enabled = 0;
+        s.c_cleared = 1;
+        s.c_len = -1;
+        s.event = 0;
+    }
+    __syncthreads();
+    const double dt = dt_req[sc];
+    if (!(dt > 0.0))
+    {
+        if (threadIdx.x == 0 && h_out) h_out[sc] = 0.0;
+        return; // nothing to do for this scene (finished)
+    }
+    // _activate_initially_penetrating_regions
+    measure_body(b, s, s.q);
+    __shared__ double m0_gap;
+    if (threadIdx.x == 0)
+    {
+        s.last_gap = s.m_gap;
+        s.last_pen = s.m_pen;
+        s.last_vn = s.m_vn;
+        m0_gap = s.m_gap;
+        if (s.phase == kInactive && s.m_gap <= 0.0)
+        {
+            s.phase = kImpacting;
+            s.dt_current = fmin(p.dt_impact, p.dt_contact);
+        }
+        s.toi = fmin(dt, region_active(s.phase) ? s.dt_current : p.dt_normal); // h_cap
+    }
+    __syncthreads();
+    const double h_cap = s.toi;
+    // _find_earliest_new_contact
+    if (s.phase == kInactive && h_cap > 0.0)
+    {
+        step_be(b, s, &s.q, &s.tr, h_cap, false);
+        measure_body(b, s, s.tr);
+        if (threadIdx.x == 0)
+            s.flag = (m0_gap > 0.0 && (s.m_gap <= 0.0 || s.m_pen > p.pen_max)) ? 1 : 0;
+        __syncthreads();
+        if (s.flag)
+        {
+            // _bisect_toi_pair
+            if (threadIdx.x == 0)
+            {
+                s.lo = 0.0;
+                s.hi = h_cap;
+                s.hm_pen = s.m_pen;
+                s.hit = 0;
+            }
+            __syncthreads();
+            for (int it = 0; it < p.max_toi_bisect_iter; ++it)
+            {
+                if (threadIdx.x == 0 && s.hi - s.lo <= p.dt_min) s.hit = 1;
+                __syncthreads();
+                if (s.hit) break;
+                const double mid = 0.5 * (s.lo + s.hi);
+                step_be(b, s, &s.q, &s.tr, mid, false);
+                measure_body(b, s, s.tr);
+                if (threadIdx.x == 0)
+                {
+                    if (s.m_gap <= 0.0 || s.m_pen > p.pen_max)
+                    {
+                        s.hi = mid;
+                        s.hm_pen = s.m_pen;
+                    }
+                    else
+                        s.lo = mid;
+                }
+                __syncthreads();
+            }
+            if (s.hi < p.dt_min && h_cap >= p.dt_min)
+            {
+                if (threadIdx.x == 0)
+                {
+                    s.hi = p.dt_min;
+                    s.hit = 1;
+                }
+                __syncthreads();
+                step_be(b, s, &s.q, &s.tr, s.hi, false);
+                measure_body(b, s, s.tr);
+                if (threadIdx.x == 0) s.hm_pen = s.m_pen;
+                __syncthreads();
+            }
+            if (threadIdx.x == 0 && s.hi > 0.0)
+            {
+                if (s.hm_pen > p.pen_max && !s.hit)
+                {
+                    s.hi = fmax(s.lo, fmin(s.hi, p.dt_min));
+                    s.hit = 1;
+                }
+                s.toi = fmin(s.hi, h_cap);
+                s.event = 1;
+            }
+            __syncthreads();
+        }
+    }
+    double h;
+    if (s.event)
+    {
+        h = s.toi;
+        step_be(b, s, &s.q, &s.q, h, region_active(s.phase));
+        if (threadIdx.x == 0)
+        {
+            s.phase = kImpacting;
+            s.dt_current = fmin(p.dt_impact, p.dt_contact);
+            s.last_toi = h;
+            if (s.hit) s.min_dt_hits += 1;
+        }
+        __syncthreads();
+        measure_body(b, s, s.q);
+        if (threadIdx.x == 0)
+        {
+            s.last_gap = s.m_gap;
+            s.last_pen = s.m_pen;
+            s.last_vn = s.m_vn;
+        }
+    }
+    else
+    {
+        h = h_cap;
+        step_be(b, s, &s.q, &s.q, h, region_active(s.phase));
+        measure_body(b, s, s.q);
+        if (threadIdx.x == 0) refresh(b, s);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        sdfo_be_scene& out = scenes[sc];
+        for (int a = 0; a < 3; ++a)
+        {
+            out.body.r[a] = s.q.r[a];
+            out.body.v[a] = s.q.v[a];
+            out.body.w[a] = s.q.w[a];
+        }
+        for (int k = 0; k < 9; ++k) out.body.R[k] = s.q.R[k];
+        out.t = s.q.t;
+        out.dt_current = s.dt_current;
+        out.last_gap = s.last_gap;
+        out.last_penetration = s.last_pen;
+        out.last_normal_velocity = s.last_vn;
+        out.last_toi = s.last_toi;
+        out.phase = s.phase;
+        out.stable_count = s.stable_count;
+        out.release_count = s.release_count;
+        out.min_dt_hits = s.min_dt_hits;
+        if (h_out) h_out[sc] = h;
+    }
+}
+
+} // namespace
+} // namespace sdfo
+
+struct sdfo_be_stepper
+{
+    const sdfo_contact_pair* pair = nullptr;
+    sdfo::BeView view{};
+    int64_t capacity = 0;
+    ~sdfo_be_stepper()
+    {
+        sdfo::device_free(view.cg);
+        sdfo::device_free(view.cgrad);
+        sdfo::device_free(view.cvalid);
+    }
+};
+
+using namespace sdfo;
+
+extern "C" {
+
+void sdfo_be_params_default(sdfo_be_params* p)
+{
+    if (!p) return;
+    p->max_iter = 20;
+    p->line_search = 1;
+    p->max_toi_bisect_iter = 60;
+    p->stable_steps = 5;
+    p->release_steps = 3;
+    p->reserved0 = 0;
+    p->tol = 1e-8;
+    p->pen_max = 1e-6;
+    p->dt_min = 1e-8;
+    p->dt_impact = 1e-7;
+    p->dt_contact = 1e-5;
+    p->dt_max_contact = 1e-4;
+    p->dt_normal = 1e-3;
+    p->dt_growth = 1.5;
+}
+
+void sdfo_be_scene_init(sdfo_be_scene* s, const sdfo_body_state* body, double t, const sdfo_be_params* p)
+{
+    if (!s) return;
+    std::memset(s, 0, sizeof(*s));
+    if (body) s->body = *body;
+    s->t = t;
+    s->dt_current = p ? p->dt_normal : 1e-3;
+    s->last_gap = INFINITY;
+    s->last_toi = INFINITY;
+    s->phase = 0;
+}
+
+int sdfo_be_stepper_create(const sdfo_contact_pair* pair, const sdfo_contact_params* contact,
+                           const sdfo_rigid_body* body_a, const sdfo_body_state* body_b,
+                           const sdfo_be_params* params, int64_t max_scenes, sdfo_be_stepper** out)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(pair && contact && body_a && body_b && params && out, SDFO_ERR_INVALID_ARGUMENT,
+                     "NULL argument");
+        *out = nullptr;
+        SDFO_REQUIRE(pair->grid != nullptr, SDFO_ERR_INVALID_ARGUMENT, "pair was created without a grid");
+        const sdfo_grid* g = pair->grid;
+        SDFO_REQUIRE(g->info.layout == SDFO_LAYOUT_DENSE && g->d.phi64 != nullptr, SDFO_ERR_UNSUPPORTED,
+                     "BE stepping samples a dense grid's FP64 values (build, load or create it from FP64 data)");
+        SDFO_REQUIRE(max_scenes > 0 && max_scenes <= 0x7fffffff, SDFO_ERR_INVALID_ARGUMENT, "bad scene count");
+        SDFO_REQUIRE(params->max_iter >= 0 && params->max_toi_bisect_iter >= 0, SDFO_ERR_INVALID_ARGUMENT,
+                     "negative iteration count");
+        SDFO_REQUIRE(body_a->mass > 0.0, SDFO_ERR_INVALID_ARGUMENT, "body mass must be positive");
+        std::unique_ptr<sdfo_be_stepper> st(new sdfo_be_stepper());
+        st->pair = pair;
+        BeView& b = st->view;
+        b.g = make_view(g);
+        b.phi64 = g->d.phi64;
+        b.nq = (int)pair->nq;
+        b.nleaves = pair->nleaves;
+        b.cull = pair->narrow_margin >= 0.0 ? 1 : 0;
+        b.px = pair->px64;
+        b.pw = pair->pw64;
+        b.pleaf = pair->pleaf;
+        b.ox = pair->ox64;
+        b.ow = pair->ow64;
+        b.leaf_box = pair->leaf_box;
+        for (int a = 0; a < 6; ++a) b.root[a] = pair->root[a];
+        for (int a = 0; a < 3; ++a)
+        {
+            b.bmin[a] = g->info.bmin[a];
+            b.bmax[a] = g->info.bmax[a];
+            b.rB[a] = body_b->r[a];
+            b.vB[a] = body_b->v[a];
+            b.wB[a] = body_b->w[a];
+            b.gravity[a] = body_a->gravity[a];
+        }
+        for (int k = 0; k < 9; ++k)
+        {
+            b.RB[k] = body_b->R[k];
+            b.Ib[k] = body_a->inertia[k];
+        }
+        b.box_margin = std::max(pair->narrow_margin, 0.05);
+        b.narrow = pair->narrow_margin;
+        b.mass = body_a->mass;
+        // np.sum of the pair's (normalised) weights: the tangent's `area`
+        double area = 0.0;
+        if (pair->nq > 0)
+        {
+            std::vector<double> w((size_t)pair->nq);
+            SDFO_CUDA(cudaMemcpy(w.data(), pair->ow64, sizeof(double) * pair->nq, cudaMemcpyDeviceToHost));
+            for (double x : w) area += x;
+        }
+        b.area = area;
+        b.c = *contact;
+        b.p = *params;
+        st->capacity = max_scenes;
+        const size_t slots = (size_t)max_scenes * (size_t)std::max<int64_t>(pair->nq, 1);
+        b.cg = dalloc<double>(slots);
+        b.cgrad = dalloc<double>(3 * slots);
+        b.cvalid = dalloc<unsigned char>(slots);
+        *out = st.release();
+    });
+}
+
+int sdfo_be_stepper_step(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n, const double* d_dt,
+                         double* d_h, void* stream)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(st != nullptr, SDFO_ERR_INVALID_ARGUMENT, "stepper is NULL");
+        SDFO_REQUIRE(n >= 0 && n <= st->capacity, SDFO_ERR_INVALID_ARGUMENT,
+                     "scene count exceeds the stepper's capacity");
+        if (n == 0) return;
+        SDFO_REQUIRE(d_scenes && d_dt, SDFO_ERR_INVALID_ARGUMENT, "scenes and step sizes are required");
+        k_be_step<<<(unsigned)n, kT, 0, as_stream(stream)>>>(st->view, d_scenes, (int)n, d_dt, d_h);
+        SDFO_CHECK_LAUNCH();
+    });
+}
+
+int sdfo_be_stepper_destroy(sdfo_be_stepper* st)
+{
+    delete st;
+    return SDFO_OK;
+}
+
+} // extern "C"

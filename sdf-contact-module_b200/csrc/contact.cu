@@ -2,9 +2,14 @@
 // the forward-mode 6x6 pose Jacobian.
 //
 // Restates SDFContactEngine.evaluate (prototype/src/dynamics/contacts_sdf.py:
-// 225-385) without its culling heuristics (AABB broad phase, point BVH, the
-// |Y_z| < margin narrow filter), which only skip points that contribute no
-// force:
+// 225-385).  Without a ContactCull every quadrature point is evaluated; with
+// one, the engine's culling is applied as the reference does it: the point
+// BVH's leaves overlapping the query box RA^T (bmin - rA) - m ..
+// RA^T (bmax - rA) + m (m = max(narrow margin, 0.05); all points when the box
+// encloses every point or no leaf overlaps it), then the narrow filter
+// |Y_z| < narrow margin.  The same pass can produce measure_pair's
+// ContactMeasure (contacts_sdf.py:171-214) over the BVH-kept points.  The
+// force law:
 //   Y = R_B^T (r_A + R_A X - r_B)                       (marker-free transform)
 //   g, grad g = SDF(Y) (Trilinear or Tricubic)           (local, raw gradient)
 //   active iff valid and k max(-g,0)^n > 1e-30
@@ -21,6 +26,8 @@
 // and stays L1/L2-resident; the grid gather and interpolation are FP32; the
 // per-point force law of active points, the Jacobian and the reductions
 // (warp shuffles, then shared memory) are FP64.
+#include <climits>
+
 #include "interp.cuh"
 
 namespace sdfo {
@@ -127,27 +134,35 @@ struct PoseFrame
 };
 
 // The SDFContactEngine.evaluate force law of quadrature point i
-// (contacts_sdf.py:256-385); returns whether the point is active (valid and
-// k max(-g,0)^n > 1e-30).  HESS also records the interpolant's Hessian for
-// the Jacobian.
+// (contacts_sdf.py:256-385).  Returns 0 when the point is outside the grid,
+// 1 when it is inside but exerts no force (k max(-g,0)^n <= 1e-30, or
+// dropped by the narrow filter |Y_z| < narrow when narrow >= 0), 2 when it
+// is active.  `gap` receives the gap of in-grid points; with need_gap false
+// a point failing the narrow filter is not sampled (status 1, gap unset).
+// HESS also records the interpolant's Hessian for the Jacobian.
 template <int MODE, bool SPARSE, int BD, bool HESS>
-__device__ __forceinline__ bool point_state(const GridView& g, const float* __restrict__ qx,
-                                            const float* __restrict__ qw, int i,
-                                            const sdfo_body_state& sA, const sdfo_body_state& sB,
-                                            const PoseFrame& f, const sdfo_contact_params& prm,
-                                            PointState& st)
+__device__ __forceinline__ int point_state(const GridView& g, const float* __restrict__ qx,
+                                           const float* __restrict__ qw, int i,
+                                           const sdfo_body_state& sA, const sdfo_body_state& sB,
+                                           const PoseFrame& f, const sdfo_contact_params& prm,
+                                           double narrow, bool need_gap, PointState& st,
+                                           double& gap_out)
 {
     const v3 X = V(__ldg(qx + 3 * i), __ldg(qx + 3 * i + 1), __ldg(qx + 3 * i + 2));
     st.off = mul(sA.R, X);                   // x_w - r_A
     const v3 Yv = mulT(sB.R, st.off) + f.tl; // body-B local point
+    const bool narrow_ok = !(narrow >= 0.0) || fabs(Yv.z) < narrow;
+    if (!narrow_ok && !need_gap) return 1;
     const double Y[3] = {Yv.x, Yv.y, Yv.z};
     float gapf;
-    if (!sample<MODE, SPARSE, BD, HESS>(g, Y, gapf, st.gl, st.Hl)) return false;
+    if (!sample<MODE, SPARSE, BD, HESS>(g, Y, gapf, st.gl, st.Hl)) return 0;
     const double gap = gapf;
+    gap_out = gap;
+    if (!narrow_ok) return 1;
     const double delta = gap < 0.0 ? -gap : 0.0;
     const double dpow = prm.order == 2.0 ? delta * delta : prm.order == 1.0 ? delta : pow(delta, prm.order);
     st.p = prm.stiffness * dpow;
-    if (!(st.p > 1e-30)) return false;
+    if (!(st.p > 1e-30)) return 1;
     st.wq = (double)__ldg(qw + i);
     const v3 xw = f.rA + st.off;
     st.rg = mul(sB.R, st.gl);
@@ -170,7 +185,7 @@ __device__ __forceinline__ bool point_state(const GridView& g, const float* __re
     st.dgdd = -prm.stiffness * (prm.order == 2.0 ? 2.0 * delta
                                 : prm.order == 1.0 ? 1.0
                                                    : prm.order * pow(delta, prm.order - 1.0));
-    return true;
+    return 2;
 }
 
 // Column j of the point's d(f, x f)/d(dx, dtheta), weighted by w.
@@ -240,12 +255,51 @@ __device__ __forceinline__ void jacobian_column(const PointState& st, const sdfo
 #define SDFO_CONTACT_JAC_MIN_BLOCKS 2
 #endif
 
-template <int MODE, bool SPARSE, int BD, bool JAC>
+// Lexicographic (gap, key) minimum for measure_pair's argmin: the reference
+// takes the first minimum in its point order, `key` is the point's position
+// in that order.
+struct MinRec
+{
+    double gap;
+    int key;
+    int i;
+};
+
+__device__ __forceinline__ bool less_rec(const MinRec& a, const MinRec& b)
+{
+    return a.gap < b.gap || (a.gap == b.gap && a.key < b.key);
+}
+
+__device__ __forceinline__ MinRec warp_min(MinRec r)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        MinRec q;
+        q.gap = __shfl_down_sync(0xffffffffu, r.gap, o);
+        q.key = __shfl_down_sync(0xffffffffu, r.key, o);
+        q.i = __shfl_down_sync(0xffffffffu, r.i, o);
+        if (less_rec(q, r)) r = q;
+    }
+    return r;
+}
+
+__device__ __forceinline__ int warp_isum(int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// EXT: the culled / measuring variant (ContactCull, measures); without it
+// every point is evaluated and no measure is produced.
+template <int MODE, bool SPARSE, int BD, bool JAC, bool EXT>
 __global__ void __launch_bounds__(kContactThreads,
                                   JAC ? SDFO_CONTACT_JAC_MIN_BLOCKS : SDFO_CONTACT_MIN_BLOCKS)
     k_contact(GridView g, const float* __restrict__ qx, const float* __restrict__ qw, int nq,
               const sdfo_body_state* __restrict__ poses, const sdfo_body_state* __restrict__ body_b,
-              sdfo_contact_params prm, double* __restrict__ ft, double* __restrict__ jac)
+              sdfo_contact_params prm, double* __restrict__ ft, double* __restrict__ jac, ContactCull cull,
+              sdfo_contact_measure* __restrict__ meas)
 {
     constexpr int kWarps = kContactThreads / 32;
     const int pose = blockIdx.x;
@@ -254,6 +308,12 @@ __global__ void __launch_bounds__(kContactThreads,
     __shared__ double sjac[JAC ? kWarps : 1][JAC ? 36 : 1];
     __shared__ int s_list[JAC ? kContactThreads : 1];
     __shared__ int s_wcnt[kWarps];
+    __shared__ unsigned s_mask[EXT ? kMaxCullLeaves / 32 : 1];
+    __shared__ double s_box[6];
+    __shared__ int s_full;
+    __shared__ MinRec s_min[EXT ? kWarps : 1];
+    __shared__ int s_cnt[EXT ? kWarps : 1][2];
+    __shared__ int s_prefix;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0)
     {
@@ -271,7 +331,52 @@ __global__ void __launch_bounds__(kContactThreads,
     f.vB = V(sB.v[0], sB.v[1], sB.v[2]);
     f.wB = V(sB.w[0], sB.w[1], sB.w[2]);
     f.tl = mulT(sB.R, f.rA - f.rB); // R_B^T (r_A - r_B)
+
+    // broad phase: AABB_BVH.query(bmin_local, bmax_local) (bvh.py:62-80)
+    bool full = true;
+    if (EXT && cull.enabled)
+    {
+        if (threadIdx.x == 0)
+        {
+            const v3 lo = mulT(sA.R, V(cull.bmin[0], cull.bmin[1], cull.bmin[2]) - f.rA);
+            const v3 hi = mulT(sA.R, V(cull.bmax[0], cull.bmax[1], cull.bmax[2]) - f.rA);
+            s_box[0] = lo.x - cull.box_margin;
+            s_box[1] = lo.y - cull.box_margin;
+            s_box[2] = lo.z - cull.box_margin;
+            s_box[3] = hi.x + cull.box_margin;
+            s_box[4] = hi.y + cull.box_margin;
+            s_box[5] = hi.z + cull.box_margin;
+            bool enc = true;
+            for (int a = 0; a < 3; ++a)
+                enc = enc && s_box[a] <= cull.root[a] && s_box[3 + a] >= cull.root[3 + a];
+            s_full = enc ? 1 : 0;
+        }
+        for (int w = threadIdx.x; w < (cull.nleaves + 31) / 32; w += kContactThreads) s_mask[w] = 0u;
+        __syncthreads();
+        full = s_full != 0;
+        if (!full)
+        {
+            bool any = false;
+            for (int l = threadIdx.x; l < cull.nleaves; l += kContactThreads)
+            {
+                const double* b = cull.leaf_box + 6 * (int64_t)l;
+                const bool skip = b[3] < s_box[0] || b[4] < s_box[1] || b[5] < s_box[2] || b[0] > s_box[3] ||
+                                  b[1] > s_box[4] || b[2] > s_box[5];
+                if (!skip)
+                {
+                    atomicOr(&s_mask[l >> 5], 1u << (l & 31));
+                    any = true;
+                }
+            }
+            full = __syncthreads_or(any) == 0; // no leaf: every point (contacts_sdf.py:268-269)
+        }
+    }
+    const double narrow = EXT && cull.enabled ? cull.narrow_margin : -1.0;
+    const bool want_force = ft != nullptr;
+    const bool want_meas = EXT && meas != nullptr;
     double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    MinRec best{INFINITY, INT_MAX, -1};
+    int nvalid = 0, nactive = 0;
 
     // block-uniform trip count: the barriers and warp reductions below see
     // every thread
@@ -281,17 +386,36 @@ __global__ void __launch_bounds__(kContactThreads,
         bool act = false;
         if (i < nq)
         {
-            PointState st;
-            act = point_state<MODE, SPARSE, BD, false>(g, qx, qw, i, sA, sB, f, prm, st);
-            if (act)
+            bool sel = true;
+            if (EXT && !full)
             {
-                const v3 tq = cross(st.off, st.fq);
-                acc[0] += st.wq * st.fq.x;
-                acc[1] += st.wq * st.fq.y;
-                acc[2] += st.wq * st.fq.z;
-                acc[3] += st.wq * tq.x;
-                acc[4] += st.wq * tq.y;
-                acc[5] += st.wq * tq.z;
+                const int l = __ldg(cull.pleaf + i);
+                sel = (s_mask[l >> 5] >> (l & 31)) & 1u;
+            }
+            if (sel)
+            {
+                PointState st;
+                double gap = 0.0;
+                const int status =
+                    point_state<MODE, SPARSE, BD, false>(g, qx, qw, i, sA, sB, f, prm, narrow, want_meas, st, gap);
+                if (want_meas && status > 0)
+                {
+                    ++nvalid;
+                    if (gap < 0.0) ++nactive;
+                    const MinRec r{gap, full ? (cull.porig ? __ldg(cull.porig + i) : i) : i, i};
+                    if (less_rec(r, best)) best = r;
+                }
+                act = status == 2 && want_force;
+                if (act)
+                {
+                    const v3 tq = cross(st.off, st.fq);
+                    acc[0] += st.wq * st.fq.x;
+                    acc[1] += st.wq * st.fq.y;
+                    acc[2] += st.wq * st.fq.z;
+                    acc[3] += st.wq * tq.x;
+                    acc[4] += st.wq * tq.y;
+                    acc[5] += st.wq * tq.z;
+                }
             }
         }
         if (!JAC) continue;
@@ -311,9 +435,10 @@ __global__ void __launch_bounds__(kContactThreads,
         if (warp * 32 < total)
         {
             PointState st;
+            double gap = 0.0;
             const bool mine = threadIdx.x < total &&
-                              point_state<MODE, SPARSE, BD, true>(g, qx, qw, s_list[threadIdx.x], sA,
-                                                                  sB, f, prm, st);
+                              point_state<MODE, SPARSE, BD, true>(g, qx, qw, s_list[threadIdx.x], sA, sB, f,
+                                                                  prm, narrow, false, st, gap) == 2;
 #pragma unroll 1
             for (int j = 0; j < 6; ++j)
             {
@@ -329,14 +454,29 @@ __global__ void __launch_bounds__(kContactThreads,
         }
         __syncthreads(); // s_list and s_wcnt are rewritten by the next chunk
     }
-#pragma unroll
-    for (int q = 0; q < 6; ++q)
+    if (want_force)
     {
-        const double s = warp_sum(acc[q]);
-        if (lane == 0) red[warp][q] = s;
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+        {
+            const double s = warp_sum(acc[q]);
+            if (lane == 0) red[warp][q] = s;
+        }
+    }
+    if (want_meas)
+    {
+        const MinRec r = warp_min(best);
+        const int nv = warp_isum(nvalid), na = warp_isum(nactive);
+        if (lane == 0)
+        {
+            s_min[warp] = r;
+            s_cnt[warp][0] = nv;
+            s_cnt[warp][1] = na;
+        }
+        if (threadIdx.x == 0) s_prefix = 0;
     }
     __syncthreads();
-    if (threadIdx.x < 6)
+    if (want_force && threadIdx.x < 6)
     {
         double s = 0.0;
 #pragma unroll
@@ -350,43 +490,127 @@ __global__ void __launch_bounds__(kContactThreads,
         for (int w = 0; w < kWarps; ++w) s += sjac[w][threadIdx.x];
         jac[36 * (int64_t)pose + threadIdx.x] = s;
     }
+    if (!want_meas) return;
+    MinRec b = s_min[0];
+    int nv = s_cnt[0][0], na = s_cnt[0][1];
+#pragma unroll
+    for (int w = 1; w < kWarps; ++w)
+    {
+        if (less_rec(s_min[w], b)) b = s_min[w];
+        nv += s_cnt[w][0];
+        na += s_cnt[w][1];
+    }
+    // position of the minimum in the broad phase's point list: the points of
+    // the kept leaves before its own
+    if (nv > 0 && !full)
+    {
+        const int lb = __ldg(cull.pleaf + b.i);
+        int part = 0;
+        for (int l = threadIdx.x; l < lb; l += kContactThreads)
+            if ((s_mask[l >> 5] >> (l & 31)) & 1u) part += __ldg(cull.leaf_start + l + 1) - __ldg(cull.leaf_start + l);
+        part = warp_isum(part);
+        if (lane == 0 && part) atomicAdd(&s_prefix, part);
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    sdfo_contact_measure out;
+    out.reserved0 = 0;
+    out.active_count = na;
+    out.valid_count = nv;
+    if (nv == 0)
+    {
+        out.gap = INFINITY;
+        out.penetration = 0.0;
+        out.normal_velocity = 0.0;
+        out.min_point_index = -1;
+    }
+    else
+    {
+        out.gap = b.gap;
+        out.penetration = b.gap < 0.0 ? -b.gap : 0.0;
+        out.min_point_index = full ? b.key : s_prefix + (b.i - __ldg(cull.leaf_start + __ldg(cull.pleaf + b.i)));
+        // normal relative velocity at the minimum (contacts_sdf.py:199-211)
+        const v3 X = V(__ldg(qx + 3 * b.i), __ldg(qx + 3 * b.i + 1), __ldg(qx + 3 * b.i + 2));
+        const v3 off = mul(sA.R, X);
+        const v3 Yv = mulT(sB.R, off) + f.tl;
+        const double Y[3] = {Yv.x, Yv.y, Yv.z};
+        float gapf;
+        v3 gl;
+        double Hl[6];
+        sample<MODE, SPARSE, BD, false>(g, Y, gapf, gl, Hl);
+        const double gn = sqrt(dot(gl, gl));
+        const v3 un = gn > 1e-30 ? (1.0 / gn) * gl : V(0.0, 0.0, 1.0);
+        v3 nw = mul(sB.R, un);
+        const double nn = sqrt(dot(nw, nw));
+        if (nn > 1e-30) nw = (1.0 / nn) * nw;
+        const v3 xw = f.rA + off;
+        const v3 uA = f.vA + cross(f.wA, off);
+        const v3 uB = f.vB + cross(f.wB, xw - f.rB);
+        out.normal_velocity = dot(uA - uB, nw);
+    }
+    meas[pose] = out;
+}
+
+struct ContactLaunch
+{
+    const float* qx;
+    const float* qw;
+    int nq;
+    const sdfo_body_state* pa;
+    int np;
+    const sdfo_body_state* pb;
+    sdfo_contact_params prm;
+    double* ft;
+    double* jac;
+    ContactCull cull;
+    sdfo_contact_measure* meas;
+};
+
+template <int MODE, bool SPARSE, int BD, bool EXT>
+void launch4(const GridView& v, const ContactLaunch& c, cudaStream_t s)
+{
+    if (c.jac)
+        k_contact<MODE, SPARSE, BD, true, EXT><<<c.np, kContactThreads, 0, s>>>(v, c.qx, c.qw, c.nq, c.pa, c.pb,
+                                                                                c.prm, c.ft, c.jac, c.cull, c.meas);
+    else
+        k_contact<MODE, SPARSE, BD, false, EXT><<<c.np, kContactThreads, 0, s>>>(v, c.qx, c.qw, c.nq, c.pa, c.pb,
+                                                                                 c.prm, c.ft, c.jac, c.cull, c.meas);
 }
 
 template <int MODE, bool SPARSE, int BD>
-void launch3(const GridView& v, const float* qx, const float* qw, int nq, const sdfo_body_state* pa,
-             int np, const sdfo_body_state* pb, const sdfo_contact_params& prm, double* ft,
-             double* jac, cudaStream_t s)
+void launch3(const GridView& v, const ContactLaunch& c, cudaStream_t s)
 {
-    if (jac)
-        k_contact<MODE, SPARSE, BD, true><<<np, kContactThreads, 0, s>>>(v, qx, qw, nq, pa, pb, prm, ft, jac);
+    if (c.cull.enabled || c.meas)
+        launch4<MODE, SPARSE, BD, true>(v, c, s);
     else
-        k_contact<MODE, SPARSE, BD, false><<<np, kContactThreads, 0, s>>>(v, qx, qw, nq, pa, pb, prm, ft, jac);
+        launch4<MODE, SPARSE, BD, false>(v, c, s);
 }
 
 template <int MODE>
-void launch2(const GridView& v, const float* qx, const float* qw, int nq, const sdfo_body_state* pa,
-             int np, const sdfo_body_state* pb, const sdfo_contact_params& prm, double* ft,
-             double* jac, cudaStream_t s)
+void launch2(const GridView& v, const ContactLaunch& c, cudaStream_t s)
 {
     if (v.layout == SDFO_LAYOUT_DENSE)
-        launch3<MODE, false, 0>(v, qx, qw, nq, pa, np, pb, prm, ft, jac, s);
+        launch3<MODE, false, 0>(v, c, s);
     else if (v.bd == 8)
-        launch3<MODE, true, 8>(v, qx, qw, nq, pa, np, pb, prm, ft, jac, s);
+        launch3<MODE, true, 8>(v, c, s);
     else
-        launch3<MODE, true, 0>(v, qx, qw, nq, pa, np, pb, prm, ft, jac, s);
+        launch3<MODE, true, 0>(v, c, s);
 }
 
 } // namespace
 
 void launch_contact(const GridView& v, int mode, const float* qx, const float* qw, int64_t nq,
                     const sdfo_body_state* pose_a, int64_t np, const sdfo_body_state* body_b,
-                    const sdfo_contact_params& prm, double* ft, double* jac, cudaStream_t s)
+                    const sdfo_contact_params& prm, double* ft, double* jac, cudaStream_t s,
+                    const ContactCull* cull, sdfo_contact_measure* meas)
 {
     if (np <= 0) return;
+    ContactLaunch c{qx, qw, (int)nq, pose_a, (int)np, body_b, prm, ft, jac, ContactCull{}, meas};
+    if (cull) c.cull = *cull;
     if (mode == SDFO_TRICUBIC)
-        launch2<SDFO_TRICUBIC>(v, qx, qw, (int)nq, pose_a, (int)np, body_b, prm, ft, jac, s);
+        launch2<SDFO_TRICUBIC>(v, c, s);
     else
-        launch2<SDFO_TRILINEAR>(v, qx, qw, (int)nq, pose_a, (int)np, body_b, prm, ft, jac, s);
+        launch2<SDFO_TRILINEAR>(v, c, s);
     SDFO_CHECK_LAUNCH();
 }
 

@@ -22,6 +22,7 @@
 // counts) are packed on the device, copied into pinned slots and written with
 // pwrite() at their file offsets, again by up to kMaxThreads threads.
 #include <fcntl.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
@@ -138,12 +139,24 @@ struct File
 {
     int fd = -1;
     int64_t size = 0;
+    unsigned char* map = nullptr; // writable mapping of an output file, or NULL
     File() = default;
     File(const File&) = delete;
     File& operator=(const File&) = delete;
     ~File()
     {
+        if (map) ::munmap(map, (size_t)size);
         if (fd >= 0) ::close(fd);
+    }
+    // Unmaps and closes; false when closing reports an error.
+    bool finish()
+    {
+        bool ok = true;
+        if (map) ok = ::munmap(map, (size_t)size) == 0;
+        map = nullptr;
+        if (fd >= 0) ok = (::close(fd) == 0) && ok;
+        fd = -1;
+        return ok;
     }
 };
 
@@ -365,7 +378,9 @@ void load_chunks(int fd, const std::vector<Chunk>& chunks, cudaStream_t s, int64
 
 // Device -> file: the copy (or packing kernel) of chunk k+T is in flight
 // while chunk k is written.
-void save_chunks(int fd, const std::vector<Chunk>& chunks, cudaStream_t s, int64_t slot_bytes,
+void put_chunk(const File& f, const void* src, int64_t bytes, int64_t off);
+
+void save_chunks(const File& f, const std::vector<Chunk>& chunks, cudaStream_t s, int64_t slot_bytes,
                  const RecordFn& pack)
 {
     if (chunks.empty()) return;
@@ -386,7 +401,7 @@ void save_chunks(int fd, const std::vector<Chunk>& chunks, cudaStream_t s, int64
         {
             if (k + (size_t)T < chunks.size()) issue(k + (size_t)T, use ^ 1);
             SDFO_CUDA(cudaEventSynchronize(e.ev[use]));
-            pwrite_full(fd, sl.h[use], chunks[k].bytes, chunks[k].off);
+            put_chunk(f, sl.h[use], chunks[k].bytes, chunks[k].off);
             use ^= 1;
         }
     });
@@ -909,12 +924,37 @@ sdfo_grid* load_sparse(const File& f, const Header& h, cudaStream_t s)
 // ---------------------------------------------------------------------------
 // save
 // ---------------------------------------------------------------------------
+// Opens, sizes and (where the file system can preallocate it, so that a full
+// disk is reported here and not as a fault on a mapped store) maps the output
+// file: the worker threads then copy chunks into the mapping in parallel,
+// which scales where concurrent pwrite() calls on one file serialise on its
+// inode lock.  Without preallocation the chunks are written with pwrite().
 void open_for_write(File& f, const char* path, int64_t size)
 {
-    f.fd = ::open(path, O_WRONLY | O_CREAT | O_TRUNC | O_CLOEXEC, 0666);
+    f.fd = ::open(path, O_RDWR | O_CREAT | O_TRUNC | O_CLOEXEC, 0666);
     if (f.fd < 0) io_error(std::string("Cannot open SdfOracle data file for writing: ") + path);
     if (::ftruncate(f.fd, (off_t)size) != 0)
         io_error(std::string("Failed to write SdfOracle data file: ") + std::strerror(errno));
+    f.size = size;
+    if (size <= 0) return;
+    // fallocate(2) itself, not posix_fallocate, whose fallback writes zeros
+    if (::fallocate(f.fd, 0, 0, (off_t)size) != 0)
+    {
+        if (errno == ENOSPC || errno == EFBIG)
+            io_error(std::string("Failed to write SdfOracle data file: ") + std::strerror(errno));
+        return; // no preallocation on this file system: pwrite
+    }
+    void* m = ::mmap(nullptr, (size_t)size, PROT_READ | PROT_WRITE, MAP_SHARED, f.fd, 0);
+    if (m != MAP_FAILED) f.map = static_cast<unsigned char*>(m);
+}
+
+// Writes one chunk's bytes at its file offset.
+void put_chunk(const File& f, const void* src, int64_t bytes, int64_t off)
+{
+    if (f.map)
+        std::memcpy(f.map + off, src, (size_t)bytes);
+    else
+        pwrite_full(f.fd, src, bytes, off);
 }
 
 // saveSdf (SdfIO.cpp:93-174): header, phi, n, H (always), witness, candidates.
@@ -969,7 +1009,7 @@ void save_dense(const sdfo_grid* g, const char* path, cudaStream_t s)
     if (sc) put_u32(hdr + 96, 4, (uint32_t)sc);
     File f;
     open_for_write(f, path, total);
-    pwrite_full(f.fd, hdr, kHeaderBytes, 0);
+    put_chunk(f, hdr, kHeaderBytes, 0);
     std::vector<Chunk> chunks;
     int64_t off = kHeaderBytes;
     for (auto& x : sec)
@@ -977,13 +1017,8 @@ void save_dense(const sdfo_grid* g, const char* path, cudaStream_t s)
         split(chunks, off, x.second, const_cast<void*>(x.first), kSlotBytes);
         off += x.second;
     }
-    save_chunks(f.fd, chunks, s, kSlotBytes, nullptr);
-    if (::close(f.fd) != 0)
-    {
-        f.fd = -1;
-        io_error("Failed to write SdfOracle data file");
-    }
-    f.fd = -1;
+    save_chunks(f, chunks, s, kSlotBytes, nullptr);
+    if (!f.finish()) io_error("Failed to write SdfOracle data file");
 }
 
 // saveSparseSdf (SdfIO.cpp:176-275): header, then per block its record.
@@ -1005,7 +1040,7 @@ void save_sparse(const sdfo_grid* g, const char* path, cudaStream_t s)
     if (sc) put_u32(hdr + 96, 24, (uint32_t)sc);
     File f;
     open_for_write(f, path, kHeaderBytes + B * r.bytes);
-    pwrite_full(f.fd, hdr, kHeaderBytes, 0);
+    put_chunk(f, hdr, kHeaderBytes, 0);
     const SparseArrays a{g->d.ijk, g->d.phin, g->d.hess6, g->d.ca_count, g->d.ca_phi32, g->d.ca_n32, g->d.ca_branch,
                          g->info.storage == SDFO_STORAGE_FP16 ? g->d.phin16 : nullptr,
                          g->info.storage == SDFO_STORAGE_FP16 ? g->d.brick_affine : nullptr};
@@ -1017,16 +1052,11 @@ void save_sparse(const sdfo_grid* g, const char* path, cudaStream_t s)
         const int64_t nb = std::min(per_chunk, B - b);
         chunks.push_back({kHeaderBytes + b * r.bytes, nb * r.bytes, nullptr, b, nb});
     }
-    save_chunks(f.fd, chunks, s, slot_bytes, [&](const Chunk& c, unsigned char* d_slot, cudaStream_t st) {
+    save_chunks(f, chunks, s, slot_bytes, [&](const Chunk& c, unsigned char* d_slot, cudaStream_t st) {
                     k_sparse_pack<<<(unsigned)c.count, kThreads, 0, st>>>(d_slot, r, c.first, a);
                     SDFO_CHECK_LAUNCH();
                 });
-    if (::close(f.fd) != 0)
-    {
-        f.fd = -1;
-        io_error("Failed to write SdfOracle data file");
-    }
-    f.fd = -1;
+    if (!f.finish()) io_error("Failed to write SdfOracle data file");
 }
 
 } // namespace

@@ -158,6 +158,33 @@ struct sdfo_grid
     ~sdfo_grid();
 };
 
+// A contact pair (contact_pair.cu): the quadrature set of body A bound to
+// body B's grid, with its point hierarchy.  Points are stored leaf by leaf
+// (px, pw, porig, pleaf) in FP32 for the contact kernels and in FP64 (px64,
+// pw64) for the BE step, which also keeps them in their original order
+// (ox64, ow64).
+struct sdfo_contact_pair
+{
+    const sdfo_grid* grid = nullptr;
+    int64_t nq = 0;
+    double narrow_margin = -1.0;
+    int nleaves = 0;
+    double root[6] = {0, 0, 0, 0, 0, 0};
+    std::vector<int32_t> h_order, h_leaf_start;
+    std::vector<double> h_leaf_box;
+    float* px = nullptr;
+    float* pw = nullptr;
+    double* px64 = nullptr;
+    double* pw64 = nullptr;
+    double* ox64 = nullptr;
+    double* ow64 = nullptr;
+    int32_t* porig = nullptr;
+    int32_t* pleaf = nullptr;
+    int32_t* leaf_start = nullptr;
+    double* leaf_box = nullptr;
+    ~sdfo_contact_pair();
+};
+
 namespace sdfo {
 
 // Largest m in [0, n) with offs[m] <= x (offs non-decreasing, offs[0] = 0):
@@ -277,9 +304,28 @@ int bvh_mode();
 void set_bvh_mode(int m);
 
 // Contact (contact.cu).
+// The culling of SDFContactEngine.evaluate / measure_pair: a point BVH over
+// the quadrature points (leaves in the order the reference's query visits
+// them, points stored leaf by leaf), the query box margin and the |Y_z|
+// narrow filter.  enabled == 0: every point, in its stored order.
+constexpr int kMaxCullLeaves = 32768;
+struct ContactCull
+{
+    int enabled;
+    int nleaves;
+    const double* leaf_box;   // (nleaves, 6): min x y z, max x y z
+    const int32_t* leaf_start; // (nleaves + 1) offsets into the point order
+    const int32_t* pleaf;      // leaf of each stored point
+    const int32_t* porig;      // original index of each stored point
+    double root[6];            // box of all points
+    double bmin[3], bmax[3];   // the grid's box (sdf.bmin / sdf.bmax)
+    double box_margin;         // max(narrow_margin, 0.05)
+    double narrow_margin;      // evaluate keeps |Y_z| < narrow_margin
+};
 void launch_contact(const GridView& v, int mode, const float* qx, const float* qw, int64_t nq,
                     const sdfo_body_state* pose_a, int64_t np, const sdfo_body_state* body_b,
-                    const sdfo_contact_params& prm, double* ft, double* jac, cudaStream_t s);
+                    const sdfo_contact_params& prm, double* ft, double* jac, cudaStream_t s,
+                    const ContactCull* cull = nullptr, sdfo_contact_measure* meas = nullptr);
 
 // FP16 re-encoding (grid.cu).
 void encode_fp16(const sdfo_grid* src, sdfo_grid* dst, cudaStream_t s);

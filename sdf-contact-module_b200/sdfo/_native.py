@@ -75,6 +75,21 @@ class ContactParams(ctypes.Structure):
                 ("regularizer", _D), ("activation_distance", _D)]
 
 
+class BEParams(ctypes.Structure):
+    _fields_ = [("max_iter", _I32), ("line_search", _I32), ("max_toi_bisect_iter", _I32),
+                ("stable_steps", _I32), ("release_steps", _I32), ("reserved0", _I32),
+                ("tol", _D), ("pen_max", _D), ("dt_min", _D), ("dt_impact", _D),
+                ("dt_contact", _D), ("dt_max_contact", _D), ("dt_normal", _D), ("dt_growth", _D)]
+
+
+class RigidBody(ctypes.Structure):
+    _fields_ = [("mass", _D), ("inertia", _D * 9), ("gravity", _D * 3)]
+
+
+class BodyState(ctypes.Structure):
+    _fields_ = [("r", _D * 3), ("R", _D * 9), ("v", _D * 3), ("w", _D * 3)]
+
+
 class BuildStats(ctypes.Structure):
     _fields_ = [("setup_ms", _D), ("bvh_ms", _D), ("fill_ms", _D), ("hessian_ms", _D),
                 ("total_ms", _D), ("voxels_filled", _I64), ("candidate_blocks", _I64),
@@ -123,6 +138,15 @@ SIGNATURES = [
     ("sdfo_grid_device_views", ctypes.c_int, [_P, ctypes.POINTER(DeviceViews)]),
     ("sdfo_grid_destroy", ctypes.c_int, [_P]),
     ("sdfo_file_probe", ctypes.c_int, [ctypes.c_char_p, _P, _P]),
+    ("sdfo_contact_pair_create", ctypes.c_int, [_P, _P, _P, _I64, _I32, _D, _I32, _P]),
+    ("sdfo_contact_pair_export_bvh", ctypes.c_int, [_P, _P, _P, _P, _P]),
+    ("sdfo_contact_pair_eval", ctypes.c_int, [_P, _I32, _P, _I64, _P, _P, _P, _P, _P, _P]),
+    ("sdfo_contact_pair_destroy", ctypes.c_int, [_P]),
+    ("sdfo_be_params_default", None, [_P]),
+    ("sdfo_be_scene_init", None, [_P, _P, _D, _P]),
+    ("sdfo_be_stepper_create", ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _P]),
+    ("sdfo_be_stepper_step", ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
+    ("sdfo_be_stepper_destroy", ctypes.c_int, [_P]),
     ("sdfo_grid_load_file", ctypes.c_int, [ctypes.c_char_p, _I32, _P, _P]),
     ("sdfo_grid_save_file", ctypes.c_int, [_P, ctypes.c_char_p, _P]),
     ("sdfo_query", ctypes.c_int, [_P, _I32, _P, _I32, _I64, _P, _P, _P, _P, _P, _P, _P]),

@@ -51,16 +51,27 @@ def rotvec_to_matrix(theta: torch.Tensor) -> torch.Tensor:
 
 
 class ContactBatch:
-    """Quadrature set of body A + contact parameters, bound to body B's grid."""
+    """Quadrature set of body A + contact parameters, bound to body B's grid.
+
+    ``narrow_margin`` None evaluates every quadrature point.  A number applies
+    SDFContactEngine's culling with that narrow margin (register_pair's
+    default is 0.01): the point-BVH cull (AABB_BVH, ``leaf_size`` points per
+    leaf) against body B's grid box with margin max(narrow_margin, 0.05),
+    then evaluate's |Y_z| < narrow_margin filter (contacts_sdf.py:244-298);
+    ``measure`` then applies the BVH cull as measure_pair does."""
 
     def __init__(self, grid, quad_x, quad_w, stiffness, order=1.0, damping=0.0, friction=0.5,
                  regularizer=1e-6, activation_distance=0.0, mode=N.TRILINEAR,
-                 normalize_weights=True, device="cuda"):
+                 normalize_weights=True, narrow_margin=None, leaf_size=16, device="cuda"):
         self.grid = grid
         qx = np.ascontiguousarray(quad_x, np.float64).reshape(-1, 3)
         qw = np.ascontiguousarray(quad_w, np.float64).reshape(-1)
         if normalize_weights and qw.sum() > 1e-30:
             qw = qw / qw.sum()  # register_pair (contacts_sdf.py:52-56)
+        self._qx64, self._qw64 = qx, qw
+        self.narrow_margin = narrow_margin
+        self.leaf_size = int(leaf_size)
+        self._pair = None
         self.qx = torch.as_tensor(qx, dtype=torch.float32, device=device).contiguous()
         self.qw = torch.as_tensor(qw, dtype=torch.float32, device=device).contiguous()
         self.nq = qx.shape[0]
@@ -70,25 +81,72 @@ class ContactBatch:
         self.mode = N.mode_id(mode)
         if self.mode not in (N.TRILINEAR, N.TRICUBIC):
             raise ValueError("contact supports Trilinear and Tricubic")
+        if narrow_margin is not None:
+            self._pair = self._make_pair(float(narrow_margin))
 
-    def evaluate(self, poses_a: torch.Tensor, body_b: torch.Tensor, jacobian=False,
-                 out=None, stream=None):
-        """poses_a (P,18), body_b (18,) float64 CUDA -> ft (P,6) [, jac (P,6,6)]."""
+    def _make_pair(self, narrow_margin):
+        out = ctypes.c_void_p()
+        N.check(N.load().sdfo_contact_pair_create(
+            self.grid.handle, self._qx64.ctypes.data_as(ctypes.c_void_p),
+            self._qw64.ctypes.data_as(ctypes.c_void_p), self.nq, 0, narrow_margin, self.leaf_size,
+            ctypes.byref(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "_pair", None) is not None and self._pair.value:
+            N.load().sdfo_contact_pair_destroy(self._pair)
+            self._pair = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _states(poses_a, body_b):
         pa = poses_a.contiguous()
         pb = body_b.reshape(18).contiguous()
         if pa.dtype != torch.float64 or pb.dtype != torch.float64:
             raise ValueError("body states must be float64")
+        return pa, pb
+
+    def evaluate(self, poses_a: torch.Tensor, body_b: torch.Tensor, jacobian=False,
+                 out=None, stream=None):
+        """poses_a (P,18), body_b (18,) float64 CUDA -> ft (P,6) [, jac (P,6,6)]."""
+        pa, pb = self._states(poses_a, body_b)
         P = pa.shape[0]
         if out is None:
             ft = torch.empty((P, 6), dtype=torch.float64, device=pa.device)
             jac = torch.empty((P, 6, 6), dtype=torch.float64, device=pa.device) if jacobian else None
         else:
             ft, jac = out
-        N.check(N.load().sdfo_contact_eval(self.grid.handle, self.mode, _t_ptr(self.qx),
-                                           _t_ptr(self.qw), self.nq, _t_ptr(pa), P, _t_ptr(pb),
-                                           ctypes.byref(self.params), _t_ptr(ft), _t_ptr(jac),
-                                           _stream_ptr(stream)))
+        if self._pair is None:
+            N.check(N.load().sdfo_contact_eval(self.grid.handle, self.mode, _t_ptr(self.qx),
+                                               _t_ptr(self.qw), self.nq, _t_ptr(pa), P, _t_ptr(pb),
+                                               ctypes.byref(self.params), _t_ptr(ft), _t_ptr(jac),
+                                               _stream_ptr(stream)))
+        else:
+            N.check(N.load().sdfo_contact_pair_eval(self._pair, self.mode, _t_ptr(pa), P, _t_ptr(pb),
+                                                    ctypes.byref(self.params), _t_ptr(ft),
+                                                    _t_ptr(jac), None, _stream_ptr(stream)))
         return (ft, jac) if jacobian else ft
+
+    def measure(self, poses_a: torch.Tensor, body_b: torch.Tensor, stream=None) -> dict:
+        """measure_pair (contacts_sdf.py:171-214) per pose: dict of CUDA
+        tensors gap, penetration, normal_velocity (float64), min_point_index,
+        active_count, valid_count (int32)."""
+        pa, pb = self._states(poses_a, body_b)
+        if self._pair is None:
+            self._pair = self._make_pair(-1.0)
+        P = pa.shape[0]
+        buf = torch.empty((P, 5), dtype=torch.float64, device=pa.device)
+        N.check(N.load().sdfo_contact_pair_eval(self._pair, self.mode, _t_ptr(pa), P, _t_ptr(pb),
+                                                ctypes.byref(self.params), None, None, _t_ptr(buf),
+                                                _stream_ptr(stream)))
+        ints = buf[:, 3:5].contiguous().view(torch.int32)
+        return dict(gap=buf[:, 0], penetration=buf[:, 1], normal_velocity=buf[:, 2],
+                    min_point_index=ints[:, 0], active_count=ints[:, 1], valid_count=ints[:, 2])
 
 
 def perturbed_poses(poses: torch.Tensor, h_lin=1e-7, h_ang=1e-6) -> torch.Tensor:
