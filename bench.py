@@ -57,10 +57,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--kernels-once", choices=["c2", "c5", "ca"], default=None,
+    ap.add_argument("--kernels-once", choices=["c2", "c5", "ca", "be"], default=None,
                     help="one launch of each query kernel on the workload (for ncu), then exit")
     ap.add_argument("--skip-ca", action="store_true",
                     help="leave out the contact-aware build / query section")
+    ap.add_argument("--skip-be", action="store_true",
+                    help="leave out the batched Backward-Euler contact step section")
     ap.add_argument("--skip-io", action="store_true",
                     help="leave out the SDFO file load / save section")
     ap.add_argument("--skip-c4", action="store_true",
@@ -534,6 +536,82 @@ def io_section(torch, cpu_ok, repeats=3):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def be_section(torch, dev, stream, steps, warmup, cpu_ok):
+    """Batched BackwardEulerIntegrator.step on the GPU (sdfo.be.BEStepper):
+    2048 ring drops on a slab (7,680 quadrature points each), `steps`
+    consecutive steps of dt = 1 ms from the drop (free flight with the
+    time-of-impact search, impact, contact at 10 us steps), each step one
+    launch for all scenes, timed with CUDA events.  CPU baseline: the NumPy
+    restatement of the reference integrator (oracle/be_port.py, which follows
+    implicit_be.py operation for operation) on the first scenes."""
+    from sdfo import SdfGrid
+    from sdfo import workloads as W
+    from sdfo.be import BEStepper
+
+    c = W.be_ring_drops(2048)
+    grid = SdfGrid.build_dense(*c["slab"], **c["build"])
+    p = c["params"]
+    st = BEStepper(grid, c["quad_x"], c["quad_w"], c["mass"], c["inertia"], p["stiffness"],
+                   order=p["order"], damping=p["damping"], friction=p["friction"],
+                   regularizer=p["regularizer"], activation_distance=p["activation_distance"],
+                   narrow_margin=0.01, max_scenes=len(c["r"]))
+    warm = st.scenes(c["r"], c["R"], c["v"], c["w"])
+    for _ in range(max(1, warmup)):
+        st.step(warm, 1e-3)
+    scenes = st.scenes(c["r"], c["R"], c["v"], c["w"])
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    hs = []
+    for a, b in evs:
+        a.record(stream)
+        hs.append(st.step(scenes, 1e-3, stream=stream))
+        b.record(stream)
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    u = st.unpack(scenes)
+    n = len(c["r"])
+    out = {"workload": "ring_drops_on_slab_2048_scenes_7680_points_dt1ms",
+           "scenes": n, "steps": steps, "step_ms": ms,
+           "scene_steps_per_s": n * steps / (sum(ms) * 1e-3),
+           "simulated_time_per_scene_s": float(u["t"].mean()),
+           "phases_after": {str(k): int((u["phase"] == k).sum()) for k in sorted(set(u["phase"].tolist()))},
+           "cpu_port_scene_steps_per_s": None}
+    if cpu_ok:
+        from oracle import be_port as P
+
+        g64 = grid.export_dense()
+        spec = dict(bmin=grid.bmin, voxel=grid.voxel, shape=grid.shape)
+        from oracle import interp_np
+
+        def qb(Y):
+            gap, grad, valid, _ = interp_np.query(spec, g64["phi"], g64["normal"], 2, Y)
+            gn = np.linalg.norm(grad, axis=1)
+            unit = np.zeros_like(grad)
+            unit[:, 2] = 1.0
+            ok = valid & (gn > 1e-30)
+            unit[ok] = grad[ok] / gn[ok, None]
+            return gap, grad, gn, unit, valid
+
+        w = c["quad_w"] / c["quad_w"].sum()
+        sc = P.Scene(qb, c["quad_x"], w, grid.bmin, grid.bmax, 0.01, p["stiffness"], p["order"],
+                     p["damping"], p["friction"], p["regularizer"], c["mass"], c["inertia"])
+        t0 = time.perf_counter()
+        done = 0
+        for i in range(4):
+            integ = P.Integrator(sc)
+            s = P.BodyState(c["r"][i].copy(), c["R"][i].copy(), c["v"][i].copy(), c["w"][i].copy())
+            for _ in range(steps):
+                integ.step(s, 1e-3)
+                done += 1
+            if time.perf_counter() - t0 > 20.0:
+                break
+        out["cpu_port_scene_steps_per_s"] = done / (time.perf_counter() - t0)
+        out["cpu_port_sample"] = f"{done} scene-steps of the first scenes, one host thread (NumPy)"
+    st.close()
+    return out
+
+
 def c4_section(torch, lib, N, dev, stream, flush, steps, warmup):
     """Config 4: 256 gear prisms (2k-60k tris, sparse 64^3..256^3, band 3):
     one batched build against 256 single builds, then 256 x 65,536 Tricubic
@@ -795,6 +873,9 @@ def run_ours(args, rank, world, local_rank):
     if not args.skip_ca:
         ca = contact_aware_section(torch, lib, N, dev, stream, flush, max(3, args.steps // 10),
                                    args.warmup, rank == 0 and world == 1)
+    be_out = None
+    if not args.skip_be:
+        be_out = be_section(torch, dev, stream, 10, 1, rank == 0 and world == 1)
     sdfo_io = None
     if not args.skip_io:
         sdfo_io = io_section(torch, rank == 0 and world == 1)
@@ -873,6 +954,7 @@ def run_ours(args, rank, world, local_rank):
         },
         "contact_aware": ca,
         "sdfo_io": sdfo_io,
+        "be_step": be_out,
         "c4": c4,
         "c5": c5,
     }
@@ -887,7 +969,8 @@ def kernels_once(which):
     regathering backward) with a 64 MB buffer written before each -- the
     program an ncu capture (-k regex:"k_query|k_backward") runs.  "ca": one
     contact-aware build of the cylinder (its fill kernels) and one
-    ContactAware query launch."""
+    ContactAware query launch.  "be": 296 ring drops (two per SM), eight
+    BE step launches (the last ones in contact)."""
     import ctypes
 
     import torch
@@ -897,6 +980,22 @@ def kernels_once(which):
     from sdfo import workloads as W
 
     lib = N.load()
+    if which == "be":
+        from sdfo.be import BEStepper
+
+        c = W.be_ring_drops(296)
+        grid = SdfGrid.build_dense(*c["slab"], **c["build"])
+        p = c["params"]
+        st = BEStepper(grid, c["quad_x"], c["quad_w"], c["mass"], c["inertia"], p["stiffness"],
+                       order=p["order"], damping=p["damping"], friction=p["friction"],
+                       regularizer=p["regularizer"], activation_distance=p["activation_distance"],
+                       narrow_margin=0.01, max_scenes=296)
+        scenes = st.scenes(c["r"], c["R"], c["v"], c["w"])
+        for _ in range(8):
+            st.step(scenes, 1e-3)
+        torch.cuda.synchronize()
+        print(json.dumps({"kernels_once": which, "scenes": 296, "steps": 8}))
+        return
     if which == "ca":
         from sdfo import meshes as M
 

@@ -98,6 +98,7 @@ struct Shared
     double c_tref[3];
     unsigned mask[kMaxCullLeaves / 32];
     int full;
+    double Rs[9], tl[3]; // R_B^T R_A and R_B^T (r_A - r_B) of the pass's pose
     double box[6];
     double red[kWarps][6];
     MinRec mins[kWarps];
@@ -179,24 +180,29 @@ __device__ bool sample64(const BeView& b, const double Y[3], double& g, double g
     return true;
 }
 
-// Y = R_B^T R_A X + R_B^T (r_A - r_B) (contacts_sdf.py:275-286).
-__device__ __forceinline__ void to_sdf(const BeView& b, const Body& s, const double X[3], double Y[3])
+// R_sdf = R_B^T R_A, t_sdf = R_B^T (r_A - r_B) of a pose (contacts_sdf.py:
+// 275-286), thread 0.
+__device__ __forceinline__ void sdf_frame(const BeView& b, const Body& s, double Rs[9], double tl[3])
 {
-    double Rs[9];
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j)
             Rs[3 * i + j] = b.RB[i] * s.R[j] + b.RB[3 + i] * s.R[3 + j] + b.RB[6 + i] * s.R[6 + j];
     double d[3] = {s.r[0] - b.rB[0], s.r[1] - b.rB[1], s.r[2] - b.rB[2]};
-    double t[3];
-    matTvec(b.RB, d, t);
-    matvec(Rs, X, Y);
-    for (int a = 0; a < 3; ++a) Y[a] = Y[a] + t[a];
+    matTvec(b.RB, d, tl);
+}
+
+// Y = R_sdf X + t_sdf with the pass's frame.
+__device__ __forceinline__ void to_sdf(const Shared& s, const double X[3], double Y[3])
+{
+    matvec(s.Rs, X, Y);
+    for (int a = 0; a < 3; ++a) Y[a] = Y[a] + s.tl[a];
 }
 
 // The broad phase of evaluate / measure_pair for the pose in s.cur
 // (contacts_sdf.py:244-269, bvh.py:62-80): leaf mask and the `full` flag.
 __device__ void broad_phase(const BeView& b, Shared& s)
 {
+    if (threadIdx.x == 0) sdf_frame(b, s.cur, s.Rs, s.tl);
     if (!b.cull)
     {
         if (threadIdx.x == 0) s.full = 1;
@@ -293,7 +299,7 @@ __device__ void eval_pass(const BeView& b, Shared& s)
         bool f = false;
         if (point_at(b, s, c0 + threadIdx.x, X, w))
         {
-            to_sdf(b, s.cur, X, Y);
+            to_sdf(s, X, Y);
             f = fabs(Y[2]) < narrow;
         }
         L += __syncthreads_count(f);
@@ -313,7 +319,7 @@ __device__ void eval_pass(const BeView& b, Shared& s)
             bool f = false;
             if (point_at(b, s, c0 + threadIdx.x, X, w))
             {
-                to_sdf(b, s.cur, X, Y);
+                to_sdf(s, X, Y);
                 f = fabs(Y[2]) < narrow;
             }
             int total;
@@ -433,7 +439,7 @@ __device__ void measure_pass(const BeView& b, Shared& s)
         const int pos = base + chunk_scan(s, kept, total);
         base += total;
         if (!kept) continue;
-        to_sdf(b, s.cur, X, Y);
+        to_sdf(s, X, Y);
         double g, gr[3];
         if (!sample64(b, Y, g, gr)) continue;
         ++nv;
@@ -482,7 +488,7 @@ __device__ void measure_pass(const BeView& b, Shared& s)
     {
         double X[3], w, Y[3], g, gr[3];
         point_at(b, s, s.mi, X, w);
-        to_sdf(b, s.cur, X, Y);
+        to_sdf(s, X, Y);
         sample64(b, Y, g, gr);
         const double gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
         double un[3] = {0.0, 0.0, 1.0};

@@ -10,10 +10,12 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <thread>
 #include <cfloat>
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -997,11 +999,31 @@ struct HostRefTree
     std::vector<RefNode> nodes;
     std::vector<int32_t> order;
     std::vector<double> lo, hi, cen;
+    std::map<int64_t, int64_t> sizes; // subtree node counts, filled before build
 
-    int build(int lo_i, int hi_i)
+    // Nodes of the subtree over n triangles (leaves of <= 8, median split);
+    // the sizes met in one tree take at most two values per level.
+    int64_t subtree_nodes(int64_t n)
     {
-        const int id = (int)nodes.size();
-        nodes.emplace_back();
+        if (n <= 8) return 1;
+        auto it = sizes.find(n);
+        if (it != sizes.end()) return it->second;
+        const int64_t v = 1 + subtree_nodes(n / 2) + subtree_nodes(n - n / 2);
+        sizes[n] = v;
+        return v;
+    }
+
+    // Read-only lookup once `sizes` holds every size of the tree.
+    int64_t node_count(int64_t n) const
+    {
+        return n <= 8 ? 1 : sizes.at(n);
+    }
+
+    // Node `id` over order[lo_i, hi_i); children get the pre-order ids
+    // id + 1 and id + 1 + |left subtree|, so disjoint subtrees can be built
+    // concurrently (`depth` levels spawn a thread for the left child).
+    void build(int lo_i, int hi_i, int id, int depth)
+    {
         double bmin[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, bmax[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
         double cmin[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, cmax[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
         for (int i = lo_i; i < hi_i; ++i)
@@ -1032,7 +1054,7 @@ struct HostRefTree
             n.start = lo_i;
             n.count = count;
             nodes[(size_t)id] = n;
-            return id;
+            return;
         }
         const double ext[3] = {cmax[0] - cmin[0], cmax[1] - cmin[1], cmax[2] - cmin[2]};
         int axis = 0;
@@ -1042,12 +1064,20 @@ struct HostRefTree
         const double* c = cen.data();
         std::nth_element(order.begin() + lo_i, order.begin() + mid, order.begin() + hi_i,
                          [c, axis](int x, int y) { return c[3 * x + axis] < c[3 * y + axis]; });
+        n.left = id + 1;
+        n.right = id + 1 + (int)node_count(mid - lo_i);
         nodes[(size_t)id] = n;
-        const int l = build(lo_i, mid);
-        const int r = build(mid, hi_i);
-        nodes[(size_t)id].left = l;
-        nodes[(size_t)id].right = r;
-        return id;
+        if (depth > 0 && count > 4096)
+        {
+            std::thread t([this, lo_i, mid, &n, depth] { build(lo_i, mid, n.left, depth - 1); });
+            build(mid, hi_i, n.right, depth - 1);
+            t.join();
+        }
+        else
+        {
+            build(lo_i, mid, n.left, 0);
+            build(mid, hi_i, n.right, 0);
+        }
     }
 };
 
@@ -1108,8 +1138,10 @@ void host_ref_tree(HostTreeData& out, const double* verts, const int32_t* tris, 
         }
         h.order[i] = (int32_t)i;
     }
-    h.nodes.reserve(2 * n);
-    h.build(0, (int)nt);
+    h.nodes.resize((size_t)h.subtree_nodes((int64_t)nt));
+    // up to 2^4 subtrees built concurrently (disjoint ranges of `order`)
+    const unsigned hw = std::thread::hardware_concurrency();
+    h.build(0, (int)nt, 0, hw >= 16 ? 4 : hw >= 8 ? 3 : hw >= 4 ? 2 : hw >= 2 ? 1 : 0);
     out.tri9.resize(9 * n);
     for (size_t sl = 0; sl < n; ++sl)
     {

@@ -4,7 +4,9 @@ on NVIDIA B200 (sm_100a) through the libsdfo_cuda C ABI (include/sdfo.h).
 Submodules:
   grid      SdfGrid -- build / query / load / save device grids
   autograd  sdf_query -- differentiable Trilinear / Tricubic queries
-  contact   ContactBatch -- fused batched contact force + 6x6 pose Jacobian
+  contact   ContactBatch -- fused batched contact force + 6x6 pose Jacobian,
+            the engine's culling and measure_pair; contact_force (autograd)
+  be        BEStepper -- batched Backward-Euler contact steps
   io        SDFO 0.1.0 file format
   meshes    procedural meshes and quadrature
   workloads seeded synthetic inputs of the benchmark configurations

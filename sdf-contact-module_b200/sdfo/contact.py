@@ -174,3 +174,57 @@ def fd_jacobian(batch: ContactBatch, poses: torch.Tensor, body_b: torch.Tensor, 
     h = torch.tensor([h_lin] * 3 + [h_ang] * 3, dtype=torch.float64, device=poses.device)
     jac = (fts[0::2] - fts[1::2]) / (2.0 * h[:, None, None])  # (6 params, P, 6 outputs)
     return ft, jac.permute(1, 2, 0).contiguous()
+
+
+def so3_left_jacobian(theta: torch.Tensor) -> torch.Tensor:
+    """J_l(theta) of exp: exp([theta + d]x) = exp([J_l d]x) exp([theta]x) to
+    first order; (P,3) -> (P,3,3), I + (1 - cos a)/a^2 K + (a - sin a)/a^3 K^2
+    with K = [theta]x, a = |theta| (series below 1e-4)."""
+    a = torch.linalg.norm(theta, dim=1)
+    K = torch.zeros(theta.shape[0], 3, 3, dtype=theta.dtype, device=theta.device)
+    K[:, 0, 1], K[:, 0, 2] = -theta[:, 2], theta[:, 1]
+    K[:, 1, 0], K[:, 1, 2] = theta[:, 2], -theta[:, 0]
+    K[:, 2, 0], K[:, 2, 1] = -theta[:, 1], theta[:, 0]
+    small = a < 1e-4
+    safe = torch.where(small, torch.ones_like(a), a)
+    c1 = torch.where(small, 0.5 - a * a / 24.0, (1.0 - torch.cos(safe)) / (safe * safe))
+    c2 = torch.where(small, 1.0 / 6.0 - a * a / 120.0, (safe - torch.sin(safe)) / (safe ** 3))
+    I = torch.eye(3, dtype=theta.dtype, device=theta.device).expand_as(K)
+    return I + c1[:, None, None] * K + c2[:, None, None] * (K @ K)
+
+
+class ContactForce(torch.autograd.Function):
+    """(F_A, tau_A) of a ContactBatch as a differentiable function of body A's
+    position r (P,3) and a rotation vector theta (P,3), R = exp([theta]x) R0.
+    The backward uses the kernel's analytic 6x6 Jacobian (forward mode, per
+    quadrature point): dL/dr = J_x^T dL/dft, dL/dtheta = J_l(theta)^T
+    J_theta^T dL/dft.  No reference counterpart (the reference tangent is a
+    finite difference, implicit_be.py:661-687)."""
+
+    @staticmethod
+    def forward(ctx, r, theta, R0, v, w, body_b, batch):
+        P = r.shape[0]
+        R = rotvec_to_matrix(theta.detach()) @ R0
+        poses = torch.cat([r.detach(), R.reshape(P, 9), v, w], dim=1).contiguous()
+        if ctx.needs_input_grad[0] or ctx.needs_input_grad[1]:
+            ft, jac = batch.evaluate(poses, body_b, jacobian=True)
+            ctx.save_for_backward(theta.detach(), jac)
+        else:
+            ft = batch.evaluate(poses, body_b)
+            ctx.save_for_backward(theta.detach(), None)
+        return ft
+
+    @staticmethod
+    def backward(ctx, dft):
+        theta, jac = ctx.saved_tensors
+        g = torch.einsum("pi,pij->pj", dft.to(jac.dtype), jac)
+        dr = g[:, :3] if ctx.needs_input_grad[0] else None
+        dth = None
+        if ctx.needs_input_grad[1]:
+            dth = torch.einsum("pij,pi->pj", so3_left_jacobian(theta), g[:, 3:])
+        return dr, dth, None, None, None, None, None
+
+
+def contact_force(batch: ContactBatch, r, theta, R0, v, w, body_b):
+    """Differentiable (F_A, tau_A) (P,6): see ContactForce."""
+    return ContactForce.apply(r, theta, R0, v, w, body_b, batch)

@@ -76,6 +76,41 @@ def c3_ring_cube(n_poses=4096, seed=2):
                             regularizer=1e-4, activation_distance=1e-5))
 
 
+def be_ring_drops(n_scenes=2048, seed=5):
+    """Batched drops of the ring of c3_ring_cube (torus R 50 mm, r 10 mm,
+    7,680 centroid quadrature points, steel) on a 0.3 x 0.3 x 0.05 m slab
+    whose top face is the plane z = 0 of its SDF frame (dense, target
+    resolution 128), with the same contact law as c3_ring_cube.  Each scene
+    starts with the ring's lowest point 0.5-3 mm above the plane, tilted by
+    at most 5 degrees, falling at 0.1-0.3 m/s with |v_xy| <= 0.1 m/s and
+    |w| <= 1 rad/s."""
+    cv, ct = M.cube(1.0)
+    sv = cv * np.array([0.3, 0.3, 0.05]) + np.array([0.0, 0.0, -0.025])
+    tv, tt = M.torus(0.05, 0.01, 192, 20)
+    qx, qw = M.centroid_quadrature(tv, tt)
+    rng = np.random.default_rng(seed)
+    phi = rng.uniform(0.0, 2.0 * np.pi, n_scenes)
+    ang = np.deg2rad(5.0) * rng.uniform(0.0, 1.0, n_scenes)
+    axis = np.stack([np.cos(phi), np.sin(phi), np.zeros(n_scenes)], 1)
+    R = _axis_angle(axis, ang)
+    low = np.einsum("nij,qj->nqi", R, qx)[:, :, 2].min(axis=1)
+    r = np.stack([rng.uniform(-0.05, 0.05, n_scenes), rng.uniform(-0.05, 0.05, n_scenes),
+                  -low + rng.uniform(0.0005, 0.003, n_scenes)], 1)
+    v = np.stack([rng.uniform(-0.07, 0.07, n_scenes), rng.uniform(-0.07, 0.07, n_scenes),
+                  -rng.uniform(0.1, 0.3, n_scenes)], 1)
+    d = rng.normal(size=(n_scenes, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    w = d * rng.uniform(0.0, 1.0, n_scenes)[:, None]
+    Rr, rr, rho = 0.05, 0.01, 7800.0
+    mass = rho * 2.0 * np.pi ** 2 * Rr * rr * rr
+    inertia = np.diag([mass * (Rr * Rr / 2 + 5 * rr * rr / 8)] * 2 + [mass * (Rr * Rr + 3 * rr * rr / 4)])
+    return dict(name="ring_drops_on_slab", slab=(sv, ct), torus=(tv, tt), quad_x=qx, quad_w=qw,
+                build=dict(target_resolution=128, max_resolution=128, padding=0.1),
+                r=r, R=R, v=v, w=w, mass=mass, inertia=inertia,
+                params=dict(stiffness=1e11, order=2, damping=1e4, friction=0.3, regularizer=1e-4,
+                            activation_distance=1e-5))
+
+
 def _axis_angle(axis, ang):
     k = axis / np.maximum(np.linalg.norm(axis, axis=1, keepdims=True), 1e-300)
     K = np.zeros((len(k), 3, 3))

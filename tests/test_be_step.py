@@ -232,14 +232,30 @@ def test_gpu_trajectories_match_port(cuda):
 
 
 @pytest.mark.gpu
-def test_gpu_integrate_reaches_end_time(cuda):
+def test_gpu_integrate_matches_port(cuda):
+    """BEStepper.integrate (BackwardEulerIntegrator.integrate: steps of at most
+    dt until t_end) for four scenes over 14 ms; the first, which meets the
+    plane after about 13 ms (then steps of 10 us), against the oracle's own
+    integrate loop."""
+    from oracle import be_port as P
+
     d = golden("be_steps.npz")
     grid, st = _stepper(d, "flat_drop", max_scenes=4)
-    r = np.array([[0.0, 0.0, 0.012], [0.01, 0.0, 0.02], [0.0, -0.02, 0.015], [0.0, 0.0, 0.05]])
-    scenes = st.scenes(r, np.tile(np.eye(3), (4, 1, 1)), v=np.tile([0.0, 0.0, -0.2], (4, 1)))
-    st.integrate(scenes, T=0.05, dt=1e-3)
+    r = np.array([[0.0, 0.0, 0.011], [0.01, 0.0, 0.02], [0.0, -0.02, 0.015], [0.0, 0.0, 0.05]])
+    R = np.tile(np.eye(3), (4, 1, 1))
+    v = np.tile([0.0, 0.0, -0.2], (4, 1))
+    scenes = st.scenes(r, R, v=v)
+    st.integrate(scenes, T=0.014, dt=1e-3)
     u = st.unpack(scenes)
-    assert np.all(np.abs(u["t"] - 0.05) <= 1e-12)
-    # lowest points 4, 12 and 7 mm above the plane reach it within 50 ms at
-    # 0.2 m/s plus gravity (22 mm); the fourth, 42 mm above, does not
-    assert np.all(u["phase"][:3] > 0) and u["phase"][3] == 0
+    assert np.all(np.abs(u["t"] - 0.014) <= 1e-12)
+    integ = P.Integrator(_port_scene(d, "flat_drop"))
+    s = P.BodyState(r[0].copy(), R[0].copy(), v[0].copy(), np.zeros(3), 0.0)
+    steps = 0
+    while s.t < 0.014 - 1e-15:
+        integ.step(s, min(1e-3, 0.014 - s.t))
+        steps += 1
+    assert steps > 50 and integ.region.phase == 3  # in contact, 10 us steps
+    assert u["phase"][0] == integ.region.phase
+    ref = np.concatenate([s.r, s.R.ravel(), s.v, s.w])
+    out = np.concatenate([u["r"][0], u["R"][0].ravel(), u["v"][0], u["w"][0]])
+    assert _close(out, ref, 1e-6, atol=1e-9), out - ref

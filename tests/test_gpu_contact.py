@@ -142,3 +142,55 @@ def test_fd_baseline_runs(ring_cube):
     ft2, jac2 = b.evaluate(_states(c, idx), _body_b(), jacobian=True)
     assert np.array_equal(ft.cpu().numpy(), ft2.cpu().numpy())
     assert jac.shape == jac2.shape == (len(idx), 6, 6)
+
+
+
+def test_contact_force_autograd(ring_cube):
+    """contact_force: dL/dr = J_x^T dL/dft and dL/dtheta = J_l(theta)^T
+    J_theta^T dL/dft, with J_l checked against central differences of
+    log(exp(theta + e) exp(theta)^-1) (scipy), at rotated poses in contact."""
+    import torch
+    from scipy.spatial.transform import Rotation
+
+    from sdfo.contact import contact_force, so3_left_jacobian
+
+    c, grid, spec, phi, nrm = ring_cube
+    cb = _batch(grid, c, 2)
+    order = np.argsort(c["r"][:, 2])
+    idx = []
+    for i in order[:400]:
+        if _oracle_eval(spec, phi, nrm, 2, c, i)[1].any():
+            idx.append(int(i))
+            if len(idx) == 6:
+                break
+    idx = np.array(idx)
+    P = len(idx)
+    dev = "cuda"
+    theta0 = np.random.default_rng(3).normal(size=(P, 3)) * 0.2
+    # R0 = exp(-[theta0]) R so that the pose rotation exp([theta0]) R0 is R
+    R0 = torch.tensor(np.einsum("pij,pjk->pik", Rotation.from_rotvec(-theta0).as_matrix(),
+                                c["R"][idx]), device=dev)
+    r = torch.tensor(c["r"][idx], dtype=torch.float64, device=dev, requires_grad=True)
+    theta = torch.tensor(theta0, dtype=torch.float64, device=dev, requires_grad=True)
+    v = torch.tensor(c["v"][idx], device=dev)
+    w = torch.tensor(c["w"][idx], device=dev)
+    ft = contact_force(cb, r, theta, R0, v, w, _body_b())
+    up = torch.randn_like(ft)
+    (ft * up).sum().backward()
+    _, jac = cb.evaluate(_states(c, idx), _body_b(), jacobian=True)
+    g = torch.einsum("pi,pij->pj", up, jac)
+    scale = float(g.abs().max())
+    assert float((r.grad - g[:, :3]).abs().max()) <= 1e-9 * scale
+    Jl = so3_left_jacobian(torch.tensor(theta0, device=dev)).cpu().numpy()
+    for p in range(P):
+        num = np.zeros((3, 3))
+        base = Rotation.from_rotvec(theta0[p])
+        for k in range(3):
+            e = np.zeros(3)
+            e[k] = 1e-6
+            dp = (Rotation.from_rotvec(theta0[p] + e) * base.inv()).as_rotvec()
+            dm = (Rotation.from_rotvec(theta0[p] - e) * base.inv()).as_rotvec()
+            num[:, k] = (dp - dm) / 2e-6
+        assert np.abs(num - Jl[p]).max() <= 1e-8
+    want = torch.einsum("pij,pi->pj", torch.tensor(Jl, device=dev), g[:, 3:])
+    assert float((theta.grad - want).abs().max()) <= 1e-9 * scale
