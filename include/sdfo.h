@@ -204,6 +204,11 @@ int sdfo_last_error(char* buf, size_t len);
 /* Checks that device `device` is usable (compute capability 10.x). */
 int sdfo_device_check(int device);
 
+/* Status word the kernels with bounded waits set instead of hanging (bit 0:
+ * a bulk-copy wait of the backward pipeline ran out); synchronous read,
+ * cleared when `clear` != 0.  0 in normal operation. */
+int sdfo_device_status(uint32_t* flags, int32_t clear);
+
 void sdfo_build_params_default(sdfo_build_params* p);
 void sdfo_sparse_build_params_default(sdfo_sparse_build_params* p);
 void sdfo_contact_aware_params_default(sdfo_contact_aware_params* p);

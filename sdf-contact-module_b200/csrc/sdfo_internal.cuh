@@ -214,6 +214,7 @@ struct GridView
     int nx, ny, nz;
     int layout;  // SDFO_LAYOUT_*
     int storage; // SDFO_STORAGE_*
+    int phin_a32; // FP32 payload on a 32-byte boundary (256-bit corner-pair loads)
     int has_hessian;
     const float4* phin;
     const float* hess6;
@@ -263,6 +264,11 @@ struct CandidateOutputs
     float* kwitness;
     int32_t* kbranch;
 };
+// dL/dp of the saved backward for the first n / 256 * 256 queries as a
+// bulk-copy pipeline (stream_bwd.cu); false when the pointers do not allow
+// it.  *done = the queries written.
+bool launch_backward_saved_bulk(int64_t n, const float* grad, const float* hess6, const float* dgap,
+                                const float* dgrad, float* dpts, cudaStream_t s, int64_t* done);
 // ContactAware on a grid with candidates (ca_query.cu).
 void launch_query_ca(const GridView& v, const void* pts, bool f64, int64_t n, const QueryOutputs& o,
                      const CandidateOutputs& co, cudaStream_t s);

@@ -1,0 +1,230 @@
+// The saved-linearisation backward for points (dL/dp = dgap * grad +
+// H dgrad) as a bulk-copy pipeline: persistent CTAs stream tiles of 256
+// queries through shared memory with cp.async.bulk (TMA bulk copies, no
+// tensor map, no multicast) completing on mbarriers, three tiles in flight per
+// CTA, and write the results back with bulk stores.  The per-query work is
+// 15 FMAs against 64 bytes of traffic, so the kernel's only job is to keep
+// enough bytes in flight to run at copy bandwidth.
+//
+// Every wait on an mbarrier is bounded: a wait that runs out sets bit 0 of
+// the device status word (sdfo_device_status), waits (bounded) for the CTA's
+// outstanding bulk stores and returns.
+#include "sdfo_internal.cuh"
+
+namespace sdfo {
+
+__device__ unsigned int g_device_status = 0;
+
+namespace {
+
+constexpr int kTile = 256;   // queries per tile (= threads per CTA)
+constexpr int kStages = 3;
+constexpr unsigned kWaitLimit = 1u << 24;
+
+// Shared-memory layout of one input stage (bytes): dgap | dgrad | grad | hess6.
+constexpr int kOffDgap = 0;
+constexpr int kOffDgrad = kOffDgap + 4 * kTile;
+constexpr int kOffGrad = kOffDgrad + 12 * kTile;
+constexpr int kOffHess = kOffGrad + 12 * kTile;
+constexpr int kStageBytes = kOffHess + 24 * kTile; // 13 KB
+constexpr int kOutBytes = 12 * kTile;              // 3 KB, double-buffered
+
+__device__ __forceinline__ unsigned smem_u32(const void* p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void bulk_wait_read()
+{
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void fence_async_shared()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// One tile's loads into stage `s`: dgap (if any), dgrad (if any), grad, hess6.
+__device__ __forceinline__ void issue_tile(unsigned char* stage, uint64_t* bar, int64_t q0, const float* dgap,
+                                           const float* dgrad, const float* grad, const float* hess6)
+{
+    const unsigned bytes = (dgap ? 4u : 0u) * kTile + (dgrad ? 12u : 0u) * kTile + 36u * kTile;
+    mbar_expect_tx(bar, bytes);
+    if (dgap) bulk_load(stage + kOffDgap, dgap + q0, 4 * kTile, bar);
+    if (dgrad) bulk_load(stage + kOffDgrad, dgrad + 3 * q0, 12 * kTile, bar);
+    bulk_load(stage + kOffGrad, grad + 3 * q0, 12 * kTile, bar);
+    bulk_load(stage + kOffHess, hess6 + 6 * q0, 24 * kTile, bar);
+}
+
+__global__ void __launch_bounds__(kTile) k_backward_saved_bulk(int64_t tiles, const float* __restrict__ grad,
+                                                               const float* __restrict__ hess6,
+                                                               const float* __restrict__ dgap,
+                                                               const float* __restrict__ dgrad,
+                                                               float* __restrict__ dpts)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bars[kStages];
+    __shared__ int s_abort;
+    __shared__ long long s_kabort; // the tile whose wait ran out
+    unsigned char* stages = smem;
+    unsigned char* outs = smem + kStages * kStageBytes;
+    const int64_t first = blockIdx.x, step = gridDim.x;
+    const int64_t mine = first < tiles ? (tiles - first + step - 1) / step : 0;
+    if (threadIdx.x == 0)
+    {
+        s_abort = 0;
+        for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int k = 0; k < kStages && k < mine; ++k)
+            issue_tile(stages + k * kStageBytes, &bars[k], (first + k * step) * kTile, dgap, dgrad, grad, hess6);
+    }
+    __syncthreads();
+    for (int64_t k = 0; k < mine; ++k)
+    {
+        const int s = (int)(k % kStages);
+        const unsigned parity = (unsigned)((k / kStages) & 1);
+        unsigned it = 0;
+        while (!mbar_try_wait(&bars[s], parity))
+            if (++it >= kWaitLimit)
+            {
+                s_abort = 1; // benign race: every writer stores the same values
+                s_kabort = k;
+                break;
+            }
+        __syncthreads();
+        if (s_abort) break;
+        const unsigned char* st = stages + s * kStageBytes;
+        const int t = threadIdx.x;
+        const float dG = dgap ? reinterpret_cast<const float*>(st + kOffDgap)[t] : 0.f;
+        float dg[3] = {0.f, 0.f, 0.f};
+        if (dgrad)
+            for (int a = 0; a < 3; ++a) dg[a] = reinterpret_cast<const float*>(st + kOffDgrad)[3 * t + a];
+        const float* gr = reinterpret_cast<const float*>(st + kOffGrad) + 3 * t;
+        const float* H = reinterpret_cast<const float*>(st + kOffHess) + 6 * t;
+        const float o0 = dG * gr[0] + H[0] * dg[0] + H[1] * dg[1] + H[2] * dg[2];
+        const float o1 = dG * gr[1] + H[1] * dg[0] + H[3] * dg[1] + H[4] * dg[2];
+        const float o2 = dG * gr[2] + H[2] * dg[0] + H[4] * dg[1] + H[5] * dg[2];
+        const int ob = (int)(k & 1);
+        float* out = reinterpret_cast<float*>(outs + ob * kOutBytes);
+        if (threadIdx.x == 0 && k >= 2) bulk_wait_read<1>(); // the store that used this buffer is done
+        __syncthreads();
+        out[3 * t] = o0;
+        out[3 * t + 1] = o1;
+        out[3 * t + 2] = o2;
+        fence_async_shared();
+        __syncthreads(); // stage s consumed, output written
+        if (threadIdx.x == 0)
+        {
+            const int64_t q0 = (first + k * step) * kTile;
+            bulk_store(dpts + 3 * q0, out, kOutBytes);
+            bulk_commit();
+            const int64_t nk = k + kStages;
+            if (nk < mine)
+                issue_tile(stages + s * kStageBytes, &bars[s], (first + nk * step) * kTile, dgap, dgrad, grad,
+                           hess6);
+        }
+    }
+    if (threadIdx.x == 0)
+    {
+        if (s_abort)
+        {
+            atomicOr(&g_device_status, 1u);
+            // the tiles issued but not consumed (s_kabort .. s_kabort + kStages
+            // - 1) complete into this CTA's shared memory: wait for them
+            // (bounded) before the CTA exits
+            for (long long j = s_kabort; j < s_kabort + kStages && j < mine; ++j)
+            {
+                unsigned it = 0;
+                while (!mbar_try_wait(&bars[j % kStages], (unsigned)((j / kStages) & 1)) && ++it < kWaitLimit)
+                {
+                }
+            }
+        }
+        bulk_wait_read<0>();
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    }
+}
+
+} // namespace
+
+bool launch_backward_saved_bulk(int64_t n, const float* grad, const float* hess6, const float* dgap,
+                                const float* dgrad, float* dpts, cudaStream_t s, int64_t* done)
+{
+    *done = 0;
+    auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    if (n < kTile || !grad || !hess6 || !dpts || !a16(grad) || !a16(hess6) || !a16(dpts) ||
+        (dgap && !a16(dgap)) || (dgrad && !a16(dgrad)))
+        return false;
+    const int64_t tiles = n / kTile;
+    static int sms = 0;
+    if (sms == 0)
+    {
+        int dev = 0;
+        SDFO_CUDA(cudaGetDevice(&dev));
+        SDFO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    const int smem = kStages * kStageBytes + 2 * kOutBytes; // 45 KB
+    const int64_t ctas = std::min<int64_t>(tiles, (int64_t)sms * 4);
+    k_backward_saved_bulk<<<(unsigned)ctas, kTile, smem, s>>>(tiles, grad, hess6, dgap, dgrad, dpts);
+    SDFO_CHECK_LAUNCH();
+    *done = tiles * kTile;
+    return true;
+}
+
+} // namespace sdfo
+
+extern "C" int sdfo_device_status(uint32_t* flags, int32_t clear)
+{
+    return sdfo::guarded([&] {
+        SDFO_REQUIRE(flags != nullptr, SDFO_ERR_INVALID_ARGUMENT, "flags is NULL");
+        unsigned v = 0;
+        SDFO_CUDA(cudaMemcpyFromSymbol(&v, sdfo::g_device_status, sizeof(v)));
+        *flags = v;
+        if (clear)
+        {
+            const unsigned z = 0;
+            SDFO_CUDA(cudaMemcpyToSymbol(sdfo::g_device_status, &z, sizeof(z)));
+        }
+    });
+}

@@ -138,6 +138,7 @@ SIGNATURES = [
     ("sdfo_grid_device_views", ctypes.c_int, [_P, ctypes.POINTER(DeviceViews)]),
     ("sdfo_grid_destroy", ctypes.c_int, [_P]),
     ("sdfo_file_probe", ctypes.c_int, [ctypes.c_char_p, _P, _P]),
+    ("sdfo_device_status", ctypes.c_int, [_P, _I32]),
     ("sdfo_contact_pair_create", ctypes.c_int, [_P, _P, _P, _I64, _I32, _D, _I32, _P]),
     ("sdfo_contact_pair_export_bvh", ctypes.c_int, [_P, _P, _P, _P, _P]),
     ("sdfo_contact_pair_eval", ctypes.c_int, [_P, _I32, _P, _I64, _P, _P, _P, _P, _P, _P]),

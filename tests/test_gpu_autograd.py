@@ -142,3 +142,34 @@ def test_saved_and_regathered_backward_agree(cuda, port, storage, mode):
     assert grid.query_backward_saved(pts, {"valid": saved["valid"]}, dgap, dgrad, mode=mode,
                                      dgrid=G3, want_points=False) is None
     assert float((G3 - G1).abs().max()) <= 1e-5 * max(float(G1.abs().max()), 1.0)
+
+
+@pytest.mark.parametrize("n", [77, 256 * 301, 256 * 301 + 77])
+def test_bulk_copy_backward_matches_regathered(cuda, port, n):
+    """dL/dp from the saved linearisation alone (the bulk-copy pipeline for
+    whole tiles of 256 queries, the staged kernel for the rest) against the
+    regathering backward, with both upstream gradients, with dgap only and
+    with dgrad only; the kernels' status word stays clear."""
+    import ctypes
+
+    import torch
+
+    from sdfo import _native as N
+
+    grid, _, g = _grid_and_ref(port, "sparse")
+    rng = np.random.default_rng(n)
+    base = g["pts"].astype(np.float32)
+    pts = torch.tensor(base[rng.integers(0, len(base), n)], device="cuda")
+    gen = torch.Generator(device="cuda").manual_seed(n)
+    dgap = torch.randn(n, device="cuda", generator=gen)
+    dgrad = torch.randn((n, 3), device="cuda", generator=gen)
+    saved = grid.query_linearize(pts, mode=3)
+    for dg, dr in ((dgap, dgrad), (dgap, None), (None, dgrad)):
+        d1 = grid.query_backward_saved(pts, saved, dg, dr, mode=3)
+        d2 = grid.query_backward(pts, dg, dr, mode=3)
+        scale = max(float(d2.abs().max()), 1e-9)
+        assert float((d1 - d2).abs().max()) <= 1e-6 * scale
+    torch.cuda.synchronize()
+    flags = ctypes.c_uint32(7)
+    N.check(N.load().sdfo_device_status(ctypes.byref(flags), 1))
+    assert flags.value == 0
