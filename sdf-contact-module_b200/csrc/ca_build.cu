@@ -137,6 +137,16 @@ __device__ int ca_point(const d3& p, const CaTri* __restrict__ tris, int nt,
                         const int* __restrict__ ids, int nids, const Tree& tree, double tol,
                         double cosMerge, CaCand* merged, int cap, int* status)
 {
+    // Pass 1: the nearest distance, and in tile order the triangles that can
+    // pass the final filter dist <= minD + tol (a triangle within the running
+    // minimum + tol when it is met: the running minimum never falls below the
+    // final one, so every accepted triangle is listed).  Pass 2 then finishes
+    // only the listed triangles, in the same order; a list that would
+    // overflow falls back to finishing every triangle of the tile.
+    constexpr int kList = 24;
+    int list[kList];
+    int nl = 0;
+    bool list_over = false;
     double minD = DBL_MAX;
     for (int q = 0; q < nids; ++q)
     {
@@ -144,6 +154,13 @@ __device__ int ca_point(const d3& p, const CaTri* __restrict__ tris, int nt,
         if (t < 0 || t >= nt) continue;
         const double d = candidate_distance(p, tris + t);
         minD = d < minD ? d : minD;
+        if (d <= minD + tol)
+        {
+            if (nl < kList)
+                list[nl++] = t;
+            else
+                list_over = true;
+        }
     }
     int fallback = -1;
     if (!isfinite(minD))
@@ -176,8 +193,15 @@ __device__ int ca_point(const d3& p, const CaTri* __restrict__ tris, int nt,
     };
     if (nids == 0)
         try_tri(fallback);
+    else if (!list_over)
+        for (int e = 0; e < nl; ++e) try_tri(list[e]);
     else
-        for (int q = 0; q < nids; ++q) try_tri(ids ? __ldg(ids + q) : q);
+        for (int q = 0; q < nids; ++q)
+        {
+            const int t = ids ? __ldg(ids + q) : q;
+            if (t < 0 || t >= nt || !(candidate_distance(p, tris + t) <= allowed)) continue;
+            try_tri(t);
+        }
     if (over) return -1;
     if (nm == 0)
     {
