@@ -426,8 +426,9 @@ def contact_aware_section(torch, lib, N, dev, stream, flush, steps, warmup, cpu_
 
     c = workload()
     cn = M.corner_normals(c["verts"], c["tris"], "face")
-    SdfGrid.build_contact_aware(c["verts"], c["tris"], cn, target_resolution=32,
-                                max_resolution=32).close()  # warm
+    cv, ct = M.cube(0.1)
+    SdfGrid.build_contact_aware(cv, ct, M.corner_normals(cv, ct, "face"), target_resolution=16,
+                                max_resolution=16).close()  # warm the kernels
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     g = SdfGrid.build_contact_aware(c["verts"], c["tris"], cn, **c["dense"])

@@ -623,6 +623,10 @@ int sdfo_be_stepper_create(const sdfo_contact_pair* pair, const sdfo_contact_par
 int sdfo_be_stepper_step(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n,
                          const double* d_dt, double* d_h, void* stream);
 
+/* Threads per scene: 256 (default; two scenes per SM) or 128 (four scenes
+ * per SM; slower on the ring-drop workload, where the point passes dominate). */
+int sdfo_be_stepper_set_threads(sdfo_be_stepper* st, int32_t threads);
+
 int sdfo_be_stepper_destroy(sdfo_be_stepper* st);
 
 #ifdef __cplusplus

@@ -40,8 +40,10 @@
 namespace sdfo {
 namespace {
 
-constexpr int kT = 256;
-constexpr int kWarps = kT / 32;
+// Threads per scene (one CTA per scene): 256 (default, two scenes per SM)
+// or 128 (four per SM, half the threads per point pass).
+constexpr int kMaxT = 256;
+constexpr int kMaxWarps = kMaxT / 32;
 
 enum : int
 {
@@ -100,10 +102,10 @@ struct Shared
     int full;
     double Rs[9], tl[3]; // R_B^T R_A and R_B^T (r_A - r_B) of the pass's pose
     double box[6];
-    double red[kWarps][6];
-    MinRec mins[kWarps];
-    int cnt[kWarps][2];
-    int scan[kWarps];
+    double red[kMaxWarps][6];
+    MinRec mins[kMaxWarps];
+    int cnt[kMaxWarps][2];
+    int scan[kMaxWarps];
     int flag, count, mi;
     double lo, hi, hm_pen, toi; // bisection bracket, its measure, the step
     int hit, event;
@@ -225,11 +227,11 @@ __device__ void broad_phase(const BeView& b, Shared& s)
         }
         s.full = enc ? 1 : 0;
     }
-    for (int w = threadIdx.x; w < (b.nleaves + 31) / 32; w += kT) s.mask[w] = 0u;
+    for (int w = threadIdx.x; w < (b.nleaves + 31) / 32; w += (int)blockDim.x) s.mask[w] = 0u;
     __syncthreads();
     if (s.full) return;
     bool any = false;
-    for (int l = threadIdx.x; l < b.nleaves; l += kT)
+    for (int l = threadIdx.x; l < b.nleaves; l += (int)blockDim.x)
     {
         const double* x = b.leaf_box + 6 * (int64_t)l;
         const bool skip = x[3] < s.box[0] || x[4] < s.box[1] || x[5] < s.box[2] || x[0] > s.box[3] ||
@@ -277,7 +279,7 @@ __device__ __forceinline__ int chunk_scan(Shared& s, bool flag, int& total)
     __syncthreads();
     int off = 0;
     total = 0;
-    for (int w = 0; w < kWarps; ++w)
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
     {
         off += w < warp ? s.scan[w] : 0;
         total += s.scan[w];
@@ -293,7 +295,7 @@ __device__ void eval_pass(const BeView& b, Shared& s)
     const double narrow = b.cull ? b.narrow : INFINITY;
     // the number of narrow-filtered points decides whether the cache is used
     int L = 0;
-    for (int c0 = 0; c0 < b.nq; c0 += kT)
+    for (int c0 = 0; c0 < b.nq; c0 += (int)blockDim.x)
     {
         double X[3], w, Y[3];
         bool f = false;
@@ -313,7 +315,7 @@ __device__ void eval_pass(const BeView& b, Shared& s)
         matTvec(b.RB, d, tsdf);
         const int64_t base_c = (int64_t)blockIdx.x * b.nq;
         int base = 0;
-        for (int c0 = 0; c0 < b.nq; c0 += kT)
+        for (int c0 = 0; c0 < b.nq; c0 += (int)blockDim.x)
         {
             double X[3], w = 0.0, Y[3];
             bool f = false;
@@ -413,7 +415,7 @@ __device__ void eval_pass(const BeView& b, Shared& s)
         for (int q = 0; q < 6; ++q)
         {
             double v = 0.0;
-            for (int w = 0; w < kWarps; ++w) v += s.red[w][q];
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += s.red[w][q];
             if (q < 3)
                 s.F[q] = v;
             else
@@ -431,7 +433,7 @@ __device__ void measure_pass(const BeView& b, Shared& s)
     MinRec best{INFINITY, INT_MAX, -1};
     int nv = 0, na = 0;
     int base = 0;
-    for (int c0 = 0; c0 < b.nq; c0 += kT)
+    for (int c0 = 0; c0 < b.nq; c0 += (int)blockDim.x)
     {
         double X[3], w, Y[3];
         const bool kept = point_at(b, s, c0 + threadIdx.x, X, w);
@@ -468,7 +470,7 @@ __device__ void measure_pass(const BeView& b, Shared& s)
     {
         MinRec m = s.mins[0];
         int v = s.cnt[0][0], a = s.cnt[0][1];
-        for (int k = 1; k < kWarps; ++k)
+        for (int k = 1; k < (int)(blockDim.x >> 5); ++k)
         {
             if (s.mins[k].gap < m.gap || (s.mins[k].gap == m.gap && s.mins[k].key < m.key)) m = s.mins[k];
             v += s.cnt[k][0];
@@ -756,7 +758,8 @@ __device__ void refresh(const BeView& b, Shared& s)
     }
 }
 
-__global__ void __launch_bounds__(kT) k_be_step(BeView b, sdfo_be_scene* __restrict__ scenes, int n,
+template <int T>
+__global__ void __launch_bounds__(T, T == 128 ? 4 : 2) k_be_step(BeView b, sdfo_be_scene* __restrict__ scenes, int n,
                                                 const double* __restrict__ dt_req, double* __restrict__ h_out)
 {
     __shared__ Shared s;
@@ -938,6 +941,7 @@ struct sdfo_be_stepper
     const sdfo_contact_pair* pair = nullptr;
     sdfo::BeView view{};
     int64_t capacity = 0;
+    int threads = 256;
     ~sdfo_be_stepper()
     {
         sdfo::device_free(view.cg);
@@ -1058,8 +1062,21 @@ int sdfo_be_stepper_step(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n
                      "scene count exceeds the stepper's capacity");
         if (n == 0) return;
         SDFO_REQUIRE(d_scenes && d_dt, SDFO_ERR_INVALID_ARGUMENT, "scenes and step sizes are required");
-        k_be_step<<<(unsigned)n, kT, 0, as_stream(stream)>>>(st->view, d_scenes, (int)n, d_dt, d_h);
+        if (st->threads == 128)
+            k_be_step<128><<<(unsigned)n, 128, 0, as_stream(stream)>>>(st->view, d_scenes, (int)n, d_dt, d_h);
+        else
+            k_be_step<256><<<(unsigned)n, 256, 0, as_stream(stream)>>>(st->view, d_scenes, (int)n, d_dt, d_h);
         SDFO_CHECK_LAUNCH();
+    });
+}
+
+int sdfo_be_stepper_set_threads(sdfo_be_stepper* st, int32_t threads)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(st != nullptr, SDFO_ERR_INVALID_ARGUMENT, "stepper is NULL");
+        SDFO_REQUIRE(threads == 128 || threads == 256, SDFO_ERR_INVALID_ARGUMENT,
+                     "threads per scene must be 128 or 256");
+        st->threads = threads;
     });
 }
 

@@ -51,7 +51,7 @@ class BEStepper:
     def __init__(self, grid, quad_x, quad_w, mass, inertia, stiffness, order=1, damping=0.0,
                  friction=0.5, regularizer=1e-6, activation_distance=0.0, narrow_margin=0.01,
                  gravity=(0.0, 0.0, -9.81), body_b=None, params=None, max_scenes=1024,
-                 leaf_size=16):
+                 leaf_size=16, threads=256):
         self.contact = ContactBatch(grid, quad_x, quad_w, stiffness, order=order, damping=damping,
                                     friction=friction, regularizer=regularizer,
                                     activation_distance=activation_distance, mode=N.TRILINEAR,
@@ -81,6 +81,7 @@ class BEStepper:
                                                 ctypes.byref(self.params), self.max_scenes,
                                                 ctypes.byref(out)))
         self._h = out
+        N.check(N.load().sdfo_be_stepper_set_threads(self._h, int(threads)))
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

@@ -259,3 +259,25 @@ def test_gpu_integrate_matches_port(cuda):
     ref = np.concatenate([s.r, s.R.ravel(), s.v, s.w])
     out = np.concatenate([u["r"][0], u["R"][0].ravel(), u["v"][0], u["w"][0]])
     assert _close(out, ref, 1e-6, atol=1e-9), out - ref
+
+
+@pytest.mark.gpu
+def test_gpu_threads_per_scene_agree(cuda):
+    """128 and 256 threads per scene: the same steps (reductions summed in
+    another order: states within 1e-12 relative)."""
+    import torch
+
+    d = golden("be_steps.npz")
+    a = d["flat_drop"]
+    outs = []
+    for th in (128, 256):
+        grid, st = _stepper(d, "flat_drop", max_scenes=len(a))
+        from sdfo import _native as N
+
+        N.check(N.load().sdfo_be_stepper_set_threads(st._h, th))
+        scenes = _rows_to_scenes(st, a[:-1])
+        h = st.step(scenes, 1e-3)
+        torch.cuda.synchronize()
+        outs.append((h.cpu().numpy(), _scenes_to_rows(st, scenes)))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert _close(outs[0][1], outs[1][1], 1e-12, atol=1e-18)
