@@ -205,7 +205,8 @@ int sdfo_last_error(char* buf, size_t len);
 int sdfo_device_check(int device);
 
 /* Status word the kernels with bounded waits set instead of hanging (bit 0:
- * a bulk-copy wait of the backward pipeline ran out); synchronous read,
+ * a bulk-copy wait of the backward pipeline ran out; bit 1: one of the
+ * pipelined query kernel); synchronous read,
  * cleared when `clear` != 0.  0 in normal operation. */
 int sdfo_device_status(uint32_t* flags, int32_t clear);
 

@@ -264,6 +264,9 @@ struct CandidateOutputs
     float* kwitness;
     int32_t* kbranch;
 };
+// Status bits of the pipelined query kernel (query.cu), read and optionally
+// cleared by sdfo_device_status.
+unsigned query_pipe_status(bool clear);
 // dL/dp of the saved backward for the first n / 256 * 256 queries as a
 // bulk-copy pipeline (stream_bwd.cu); false when the pointers do not allow
 // it.  *done = the queries written.

@@ -9,6 +9,7 @@
 // Every wait on an mbarrier is bounded: a wait that runs out sets bit 0 of
 // the device status word (sdfo_device_status), waits (bounded) for the CTA's
 // outstanding bulk stores and returns.
+#include "bulk.cuh"
 #include "sdfo_internal.cuh"
 
 namespace sdfo {
@@ -16,6 +17,8 @@ namespace sdfo {
 __device__ unsigned int g_device_status = 0;
 
 namespace {
+
+using namespace bulk;
 
 constexpr int kTile = 256;   // queries per tile (= threads per CTA)
 constexpr int kStages = 3;
@@ -28,62 +31,6 @@ constexpr int kOffGrad = kOffDgrad + 12 * kTile;
 constexpr int kOffHess = kOffGrad + 12 * kTile;
 constexpr int kStageBytes = kOffHess + 24 * kTile; // 13 KB
 constexpr int kOutBytes = 12 * kTile;              // 3 KB, double-buffered
-
-__device__ __forceinline__ unsigned smem_u32(const void* p)
-{
-    return (unsigned)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
-{
-    unsigned ok;
-    asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                 "selp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(ok)
-                 : "r"(smem_u32(bar)), "r"(parity)
-                 : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void bulk_store(void* dst, const void* src, unsigned bytes)
-{
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-
-template <int N>
-__device__ __forceinline__ void bulk_wait_read()
-{
-    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
-}
-
-__device__ __forceinline__ void fence_async_shared()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
 
 // One tile's loads into stage `s`: dgap (if any), dgrad (if any), grad, hess6.
 __device__ __forceinline__ void issue_tile(unsigned char* stage, uint64_t* bar, int64_t q0, const float* dgap,
@@ -220,7 +167,7 @@ extern "C" int sdfo_device_status(uint32_t* flags, int32_t clear)
         SDFO_REQUIRE(flags != nullptr, SDFO_ERR_INVALID_ARGUMENT, "flags is NULL");
         unsigned v = 0;
         SDFO_CUDA(cudaMemcpyFromSymbol(&v, sdfo::g_device_status, sizeof(v)));
-        *flags = v;
+        *flags = v | sdfo::query_pipe_status(clear != 0);
         if (clear)
         {
             const unsigned z = 0;
