@@ -40,8 +40,9 @@
 namespace sdfo {
 namespace {
 
-// Threads per scene (one CTA per scene): 256 (default, two scenes per SM)
-// or 128 (four per SM, half the threads per point pass).
+// Threads per scene: 256 (one CTA per scene, two scenes per SM), 128 (four
+// per SM) or 32 (one warp per scene, eight scenes per CTA, sixteen per SM:
+// warp-level synchronisation instead of CTA barriers).
 constexpr int kMaxT = 256;
 constexpr int kMaxWarps = kMaxT / 32;
 
@@ -109,6 +110,7 @@ struct Shared
     int flag, count, mi;
     double lo, hi, hm_pen, toi; // bisection bracket, its measure, the step
     int hit, event;
+    int scene;                  // index of the scene in the batch
     double alpha;               // line search
     int found;
 };
@@ -147,6 +149,35 @@ __device__ __forceinline__ int warp_isum(int v)
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     return v;
 }
+
+// The threads working on one scene: a whole CTA (Grp<false>) or one warp
+// (Grp<true>, several scenes per CTA).
+template <bool W>
+struct Grp;
+
+template <>
+struct Grp<false>
+{
+    __device__ static int rank() { return (int)threadIdx.x; }
+    __device__ static int size() { return (int)blockDim.x; }
+    __device__ static void sync() { __syncthreads(); }
+    __device__ static int count(bool f) { return __syncthreads_count(f); }
+    __device__ static bool any(bool f) { return __syncthreads_or(f) != 0; }
+    __device__ static int warp() { return (int)(threadIdx.x >> 5); }
+    __device__ static int warps() { return (int)(blockDim.x >> 5); }
+};
+
+template <>
+struct Grp<true>
+{
+    __device__ static int rank() { return (int)(threadIdx.x & 31); }
+    __device__ static int size() { return 32; }
+    __device__ static void sync() { __syncwarp(); }
+    __device__ static int count(bool f) { return __popc(__ballot_sync(0xffffffffu, f)); }
+    __device__ static bool any(bool f) { return __any_sync(0xffffffffu, f) != 0; }
+    __device__ static int warp() { return 0; }
+    __device__ static int warps() { return 1; }
+};
 
 // TrilinearSDFGrid.query_batch for one point (sdf_grid.py:138-204).
 __device__ bool sample64(const BeView& b, const double Y[3], double& g, double grad[3])
@@ -202,16 +233,17 @@ __device__ __forceinline__ void to_sdf(const Shared& s, const double X[3], doubl
 
 // The broad phase of evaluate / measure_pair for the pose in s.cur
 // (contacts_sdf.py:244-269, bvh.py:62-80): leaf mask and the `full` flag.
+template <bool W>
 __device__ void broad_phase(const BeView& b, Shared& s)
 {
-    if (threadIdx.x == 0) sdf_frame(b, s.cur, s.Rs, s.tl);
+    if (Grp<W>::rank() == 0) sdf_frame(b, s.cur, s.Rs, s.tl);
     if (!b.cull)
     {
-        if (threadIdx.x == 0) s.full = 1;
-        __syncthreads();
+        if (Grp<W>::rank() == 0) s.full = 1;
+        Grp<W>::sync();
         return;
     }
-    if (threadIdx.x == 0)
+    if (Grp<W>::rank() == 0)
     {
         double lo[3], hi[3], d[3];
         for (int a = 0; a < 3; ++a) d[a] = b.bmin[a] - s.cur.r[a];
@@ -227,11 +259,11 @@ __device__ void broad_phase(const BeView& b, Shared& s)
         }
         s.full = enc ? 1 : 0;
     }
-    for (int w = threadIdx.x; w < (b.nleaves + 31) / 32; w += (int)blockDim.x) s.mask[w] = 0u;
-    __syncthreads();
+    for (int w = Grp<W>::rank(); w < (b.nleaves + 31) / 32; w += Grp<W>::size()) s.mask[w] = 0u;
+    Grp<W>::sync();
     if (s.full) return;
     bool any = false;
-    for (int l = threadIdx.x; l < b.nleaves; l += (int)blockDim.x)
+    for (int l = Grp<W>::rank(); l < b.nleaves; l += Grp<W>::size())
     {
         const double* x = b.leaf_box + 6 * (int64_t)l;
         const bool skip = x[3] < s.box[0] || x[4] < s.box[1] || x[5] < s.box[2] || x[0] > s.box[3] ||
@@ -242,9 +274,9 @@ __device__ void broad_phase(const BeView& b, Shared& s)
             any = true;
         }
     }
-    const int none = __syncthreads_or(any) == 0;
-    if (threadIdx.x == 0 && none) s.full = 1;
-    __syncthreads();
+    const int none = Grp<W>::any(any) ? 0 : 1;
+    if (Grp<W>::rank() == 0 && none) s.full = 1;
+    Grp<W>::sync();
 }
 
 // Point i of the kept list in the reference's order (original order when
@@ -271,40 +303,42 @@ __device__ __forceinline__ bool point_at(const BeView& b, const Shared& s, int i
 }
 
 // Block-wide exclusive position of `flag` within the chunk; *total = count.
+template <bool W>
 __device__ __forceinline__ int chunk_scan(Shared& s, bool flag, int& total)
 {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = Grp<W>::warp(), lane = (int)(threadIdx.x & 31);
     const unsigned bal = __ballot_sync(0xffffffffu, flag);
     if (lane == 0) s.scan[warp] = __popc(bal);
-    __syncthreads();
+    Grp<W>::sync();
     int off = 0;
     total = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+    for (int w = 0; w < Grp<W>::warps(); ++w)
     {
         off += w < warp ? s.scan[w] : 0;
         total += s.scan[w];
     }
-    __syncthreads();
+    Grp<W>::sync();
     return off + __popc(bal & ((1u << lane) - 1u));
 }
 
 // SDFContactEngine.evaluate for s.cur with the cache (F, tau into shared).
+template <bool W>
 __device__ void eval_pass(const BeView& b, Shared& s)
 {
-    broad_phase(b, s);
+    broad_phase<W>(b, s);
     const double narrow = b.cull ? b.narrow : INFINITY;
     // the number of narrow-filtered points decides whether the cache is used
     int L = 0;
-    for (int c0 = 0; c0 < b.nq; c0 += (int)blockDim.x)
+    for (int c0 = 0; c0 < b.nq; c0 += Grp<W>::size())
     {
         double X[3], w, Y[3];
         bool f = false;
-        if (point_at(b, s, c0 + threadIdx.x, X, w))
+        if (point_at(b, s, c0 + Grp<W>::rank(), X, w))
         {
             to_sdf(s, X, Y);
             f = fabs(Y[2]) < narrow;
         }
-        L += __syncthreads_count(f);
+        L += Grp<W>::count(f);
     }
     double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (L > 0)
@@ -313,19 +347,19 @@ __device__ void eval_pass(const BeView& b, Shared& s)
         const bool store = !use && s.c_enabled;
         double tsdf[3], d[3] = {s.cur.r[0] - b.rB[0], s.cur.r[1] - b.rB[1], s.cur.r[2] - b.rB[2]};
         matTvec(b.RB, d, tsdf);
-        const int64_t base_c = (int64_t)blockIdx.x * b.nq;
+        const int64_t base_c = (int64_t)s.scene * b.nq;
         int base = 0;
-        for (int c0 = 0; c0 < b.nq; c0 += (int)blockDim.x)
+        for (int c0 = 0; c0 < b.nq; c0 += Grp<W>::size())
         {
             double X[3], w = 0.0, Y[3];
             bool f = false;
-            if (point_at(b, s, c0 + threadIdx.x, X, w))
+            if (point_at(b, s, c0 + Grp<W>::rank(), X, w))
             {
                 to_sdf(s, X, Y);
                 f = fabs(Y[2]) < narrow;
             }
             int total;
-            const int pos = base + chunk_scan(s, f, total);
+            const int pos = base + chunk_scan<W>(s, f, total);
             base += total;
             if (!f) continue;
             double g, gr[3];
@@ -396,49 +430,50 @@ __device__ void eval_pass(const BeView& b, Shared& s)
                 acc[3 + a] += w * tq[a];
             }
         }
-        if (threadIdx.x == 0 && store)
+        if (Grp<W>::rank() == 0 && store)
         {
             for (int a = 0; a < 3; ++a) s.c_tref[a] = tsdf[a];
             s.c_len = L;
             s.c_cleared = 0;
         }
     }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = Grp<W>::warp(), lane = (int)(threadIdx.x & 31);
     for (int q = 0; q < 6; ++q)
     {
         const double v = warp_dsum(acc[q]);
         if (lane == 0) s.red[warp][q] = v;
     }
-    __syncthreads();
-    if (threadIdx.x == 0)
+    Grp<W>::sync();
+    if (Grp<W>::rank() == 0)
     {
         for (int q = 0; q < 6; ++q)
         {
             double v = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += s.red[w][q];
+            for (int w = 0; w < Grp<W>::warps(); ++w) v += s.red[w][q];
             if (q < 3)
                 s.F[q] = v;
             else
                 s.tau[q - 3] = v;
         }
     }
-    __syncthreads();
+    Grp<W>::sync();
 }
 
 // measure_pair for s.cur (contacts_sdf.py:171-214): m_gap, m_pen, m_vn,
 // m_active, m_valid.
+template <bool W>
 __device__ void measure_pass(const BeView& b, Shared& s)
 {
-    broad_phase(b, s);
+    broad_phase<W>(b, s);
     MinRec best{INFINITY, INT_MAX, -1};
     int nv = 0, na = 0;
     int base = 0;
-    for (int c0 = 0; c0 < b.nq; c0 += (int)blockDim.x)
+    for (int c0 = 0; c0 < b.nq; c0 += Grp<W>::size())
     {
         double X[3], w, Y[3];
-        const bool kept = point_at(b, s, c0 + threadIdx.x, X, w);
+        const bool kept = point_at(b, s, c0 + Grp<W>::rank(), X, w);
         int total;
-        const int pos = base + chunk_scan(s, kept, total);
+        const int pos = base + chunk_scan<W>(s, kept, total);
         base += total;
         if (!kept) continue;
         to_sdf(s, X, Y);
@@ -446,9 +481,9 @@ __device__ void measure_pass(const BeView& b, Shared& s)
         if (!sample64(b, Y, g, gr)) continue;
         ++nv;
         if (g < 0.0) ++na;
-        if (g < best.gap || (g == best.gap && pos < best.key)) best = MinRec{g, pos, c0 + (int)threadIdx.x};
+        if (g < best.gap || (g == best.gap && pos < best.key)) best = MinRec{g, pos, c0 + Grp<W>::rank()};
     }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = Grp<W>::warp(), lane = (int)(threadIdx.x & 31);
     for (int o = 16; o > 0; o >>= 1)
     {
         MinRec q;
@@ -465,12 +500,12 @@ __device__ void measure_pass(const BeView& b, Shared& s)
         s.cnt[warp][0] = nv;
         s.cnt[warp][1] = na;
     }
-    __syncthreads();
-    if (threadIdx.x == 0)
+    Grp<W>::sync();
+    if (Grp<W>::rank() == 0)
     {
         MinRec m = s.mins[0];
         int v = s.cnt[0][0], a = s.cnt[0][1];
-        for (int k = 1; k < (int)(blockDim.x >> 5); ++k)
+        for (int k = 1; k < Grp<W>::warps(); ++k)
         {
             if (s.mins[k].gap < m.gap || (s.mins[k].gap == m.gap && s.mins[k].key < m.key)) m = s.mins[k];
             v += s.cnt[k][0];
@@ -484,9 +519,9 @@ __device__ void measure_pass(const BeView& b, Shared& s)
         s.count = v ? m.key : -1;
         s.mi = v ? m.i : -1;
     }
-    __syncthreads();
+    Grp<W>::sync();
     // normal relative velocity at the minimum point (contacts_sdf.py:199-211)
-    if (threadIdx.x == 0 && s.mi >= 0)
+    if (Grp<W>::rank() == 0 && s.mi >= 0)
     {
         double X[3], w, Y[3], g, gr[3];
         point_at(b, s, s.mi, X, w);
@@ -512,7 +547,7 @@ __device__ void measure_pass(const BeView& b, Shared& s)
         double du[3] = {uA[0] - uB[0], uA[1] - uB[1], uA[2] - uB[2]};
         s.m_vn = dot3(du, n);
     }
-    __syncthreads();
+    Grp<W>::sync();
 }
 
 // _kinematic_update (implicit_be.py:507-534), thread 0.
@@ -547,12 +582,13 @@ __device__ void kinematic(const Body& q0, const double V[6], double dt, Body& ou
 }
 
 // _residual at V = z (implicit_be.py:536-604): s.res, s.err, s.Iw, s.cur.
+template <bool W>
 __device__ void residual(const BeView& b, Shared& s, const double* z, double dt, bool allowed)
 {
-    if (threadIdx.x == 0) kinematic(s.q0, z, dt, s.cur);
-    __syncthreads();
-    if (allowed) eval_pass(b, s);
-    if (threadIdx.x == 0)
+    if (Grp<W>::rank() == 0) kinematic(s.q0, z, dt, s.cur);
+    Grp<W>::sync();
+    if (allowed) eval_pass<W>(b, s);
+    if (Grp<W>::rank() == 0)
     {
         double RI[9];
         for (int i = 0; i < 3; ++i)
@@ -589,14 +625,15 @@ __device__ void residual(const BeView& b, Shared& s, const double* z, double dt,
         for (int a = 0; a < 6; ++a) err = fmax(err, fabs(s.res[a]));
         s.err = err;
     }
-    __syncthreads();
+    Grp<W>::sync();
 }
 
 // _step_be (implicit_be.py:468-505): src -> dst (thread-0 copies), contact
 // forces of the pair when `allowed`.
+template <bool W>
 __device__ void step_be(const BeView& b, Shared& s, const Body* src, Body* dst, double dt, bool allowed)
 {
-    if (threadIdx.x == 0)
+    if (Grp<W>::rank() == 0)
     {
         s.q0 = *src;
         for (int a = 0; a < 3; ++a)
@@ -607,12 +644,12 @@ __device__ void step_be(const BeView& b, Shared& s, const Body* src, Body* dst, 
         s.c_enabled = allowed ? 1 : 0;
         s.c_cleared = 1;
     }
-    __syncthreads();
-    residual(b, s, s.z, dt, allowed);
+    Grp<W>::sync();
+    residual<W>(b, s, s.z, dt, allowed);
     for (int it = 0; it < b.p.max_iter; ++it)
     {
         if (s.err < b.p.tol) break;
-        if (threadIdx.x == 0)
+        if (Grp<W>::rank() == 0)
         {
             // tangent (_tangent / _contact_tangent): M/h + diag(Kc) on the
             // translational rows; the two diagonal blocks solved exactly
@@ -651,16 +688,16 @@ __device__ void step_be(const BeView& b, Shared& s, const Body* src, Body* dst, 
             s.found = 0;
             s.alpha = 1.0;
         }
-        __syncthreads();
+        Grp<W>::sync();
         if (b.p.line_search)
         {
             const double alphas[5] = {1.0, 0.5, 0.25, 0.125, 0.0625};
             for (int k = 0; k < 5; ++k)
             {
-                if (threadIdx.x < 6) s.zt[threadIdx.x] = s.z[threadIdx.x] + alphas[k] * s.dz[threadIdx.x];
-                __syncthreads();
-                residual(b, s, s.zt, dt, allowed);
-                if (threadIdx.x == 0)
+                if (Grp<W>::rank() < 6) s.zt[Grp<W>::rank()] = s.z[Grp<W>::rank()] + alphas[k] * s.dz[Grp<W>::rank()];
+                Grp<W>::sync();
+                residual<W>(b, s, s.zt, dt, allowed);
+                if (Grp<W>::rank() == 0)
                 {
                     double nr = 0.0;
                     for (int a = 0; a < 6; ++a) nr += s.res[a] * s.res[a];
@@ -670,19 +707,19 @@ __device__ void step_be(const BeView& b, Shared& s, const Body* src, Body* dst, 
                         s.found = 1;
                     }
                 }
-                __syncthreads();
+                Grp<W>::sync();
                 if (s.found) break;
             }
         }
-        if (threadIdx.x == 0)
+        if (Grp<W>::rank() == 0)
         {
             const double alpha = s.found ? s.alpha : 1.0;
             for (int a = 0; a < 6; ++a) s.z[a] = s.z[a] + alpha * s.dz[a];
         }
-        __syncthreads();
-        residual(b, s, s.z, dt, allowed);
+        Grp<W>::sync();
+        residual<W>(b, s, s.z, dt, allowed);
     }
-    if (threadIdx.x == 0)
+    if (Grp<W>::rank() == 0)
     {
         Body out;
         kinematic(s.q0, s.z, dt, out);
@@ -691,14 +728,15 @@ __device__ void step_be(const BeView& b, Shared& s, const Body* src, Body* dst, 
         s.c_enabled = 0;
         s.c_cleared = 1;
     }
-    __syncthreads();
+    Grp<W>::sync();
 }
 
+template <bool W>
 __device__ void measure_body(const BeView& b, Shared& s, const Body& body)
 {
-    if (threadIdx.x == 0) s.cur = body;
-    __syncthreads();
-    measure_pass(b, s);
+    if (Grp<W>::rank() == 0) s.cur = body;
+    Grp<W>::sync();
+    measure_pass<W>(b, s);
 }
 
 __device__ __forceinline__ bool region_active(int ph)
@@ -758,15 +796,20 @@ __device__ void refresh(const BeView& b, Shared& s)
     }
 }
 
-template <int T>
-__global__ void __launch_bounds__(T, T == 128 ? 4 : 2) k_be_step(BeView b, sdfo_be_scene* __restrict__ scenes, int n,
+// T threads per CTA; W: one warp per scene (T / 32 scenes per CTA), else
+// the whole CTA on one scene.
+template <int T, bool W>
+__global__ void __launch_bounds__(T, (W || T == 256) ? 2 : 4) k_be_step(BeView b, sdfo_be_scene* __restrict__ scenes, int n,
                                                 const double* __restrict__ dt_req, double* __restrict__ h_out)
 {
-    __shared__ Shared s;
-    const int sc = blockIdx.x;
+    __shared__ Shared shared_scenes[W ? T / 32 : 1];
+    const int sc = W ? (int)(blockIdx.x * (T / 32) + (threadIdx.x >> 5)) : (int)blockIdx.x;
+    if (sc >= n) return; // (warps) whole warps past the last scene
+    Shared& s = shared_scenes[W ? (threadIdx.x >> 5) : 0];
     const sdfo_be_params& p = b.p;
-    if (threadIdx.x == 0)
+    if (Grp<W>::rank() == 0)
     {
+        s.scene = sc;
         const sdfo_be_scene& in = scenes[sc];
         for (int a = 0; a < 3; ++a)
         {
@@ -790,17 +833,17 @@ __global__ void __launch_bounds__(T, T == 128 ? 4 : 2) k_be_step(BeView b, sdfo_
         s.c_len = -1;
         s.event = 0;
     }
-    __syncthreads();
+    Grp<W>::sync();
     const double dt = dt_req[sc];
     if (!(dt > 0.0))
     {
-        if (threadIdx.x == 0 && h_out) h_out[sc] = 0.0;
+        if (Grp<W>::rank() == 0 && h_out) h_out[sc] = 0.0;
         return; // nothing to do for this scene (finished)
     }
     // _activate_initially_penetrating_regions
-    measure_body(b, s, s.q);
+    measure_body<W>(b, s, s.q);
     __shared__ double m0_gap;
-    if (threadIdx.x == 0)
+    if (Grp<W>::rank() == 0)
     {
         s.last_gap = s.m_gap;
         s.last_pen = s.m_pen;
@@ -813,36 +856,36 @@ __global__ void __launch_bounds__(T, T == 128 ? 4 : 2) k_be_step(BeView b, sdfo_
         }
         s.toi = fmin(dt, region_active(s.phase) ? s.dt_current : p.dt_normal); // h_cap
     }
-    __syncthreads();
+    Grp<W>::sync();
     const double h_cap = s.toi;
     // _find_earliest_new_contact
     if (s.phase == kInactive && h_cap > 0.0)
     {
-        step_be(b, s, &s.q, &s.tr, h_cap, false);
-        measure_body(b, s, s.tr);
-        if (threadIdx.x == 0)
+        step_be<W>(b, s, &s.q, &s.tr, h_cap, false);
+        measure_body<W>(b, s, s.tr);
+        if (Grp<W>::rank() == 0)
             s.flag = (m0_gap > 0.0 && (s.m_gap <= 0.0 || s.m_pen > p.pen_max)) ? 1 : 0;
-        __syncthreads();
+        Grp<W>::sync();
         if (s.flag)
         {
             // _bisect_toi_pair
-            if (threadIdx.x == 0)
+            if (Grp<W>::rank() == 0)
             {
                 s.lo = 0.0;
                 s.hi = h_cap;
                 s.hm_pen = s.m_pen;
                 s.hit = 0;
             }
-            __syncthreads();
+            Grp<W>::sync();
             for (int it = 0; it < p.max_toi_bisect_iter; ++it)
             {
-                if (threadIdx.x == 0 && s.hi - s.lo <= p.dt_min) s.hit = 1;
-                __syncthreads();
+                if (Grp<W>::rank() == 0 && s.hi - s.lo <= p.dt_min) s.hit = 1;
+                Grp<W>::sync();
                 if (s.hit) break;
                 const double mid = 0.5 * (s.lo + s.hi);
-                step_be(b, s, &s.q, &s.tr, mid, false);
-                measure_body(b, s, s.tr);
-                if (threadIdx.x == 0)
+                step_be<W>(b, s, &s.q, &s.tr, mid, false);
+                measure_body<W>(b, s, s.tr);
+                if (Grp<W>::rank() == 0)
                 {
                     if (s.m_gap <= 0.0 || s.m_pen > p.pen_max)
                     {
@@ -852,22 +895,22 @@ __global__ void __launch_bounds__(T, T == 128 ? 4 : 2) k_be_step(BeView b, sdfo_
                     else
                         s.lo = mid;
                 }
-                __syncthreads();
+                Grp<W>::sync();
             }
             if (s.hi < p.dt_min && h_cap >= p.dt_min)
             {
-                if (threadIdx.x == 0)
+                if (Grp<W>::rank() == 0)
                 {
                     s.hi = p.dt_min;
                     s.hit = 1;
                 }
-                __syncthreads();
-                step_be(b, s, &s.q, &s.tr, s.hi, false);
-                measure_body(b, s, s.tr);
-                if (threadIdx.x == 0) s.hm_pen = s.m_pen;
-                __syncthreads();
+                Grp<W>::sync();
+                step_be<W>(b, s, &s.q, &s.tr, s.hi, false);
+                measure_body<W>(b, s, s.tr);
+                if (Grp<W>::rank() == 0) s.hm_pen = s.m_pen;
+                Grp<W>::sync();
             }
-            if (threadIdx.x == 0 && s.hi > 0.0)
+            if (Grp<W>::rank() == 0 && s.hi > 0.0)
             {
                 if (s.hm_pen > p.pen_max && !s.hit)
                 {
@@ -877,24 +920,24 @@ __global__ void __launch_bounds__(T, T == 128 ? 4 : 2) k_be_step(BeView b, sdfo_
                 s.toi = fmin(s.hi, h_cap);
                 s.event = 1;
             }
-            __syncthreads();
+            Grp<W>::sync();
         }
     }
     double h;
     if (s.event)
     {
         h = s.toi;
-        step_be(b, s, &s.q, &s.q, h, region_active(s.phase));
-        if (threadIdx.x == 0)
+        step_be<W>(b, s, &s.q, &s.q, h, region_active(s.phase));
+        if (Grp<W>::rank() == 0)
         {
             s.phase = kImpacting;
             s.dt_current = fmin(p.dt_impact, p.dt_contact);
             s.last_toi = h;
             if (s.hit) s.min_dt_hits += 1;
         }
-        __syncthreads();
-        measure_body(b, s, s.q);
-        if (threadIdx.x == 0)
+        Grp<W>::sync();
+        measure_body<W>(b, s, s.q);
+        if (Grp<W>::rank() == 0)
         {
             s.last_gap = s.m_gap;
             s.last_pen = s.m_pen;
@@ -904,12 +947,12 @@ __global__ void __launch_bounds__(T, T == 128 ? 4 : 2) k_be_step(BeView b, sdfo_
     else
     {
         h = h_cap;
-        step_be(b, s, &s.q, &s.q, h, region_active(s.phase));
-        measure_body(b, s, s.q);
-        if (threadIdx.x == 0) refresh(b, s);
+        step_be<W>(b, s, &s.q, &s.q, h, region_active(s.phase));
+        measure_body<W>(b, s, s.q);
+        if (Grp<W>::rank() == 0) refresh(b, s);
     }
-    __syncthreads();
-    if (threadIdx.x == 0)
+    Grp<W>::sync();
+    if (Grp<W>::rank() == 0)
     {
         sdfo_be_scene& out = scenes[sc];
         for (int a = 0; a < 3; ++a)
@@ -1062,10 +1105,13 @@ int sdfo_be_stepper_step(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n
                      "scene count exceeds the stepper's capacity");
         if (n == 0) return;
         SDFO_REQUIRE(d_scenes && d_dt, SDFO_ERR_INVALID_ARGUMENT, "scenes and step sizes are required");
-        if (st->threads == 128)
-            k_be_step<128><<<(unsigned)n, 128, 0, as_stream(stream)>>>(st->view, d_scenes, (int)n, d_dt, d_h);
+        cudaStream_t s = as_stream(stream);
+        if (st->threads == 32)
+            k_be_step<256, true><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(st->view, d_scenes, (int)n, d_dt, d_h);
+        else if (st->threads == 128)
+            k_be_step<128, false><<<(unsigned)n, 128, 0, s>>>(st->view, d_scenes, (int)n, d_dt, d_h);
         else
-            k_be_step<256><<<(unsigned)n, 256, 0, as_stream(stream)>>>(st->view, d_scenes, (int)n, d_dt, d_h);
+            k_be_step<256, false><<<(unsigned)n, 256, 0, s>>>(st->view, d_scenes, (int)n, d_dt, d_h);
         SDFO_CHECK_LAUNCH();
     });
 }
@@ -1074,8 +1120,8 @@ int sdfo_be_stepper_set_threads(sdfo_be_stepper* st, int32_t threads)
 {
     return guarded([&] {
         SDFO_REQUIRE(st != nullptr, SDFO_ERR_INVALID_ARGUMENT, "stepper is NULL");
-        SDFO_REQUIRE(threads == 128 || threads == 256, SDFO_ERR_INVALID_ARGUMENT,
-                     "threads per scene must be 128 or 256");
+        SDFO_REQUIRE(threads == 32 || threads == 128 || threads == 256, SDFO_ERR_INVALID_ARGUMENT,
+                     "threads per scene must be 32, 128 or 256");
         st->threads = threads;
     });
 }

@@ -263,14 +263,14 @@ def test_gpu_integrate_matches_port(cuda):
 
 @pytest.mark.gpu
 def test_gpu_threads_per_scene_agree(cuda):
-    """128 and 256 threads per scene: the same steps (reductions summed in
-    another order: states within 1e-12 relative)."""
+    """One warp (32 threads), 128 and 256 threads per scene: the same steps
+    (reductions summed in another order: states within 1e-12 relative)."""
     import torch
 
     d = golden("be_steps.npz")
     a = d["flat_drop"]
     outs = []
-    for th in (128, 256):
+    for th in (256, 128, 32):
         grid, st = _stepper(d, "flat_drop", max_scenes=len(a))
         from sdfo import _native as N
 
@@ -279,5 +279,6 @@ def test_gpu_threads_per_scene_agree(cuda):
         h = st.step(scenes, 1e-3)
         torch.cuda.synchronize()
         outs.append((h.cpu().numpy(), _scenes_to_rows(st, scenes)))
-    assert np.array_equal(outs[0][0], outs[1][0])
-    assert _close(outs[0][1], outs[1][1], 1e-12, atol=1e-18)
+    for k in (1, 2):
+        assert np.array_equal(outs[0][0], outs[k][0])
+        assert _close(outs[0][1], outs[k][1], 1e-12, atol=1e-18)
