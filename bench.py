@@ -560,6 +560,7 @@ def be_section(torch, dev, stream, steps, warmup, cpu_ok):
     for _ in range(max(1, warmup)):
         st.step(warm, 1e-3)
     scenes = st.scenes(c["r"], c["R"], c["v"], c["w"])
+    graph_scenes = scenes.clone()
     torch.cuda.synchronize()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(steps)]
@@ -570,11 +571,26 @@ def be_section(torch, dev, stream, steps, warmup, cpu_ok):
         b.record(stream)
     torch.cuda.synchronize()
     ms = [a.elapsed_time(b) for a, b in evs]
+    # the same steps as integrate runs them: one CUDA graph of `steps`
+    # launches (t_end far enough that every step is the full 1 ms request)
+    start = graph_scenes.clone()
+    t_end = graph_scenes[:, 18] + 1.0
+    st.advance(graph_scenes, t_end, 1e-3, launches=steps, stream=stream)  # captured here (untimed)
+    torch.cuda.synchronize()
+    graph_scenes.copy_(start)
+    ga, gb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ga.record(stream)
+    st.advance(graph_scenes, t_end, 1e-3, launches=steps, stream=stream)
+    gb.record(stream)
+    torch.cuda.synchronize()
     u = st.unpack(scenes)
     n = len(c["r"])
     out = {"workload": "ring_drops_on_slab_2048_scenes_7680_points_dt1ms",
            "scenes": n, "steps": steps, "step_ms": ms,
            "scene_steps_per_s": n * steps / (sum(ms) * 1e-3),
+           "graph_ms": ga.elapsed_time(gb),
+           "graph_matches_steps": bool(torch.equal(graph_scenes, scenes)),
            "simulated_time_per_scene_s": float(u["t"].mean()),
            "phases_after": {str(k): int((u["phase"] == k).sum()) for k in sorted(set(u["phase"].tolist()))},
            "cpu_port_scene_steps_per_s": None}
@@ -913,7 +929,7 @@ def run_ours(args, rank, world, local_rank):
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                     "kernel": "k_query<Tricubic,dense>",
+                     "kernel": "k_query_pipe<Tricubic,dense>",
                      "bytes_per_query": BYTES_PER_QUERY,
                      "note": "16 MB grid is L2-resident after the first touch; achieved "
                              "counts gather-model bytes, DRAM traffic is lower"},

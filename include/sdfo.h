@@ -631,6 +631,29 @@ int sdfo_be_stepper_step(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n
  * small quadrature sets. */
 int sdfo_be_stepper_set_threads(sdfo_be_stepper* st, int32_t threads);
 
+/* BackwardEulerIntegrator.integrate (implicit_be.py:113-129), `launches`
+ * steps of it for every scene: a scene with t < t_end - 1e-15 (d_t_end (n),
+ * device) takes one step of at most min(dt, t_end - t), with the loop's
+ * zero-progress fail-safe (a plain BE step of min(dt_min, t_end - t) when a
+ * step makes no progress); the others are left as they are.  The launches
+ * run as one CUDA graph, captured on the first call with a set of arguments
+ * and replayed while they stay the same.  d_unfinished (device, may be NULL)
+ * receives the number of scenes still short of t_end after the last launch.
+ * Asynchronous. */
+int sdfo_be_stepper_advance(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n,
+                            const double* d_t_end, double dt, int32_t launches,
+                            int32_t* d_unfinished, void* stream);
+
+/* The whole integrate loop: sdfo_be_stepper_advance of launches_per_check
+ * launches, then a 4-byte read of the unfinished count, until every scene
+ * has reached t_end or max_launches launches are made.  Synchronises
+ * `stream`.  *launches_out: launches made; *unfinished_out: scenes still
+ * short of t_end (0 unless max_launches ran out).  Both may be NULL. */
+int sdfo_be_stepper_integrate(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n,
+                              const double* d_t_end, double dt, int32_t launches_per_check,
+                              int64_t max_launches, int64_t* launches_out,
+                              int32_t* unfinished_out, void* stream);
+
 int sdfo_be_stepper_destroy(sdfo_be_stepper* st);
 
 #ifdef __cplusplus

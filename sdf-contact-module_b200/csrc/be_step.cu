@@ -109,6 +109,7 @@ struct Shared
     int scan[kMaxWarps];
     int flag, count, mi;
     double lo, hi, hm_pen, toi; // bisection bracket, its measure, the step
+    double m0_gap;              // gap at the start of the step
     int hit, event;
     int scene;                  // index of the scene in the batch
     double alpha;               // line search
@@ -800,7 +801,9 @@ __device__ void refresh(const BeView& b, Shared& s)
 // the whole CTA on one scene.
 template <int T, bool W>
 __global__ void __launch_bounds__(T, (W || T == 256) ? 2 : 4) k_be_step(BeView b, sdfo_be_scene* __restrict__ scenes, int n,
-                                                const double* __restrict__ dt_req, double* __restrict__ h_out)
+                                                const double* __restrict__ dt_req, double* __restrict__ h_out,
+                                                const double* __restrict__ t_end, double dt_max,
+                                                int* __restrict__ unfinished)
 {
     __shared__ Shared shared_scenes[W ? T / 32 : 1];
     const int sc = W ? (int)(blockIdx.x * (T / 32) + (threadIdx.x >> 5)) : (int)blockIdx.x;
@@ -834,7 +837,9 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 2 : 4) k_be_step(BeView b
         s.event = 0;
     }
     Grp<W>::sync();
-    const double dt = dt_req[sc];
+    // integrate mode (implicit_be.py:121-122): while t < t_end - 1e-15, a
+    // step of at most min(dt, t_end - t); otherwise the requested step
+    const double dt = t_end ? (s.q.t < t_end[sc] - 1e-15 ? fmin(dt_max, t_end[sc] - s.q.t) : 0.0) : dt_req[sc];
     if (!(dt > 0.0))
     {
         if (Grp<W>::rank() == 0 && h_out) h_out[sc] = 0.0;
@@ -842,13 +847,12 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 2 : 4) k_be_step(BeView b
     }
     // _activate_initially_penetrating_regions
     measure_body<W>(b, s, s.q);
-    __shared__ double m0_gap;
     if (Grp<W>::rank() == 0)
     {
         s.last_gap = s.m_gap;
         s.last_pen = s.m_pen;
         s.last_vn = s.m_vn;
-        m0_gap = s.m_gap;
+        s.m0_gap = s.m_gap;
         if (s.phase == kInactive && s.m_gap <= 0.0)
         {
             s.phase = kImpacting;
@@ -864,7 +868,7 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 2 : 4) k_be_step(BeView b
         step_be<W>(b, s, &s.q, &s.tr, h_cap, false);
         measure_body<W>(b, s, s.tr);
         if (Grp<W>::rank() == 0)
-            s.flag = (m0_gap > 0.0 && (s.m_gap <= 0.0 || s.m_pen > p.pen_max)) ? 1 : 0;
+            s.flag = (s.m0_gap > 0.0 && (s.m_gap <= 0.0 || s.m_pen > p.pen_max)) ? 1 : 0;
         Grp<W>::sync();
         if (s.flag)
         {
@@ -952,6 +956,14 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 2 : 4) k_be_step(BeView b
         if (Grp<W>::rank() == 0) refresh(b, s);
     }
     Grp<W>::sync();
+    if (t_end && !(h > 0.0))
+    {
+        // the integrate loop's zero-progress fail-safe (implicit_be.py:124-127):
+        // one plain BE step of min(dt_min, t_end - t), nothing re-measured
+        h = fmin(p.dt_min, t_end[sc] - s.q.t);
+        step_be<W>(b, s, &s.q, &s.q, h, region_active(s.phase));
+        Grp<W>::sync();
+    }
     if (Grp<W>::rank() == 0)
     {
         sdfo_be_scene& out = scenes[sc];
@@ -973,11 +985,29 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 2 : 4) k_be_step(BeView b
         out.release_count = s.release_count;
         out.min_dt_hits = s.min_dt_hits;
         if (h_out) h_out[sc] = h;
+        if (unfinished && s.q.t < t_end[sc] - 1e-15) atomicAdd(unfinished, 1);
     }
 }
 
 } // namespace
 } // namespace sdfo
+
+// The arguments a captured run of integrate-mode launches was recorded with.
+struct BeGraphKey
+{
+    void* scenes = nullptr;
+    int64_t n = -1;
+    const double* t_end = nullptr;
+    double dt = 0.0;
+    int launches = 0;
+    int* unfinished = nullptr;
+    int threads = 0;
+    bool operator==(const BeGraphKey& o) const
+    {
+        return scenes == o.scenes && n == o.n && t_end == o.t_end && dt == o.dt && launches == o.launches &&
+               unfinished == o.unfinished && threads == o.threads;
+    }
+};
 
 struct sdfo_be_stepper
 {
@@ -985,13 +1015,97 @@ struct sdfo_be_stepper
     sdfo::BeView view{};
     int64_t capacity = 0;
     int threads = 256;
+    // integrate mode: the last captured graph, the stream it was captured
+    // on, and the unfinished-scene counter (device) with its pinned mirror
+    BeGraphKey key{};
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t capture = nullptr;
+    int* d_unfinished = nullptr;
+    int* h_unfinished = nullptr;
     ~sdfo_be_stepper()
     {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (capture) cudaStreamDestroy(capture);
+        if (h_unfinished) cudaFreeHost(h_unfinished);
+        sdfo::device_free(d_unfinished);
         sdfo::device_free(view.cg);
         sdfo::device_free(view.cgrad);
         sdfo::device_free(view.cvalid);
     }
 };
+
+namespace sdfo {
+namespace {
+
+void launch_step(const sdfo_be_stepper* st, sdfo_be_scene* scenes, int64_t n, const double* dt, double* h,
+                 const double* t_end, double dt_max, int* unfinished, cudaStream_t s)
+{
+    if (st->threads == 32)
+        k_be_step<256, true><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(st->view, scenes, (int)n, dt, h, t_end, dt_max,
+                                                                      unfinished);
+    else if (st->threads == 128)
+        k_be_step<128, false><<<(unsigned)n, 128, 0, s>>>(st->view, scenes, (int)n, dt, h, t_end, dt_max, unfinished);
+    else
+        k_be_step<256, false><<<(unsigned)n, 256, 0, s>>>(st->view, scenes, (int)n, dt, h, t_end, dt_max, unfinished);
+    SDFO_CHECK_LAUNCH();
+}
+
+// Records `k.launches` integrate-mode launches (the counter cleared first,
+// the last launch counting the scenes still short of t_end) as one graph.
+cudaGraphExec_t capture_advance(sdfo_be_stepper* st, const BeGraphKey& k)
+{
+    if (!st->capture) SDFO_CUDA(cudaStreamCreateWithFlags(&st->capture, cudaStreamNonBlocking));
+    cudaStream_t cs = st->capture;
+    SDFO_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    try
+    {
+        if (k.unfinished) SDFO_CUDA(cudaMemsetAsync(k.unfinished, 0, sizeof(int), cs));
+        for (int i = 0; i < k.launches; ++i)
+            launch_step(st, static_cast<sdfo_be_scene*>(k.scenes), k.n, nullptr, nullptr, k.t_end, k.dt,
+                        i + 1 == k.launches ? k.unfinished : nullptr, cs);
+    }
+    catch (...)
+    {
+        cudaStreamEndCapture(cs, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        throw;
+    }
+    SDFO_CUDA(cudaStreamEndCapture(cs, &graph));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    SDFO_CUDA(e);
+    return exec;
+}
+
+void advance(sdfo_be_stepper* st, sdfo_be_scene* scenes, int64_t n, const double* t_end, double dt, int launches,
+             int* unfinished, cudaStream_t s)
+{
+    BeGraphKey k;
+    k.scenes = scenes;
+    k.n = n;
+    k.t_end = t_end;
+    k.dt = dt;
+    k.launches = launches;
+    k.unfinished = unfinished;
+    k.threads = st->threads;
+    if (!st->exec || !(st->key == k))
+    {
+        if (st->exec)
+        {
+            cudaGraphExecDestroy(st->exec);
+            st->exec = nullptr;
+        }
+        st->exec = capture_advance(st, k);
+        st->key = k;
+    }
+    SDFO_CUDA(cudaGraphLaunch(st->exec, s));
+}
+
+} // namespace
+} // namespace sdfo
 
 using namespace sdfo;
 
@@ -1105,14 +1219,61 @@ int sdfo_be_stepper_step(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n
                      "scene count exceeds the stepper's capacity");
         if (n == 0) return;
         SDFO_REQUIRE(d_scenes && d_dt, SDFO_ERR_INVALID_ARGUMENT, "scenes and step sizes are required");
+        launch_step(st, d_scenes, n, d_dt, d_h, nullptr, 0.0, nullptr, as_stream(stream));
+    });
+}
+
+int sdfo_be_stepper_advance(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n, const double* d_t_end,
+                            double dt, int32_t launches, int32_t* d_unfinished, void* stream)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(st != nullptr, SDFO_ERR_INVALID_ARGUMENT, "stepper is NULL");
+        SDFO_REQUIRE(n >= 0 && n <= st->capacity, SDFO_ERR_INVALID_ARGUMENT,
+                     "scene count exceeds the stepper's capacity");
+        SDFO_REQUIRE(dt > 0.0, SDFO_ERR_INVALID_ARGUMENT, "dt must be positive");
+        SDFO_REQUIRE(launches >= 1 && launches <= 4096, SDFO_ERR_INVALID_ARGUMENT,
+                     "launches must be in [1, 4096]");
         cudaStream_t s = as_stream(stream);
-        if (st->threads == 32)
-            k_be_step<256, true><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(st->view, d_scenes, (int)n, d_dt, d_h);
-        else if (st->threads == 128)
-            k_be_step<128, false><<<(unsigned)n, 128, 0, s>>>(st->view, d_scenes, (int)n, d_dt, d_h);
-        else
-            k_be_step<256, false><<<(unsigned)n, 256, 0, s>>>(st->view, d_scenes, (int)n, d_dt, d_h);
-        SDFO_CHECK_LAUNCH();
+        if (n == 0)
+        {
+            if (d_unfinished) SDFO_CUDA(cudaMemsetAsync(d_unfinished, 0, sizeof(int32_t), s));
+            return;
+        }
+        SDFO_REQUIRE(d_scenes && d_t_end, SDFO_ERR_INVALID_ARGUMENT, "scenes and end times are required");
+        advance(st, d_scenes, n, d_t_end, dt, launches, d_unfinished, s);
+    });
+}
+
+int sdfo_be_stepper_integrate(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n, const double* d_t_end,
+                              double dt, int32_t launches_per_check, int64_t max_launches, int64_t* launches_out,
+                              int32_t* unfinished_out, void* stream)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(st != nullptr, SDFO_ERR_INVALID_ARGUMENT, "stepper is NULL");
+        SDFO_REQUIRE(n >= 0 && n <= st->capacity, SDFO_ERR_INVALID_ARGUMENT,
+                     "scene count exceeds the stepper's capacity");
+        SDFO_REQUIRE(dt > 0.0, SDFO_ERR_INVALID_ARGUMENT, "dt must be positive");
+        SDFO_REQUIRE(launches_per_check >= 1 && launches_per_check <= 4096, SDFO_ERR_INVALID_ARGUMENT,
+                     "launches_per_check must be in [1, 4096]");
+        SDFO_REQUIRE(max_launches >= 1, SDFO_ERR_INVALID_ARGUMENT, "max_launches must be positive");
+        if (launches_out) *launches_out = 0;
+        if (unfinished_out) *unfinished_out = 0;
+        if (n == 0) return;
+        SDFO_REQUIRE(d_scenes && d_t_end, SDFO_ERR_INVALID_ARGUMENT, "scenes and end times are required");
+        if (!st->d_unfinished) st->d_unfinished = dalloc<int>(1);
+        if (!st->h_unfinished) SDFO_CUDA(cudaHostAlloc(&st->h_unfinished, sizeof(int), cudaHostAllocDefault));
+        cudaStream_t s = as_stream(stream);
+        int64_t made = 0;
+        while (made < max_launches)
+        {
+            advance(st, d_scenes, n, d_t_end, dt, launches_per_check, st->d_unfinished, s);
+            made += launches_per_check;
+            SDFO_CUDA(cudaMemcpyAsync(st->h_unfinished, st->d_unfinished, sizeof(int), cudaMemcpyDeviceToHost, s));
+            SDFO_CUDA(cudaStreamSynchronize(s));
+            if (*st->h_unfinished == 0) break;
+        }
+        if (launches_out) *launches_out = made;
+        if (unfinished_out) *unfinished_out = *st->h_unfinished;
     });
 }
 

@@ -356,9 +356,10 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 
 // symmetric Hessian:
 // each CTA walks tiles of kThreads queries; point tiles arrive by
 // cp.async.bulk three tiles ahead (so no query waits on its point load), the
-// output tiles are written to shared memory and leave by bulk stores.  Whole
-// tiles only; the caller runs k_query on the remainder.  Bounded waits, as
-// in stream_bwd.cu (status bit 1 when one runs out).
+// output tiles are written to shared memory and leave by bulk stores.  The
+// last n mod kThreads points take plain loads and stores in the last CTA,
+// which takes no tile.  Bounded waits, as in stream_bwd.cu (status bit 1 when
+// one runs out).
 constexpr int kPipeStages = 3;
 constexpr unsigned kPipeWaitLimit = 1u << 24;
 __device__ unsigned int g_pipe_status = 0;
@@ -375,7 +376,7 @@ struct PipeLayout
 
 template <int MODE, bool SPARSE, int BD, bool HESS>
 __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS>())
-    k_query_pipe(GridView g, const float* __restrict__ pts, int64_t tiles, QueryOutputs o)
+    k_query_pipe(GridView g, const float* __restrict__ pts, int64_t n, QueryOutputs o)
 {
     using L = PipeLayout<HESS>;
     using namespace bulk;
@@ -385,7 +386,34 @@ __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS>())
     __shared__ long long s_kabort;
     unsigned char* stages = smem;
     unsigned char* outs = smem + kPipeStages * L::pts;
-    const int64_t first = blockIdx.x, step = gridDim.x;
+    const int64_t tiles = n / kThreads;
+    // with a remainder the last CTA takes it (plain loads and stores) and
+    // leaves; the others walk the whole tiles
+    const bool rem = (n % kThreads) != 0;
+    if (rem && blockIdx.x == gridDim.x - 1)
+    {
+        const int64_t q = tiles * kThreads + threadIdx.x;
+        if (q >= n) return;
+        const double p[3] = {pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]};
+        Interp r;
+        float unit[3];
+        const bool valid = evaluate<MODE, SPARSE, BD, HESS>(g, p, r, unit, false);
+        if (!valid)
+        {
+            r.gap = 0.f;
+            r.g[0] = r.g[1] = r.g[2] = 0.f;
+#pragma unroll
+            for (int a = 0; a < 6; ++a) r.H[a] = 0.f;
+        }
+        o.gap[q] = r.gap;
+        if (o.grad)
+            for (int a = 0; a < 3; ++a) o.grad[3 * q + a] = r.g[a];
+        if (o.valid) o.valid[q] = valid ? 1 : 0;
+        if (HESS && o.hess6)
+            for (int a = 0; a < 6; ++a) o.hess6[6 * q + a] = r.H[a];
+        return;
+    }
+    const int64_t first = blockIdx.x, step = gridDim.x - (rem ? 1 : 0);
     const int64_t mine = first < tiles ? (tiles - first + step - 1) / step : 0;
     if (threadIdx.x == 0)
     {
@@ -477,15 +505,15 @@ __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS>())
     }
 }
 
-// The whole tiles of a float32 query through k_query_pipe when the outputs
-// allow it (gap, grad, valid, hess6 only; 16-byte aligned); returns the
-// number of queries done (0: not taken).
+// A float32 query through k_query_pipe when the outputs allow it (gap, grad,
+// valid, hess6 only; 16-byte aligned) and there is at least one whole tile;
+// returns whether it was taken.
 template <int MODE, bool SPARSE, int BD>
-int64_t launch_pipe(const GridView& v, const float* pts, int64_t n, const QueryOutputs& o, cudaStream_t s)
+bool launch_pipe(const GridView& v, const float* pts, int64_t n, const QueryOutputs& o, cudaStream_t s)
 {
     if (n < kThreads || o.unit || o.witness || o.hess || !o.gap || !aligned16(pts) || !aligned16(o.gap) ||
         !aligned16(o.grad) || !aligned16(o.valid) || !aligned16(o.hess6))
-        return 0;
+        return false;
     static int sms = 0;
     if (sms == 0)
     {
@@ -494,48 +522,32 @@ int64_t launch_pipe(const GridView& v, const float* pts, int64_t n, const QueryO
         SDFO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     }
     const int64_t tiles = n / kThreads;
+    const int64_t rem = n % kThreads ? 1 : 0; // one more CTA, for the remainder
     if (o.hess6)
     {
-        const int64_t ctas = std::min<int64_t>(tiles, (int64_t)sms * query_min_blocks<true>());
+        const int64_t ctas = std::min<int64_t>(tiles, (int64_t)sms * query_min_blocks<true>() - rem) + rem;
         k_query_pipe<MODE, SPARSE, BD, true>
-            <<<(unsigned)ctas, kThreads, PipeLayout<true>::total, s>>>(v, pts, tiles, o);
+            <<<(unsigned)ctas, kThreads, PipeLayout<true>::total, s>>>(v, pts, n, o);
     }
     else
     {
-        const int64_t ctas = std::min<int64_t>(tiles, (int64_t)sms * query_min_blocks<false>());
+        const int64_t ctas = std::min<int64_t>(tiles, (int64_t)sms * query_min_blocks<false>() - rem) + rem;
         k_query_pipe<MODE, SPARSE, BD, false>
-            <<<(unsigned)ctas, kThreads, PipeLayout<false>::total, s>>>(v, pts, tiles, o);
+            <<<(unsigned)ctas, kThreads, PipeLayout<false>::total, s>>>(v, pts, n, o);
     }
     SDFO_CHECK_LAUNCH();
-    return tiles * kThreads;
+    return true;
 }
 
 template <int MODE, bool SPARSE, int BD>
-void launch_pt(const GridView& v, const void* pts_in, bool f64, int64_t n_in, const QueryOutputs& o_in,
-               cudaStream_t s)
+void launch_pt(const GridView& v, const void* pts, bool f64, int64_t n, const QueryOutputs& o, cudaStream_t s)
 {
-    const void* pts = pts_in;
-    int64_t n = n_in;
-    QueryOutputs o = o_in;
     // Dense grids only: on sparse grids the gathers' latency varies with the
     // brick lookups, and the per-tile barriers of a persistent CTA then cost
     // more than the prefetched points save (measured: C5 forward -11%).
     if constexpr (!SPARSE && (MODE == SDFO_TRILINEAR || MODE == SDFO_TRICUBIC))
     {
-        if (!f64)
-        {
-            const int64_t done = launch_pipe<MODE, SPARSE, BD>(v, static_cast<const float*>(pts), n, o, s);
-            if (done == n) return;
-            if (done > 0)
-            {
-                pts = static_cast<const float*>(pts) + 3 * done;
-                n -= done;
-                o.gap += done;
-                if (o.grad) o.grad += 3 * done;
-                if (o.valid) o.valid += done;
-                if (o.hess6) o.hess6 += 6 * done;
-            }
-        }
+        if (!f64 && launch_pipe<MODE, SPARSE, BD>(v, static_cast<const float*>(pts), n, o, s)) return;
     }
     const bool staged = !f64 && aligned16(pts) && aligned16(o.grad) && aligned16(o.unit) &&
                         aligned16(o.witness) && aligned16(o.hess6);

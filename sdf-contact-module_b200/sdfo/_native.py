@@ -148,6 +148,9 @@ SIGNATURES = [
     ("sdfo_be_stepper_create", ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _P]),
     ("sdfo_be_stepper_step", ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
     ("sdfo_be_stepper_set_threads", ctypes.c_int, [_P, _I32]),
+    ("sdfo_be_stepper_advance", ctypes.c_int, [_P, _P, _I64, _P, ctypes.c_double, _I32, _P, _P]),
+    ("sdfo_be_stepper_integrate", ctypes.c_int,
+     [_P, _P, _I64, _P, ctypes.c_double, _I32, _I64, _P, _P, _P]),
     ("sdfo_be_stepper_destroy", ctypes.c_int, [_P]),
     ("sdfo_grid_load_file", ctypes.c_int, [ctypes.c_char_p, _I32, _P, _P]),
     ("sdfo_grid_save_file", ctypes.c_int, [_P, ctypes.c_char_p, _P]),

@@ -8,7 +8,8 @@ SDFContactEngine's culling and linearisation cache
 (prototype/src/dynamics/contacts_sdf.py).  One CUDA thread block advances
 one scene through its whole adaptive step -- time-of-impact bisection with
 trial BE solves, Newton iterations with line search, the contact phase state
-machine -- so a step of every scene is one kernel launch.
+machine -- so a step of every scene is one kernel launch, and integrate's
+steps replay as CUDA graphs of such launches.
 
 Scenes live in a float64 CUDA tensor (n, 26) laid out as sdfo_be_scene:
 r (3), R row-major (9), v (3), w (3), t, dt_current, last_gap,
@@ -142,8 +143,7 @@ class BEStepper:
         """One BackwardEulerIntegrator.step of every scene (in place); dt a
         float or an (n,) float64 CUDA tensor (<= 0 leaves a scene as it is).
         Returns the step each scene took."""
-        if scenes.dtype != torch.float64 or scenes.shape[1] != SCENE_DOUBLES or not scenes.is_contiguous():
-            raise ValueError("scenes must be a contiguous (n, 26) float64 CUDA tensor")
+        self._check(scenes)
         n = scenes.shape[0]
         if not torch.is_tensor(dt):
             dt = torch.full((n,), float(dt), dtype=torch.float64, device=scenes.device)
@@ -153,18 +153,48 @@ class BEStepper:
                                               _stream_ptr(stream)))
         return h
 
-    def integrate(self, scenes: torch.Tensor, T: float, dt: float, check_every=8, max_launches=100000):
-        """BackwardEulerIntegrator.integrate (implicit_be.py:109-129) for every
+    def advance(self, scenes: torch.Tensor, t_end: torch.Tensor, dt: float, launches: int = 8,
+                unfinished: torch.Tensor = None, stream=None) -> None:
+        """`launches` steps of BackwardEulerIntegrator.integrate's loop
+        (implicit_be.py:121-127) for every scene short of its t_end (an (n,)
+        float64 CUDA tensor), replayed as one CUDA graph.  `unfinished` (a
+        one-element int32 CUDA tensor) receives the number of scenes still
+        short of t_end.  Asynchronous."""
+        self._check(scenes)
+        t_end = self._t_end(scenes, t_end)
+        if unfinished is not None and (unfinished.dtype != torch.int32 or unfinished.numel() < 1):
+            raise ValueError("unfinished must be an int32 CUDA tensor")
+        N.check(N.load().sdfo_be_stepper_advance(
+            self._h, _t_ptr(scenes), scenes.shape[0], _t_ptr(t_end), float(dt), int(launches),
+            _t_ptr(unfinished) if unfinished is not None else None, _stream_ptr(stream)))
+
+    def integrate(self, scenes: torch.Tensor, T: float, dt: float, check_every=8, max_launches=100000,
+                  stream=None) -> int:
+        """BackwardEulerIntegrator.integrate (implicit_be.py:113-129) for every
         scene: steps of at most dt until each scene's t reaches its start
-        time + T.  Returns the number of launches."""
-        t_end = scenes[:, 18].clone() + T
-        launches = 0
-        while launches < max_launches:
-            for _ in range(check_every):
-                rem = t_end - scenes[:, 18]
-                req = torch.where(rem > 1e-15, torch.clamp(rem, max=dt), torch.zeros_like(rem))
-                self.step(scenes, req)
-                launches += 1
-            if not bool((t_end - scenes[:, 18] > 1e-15).any()):
-                break
-        return launches
+        time + T.  The steps run as CUDA graphs of `check_every` launches
+        with a 4-byte read of the unfinished count after each.  Returns the
+        number of launches; raises if max_launches ran out first."""
+        self._check(scenes)
+        t_end = (scenes[:, 18] + T).contiguous()
+        made = ctypes.c_int64(0)
+        left = ctypes.c_int32(0)
+        N.check(N.load().sdfo_be_stepper_integrate(
+            self._h, _t_ptr(scenes), scenes.shape[0], _t_ptr(t_end), float(dt), int(check_every),
+            int(max_launches), ctypes.byref(made), ctypes.byref(left), _stream_ptr(stream)))
+        if left.value:
+            raise RuntimeError(f"{left.value} scenes short of their end time after {made.value} launches")
+        return made.value
+
+    @staticmethod
+    def _check(scenes):
+        if scenes.dtype != torch.float64 or scenes.dim() != 2 or scenes.shape[1] != SCENE_DOUBLES \
+                or not scenes.is_contiguous() or not scenes.is_cuda:
+            raise ValueError("scenes must be a contiguous (n, 26) float64 CUDA tensor")
+
+    @staticmethod
+    def _t_end(scenes, t_end):
+        if not torch.is_tensor(t_end) or t_end.dtype != torch.float64 or t_end.numel() != scenes.shape[0] \
+                or not t_end.is_cuda:
+            raise ValueError("t_end must be an (n,) float64 CUDA tensor")
+        return t_end.contiguous()

@@ -262,6 +262,44 @@ def test_gpu_integrate_matches_port(cuda):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("threads", [256, 32])
+def test_gpu_advance_graph_matches_steps(cuda, threads):
+    """sdfo_be_stepper_advance (integrate's steps replayed as one CUDA graph,
+    each scene's step size min(dt, t_end - t) worked out on the device) gives
+    the same states, bit for bit, as single steps whose sizes the host works
+    out by implicit_be.py:121-122; the graph is replayed with the same
+    arguments, and the unfinished count matches the host's."""
+    import torch
+
+    from sdfo import _native as N
+
+    d = golden("be_steps.npz")
+    grid, st = _stepper(d, "flat_drop", max_scenes=5)
+    N.check(N.load().sdfo_be_stepper_set_threads(st._h, threads))
+    r = np.array([[0.0, 0.0, 0.0115], [0.01, 0.0, 0.02], [0.0, -0.02, 0.012], [0.0, 0.0, 0.05],
+                  [0.0, 0.0, 0.03]])
+    R = np.tile(np.eye(3), (5, 1, 1))
+    v = np.tile([0.0, 0.0, -0.2], (5, 1))
+    a = st.scenes(r, R, v=v)
+    b = a.clone()
+    # scene 3 runs 2.5 ms, scene 4 is already at its end time
+    t_end = a[:, 18] + torch.tensor([0.006, 0.006, 0.006, 0.0025, 0.0], dtype=torch.float64, device="cuda")
+    unfinished = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+    for _ in range(2):
+        st.advance(a, t_end, 1e-3, launches=4, unfinished=unfinished)
+    te = t_end.cpu().numpy()
+    for _ in range(8):
+        t = b[:, 18].cpu().numpy()
+        req = np.where(t < te - 1e-15, np.minimum(1e-3, te - t), 0.0)
+        st.step(b, torch.as_tensor(req, device="cuda"))
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    t = a[:, 18].cpu().numpy()
+    assert int(unfinished.item()) == int(np.sum(t < te - 1e-15))
+    assert t[4] == 0.0 and abs(t[3] - 0.0025) <= 1e-15
+
+
+@pytest.mark.gpu
 def test_gpu_threads_per_scene_agree(cuda):
     """One warp (32 threads), 128 and 256 threads per scene: the same steps
     (reductions summed in another order: states within 1e-12 relative)."""
