@@ -753,6 +753,9 @@ def run_ours(args, rank, world, local_rank):
     lb.close()
     N.check(lib.sdfo_set_bvh_mode(N.BVH_REFERENCE))
     n_vox = int(np.prod(dense.shape))
+    # traversal work per voxel of the dense fill (instrumented copy, untimed)
+    trav = SdfGrid.traversal_stats(c["verts"], c["tris"], **c["dense"])
+    trav.pop("totals")
 
     h = float(dense.voxel[0])
     pts_np = points_for(c, h)
@@ -941,7 +944,8 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk,
         "build": {
             "dense_voxels_per_s": n_vox / t_dense,
-            "dense_ms": 1e3 * t_dense, "dense_fill_kernel_ms": st_dense["fill_ms"],
+            "dense_ms": 1e3 * t_dense, "dense_setup_alloc_ms": st_dense["setup_ms"],
+            "dense_fill_kernel_ms": st_dense["fill_ms"],
             "dense_bvh_ms": st_dense["bvh_ms"], "dense_hessian_ms": st_dense["hessian_ms"],
             "dense_fill_voxels_per_s": n_vox / (1e-3 * st_dense["fill_ms"]),
             "lbvh_dense_ms": 1e3 * t_lbvh, "lbvh_bvh_ms": st_lbvh["bvh_ms"],
@@ -950,6 +954,7 @@ def run_ours(args, rank, world, local_rank):
             "sparse_stored_voxels_per_s": sparse.stored_voxels / t_sparse,
             "sparse_fill_ms": st_sparse["fill_ms"],
             "cpu_reference_dense_voxels_per_s": cpu_build,
+            "dense_fill_traversal": trav,
         },
         "queries": {
             "dense_tricubic_fwd_per_s": n / per_launch_s,

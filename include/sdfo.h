@@ -171,7 +171,9 @@ typedef struct
     int32_t reserved0;
 } sdfo_contact_measure;
 
-/* Build statistics of the last build on a handle. */
+/* Build statistics of the last build on a handle: setup_ms = host grid
+ * setup and the grid's device allocations, bvh_ms = acceleration structure,
+ * fill_ms = distance / sign fill, hessian_ms = Hessian and query layouts. */
 typedef struct
 {
     double setup_ms, bvh_ms, fill_ms, hessian_ms, total_ms;
@@ -271,6 +273,22 @@ int sdfo_grid_build_sparse_batched(const sdfo_mesh_desc* meshes, int32_t n, void
 int sdfo_set_fill_ctas_per_sm(int32_t ctas);
 
 int sdfo_grid_build_stats(const sdfo_grid* g, sdfo_build_stats* out);
+
+/* Traversal work of the dense fill (no reference counterpart; for
+ * profiling): the nearest-triangle searches (KdTree::findNearest) and the
+ * parity-ray counts (countRayIntersections) of every voxel of the grid that
+ * `p` gives, on the current acceleration structure, run by an instrumented
+ * copy of the fill kernel that counts instead of storing.  Synchronous. */
+typedef struct
+{
+    int64_t voxels;
+    int64_t nearest_nodes;     /* nodes whose children or triangles were examined */
+    int64_t nearest_triangles; /* closest-point tests */
+    int64_t ray_nodes;         /* ray-box tests */
+    int64_t ray_triangles;     /* ray-triangle tests */
+} sdfo_traversal_stats;
+int sdfo_build_traversal_stats(const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
+                               const sdfo_build_params* p, void* stream, sdfo_traversal_stats* out);
 
 /* Selects the acceleration structure of subsequent builds (process-wide;
  * default SDFO_BVH_REFERENCE).  No reference counterpart: the reference has

@@ -48,6 +48,7 @@ def lib():
         L.port_bvh_free.argtypes = [_P]
         L.port_signed_nearest.argtypes = [_P, _P, _L, _P, _P, _P, _P, _P]
         L.port_nearest_distance.argtypes = [_P, _P, _L, _P]
+        L.port_traversal_counts.argtypes = [_P, _P, _L, _P]
         L.port_build_dense.argtypes = [_P, ctypes.POINTER(_Spec), _P, _P, _P, _P]
         L.port_dense_hessian.argtypes = [ctypes.POINTER(_Spec), _P, _P]
         L.port_sparse_activate.argtypes = [_P, ctypes.POINTER(_Spec), _I, _I, _D, _P]
@@ -135,6 +136,14 @@ class Bvh:
         lib().port_signed_nearest(self.h, _ptr(p), n, _ptr(sd), _ptr(cp), _ptr(fn), _ptr(tri),
                                   _ptr(hits))
         return dict(sd=sd, cp=cp, fn=fn, tri=tri, hits=hits)
+
+    def traversal_counts(self, pts):
+        """[nodes entered past the nearest search's cut, closest-point tests,
+        ray-box tests, ray-triangle tests] summed over the points."""
+        p = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+        c = np.zeros(4, np.int64)
+        lib().port_traversal_counts(self.h, _ptr(p), len(p), _ptr(c))
+        return c
 
     def nearest_distance(self, pts):
         p = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)

@@ -385,13 +385,20 @@ typedef struct
     double cp[3];
 } nearest_t;
 
+/* Traversal work counted by port_traversal_counts (NULL otherwise): nodes
+ * entered past the nearest search's box cut and their closest-point tests;
+ * ray-box tests and ray-triangle tests. */
+static thread_local int64_t* t_count = NULL;
+
 /* searchNearest (KdTree.h:266-328): near-first depth-first branch and bound. */
 static void nearest_rec(const port_bvh* b, int id, const double* p, nearest_t* best)
 {
     const pnode* n = &b->nodes[id];
     if (box_dist_sq(p, n->lo, n->hi) > best->sq) return;
+    if (t_count) ++t_count[0];
     if (n->count > 0)
     {
+        if (t_count) t_count[1] += n->count;
         for (int i = n->start; i < n->start + n->count; ++i)
         {
             const int t = b->order[i];
@@ -459,9 +466,11 @@ static int ray_box(const port_bvh* b, const double* o, const pnode* n)
 static int ray_count_rec(const port_bvh* b, int id, const double* o)
 {
     const pnode* n = &b->nodes[id];
+    if (t_count) ++t_count[2];
     if (!ray_box(b, o, n)) return 0;
     if (n->count > 0)
     {
+        if (t_count) t_count[3] += n->count;
         int hits = 0;
         for (int i = n->start; i < n->start + n->count; ++i)
         {
@@ -517,6 +526,18 @@ void port_signed_nearest(const port_bvh* b, const double* pts, int64_t n, double
     for (int64_t i = 0; i < n; ++i)
         signed_nearest_one(b, pts + 3 * i, sd + i, cp ? cp + 3 * i : NULL, fn ? fn + 3 * i : NULL,
                            tri ? tri + i : NULL, hits ? hits + i : NULL);
+}
+
+void port_traversal_counts(const port_bvh* b, const double* pts, int64_t n, int64_t* counts)
+{
+    counts[0] = counts[1] = counts[2] = counts[3] = 0;
+    for (int64_t i = 0; i < n; ++i)
+    {
+        double sd;
+        t_count = counts;
+        signed_nearest_one(b, pts + 3 * i, &sd, NULL, NULL, NULL, NULL);
+        t_count = NULL;
+    }
 }
 
 void port_nearest_distance(const port_bvh* b, const double* pts, int64_t n, double* dist)

@@ -57,6 +57,10 @@ void port_signed_nearest(const port_bvh* b, const double* pts, int64_t n, double
                          double* cp, double* fn, int* tri, int* hits);
 /* Unsigned nearest distance only (used for sparse block activation). */
 void port_nearest_distance(const port_bvh* b, const double* pts, int64_t n, double* dist);
+/* The findSignedNearest traversals of n points, counted (serial): counts[0]
+ * nodes entered past the nearest search's cut, [1] closest-point tests,
+ * [2] ray-box tests, [3] ray-triangle tests. */
+void port_traversal_counts(const port_bvh* b, const double* pts, int64_t n, int64_t* counts);
 
 /* Dense build: computeSdfAndNormals (SdfBuilder.cpp:1039-1101) then
  * estimateHessian (SdfBuilder.cpp:1105-1152).  Arrays are x-fastest,

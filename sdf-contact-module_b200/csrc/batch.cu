@@ -241,8 +241,9 @@ std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n
                 {
                     try
                     {
+                        // one host thread per mesh: the pool runs the meshes side by side
                         host_ref_tree(host[(size_t)m], meshes[m].h_verts, meshes[m].h_tris,
-                                      meshes[m].nt);
+                                      meshes[m].nt, 1);
                     }
                     catch (...)
                     {

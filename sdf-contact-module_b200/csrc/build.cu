@@ -105,13 +105,7 @@ sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int
     const int64_t N = (int64_t)g->info.shape[0] * g->info.shape[1] * g->info.shape[2];
     g->stored_voxels = N;
     g->stats.triangles = (int32_t)nt;
-    g->stats.setup_ms =
-        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    Timer tm(s);
-    AnyTree tree{bvh_mode()};
-    tree.build(verts, nv, tris, nt, scene_extent(verts, nv, g->info), s);
-    g->stats.bvh_nodes = tree.node_count(nt);
-    g->stats.bvh_ms = tm.lap();
+    // the grid's storage (setup_ms counts these allocations)
     g->d.phin = dalloc<float4>((size_t)N);
     g->d.phi64 = dalloc<double>((size_t)N);
     g->d.n64 = dalloc<double>((size_t)N * 3);
@@ -120,6 +114,13 @@ sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int
     g->d.hess6 = dalloc<float>((size_t)N * 6);
     DeviceBuffer<int> status(1);
     SDFO_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), s));
+    g->stats.setup_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    Timer tm(s);
+    AnyTree tree{bvh_mode()};
+    tree.build(verts, nv, tris, nt, scene_extent(verts, nv, g->info), s);
+    g->stats.bvh_nodes = tree.node_count(nt);
+    g->stats.bvh_ms = tm.lap();
     const SpecD sp = spec_of(g->info);
     const dim3 grid((sp.n[0] + 7) / 8, (sp.n[1] + 7) / 8, (sp.n[2] + 3) / 4);
     tree.visit([&](auto view) {
@@ -137,6 +138,30 @@ sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int
     g->stats.total_ms =
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return g.release();
+}
+
+void count_dense_traversal(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
+                           const sdfo_build_params& p, cudaStream_t s, sdfo_traversal_stats* out)
+{
+    const sdfo_grid_info info = setup_grid(verts, nv, p);
+    AnyTree tree{bvh_mode()};
+    tree.build(verts, nv, tris, nt, scene_extent(verts, nv, info), s);
+    DeviceBuffer<int> status(1);
+    DeviceBuffer<unsigned long long> sums(4);
+    SDFO_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), s));
+    SDFO_CUDA(cudaMemsetAsync(sums.get(), 0, 4 * sizeof(unsigned long long), s));
+    const SpecD sp = spec_of(info);
+    const dim3 grid((sp.n[0] + 7) / 8, (sp.n[1] + 7) / 8, (sp.n[2] + 3) / 4);
+    tree.visit([&](auto view) { k_dense_count<<<grid, 256, 0, s>>>(view, sp, sums.get(), status.get()); });
+    SDFO_CHECK_LAUNCH();
+    unsigned long long h[4] = {0, 0, 0, 0};
+    SDFO_CUDA(cudaMemcpyAsync(h, sums.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
+    check_status(status, s); // synchronises s
+    out->voxels = (int64_t)info.shape[0] * info.shape[1] * info.shape[2];
+    out->nearest_nodes = (int64_t)h[0];
+    out->nearest_triangles = (int64_t)h[1];
+    out->ray_nodes = (int64_t)h[2];
+    out->ray_triangles = (int64_t)h[3];
 }
 
 sdfo_grid* build_sparse(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,

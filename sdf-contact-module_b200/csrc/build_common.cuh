@@ -318,6 +318,15 @@ __device__ __forceinline__ void test_triangle(const LbvhView& b, const d3& p, in
     }
 }
 
+// Traversal work of one query, counted only by the instrumented (COUNT)
+// instantiations of the traversals below: nodes whose children (or
+// triangles) were examined and triangles tested, for the nearest search and
+// for the parity ray.
+struct TravCount
+{
+    int nearest_nodes = 0, nearest_tris = 0, ray_nodes = 0, ray_tris = 0;
+};
+
 // Upper bound used for FP32 culling: bestSq rounded up, plus a relative slack
 // covering FP32 rounding of the box distance.
 __device__ __forceinline__ float cull_limit(double sq)
@@ -325,7 +334,8 @@ __device__ __forceinline__ float cull_limit(double sq)
     return sq >= 3.0e38 ? INFINITY : __double2float_ru(sq) * 1.000002f;
 }
 
-__device__ Nearest tree_nearest(const LbvhView& b, const d3& p, int* status)
+template <bool COUNT = false>
+__device__ Nearest tree_nearest(const LbvhView& b, const d3& p, int* status, TravCount* tc = nullptr)
 {
     Nearest best;
     best.sq = 1.0e308 * 10.0; // +inf
@@ -334,6 +344,7 @@ __device__ Nearest tree_nearest(const LbvhView& b, const d3& p, int* status)
     best.cp = p;
     if (b.n == 1)
     {
+        if constexpr (COUNT) ++tc->nearest_tris;
         test_triangle(b, p, 0, best);
         return best;
     }
@@ -346,10 +357,12 @@ __device__ Nearest tree_nearest(const LbvhView& b, const d3& p, int* status)
     {
         if (node < 0)
         {
+            if constexpr (COUNT) ++tc->nearest_tris;
             test_triangle(b, p, ~node, best);
         }
         else
         {
+            if constexpr (COUNT) ++tc->nearest_nodes;
             const float4 n0 = __ldg(b.nodes + 4 * (int64_t)node);
             const float4 n1 = __ldg(b.nodes + 4 * (int64_t)node + 1);
             const float4 n2 = __ldg(b.nodes + 4 * (int64_t)node + 2);
@@ -422,11 +435,15 @@ __device__ __forceinline__ bool ray_box(const float o[3], const float inv[3], fl
 
 // countRayIntersections (KdTree.h:398-441): number of triangles the fixed
 // ray hits (exact FP64 test on every triangle whose widened box it crosses).
-__device__ int tree_ray_count(const LbvhView& b, const d3& p, int* status)
+template <bool COUNT = false>
+__device__ int tree_ray_count(const LbvhView& b, const d3& p, int* status, TravCount* tc = nullptr)
 {
     const d3 dir = mk(b.dir[0], b.dir[1], b.dir[2]);
     if (b.n == 1)
+    {
+        if constexpr (COUNT) ++tc->ray_tris;
         return ray_hits(p, dir, tri_vertex(b, 0, 0), tri_vertex(b, 0, 1), tri_vertex(b, 0, 2)) ? 1 : 0;
+    }
     const float o[3] = {(float)p.x, (float)p.y, (float)p.z};
     int stack[kStackDepth];
     int sp = 0;
@@ -436,11 +453,13 @@ __device__ int tree_ray_count(const LbvhView& b, const d3& p, int* status)
     {
         if (node < 0)
         {
+            if constexpr (COUNT) ++tc->ray_tris;
             const int s = ~node;
             hits += ray_hits(p, dir, tri_vertex(b, s, 0), tri_vertex(b, s, 1), tri_vertex(b, s, 2)) ? 1 : 0;
         }
         else
         {
+            if constexpr (COUNT) ++tc->ray_nodes;
             const float4 n0 = __ldg(b.nodes + 4 * (int64_t)node);
             const float4 n1 = __ldg(b.nodes + 4 * (int64_t)node + 1);
             const float4 n2 = __ldg(b.nodes + 4 * (int64_t)node + 2);
@@ -536,7 +555,8 @@ __device__ __forceinline__ double box_dist_sq(const d3& p, const double lo[3], c
 // "box distance > best" cut when a subtree is entered, and triangles replace
 // the best only on a strictly smaller squared distance -- so the triangle
 // found is the reference's, ties included.
-__device__ Nearest tree_nearest(const RefTreeView& b, const d3& p, int* status)
+template <bool COUNT = false>
+__device__ Nearest tree_nearest(const RefTreeView& b, const d3& p, int* status, TravCount* tc = nullptr)
 {
     Nearest best;
     best.sq = DBL_MAX;
@@ -559,10 +579,12 @@ __device__ Nearest tree_nearest(const RefTreeView& b, const d3& p, int* status)
         --sp;
         const int node = stack[sp];
         if (sdist[sp] > best.sq) continue;
+        if constexpr (COUNT) ++tc->nearest_nodes;
         const RefNode* nd = b.nodes + node;
         const int4 meta = __ldg(reinterpret_cast<const int4*>(nd) + 3);
         if (meta.w > 0)
         {
+            if constexpr (COUNT) tc->nearest_tris += meta.w;
             for (int s = meta.z; s < meta.z + meta.w; ++s)
             {
                 const d3 a = tri_vertex(b, s, 0), bb = tri_vertex(b, s, 1), c = tri_vertex(b, s, 2);
@@ -634,7 +656,8 @@ __device__ __forceinline__ bool ray_box_ref(const d3& o, const double dir[3], co
 }
 
 // countRayIntersectionsRecursive (KdTree.h:398-441) over the same tree.
-__device__ int tree_ray_count(const RefTreeView& b, const d3& p, int* status)
+template <bool COUNT = false>
+__device__ int tree_ray_count(const RefTreeView& b, const d3& p, int* status, TravCount* tc = nullptr)
 {
     if (b.nnodes == 0) return 0;
     const d3 dir = mk(b.dir[0], b.dir[1], b.dir[2]);
@@ -648,10 +671,12 @@ __device__ int tree_ray_count(const RefTreeView& b, const d3& p, int* status)
         const RefNode* nd = b.nodes + node;
         double lo[3], hi[3];
         load_box(nd, lo, hi);
+        if constexpr (COUNT) ++tc->ray_nodes;
         if (!ray_box_ref(p, b.dir, lo, hi)) continue;
         const int4 meta = __ldg(reinterpret_cast<const int4*>(nd) + 3);
         if (meta.w > 0)
         {
+            if constexpr (COUNT) tc->ray_tris += meta.w;
             for (int s = meta.z; s < meta.z + meta.w; ++s)
                 hits += ray_hits(p, dir, tri_vertex(b, s, 0), tri_vertex(b, s, 1), tri_vertex(b, s, 2)) ? 1 : 0;
             continue;
@@ -675,17 +700,17 @@ struct SignedResult
 };
 
 // findSignedNearest (KdTree.h:143-165).
-template <class Tree>
-__device__ SignedResult signed_nearest(const Tree& b, const d3& p, int* status)
+template <class Tree, bool COUNT = false>
+__device__ SignedResult signed_nearest(const Tree& b, const d3& p, int* status, TravCount* tc = nullptr)
 {
-    const Nearest best = tree_nearest(b, p, status);
+    const Nearest best = tree_nearest<COUNT>(b, p, status, tc);
     SignedResult r;
     const double dist = sqrt(best.sq);
     r.cp = best.cp;
     r.fn = best.slot >= 0 ? face_normal(tri_vertex(b, best.slot, 0), tri_vertex(b, best.slot, 1),
                                         tri_vertex(b, best.slot, 2))
                           : mk(0.0, 0.0, 1.0);
-    const int hits = tree_ray_count(b, p, status);
+    const int hits = tree_ray_count<COUNT>(b, p, status, tc);
     if (hits > 0)
         r.sd = (hits % 2) == 1 ? -dist : dist;
     else
@@ -744,6 +769,28 @@ __global__ void __launch_bounds__(256) k_dense_fill(Tree b, SpecD s, double* __r
         w64[3 * idx + 2] = r.cp.z;
     }
     phin[idx] = make_float4((float)r.sd, (float)g.x, (float)g.y, (float)g.z);
+}
+
+// The dense fill's traversals over the same voxels and tiles, counted
+// (TravCount) and summed into out[4] instead of stored.
+template <class Tree>
+__global__ void __launch_bounds__(256) k_dense_count(Tree b, SpecD s, unsigned long long* out, int* status)
+{
+    const int tx = threadIdx.x;
+    const int i = blockIdx.x * 8 + (tx & 7);
+    const int j = blockIdx.y * 8 + ((tx >> 3) & 7);
+    const int k = blockIdx.z * 4 + (tx >> 6);
+    TravCount tc;
+    if (i < s.n[0] && j < s.n[1] && k < s.n[2])
+        (void)signed_nearest<Tree, true>(b, voxel_center(s, i, j, k), status, &tc);
+    unsigned long long v[4] = {(unsigned long long)tc.nearest_nodes, (unsigned long long)tc.nearest_tris,
+                               (unsigned long long)tc.ray_nodes, (unsigned long long)tc.ray_tris};
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+    {
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+        if ((tx & 31) == 0) atomicAdd(out + q, v[q]);
+    }
 }
 
 // Symmetrised central-difference Hessian of the normal field
@@ -994,11 +1041,28 @@ struct DeviceLbvh
 // numbered in creation (pre-)order.  Restated because tie resolution of the
 // nearest search (and with it the face-normal sign fallback) depends on this
 // exact tree.
+//
+// The reference partitions an index array whose comparator reads the
+// centroid arrays; here the partition runs over 32-byte records {centroid,
+// triangle id} kept contiguous, so every pass streams through memory instead
+// of gathering.  std::nth_element makes the same comparisons and the same
+// moves whatever the element type, so the permutation of triangle ids -- and
+// the tree -- is the same as with the index array.  Node boxes are
+// unions of the children's boxes, computed after the children: min and max
+// are exact, so they equal the reference's min / max over the node's
+// triangles.
 struct HostRefTree
 {
+    struct Rec
+    {
+        double c[3];
+        int32_t id;
+        int32_t pad;
+    };
     std::vector<RefNode> nodes;
-    std::vector<int32_t> order;
-    std::vector<double> lo, hi, cen;
+    std::vector<Rec> rec;
+    const double* verts = nullptr;
+    const int32_t* tris = nullptr;
     std::map<int64_t, int64_t> sizes; // subtree node counts, filled before build
 
     // Nodes of the subtree over n triangles (leaves of <= 8, median split);
@@ -1019,57 +1083,70 @@ struct HostRefTree
         return n <= 8 ? 1 : sizes.at(n);
     }
 
-    // Node `id` over order[lo_i, hi_i); children get the pre-order ids
-    // id + 1 and id + 1 + |left subtree|, so disjoint subtrees can be built
+    // Node `id` over rec[lo_i, hi_i); children get the pre-order ids id + 1
+    // and id + 1 + |left subtree|, so disjoint subtrees can be built
     // concurrently (`depth` levels spawn a thread for the left child).
     void build(int lo_i, int hi_i, int id, int depth)
     {
-        double bmin[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, bmax[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-        double cmin[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, cmax[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-        for (int i = lo_i; i < hi_i; ++i)
-        {
-            const int t = order[(size_t)i];
-            for (int a = 0; a < 3; ++a)
-            {
-                const double l = lo[3 * (size_t)t + a], h = hi[3 * (size_t)t + a],
-                             c = cen[3 * (size_t)t + a];
-                bmin[a] = l < bmin[a] ? l : bmin[a];
-                bmax[a] = bmax[a] < h ? h : bmax[a];
-                cmin[a] = c < cmin[a] ? c : cmin[a];
-                cmax[a] = cmax[a] < c ? c : cmax[a];
-            }
-        }
         RefNode n{};
-        for (int a = 0; a < 3; ++a)
-        {
-            n.lo[a] = bmin[a];
-            n.hi[a] = bmax[a];
-        }
         n.left = n.right = -1;
         n.start = -1;
         n.count = 0;
         const int count = hi_i - lo_i;
         if (count <= 8)
         {
+            // box over the triangles' own boxes (a.cwiseMin(b).cwiseMin(c),
+            // a.cwiseMax(b).cwiseMax(c))
+            for (int a = 0; a < 3; ++a)
+            {
+                n.lo[a] = DBL_MAX;
+                n.hi[a] = -DBL_MAX;
+            }
+            for (int i = lo_i; i < hi_i; ++i)
+            {
+                const int32_t* t = tris + 3 * (size_t)rec[(size_t)i].id;
+                const double* A = verts + 3 * (size_t)t[0];
+                const double* B = verts + 3 * (size_t)t[1];
+                const double* C = verts + 3 * (size_t)t[2];
+                for (int a = 0; a < 3; ++a)
+                {
+                    double mn = B[a] < A[a] ? B[a] : A[a];
+                    mn = C[a] < mn ? C[a] : mn;
+                    double mx = A[a] < B[a] ? B[a] : A[a];
+                    mx = mx < C[a] ? C[a] : mx;
+                    n.lo[a] = mn < n.lo[a] ? mn : n.lo[a];
+                    n.hi[a] = n.hi[a] < mx ? mx : n.hi[a];
+                }
+            }
             n.start = lo_i;
             n.count = count;
             nodes[(size_t)id] = n;
             return;
+        }
+        double cmin[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, cmax[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+        for (int i = lo_i; i < hi_i; ++i)
+        {
+            const Rec& r = rec[(size_t)i];
+            for (int a = 0; a < 3; ++a)
+            {
+                const double c = r.c[a];
+                cmin[a] = c < cmin[a] ? c : cmin[a];
+                cmax[a] = cmax[a] < c ? c : cmax[a];
+            }
         }
         const double ext[3] = {cmax[0] - cmin[0], cmax[1] - cmin[1], cmax[2] - cmin[2]};
         int axis = 0;
         if (ext[1] > ext[0]) axis = 1;
         if (ext[2] > ext[axis]) axis = 2;
         const int mid = lo_i + count / 2;
-        const double* c = cen.data();
-        std::nth_element(order.begin() + lo_i, order.begin() + mid, order.begin() + hi_i,
-                         [c, axis](int x, int y) { return c[3 * x + axis] < c[3 * y + axis]; });
+        std::nth_element(rec.begin() + lo_i, rec.begin() + mid, rec.begin() + hi_i,
+                         [axis](const Rec& x, const Rec& y) { return x.c[axis] < y.c[axis]; });
         n.left = id + 1;
         n.right = id + 1 + (int)node_count(mid - lo_i);
-        nodes[(size_t)id] = n;
         if (depth > 0 && count > 4096)
         {
-            std::thread t([this, lo_i, mid, &n, depth] { build(lo_i, mid, n.left, depth - 1); });
+            const int left = n.left;
+            std::thread t([this, lo_i, mid, left, depth] { build(lo_i, mid, left, depth - 1); });
             build(mid, hi_i, n.right, depth - 1);
             t.join();
         }
@@ -1078,8 +1155,38 @@ struct HostRefTree
             build(lo_i, mid, n.left, 0);
             build(mid, hi_i, n.right, 0);
         }
+        const RefNode& L = nodes[(size_t)n.left];
+        const RefNode& R = nodes[(size_t)n.right];
+        for (int a = 0; a < 3; ++a)
+        {
+            n.lo[a] = R.lo[a] < L.lo[a] ? R.lo[a] : L.lo[a];
+            n.hi[a] = L.hi[a] < R.hi[a] ? R.hi[a] : L.hi[a];
+        }
+        nodes[(size_t)id] = n;
     }
 };
+
+// Runs body(lo, hi) over [0, n) on up to `threads` host threads.
+template <class F>
+void host_parallel_for(size_t n, unsigned threads, F&& body)
+{
+    const size_t min_chunk = 65536;
+    threads = (unsigned)std::max<size_t>(1, std::min<size_t>(threads, (n + min_chunk - 1) / min_chunk));
+    if (threads <= 1)
+    {
+        body(size_t(0), n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t step = (n + threads - 1) / threads;
+    for (unsigned t = 1; t < threads; ++t)
+    {
+        const size_t lo = std::min(n, t * step), hi = std::min(n, lo + step);
+        pool.emplace_back([&body, lo, hi] { body(lo, hi); });
+    }
+    body(size_t(0), std::min(n, step));
+    for (auto& th : pool) th.join();
+}
 
 struct DeviceRefTree
 {
@@ -1110,48 +1217,52 @@ struct HostTreeData
     std::vector<int32_t> tri_id;
 };
 
-void host_ref_tree(HostTreeData& out, const double* verts, const int32_t* tris, int64_t nt)
+// `threads`: host threads the build may use (0: all of the machine's).
+void host_ref_tree(HostTreeData& out, const double* verts, const int32_t* tris, int64_t nt,
+                   unsigned threads = 0)
 {
+    if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
     HostRefTree h;
     const size_t n = (size_t)nt;
-    h.lo.resize(3 * n);
-    h.hi.resize(3 * n);
-    h.cen.resize(3 * n);
-    h.order.resize(n);
-    for (size_t i = 0; i < n; ++i)
-    {
-        const double* a = verts + 3 * (size_t)tris[3 * i];
-        const double* b = verts + 3 * (size_t)tris[3 * i + 1];
-        const double* c = verts + 3 * (size_t)tris[3 * i + 2];
-        for (int q = 0; q < 3; ++q)
+    h.verts = verts;
+    h.tris = tris;
+    h.rec.resize(n);
+    host_parallel_for(n, threads, [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i)
         {
-            // a.cwiseMin(b).cwiseMin(c), a.cwiseMax(b).cwiseMax(c), (a + b + c) / 3.0
-            double mn = b[q] < a[q] ? b[q] : a[q];
-            mn = c[q] < mn ? c[q] : mn;
-            double mx = a[q] < b[q] ? b[q] : a[q];
-            mx = mx < c[q] ? c[q] : mx;
-            h.lo[3 * i + q] = mn;
-            h.hi[3 * i + q] = mx;
-            volatile double sum = a[q] + b[q];
-            sum = sum + c[q];
-            h.cen[3 * i + q] = sum / 3.0;
-        }
-        h.order[i] = (int32_t)i;
-    }
-    h.nodes.resize((size_t)h.subtree_nodes((int64_t)nt));
-    // up to 2^4 subtrees built concurrently (disjoint ranges of `order`)
-    const unsigned hw = std::thread::hardware_concurrency();
-    h.build(0, (int)nt, 0, hw >= 16 ? 4 : hw >= 8 ? 3 : hw >= 4 ? 2 : hw >= 2 ? 1 : 0);
-    out.tri9.resize(9 * n);
-    for (size_t sl = 0; sl < n; ++sl)
-    {
-        const int32_t ti = h.order[sl];
-        for (int v = 0; v < 3; ++v)
+            const double* a = verts + 3 * (size_t)tris[3 * i];
+            const double* b = verts + 3 * (size_t)tris[3 * i + 1];
+            const double* c = verts + 3 * (size_t)tris[3 * i + 2];
+            HostRefTree::Rec& r = h.rec[i];
             for (int q = 0; q < 3; ++q)
-                out.tri9[9 * sl + 3 * v + q] = verts[3 * (size_t)tris[3 * (size_t)ti + v] + q];
-    }
+            {
+                // (a + b + c) / 3.0, summed left to right
+                volatile double sum = a[q] + b[q];
+                sum = sum + c[q];
+                r.c[q] = sum / 3.0;
+            }
+            r.id = (int32_t)i;
+            r.pad = 0;
+        }
+    });
+    h.nodes.resize((size_t)h.subtree_nodes((int64_t)nt));
+    // up to 2^depth subtrees built concurrently (disjoint ranges of `rec`)
+    int depth = 0;
+    while (depth < 4 && (2u << depth) <= threads) ++depth;
+    h.build(0, (int)nt, 0, depth);
+    out.tri9.resize(9 * n);
+    out.tri_id.resize(n);
+    host_parallel_for(n, threads, [&](size_t lo, size_t hi) {
+        for (size_t sl = lo; sl < hi; ++sl)
+        {
+            const int32_t ti = h.rec[sl].id;
+            out.tri_id[sl] = ti;
+            for (int v = 0; v < 3; ++v)
+                for (int q = 0; q < 3; ++q)
+                    out.tri9[9 * sl + 3 * v + q] = verts[3 * (size_t)tris[3 * (size_t)ti + v] + q];
+        }
+    });
     out.nodes = std::move(h.nodes);
-    out.tri_id = std::move(h.order);
 }
 
 void build_ref_tree(DeviceRefTree& t, const double* verts, int64_t nv, const int32_t* tris, int64_t nt,

@@ -125,6 +125,18 @@ int sdfo_grid_build_dense(const double* h_verts, int64_t nv, const int32_t* h_tr
     });
 }
 
+int sdfo_build_traversal_stats(const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
+                               const sdfo_build_params* p, void* stream, sdfo_traversal_stats* out)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(out != nullptr, SDFO_ERR_INVALID_ARGUMENT, "out is NULL");
+        std::memset(out, 0, sizeof(*out));
+        check_mesh(h_verts, nv, h_tris, nt);
+        check_build_params(p);
+        count_dense_traversal(h_verts, nv, h_tris, nt, *p, as_stream(stream), out);
+    });
+}
+
 int sdfo_grid_build_sparse(const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
                            const sdfo_sparse_build_params* p, void* stream, sdfo_grid** out)
 {

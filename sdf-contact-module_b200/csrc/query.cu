@@ -596,27 +596,11 @@ void launch_saved3(const GridView& v, const SavedBackward& b, cudaStream_t s)
 }
 
 template <int MODE, bool SPARSE, int BD>
-void launch_saved2(const GridView& v, const SavedBackward& b_in, cudaStream_t s)
+void launch_saved2(const GridView& v, const SavedBackward& b, cudaStream_t s)
 {
-    SavedBackward b = b_in;
-    if (b.dpts && !b.dgrid)
-    {
-        // dL/dp alone: the bulk-copy pipeline for whole tiles, the staged
-        // kernel for the tail
-        int64_t done = 0;
-        if (launch_backward_saved_bulk(b.n, b.grad, b.hess6, b.dgap, b.dgrad, b.dpts, s, &done) && done > 0)
-        {
-            if (done == b.n) return;
-            b.pts = b.pts ? b.pts + 3 * done : nullptr;
-            b.grad += 3 * done;
-            b.hess6 += 6 * done;
-            b.valid = b.valid ? b.valid + done : nullptr;
-            b.dgap = b.dgap ? b.dgap + done : nullptr;
-            b.dgrad = b.dgrad ? b.dgrad + 3 * done : nullptr;
-            b.dpts += 3 * done;
-            b.n -= done;
-        }
-    }
+    // dL/dp alone: the bulk-copy pipeline when there is a whole tile
+    if (b.dpts && !b.dgrid && launch_backward_saved_bulk(b.n, b.grad, b.hess6, b.dgap, b.dgrad, b.dpts, s))
+        return;
     const bool staged = aligned16(b.pts) && aligned16(b.grad) && aligned16(b.hess6) &&
                         aligned16(b.dgrad) && aligned16(b.dpts);
     if (staged)

@@ -267,11 +267,11 @@ struct CandidateOutputs
 // Status bits of the pipelined query kernel (query.cu), read and optionally
 // cleared by sdfo_device_status.
 unsigned query_pipe_status(bool clear);
-// dL/dp of the saved backward for the first n / 256 * 256 queries as a
-// bulk-copy pipeline (stream_bwd.cu); false when the pointers do not allow
-// it.  *done = the queries written.
+// dL/dp of the saved backward for all n queries as a bulk-copy pipeline
+// (stream_bwd.cu); false (nothing launched) when n < 256 or the pointers are
+// not 16-byte aligned.
 bool launch_backward_saved_bulk(int64_t n, const float* grad, const float* hess6, const float* dgap,
-                                const float* dgrad, float* dpts, cudaStream_t s, int64_t* done);
+                                const float* dgrad, float* dpts, cudaStream_t s);
 // ContactAware on a grid with candidates (ca_query.cu).
 void launch_query_ca(const GridView& v, const void* pts, bool f64, int64_t n, const QueryOutputs& o,
                      const CandidateOutputs& co, cudaStream_t s);
@@ -302,6 +302,9 @@ sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int
 sdfo_grid* build_sparse(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
                         const sdfo_sparse_build_params& p, cudaStream_t s);
 sdfo_grid_info setup_grid(const double* verts, int64_t nv, const sdfo_build_params& p);
+// The dense fill's traversals counted over the grid of p (build.cu).
+void count_dense_traversal(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
+                           const sdfo_build_params& p, cudaStream_t s, sdfo_traversal_stats* out);
 // Batched sparse build (batch.cu): one grid per mesh, storage in one arena.
 std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n, cudaStream_t s);
 void set_fill_ctas_per_sm(int k);

@@ -4,7 +4,8 @@
 // tensor map, no multicast) completing on mbarriers, three tiles in flight per
 // CTA, and write the results back with bulk stores.  The per-query work is
 // 15 FMAs against 64 bytes of traffic, so the kernel's only job is to keep
-// enough bytes in flight to run at copy bandwidth.
+// enough bytes in flight to run at copy bandwidth.  The last n mod 256
+// queries take plain loads and stores in one extra CTA of the same launch.
 //
 // Every wait on an mbarrier is bounded: a wait that runs out sets bit 0 of
 // the device status word (sdfo_device_status), waits (bounded) for the CTA's
@@ -44,7 +45,7 @@ __device__ __forceinline__ void issue_tile(unsigned char* stage, uint64_t* bar, 
     bulk_load(stage + kOffHess, hess6 + 6 * q0, 24 * kTile, bar);
 }
 
-__global__ void __launch_bounds__(kTile) k_backward_saved_bulk(int64_t tiles, const float* __restrict__ grad,
+__global__ void __launch_bounds__(kTile) k_backward_saved_bulk(int64_t n, const float* __restrict__ grad,
                                                                const float* __restrict__ hess6,
                                                                const float* __restrict__ dgap,
                                                                const float* __restrict__ dgrad,
@@ -56,7 +57,25 @@ __global__ void __launch_bounds__(kTile) k_backward_saved_bulk(int64_t tiles, co
     __shared__ long long s_kabort; // the tile whose wait ran out
     unsigned char* stages = smem;
     unsigned char* outs = smem + kStages * kStageBytes;
-    const int64_t first = blockIdx.x, step = gridDim.x;
+    const int64_t tiles = n / kTile;
+    const bool rem = (n % kTile) != 0;
+    if (rem && blockIdx.x == gridDim.x - 1)
+    {
+        // the remainder, one query per thread
+        const int64_t q = tiles * kTile + threadIdx.x;
+        if (q >= n) return;
+        const float dG = dgap ? dgap[q] : 0.f;
+        float dg[3] = {0.f, 0.f, 0.f};
+        if (dgrad)
+            for (int a = 0; a < 3; ++a) dg[a] = dgrad[3 * q + a];
+        const float* gr = grad + 3 * q;
+        const float* H = hess6 + 6 * q;
+        dpts[3 * q] = dG * gr[0] + H[0] * dg[0] + H[1] * dg[1] + H[2] * dg[2];
+        dpts[3 * q + 1] = dG * gr[1] + H[1] * dg[0] + H[3] * dg[1] + H[4] * dg[2];
+        dpts[3 * q + 2] = dG * gr[2] + H[2] * dg[0] + H[4] * dg[1] + H[5] * dg[2];
+        return;
+    }
+    const int64_t first = blockIdx.x, step = gridDim.x - (rem ? 1 : 0);
     const int64_t mine = first < tiles ? (tiles - first + step - 1) / step : 0;
     if (threadIdx.x == 0)
     {
@@ -136,9 +155,8 @@ __global__ void __launch_bounds__(kTile) k_backward_saved_bulk(int64_t tiles, co
 } // namespace
 
 bool launch_backward_saved_bulk(int64_t n, const float* grad, const float* hess6, const float* dgap,
-                                const float* dgrad, float* dpts, cudaStream_t s, int64_t* done)
+                                const float* dgrad, float* dpts, cudaStream_t s)
 {
-    *done = 0;
     auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
     if (n < kTile || !grad || !hess6 || !dpts || !a16(grad) || !a16(hess6) || !a16(dpts) ||
         (dgap && !a16(dgap)) || (dgrad && !a16(dgrad)))
@@ -152,10 +170,10 @@ bool launch_backward_saved_bulk(int64_t n, const float* grad, const float* hess6
         SDFO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     }
     const int smem = kStages * kStageBytes + 2 * kOutBytes; // 45 KB
-    const int64_t ctas = std::min<int64_t>(tiles, (int64_t)sms * 4);
-    k_backward_saved_bulk<<<(unsigned)ctas, kTile, smem, s>>>(tiles, grad, hess6, dgap, dgrad, dpts);
+    const int64_t rem = n % kTile ? 1 : 0; // one more CTA, for the remainder
+    const int64_t ctas = std::min<int64_t>(tiles, (int64_t)sms * 4 - rem) + rem;
+    k_backward_saved_bulk<<<(unsigned)ctas, kTile, smem, s>>>(n, grad, hess6, dgap, dgrad, dpts);
     SDFO_CHECK_LAUNCH();
-    *done = tiles * kTile;
     return true;
 }
 

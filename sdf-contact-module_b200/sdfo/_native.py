@@ -96,6 +96,11 @@ class BuildStats(ctypes.Structure):
                 ("triangles", _I32), ("bvh_nodes", _I32)]
 
 
+class TraversalStats(ctypes.Structure):
+    _fields_ = [("voxels", _I64), ("nearest_nodes", _I64), ("nearest_triangles", _I64),
+                ("ray_nodes", _I64), ("ray_triangles", _I64)]
+
+
 class DeviceViews(ctypes.Structure):
     _fields_ = [("phin", _P), ("hessian6", _P), ("table", _P), ("block_ijk", _P),
                 ("stored_voxels", _I64), ("table_dims", _I32 * 3), ("reserved0", _I32)]
@@ -121,6 +126,8 @@ SIGNATURES = [
      [ctypes.POINTER(MeshDesc), _I32, _P, ctypes.POINTER(_P)]),
     ("sdfo_set_fill_ctas_per_sm", ctypes.c_int, [_I32]),
     ("sdfo_grid_build_stats", ctypes.c_int, [_P, ctypes.POINTER(BuildStats)]),
+    ("sdfo_build_traversal_stats", ctypes.c_int,
+     [_P, _I64, _P, _I64, _P, _P, ctypes.POINTER(TraversalStats)]),
     ("sdfo_set_bvh_mode", ctypes.c_int, [_I32]),
     ("sdfo_get_bvh_mode", ctypes.c_int, []),
     ("sdfo_grid_create_dense", ctypes.c_int,

@@ -118,6 +118,26 @@ class SdfGrid:
         return cls(out.value, mode)
 
     @classmethod
+    def traversal_stats(cls, verts, tris, padding=0.1, voxel_size=0.0, target_resolution=128,
+                        max_resolution=512, stream=None) -> dict:
+        """Per-voxel traversal work of build_dense's fill on the same grid
+        (nearest search: nodes examined, closest-point tests; parity ray:
+        box tests, triangle tests), counted on the device."""
+        v, t = cls._mesh(verts, tris)
+        p = N.BuildParams(padding, voxel_size, target_resolution, max_resolution)
+        st = N.TraversalStats()
+        N.check(N.load().sdfo_build_traversal_stats(_np_ptr(v), len(v), _np_ptr(t), len(t),
+                                                    ctypes.byref(p), _stream_ptr(stream),
+                                                    ctypes.byref(st)))
+        n = max(st.voxels, 1)
+        return {"voxels": st.voxels,
+                "totals": [st.nearest_nodes, st.nearest_triangles, st.ray_nodes, st.ray_triangles],
+                "nearest_nodes_per_voxel": st.nearest_nodes / n,
+                "nearest_triangle_tests_per_voxel": st.nearest_triangles / n,
+                "ray_box_tests_per_voxel": st.ray_nodes / n,
+                "ray_triangle_tests_per_voxel": st.ray_triangles / n}
+
+    @classmethod
     def build_sparse(cls, verts, tris, padding=0.1, voxel_size=0.0, target_resolution=128,
                      max_resolution=512, block_dim=8, halo_voxels=2, band_voxels=8,
                      band_distance=0.0, store_hessian=True, mode=N.TRILINEAR,

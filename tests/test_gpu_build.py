@@ -169,6 +169,29 @@ def test_lbvh_mode_distances(cuda, port, name):
     assert np.array_equal(np.signbit(d["phi"][decided]), np.signbit(P["phi"][decided]))
 
 
+@pytest.mark.parametrize("name,res", [("cube", 32), ("cyl", 48), ("torus", 40), ("gear", 64)])
+def test_traversal_counts_match_reference_order(cuda, port, name, res):
+    """The dense fill's traversal work counted on the device
+    (sdfo_build_traversal_stats) equals the oracle's recursive KdTree
+    traversal count for count: nodes entered past the nearest search's cut,
+    closest-point tests, ray-box tests and ray-triangle tests.  Equal totals
+    over every voxel follow from the same visit order and the same cuts."""
+    from sdfo import SdfGrid
+
+    _set_mode(0)
+    v, t = _meshes()[name]
+    st = SdfGrid.traversal_stats(v, t, padding=0.1, target_resolution=res, max_resolution=res)
+    spec = port.setup_grid(v, padding=0.1, target_resolution=res, max_resolution=res)
+    nx, ny, nz = spec["shape"]
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    idx = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1).astype(np.float64)
+    centres = spec["bmin"][None, :] + spec["voxel"][None, :] * (idx + 0.5)
+    ref = port.Bvh(v, t).traversal_counts(centres)
+    n = nx * ny * nz
+    assert st["voxels"] == n
+    assert np.array_equal(np.array(st["totals"], np.int64), ref), (st["totals"], ref)
+
+
 def test_empty_mesh_raises(cuda):
     from sdfo import SdfGrid, SdfoError
 
