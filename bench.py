@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--kernels-once", choices=["c2", "c5", "ca", "be"], default=None,
+    ap.add_argument("--kernels-once", choices=["c2", "c5", "ca", "be", "build"], default=None,
                     help="one launch of each query kernel on the workload (for ncu), then exit")
     ap.add_argument("--skip-ca", action="store_true",
                     help="leave out the contact-aware build / query section")
@@ -249,8 +249,9 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def timed(torch, fn, steps, warmup, flush, stream):
-    """Sum of per-step CUDA-event durations, L2 flushed before each step."""
+def timed(torch, fn, steps, warmup, flush, stream, per_step=None):
+    """Sum of per-step CUDA-event durations, L2 flushed before each step
+    (the durations are appended to per_step when it is a list)."""
     for _ in range(warmup):
         flush()
         fn()
@@ -263,7 +264,10 @@ def timed(torch, fn, steps, warmup, flush, stream):
         fn()
         e.record(stream)
     torch.cuda.synchronize()
-    return sum(s.elapsed_time(e) for s, e in evs)
+    ms = [s.elapsed_time(e) for s, e in evs]
+    if per_step is not None:
+        per_step.extend(ms)
+    return sum(ms)
 
 
 # algorithmic bytes per C5 query (sparse, 8^3 bricks): forward = point 12 +
@@ -789,7 +793,8 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    total_ms = timed(torch, lambda: query(dense), args.steps, args.warmup, flush, stream)
+    head_steps = []
+    total_ms = timed(torch, lambda: query(dense), args.steps, args.warmup, flush, stream, head_steps)
     t_local = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if world > 1:
         torch.distributed.barrier()
@@ -941,6 +946,8 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": 17 * n,
                 "path": "sdfo_query_host, pinned host buffers, synchronous"},
         "gpu_launches": args.steps,
+        "step_us": {"min": 1e3 * min(head_steps), "median": 1e3 * float(np.median(head_steps)),
+                    "max": 1e3 * max(head_steps)},
         "clocks": clk,
         "build": {
             "dense_voxels_per_s": n_vox / t_dense,
@@ -992,7 +999,9 @@ def kernels_once(which):
     program an ncu capture (-k regex:"k_query|k_backward") runs.  "ca": one
     contact-aware build of the cylinder (its fill kernels) and one
     ContactAware query launch.  "be": 296 ring drops (two per SM), eight
-    BE step launches (the last ones in contact)."""
+    BE step launches (the last ones in contact).  "build": one dense and one
+    sparse (band 3) reference-order build of the hollow cylinder
+    (k_dense_fill, k_dense_hessian, k_sparse_activate, k_sparse_fill)."""
     import ctypes
 
     import torch
@@ -1002,6 +1011,15 @@ def kernels_once(which):
     from sdfo import workloads as W
 
     lib = N.load()
+    if which == "build":
+        c = W.c2_cylinder()
+        N.check(lib.sdfo_set_bvh_mode(N.BVH_REFERENCE))
+        d = SdfGrid.build_dense(c["verts"], c["tris"], **c["dense"])
+        s = SdfGrid.build_sparse(c["verts"], c["tris"], **c["sparse"])
+        torch.cuda.synchronize()
+        print(json.dumps({"kernels_once": which, "dense_voxels": int(np.prod(d.shape)),
+                          "sparse_blocks": s.block_count}))
+        return
     if which == "be":
         from sdfo.be import BEStepper
 

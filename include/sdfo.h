@@ -206,6 +206,14 @@ int sdfo_last_error(char* buf, size_t len);
 /* Checks that device `device` is usable (compute capability 10.x). */
 int sdfo_device_check(int device);
 
+/* Device memory the library frees (grids, build temporaries) is kept for
+ * reuse by later requests of the same size class, up to `limit` bytes per
+ * device (default 1 GiB).  A free still synchronises the device first, as
+ * cudaFree does.  limit < 0 leaves the limit as it is; 0 releases every
+ * cached block of the current device and turns the cache off.  *held (may
+ * be NULL) receives the bytes now cached on the current device. */
+int sdfo_device_cache(int64_t limit, int64_t* held);
+
 /* Status word the kernels with bounded waits set instead of hanging (bit 0:
  * a bulk-copy wait of the backward pipeline ran out; bit 1: one of the
  * pipelined query kernel); synchronous read,

@@ -743,9 +743,14 @@ __device__ __forceinline__ d3 voxel_center(const SpecD& s, int i, int j, int k)
               s.bmin[2] + s.voxel[2] * (k + 0.5));
 }
 
+// Resident CTAs per SM the fill kernels ask the register allocator for.
+#ifndef SDFO_FILL_MIN_BLOCKS
+#define SDFO_FILL_MIN_BLOCKS 1
+#endif
+
 // Dense fill: CTA = 8x8x4 voxel tile (coherent traversals), thread = voxel.
 template <class Tree>
-__global__ void __launch_bounds__(256) k_dense_fill(Tree b, SpecD s, double* __restrict__ phi64,
+__global__ void __launch_bounds__(256, SDFO_FILL_MIN_BLOCKS) k_dense_fill(Tree b, SpecD s, double* __restrict__ phi64,
                                                     double* __restrict__ n64, double* __restrict__ w64,
                                                     float4* __restrict__ phin, int* status)
 {
@@ -897,7 +902,7 @@ __device__ __forceinline__ float4 brick_voxel(const Tree& b, const SpecD& s, int
 
 // Brick fill: one CTA per stored block.
 template <class Tree>
-__global__ void __launch_bounds__(256) k_sparse_fill(Tree b, SpecD s, int bd,
+__global__ void __launch_bounds__(256, SDFO_FILL_MIN_BLOCKS) k_sparse_fill(Tree b, SpecD s, int bd,
                                                      const int32_t* __restrict__ ijk,
                                                      float4* __restrict__ phin, int* status)
 {

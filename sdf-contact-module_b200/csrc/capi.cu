@@ -125,6 +125,11 @@ int sdfo_grid_build_dense(const double* h_verts, int64_t nv, const int32_t* h_tr
     });
 }
 
+int sdfo_device_cache(int64_t limit, int64_t* held)
+{
+    return guarded([&] { device_cache_control(limit, held); });
+}
+
 int sdfo_build_traversal_stats(const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
                                const sdfo_build_params* p, void* stream, sdfo_traversal_stats* out)
 {

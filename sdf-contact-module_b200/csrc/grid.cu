@@ -4,6 +4,9 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
 
 #include "sdfo_internal.cuh"
 
@@ -25,11 +28,100 @@ void throw_cuda(cudaError_t e, const char* what, const char* file, int line)
     throw Error(SDFO_ERR_CUDA, buf);
 }
 
+// ---------------------------------------------------------------------------
+// Device memory: cudaMalloc and cudaFree each cost about 0.3 ms whatever the
+// size, and a build makes a dozen of them.  Freed blocks are therefore kept
+// per device, by size class, and handed out again for a request of the same
+// class.  A free first synchronises the device, as cudaFree does, so no block
+// is handed out while work queued before its free can still touch it.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Live
+{
+    size_t bytes;
+    int device;
+};
+
+struct Cache
+{
+    std::mutex mu;
+    std::unordered_map<void*, Live> live;              // handed out
+    std::vector<std::vector<std::pair<void*, size_t>>> free_blocks; // per device, oldest first
+    std::vector<size_t> held;                           // per device
+    int64_t limit = int64_t(1) << 30;                   // per device
+};
+
+Cache& cache()
+{
+    static Cache* c = new Cache(); // never destroyed: frees may run during exit
+    return *c;
+}
+
+// Size class: powers of two up to 2 MiB, then multiples of 2 MiB.
+size_t size_class(size_t b)
+{
+    const size_t mb2 = size_t(2) << 20;
+    if (b >= mb2) return (b + mb2 - 1) / mb2 * mb2;
+    size_t c = 512;
+    while (c < b) c <<= 1;
+    return c;
+}
+
+void ensure_device(Cache& c, int dev)
+{
+    if ((int)c.free_blocks.size() <= dev)
+    {
+        c.free_blocks.resize((size_t)dev + 1);
+        c.held.resize((size_t)dev + 1, 0);
+    }
+}
+
+// cudaFree of every cached block of `dev` (the current device) above `keep`
+// bytes, oldest first; the caller holds the lock.
+void trim_locked(Cache& c, int dev, size_t keep)
+{
+    auto& fl = c.free_blocks[(size_t)dev];
+    size_t i = 0;
+    while (c.held[(size_t)dev] > keep && i < fl.size())
+    {
+        cudaFree(fl[i].first);
+        c.held[(size_t)dev] -= fl[i].second;
+        ++i;
+    }
+    fl.erase(fl.begin(), fl.begin() + (std::ptrdiff_t)i);
+}
+
+} // namespace
+
 void* device_alloc(size_t bytes)
 {
     if (bytes == 0) return nullptr;
+    const size_t cls = size_class(bytes);
+    int dev = 0;
+    SDFO_CUDA(cudaGetDevice(&dev));
+    Cache& c = cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    ensure_device(c, dev);
+    auto& fl = c.free_blocks[(size_t)dev];
+    for (size_t i = fl.size(); i-- > 0;)
+        if (fl[i].second == cls)
+        {
+            void* p = fl[i].first;
+            fl.erase(fl.begin() + (std::ptrdiff_t)i);
+            c.held[(size_t)dev] -= cls;
+            c.live[p] = Live{cls, dev};
+            return p;
+        }
     void* p = nullptr;
-    const cudaError_t e = cudaMalloc(&p, bytes);
+    cudaError_t e = cudaMalloc(&p, cls);
+    if (e == cudaErrorMemoryAllocation && c.held[(size_t)dev] > 0)
+    {
+        // give the cached blocks back and try once more
+        (void)cudaGetLastError();
+        trim_locked(c, dev, 0);
+        e = cudaMalloc(&p, cls);
+    }
     if (e != cudaSuccess)
     {
         (void)cudaGetLastError();
@@ -38,12 +130,53 @@ void* device_alloc(size_t bytes)
                       cudaGetErrorString(e));
         throw Error(e == cudaErrorMemoryAllocation ? SDFO_ERR_OUT_OF_MEMORY : SDFO_ERR_CUDA, buf);
     }
+    c.live[p] = Live{cls, dev};
     return p;
 }
 
 void device_free(void* p)
 {
-    if (p) cudaFree(p);
+    if (!p) return;
+    Cache& c = cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    auto it = c.live.find(p);
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = -1;
+    if (it == c.live.end() || it->second.device != dev || c.limit <= 0 ||
+        (int64_t)it->second.bytes > c.limit)
+    {
+        if (it != c.live.end()) c.live.erase(it);
+        cudaFree(p);
+        return;
+    }
+    const size_t bytes = it->second.bytes;
+    c.live.erase(it);
+    // the synchronisation cudaFree would make
+    if (cudaDeviceSynchronize() != cudaSuccess)
+    {
+        (void)cudaGetLastError();
+        cudaFree(p);
+        return;
+    }
+    ensure_device(c, dev);
+    c.free_blocks[(size_t)dev].emplace_back(p, bytes);
+    c.held[(size_t)dev] += bytes;
+    trim_locked(c, dev, (size_t)c.limit);
+}
+
+void device_cache_control(int64_t limit, int64_t* held)
+{
+    int dev = 0;
+    SDFO_CUDA(cudaGetDevice(&dev));
+    Cache& c = cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    ensure_device(c, dev);
+    if (limit >= 0)
+    {
+        c.limit = limit;
+        trim_locked(c, dev, (size_t)limit);
+    }
+    if (held) *held = (int64_t)c.held[(size_t)dev];
 }
 
 GridView make_view(const sdfo_grid* g)

@@ -73,6 +73,10 @@ int guarded(F&& f)
 void* device_alloc(size_t bytes);
 void device_free(void* p);
 
+// Limit (bytes per device; < 0 leaves it, 0 releases all and disables) and
+// current size of the cache of freed device blocks (grid.cu).
+void device_cache_control(int64_t limit, int64_t* held);
+
 template <class T>
 T* dalloc(size_t count)
 {

@@ -126,6 +126,7 @@ SIGNATURES = [
      [ctypes.POINTER(MeshDesc), _I32, _P, ctypes.POINTER(_P)]),
     ("sdfo_set_fill_ctas_per_sm", ctypes.c_int, [_I32]),
     ("sdfo_grid_build_stats", ctypes.c_int, [_P, ctypes.POINTER(BuildStats)]),
+    ("sdfo_device_cache", ctypes.c_int, [_I64, _P]),
     ("sdfo_build_traversal_stats", ctypes.c_int,
      [_P, _I64, _P, _I64, _P, _P, ctypes.POINTER(TraversalStats)]),
     ("sdfo_set_bvh_mode", ctypes.c_int, [_I32]),

@@ -192,6 +192,36 @@ def test_traversal_counts_match_reference_order(cuda, port, name, res):
     assert np.array_equal(np.array(st["totals"], np.int64), ref), (st["totals"], ref)
 
 
+def test_device_cache_reuse(cuda):
+    """Freed grid storage is cached and reused: a second identical build
+    gives identical data, the cache holds the freed blocks, and a zero limit
+    releases them."""
+    import ctypes
+
+    from sdfo import SdfGrid
+    from sdfo import _native as N
+
+    lib = N.load()
+    held = ctypes.c_int64(-1)
+    try:
+        N.check(lib.sdfo_device_cache(1 << 30, ctypes.byref(held)))
+        v, t = _meshes()["torus"]
+        a = SdfGrid.build_dense(v, t, target_resolution=40, max_resolution=40)
+        ea = a.export_dense()
+        a.close()
+        N.check(lib.sdfo_device_cache(-1, ctypes.byref(held)))
+        assert held.value > 0
+        b = SdfGrid.build_dense(v, t, target_resolution=40, max_resolution=40)
+        eb = b.export_dense()
+        for k in ("phi", "normal", "witness", "hessian"):
+            assert np.array_equal(ea[k], eb[k]), k
+        b.close()
+        N.check(lib.sdfo_device_cache(0, ctypes.byref(held)))
+        assert held.value == 0
+    finally:
+        N.check(lib.sdfo_device_cache(1 << 30, None))
+
+
 def test_empty_mesh_raises(cuda):
     from sdfo import SdfGrid, SdfoError
 
