@@ -57,7 +57,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--kernels-once", choices=["c2", "c5", "ca", "be", "build"], default=None,
+    ap.add_argument("--kernels-once", choices=["c2", "c5", "ca", "be", "build", "build5"], default=None,
                     help="one launch of each query kernel on the workload (for ncu), then exit")
     ap.add_argument("--skip-ca", action="store_true",
                     help="leave out the contact-aware build / query section")
@@ -1001,7 +1001,8 @@ def kernels_once(which):
     ContactAware query launch.  "be": 296 ring drops (two per SM), eight
     BE step launches (the last ones in contact).  "build": one dense and one
     sparse (band 3) reference-order build of the hollow cylinder
-    (k_dense_fill, k_dense_hessian, k_sparse_activate, k_sparse_fill)."""
+    (k_dense_fill, k_dense_hessian, k_sparse_activate, k_sparse_fill);
+    "build5": the same sparse build of the 1.31M-triangle icosphere at 512³."""
     import ctypes
 
     import torch
@@ -1011,6 +1012,14 @@ def kernels_once(which):
     from sdfo import workloads as W
 
     lib = N.load()
+    if which == "build5":
+        c = W.c5_icosphere()
+        N.check(lib.sdfo_set_bvh_mode(N.BVH_REFERENCE))
+        s = SdfGrid.build_sparse(c["verts"], c["tris"], **c["sparse"])
+        torch.cuda.synchronize()
+        print(json.dumps({"kernels_once": which, "sparse_blocks": s.block_count,
+                          "stats": s.build_stats()}))
+        return
     if which == "build":
         c = W.c2_cylinder()
         N.check(lib.sdfo_set_bvh_mode(N.BVH_REFERENCE))

@@ -1064,8 +1064,8 @@ struct HostRefTree
         int32_t id;
         int32_t pad;
     };
-    std::vector<RefNode> nodes;
-    std::vector<Rec> rec;
+    RefNode* nodes = nullptr; // subtree_nodes(n) nodes, caller-provided storage
+    Rec* rec = nullptr;       // n records, caller-provided storage
     const double* verts = nullptr;
     const int32_t* tris = nullptr;
     std::map<int64_t, int64_t> sizes; // subtree node counts, filled before build
@@ -1144,7 +1144,7 @@ struct HostRefTree
         if (ext[1] > ext[0]) axis = 1;
         if (ext[2] > ext[axis]) axis = 2;
         const int mid = lo_i + count / 2;
-        std::nth_element(rec.begin() + lo_i, rec.begin() + mid, rec.begin() + hi_i,
+        std::nth_element(rec + lo_i, rec + mid, rec + hi_i,
                          [axis](const Rec& x, const Rec& y) { return x.c[axis] < y.c[axis]; });
         n.left = id + 1;
         n.right = id + 1 + (int)node_count(mid - lo_i);
@@ -1222,16 +1222,17 @@ struct HostTreeData
     std::vector<int32_t> tri_id;
 };
 
+// The records of every triangle (centroid (a + b + c) / 3, summed left to
+// right as the reference's Eigen expression does; the host code is compiled
+// without contraction or reassociation) and the tree over them, into the
+// storage h.rec (nt records) and h.nodes (h.subtree_nodes(nt) nodes).
 // `threads`: host threads the build may use (0: all of the machine's).
-void host_ref_tree(HostTreeData& out, const double* verts, const int32_t* tris, int64_t nt,
-                   unsigned threads = 0)
+void host_tree_core(HostRefTree& h, const double* verts, const int32_t* tris, int64_t nt, unsigned threads)
 {
     if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
-    HostRefTree h;
     const size_t n = (size_t)nt;
     h.verts = verts;
     h.tris = tris;
-    h.rec.resize(n);
     host_parallel_for(n, threads, [&](size_t lo, size_t hi) {
         for (size_t i = lo; i < hi; ++i)
         {
@@ -1239,54 +1240,119 @@ void host_ref_tree(HostTreeData& out, const double* verts, const int32_t* tris, 
             const double* b = verts + 3 * (size_t)tris[3 * i + 1];
             const double* c = verts + 3 * (size_t)tris[3 * i + 2];
             HostRefTree::Rec& r = h.rec[i];
-            for (int q = 0; q < 3; ++q)
-            {
-                // (a + b + c) / 3.0, summed left to right
-                volatile double sum = a[q] + b[q];
-                sum = sum + c[q];
-                r.c[q] = sum / 3.0;
-            }
+            for (int q = 0; q < 3; ++q) r.c[q] = (a[q] + b[q] + c[q]) / 3.0;
             r.id = (int32_t)i;
             r.pad = 0;
         }
     });
-    h.nodes.resize((size_t)h.subtree_nodes((int64_t)nt));
     // up to 2^depth subtrees built concurrently (disjoint ranges of `rec`)
     int depth = 0;
     while (depth < 4 && (2u << depth) <= threads) ++depth;
     h.build(0, (int)nt, 0, depth);
+}
+
+// The reference tree of one mesh on the host, with the triangles in slot
+// order (for the batched build, which concatenates many meshes).
+void host_ref_tree(HostTreeData& out, const double* verts, const int32_t* tris, int64_t nt,
+                   unsigned threads = 0)
+{
+    if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
+    const size_t n = (size_t)nt;
+    HostRefTree h;
+    std::vector<HostRefTree::Rec> rec(n);
+    out.nodes.resize((size_t)h.subtree_nodes(nt));
+    h.rec = rec.data();
+    h.nodes = out.nodes.data();
+    host_tree_core(h, verts, tris, nt, threads);
     out.tri9.resize(9 * n);
     out.tri_id.resize(n);
     host_parallel_for(n, threads, [&](size_t lo, size_t hi) {
         for (size_t sl = lo; sl < hi; ++sl)
         {
-            const int32_t ti = h.rec[sl].id;
+            const int32_t ti = rec[sl].id;
             out.tri_id[sl] = ti;
             for (int v = 0; v < 3; ++v)
                 for (int q = 0; q < 3; ++q)
                     out.tri9[9 * sl + 3 * v + q] = verts[3 * (size_t)tris[3 * (size_t)ti + v] + q];
         }
     });
-    out.nodes = std::move(h.nodes);
+}
+
+// Host memory reused by single-mesh tree builds: the records, and a pinned
+// block holding the nodes and the slot order so that they upload at copy
+// bandwidth and fresh pages are not faulted in on every build.  Builds that
+// run at the same time take turns on it.
+struct TreeStaging
+{
+    std::mutex mu;
+    std::vector<HostRefTree::Rec> rec;
+    unsigned char* pinned = nullptr;
+    size_t pinned_bytes = 0;
+};
+
+TreeStaging& tree_staging()
+{
+    static TreeStaging* st = new TreeStaging(); // never destroyed: kept for the process
+    return *st;
+}
+
+__global__ void k_gather_tri9(const double* __restrict__ verts, const int32_t* __restrict__ tris,
+                              const int32_t* __restrict__ ids, int n, double* __restrict__ tri9)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int t = ids[s];
+    for (int v = 0; v < 3; ++v)
+    {
+        const int vi = tris[3 * (int64_t)t + v];
+        for (int a = 0; a < 3; ++a) tri9[9 * (int64_t)s + 3 * v + a] = verts[3 * (int64_t)vi + a];
+    }
 }
 
 void build_ref_tree(DeviceRefTree& t, const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
                     cudaStream_t s)
 {
-    (void)nv;
-    HostTreeData h;
-    host_ref_tree(h, verts, tris, nt);
     const size_t n = (size_t)nt;
+    HostRefTree h;
+    const size_t nnodes = (size_t)h.subtree_nodes(nt);
+    const size_t node_bytes = sizeof(RefNode) * nnodes;
+    const size_t need = node_bytes + sizeof(int32_t) * n;
+    TreeStaging& st = tree_staging();
+    std::lock_guard<std::mutex> lock(st.mu);
+    if (st.pinned_bytes < need)
+    {
+        if (st.pinned) cudaFreeHost(st.pinned);
+        st.pinned = nullptr;
+        st.pinned_bytes = 0;
+        const size_t want = need + need / 4;
+        SDFO_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&st.pinned), want, cudaHostAllocDefault));
+        st.pinned_bytes = want;
+    }
+    if (st.rec.size() < n) st.rec.resize(n);
+    h.rec = st.rec.data();
+    h.nodes = reinterpret_cast<RefNode*>(st.pinned);
+    const unsigned threads = std::max(1u, std::thread::hardware_concurrency());
+    host_tree_core(h, verts, tris, nt, threads);
+    int32_t* ids = reinterpret_cast<int32_t*>(st.pinned + node_bytes);
+    host_parallel_for(n, threads, [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) ids[i] = st.rec[i].id;
+    });
     t.n = (int)nt;
-    t.nnodes = (int)h.nodes.size();
-    t.nodes.reset(h.nodes.size());
+    t.nnodes = (int)nnodes;
+    t.nodes.reset(nnodes);
     t.tri9.reset(9 * n);
     t.tri_id.reset(n);
-    SDFO_CUDA(cudaMemcpyAsync(t.nodes.get(), h.nodes.data(), sizeof(RefNode) * h.nodes.size(),
-                              cudaMemcpyHostToDevice, s));
-    SDFO_CUDA(cudaMemcpyAsync(t.tri9.get(), h.tri9.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, s));
-    SDFO_CUDA(cudaMemcpyAsync(t.tri_id.get(), h.tri_id.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
-    // the host vectors above are freed on return: finish the copies first
+    DeviceBuffer<double> dverts((size_t)nv * 3);
+    DeviceBuffer<int32_t> dtris(n * 3);
+    SDFO_CUDA(cudaMemcpyAsync(t.nodes.get(), st.pinned, node_bytes, cudaMemcpyHostToDevice, s));
+    SDFO_CUDA(cudaMemcpyAsync(t.tri_id.get(), ids, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+    SDFO_CUDA(cudaMemcpyAsync(dverts.get(), verts, sizeof(double) * 3 * (size_t)nv, cudaMemcpyHostToDevice, s));
+    SDFO_CUDA(cudaMemcpyAsync(dtris.get(), tris, sizeof(int32_t) * 3 * n, cudaMemcpyHostToDevice, s));
+    k_gather_tri9<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(dverts.get(), dtris.get(), t.tri_id.get(), (int)nt,
+                                                             t.tri9.get());
+    SDFO_CHECK_LAUNCH();
+    // the staging block is reused by the next build and the temporaries are
+    // freed on return: finish the copies and the gather first
     SDFO_CUDA(cudaStreamSynchronize(s));
 }
 
