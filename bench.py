@@ -54,7 +54,10 @@ L2_FLUSH_BYTES = 256 << 20
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    # 2000 headline steps (about 150 ms with the flushes) so that one stall of
+    # the device (about 1 ms was seen in single steps) moves the number by
+    # about 1 %, not 15 %
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--kernels-once", choices=["c2", "c5", "ca", "be", "build", "build5"], default=None,

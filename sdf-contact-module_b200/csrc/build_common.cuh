@@ -334,11 +334,13 @@ __device__ __forceinline__ float cull_limit(double sq)
     return sq >= 3.0e38 ? INFINITY : __double2float_ru(sq) * 1.000002f;
 }
 
+// init_sq: a triangle is recorded only below it (default +inf).
 template <bool COUNT = false>
-__device__ Nearest tree_nearest(const LbvhView& b, const d3& p, int* status, TravCount* tc = nullptr)
+__device__ Nearest tree_nearest(const LbvhView& b, const d3& p, int* status, TravCount* tc = nullptr,
+                                double init_sq = 1.0e308 * 10.0)
 {
     Nearest best;
-    best.sq = 1.0e308 * 10.0; // +inf
+    best.sq = init_sq;
     best.slot = -1;
     best.id = 0x7fffffff;
     best.cp = p;
@@ -555,11 +557,14 @@ __device__ __forceinline__ double box_dist_sq(const d3& p, const double lo[3], c
 // "box distance > best" cut when a subtree is entered, and triangles replace
 // the best only on a strictly smaller squared distance -- so the triangle
 // found is the reference's, ties included.
+// init_sq: a triangle is recorded only below it (default: the reference's
+// DBL_MAX start).
 template <bool COUNT = false>
-__device__ Nearest tree_nearest(const RefTreeView& b, const d3& p, int* status, TravCount* tc = nullptr)
+__device__ Nearest tree_nearest(const RefTreeView& b, const d3& p, int* status, TravCount* tc = nullptr,
+                                double init_sq = DBL_MAX)
 {
     Nearest best;
-    best.sq = DBL_MAX;
+    best.sq = init_sq;
     best.slot = -1;
     best.id = -1;
     best.cp = mk(0.0, 0.0, 0.0);
@@ -841,6 +846,17 @@ __global__ void k_dense_hessian(SpecD s, const double* __restrict__ n64, double*
 
 // Sparse block activation (SdfBuilder.cpp:869-890): distance from the block's
 // geometric centre to the mesh against band + halo*h + (sqrt(3)/2)*bd*h.
+//
+// Most candidate blocks lie far from the surface, where the reference's
+// nearest search visits many nodes.  A first search starts with the best
+// squared distance set to activation^2 (1 + 1e-9), so it prunes everything
+// farther.  If it records no triangle, every triangle's computed squared
+// distance is above activation^2: the tested ones by that test, and those
+// in pruned subtrees because they lie no nearer than their box, whose
+// distance was above the start value.  The reference's search would then
+// also return a distance above the activation distance, with a margin far
+// beyond FP64 rounding, and the block is inactive.  Otherwise the block
+// runs the reference's full search, and its result decides.
 template <class Tree>
 __device__ __forceinline__ int32_t block_active(const Tree& b, const SpecD& s, int bd, int nbx,
                                                 int nby, int bl, double activation, int* status)
@@ -851,6 +867,8 @@ __device__ __forceinline__ int32_t block_active(const Tree& b, const SpecD& s, i
     const d3 c = mk(s.bmin[0] + s.voxel[0] * (0.5 * (double)(i0 + i1)),
                     s.bmin[1] + s.voxel[1] * (0.5 * (double)(j0 + j1)),
                     s.bmin[2] + s.voxel[2] * (0.5 * (double)(k0 + k1)));
+    const Nearest near = tree_nearest(b, c, status, nullptr, activation * activation * (1.0 + 1e-9));
+    if (near.slot < 0) return 0;
     const Nearest best = tree_nearest(b, c, status);
     const double dist = sqrt(best.sq);
     return fabs(dist) <= activation ? 1 : 0;
