@@ -449,11 +449,18 @@ __global__ void k_ca_sparse_activate(CaView v, Tree tree, SpecD s, int bd, int n
         const d3 c = mk(s.bmin[0] + s.voxel[0] * (0.5 * (double)(i0 + i1)),
                         s.bmin[1] + s.voxel[1] * (0.5 * (double)(j0 + j1)),
                         s.bmin[2] + s.voxel[2] * (0.5 * (double)(k0 + k1)));
-        const Nearest nb = tree_nearest(tree, c, status);
-        const double dist = nb.slot >= 0 ? sqrt(nb.sq) : DBL_MAX;
         const double h = fmax(s.voxel[0], fmax(s.voxel[1], s.voxel[2]));
         const double blockRadius = 0.5 * sqrt(3.0) * (double)bd * h;
-        act = dist <= activation + blockRadius;
+        const double limit = activation + blockRadius;
+        // exact far-block reject, as block_active (build_common.cuh) argues:
+        // nothing recorded below limit^2 (1 + 1e-9) means the full search's
+        // distance is above the limit too
+        if (tree_nearest(tree, c, status, nullptr, limit * limit * (1.0 + 1e-9)).slot >= 0)
+        {
+            const Nearest nb = tree_nearest(tree, c, status);
+            const double dist = nb.slot >= 0 ? sqrt(nb.sq) : DBL_MAX;
+            act = dist <= limit;
+        }
     }
     flags[bl] = act ? 1 : 0;
 }
