@@ -650,8 +650,8 @@ int sdfo_be_stepper_create(const sdfo_contact_pair* pair, const sdfo_contact_par
 int sdfo_be_stepper_step(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int64_t n,
                          const double* d_dt, double* d_h, void* stream);
 
-/* Threads per scene: 256 (default; one CTA per scene, two scenes per SM),
- * 128 (four scenes per SM) or 32 (one warp per scene, sixteen per SM).  On
+/* Threads per scene: 256 (default; one CTA per scene, three scenes per SM),
+ * 128 (four scenes per SM) or 32 (one warp per scene, 24 per SM).  On
  * 2048 drops of a 7,680-point ring, 128 and 256 run within 5 % of each other
  * and 32 takes twice as long (its point passes are 8x longer); 32 suits
  * small quadrature sets. */

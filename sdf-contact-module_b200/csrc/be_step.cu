@@ -800,7 +800,7 @@ __device__ void refresh(const BeView& b, Shared& s)
 // T threads per CTA; W: one warp per scene (T / 32 scenes per CTA), else
 // the whole CTA on one scene.
 template <int T, bool W>
-__global__ void __launch_bounds__(T, (W || T == 256) ? 2 : 4) k_be_step(BeView b, sdfo_be_scene* __restrict__ scenes, int n,
+__global__ void __launch_bounds__(T, (W || T == 256) ? 3 : 4) k_be_step(BeView b, sdfo_be_scene* __restrict__ scenes, int n,
                                                 const double* __restrict__ dt_req, double* __restrict__ h_out,
                                                 const double* __restrict__ t_end, double dt_max,
                                                 int* __restrict__ unfinished)
