@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--kernels-once", choices=["c2", "c5", "ca", "be", "build", "build5"], default=None,
+    ap.add_argument("--kernels-once", choices=["c2", "c5", "ca", "be", "build", "build5", "contact"],
+                    default=None,
                     help="one launch of each query kernel on the workload (for ncu), then exit")
     ap.add_argument("--skip-ca", action="store_true",
                     help="leave out the contact-aware build / query section")
@@ -1005,7 +1006,10 @@ def kernels_once(which):
     BE step launches (the last ones in contact).  "build": one dense and one
     sparse (band 3) reference-order build of the hollow cylinder
     (k_dense_fill, k_dense_hessian, k_sparse_activate, k_sparse_fill);
-    "build5": the same sparse build of the 1.31M-triangle icosphere at 512³."""
+    "build5": the same sparse build of the 1.31M-triangle icosphere at 512³.
+    "contact": the ring-on-cube contact batch (4096 poses x 7680 points),
+    one Trilinear forward, one Trilinear forward + Jacobian and one
+    Tricubic forward + Jacobian launch."""
     import ctypes
 
     import torch
@@ -1015,6 +1019,21 @@ def kernels_once(which):
     from sdfo import workloads as W
 
     lib = N.load()
+    if which == "contact":
+        from sdfo.contact import ContactBatch, pack_states
+
+        cc = W.c3_ring_cube(n_poses=4096)
+        cube = SdfGrid.build_dense(*cc["cube"], **cc["build"])
+        poses = pack_states(cc["r"], cc["R"], cc["v"], cc["w"], device="cuda")
+        body_b = pack_states(np.zeros((1, 3)), np.eye(3)[None], device="cuda")[0]
+        b2 = ContactBatch(cube, cc["quad_x"], cc["quad_w"], mode=2, **cc["params"])
+        b3 = ContactBatch(cube, cc["quad_x"], cc["quad_w"], mode=3, **cc["params"])
+        b2.evaluate(poses, body_b)
+        b2.evaluate(poses, body_b, jacobian=True)
+        b3.evaluate(poses, body_b, jacobian=True)
+        torch.cuda.synchronize()
+        print(json.dumps({"kernels_once": which, "poses": 4096, "points": int(len(cc["quad_x"]))}))
+        return
     if which == "build5":
         c = W.c5_icosphere()
         N.check(lib.sdfo_set_bvh_mode(N.BVH_REFERENCE))
