@@ -243,7 +243,7 @@ std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n
                     {
                         // one host thread per mesh: the pool runs the meshes side by side
                         host_ref_tree(host[(size_t)m], meshes[m].h_verts, meshes[m].h_tris,
-                                      meshes[m].nt, 1);
+                                      meshes[m].nt, 1, false);
                     }
                     catch (...)
                     {
@@ -262,24 +262,42 @@ std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n
         }
         total_nodes = node_off[(size_t)n];
         std::vector<RefNode> nodes((size_t)total_nodes);
-        std::vector<double> tri9((size_t)tri_off[(size_t)n] * 9);
         std::vector<int32_t> tri_id((size_t)tri_off[(size_t)n]);
+        std::vector<int64_t> vert_off((size_t)n + 1, 0);
         for (int m = 0; m < n; ++m)
         {
             const HostTreeData& h = host[(size_t)m];
             std::copy(h.nodes.begin(), h.nodes.end(), nodes.begin() + node_off[(size_t)m]);
-            std::copy(h.tri9.begin(), h.tri9.end(), tri9.begin() + 9 * tri_off[(size_t)m]);
             std::copy(h.tri_id.begin(), h.tri_id.end(), tri_id.begin() + tri_off[(size_t)m]);
+            vert_off[(size_t)m + 1] = vert_off[(size_t)m] + meshes[m].nv;
         }
         ref_nodes.reset(nodes.size());
-        ref_tri9.reset(tri9.size());
+        ref_tri9.reset((size_t)tri_off[(size_t)n] * 9);
         ref_tri_id.reset(tri_id.size());
         SDFO_CUDA(cudaMemcpyAsync(ref_nodes.get(), nodes.data(), sizeof(RefNode) * nodes.size(),
                                   cudaMemcpyHostToDevice, s));
-        SDFO_CUDA(cudaMemcpyAsync(ref_tri9.get(), tri9.data(), sizeof(double) * tri9.size(),
-                                  cudaMemcpyHostToDevice, s));
         SDFO_CUDA(cudaMemcpyAsync(ref_tri_id.get(), tri_id.data(), sizeof(int32_t) * tri_id.size(),
                                   cudaMemcpyHostToDevice, s));
+        // the triangles in slot order are gathered on the device from each
+        // mesh's vertices and (mesh-local) triangles
+        DeviceBuffer<double> dverts((size_t)vert_off[(size_t)n] * 3);
+        DeviceBuffer<int32_t> dtris((size_t)tri_off[(size_t)n] * 3);
+        for (int m = 0; m < n; ++m)
+        {
+            SDFO_CUDA(cudaMemcpyAsync(dverts.get() + 3 * vert_off[(size_t)m], meshes[m].h_verts,
+                                      sizeof(double) * 3 * (size_t)meshes[m].nv, cudaMemcpyHostToDevice, s));
+            SDFO_CUDA(cudaMemcpyAsync(dtris.get() + 3 * tri_off[(size_t)m], meshes[m].h_tris,
+                                      sizeof(int32_t) * 3 * (size_t)meshes[m].nt, cudaMemcpyHostToDevice, s));
+        }
+        for (int m = 0; m < n; ++m)
+        {
+            const int64_t nt_m = meshes[m].nt;
+            if (nt_m <= 0) continue;
+            k_gather_tri9<<<(unsigned)((nt_m + 255) / 256), 256, 0, s>>>(
+                dverts.get() + 3 * vert_off[(size_t)m], dtris.get() + 3 * tri_off[(size_t)m],
+                ref_tri_id.get() + tri_off[(size_t)m], (int)nt_m, ref_tri9.get() + 9 * tri_off[(size_t)m]);
+            SDFO_CHECK_LAUNCH();
+        }
         ref_views.resize((size_t)n);
         for (int m = 0; m < n; ++m)
         {

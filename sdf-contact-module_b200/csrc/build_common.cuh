@@ -1269,10 +1269,10 @@ void host_tree_core(HostRefTree& h, const double* verts, const int32_t* tris, in
     h.build(0, (int)nt, 0, depth);
 }
 
-// The reference tree of one mesh on the host, with the triangles in slot
-// order (for the batched build, which concatenates many meshes).
+// The reference tree of one mesh on the host, with the slot order and (if
+// with_tri9) the triangles in slot order.
 void host_ref_tree(HostTreeData& out, const double* verts, const int32_t* tris, int64_t nt,
-                   unsigned threads = 0)
+                   unsigned threads = 0, bool with_tri9 = true)
 {
     if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
     const size_t n = (size_t)nt;
@@ -1282,13 +1282,14 @@ void host_ref_tree(HostTreeData& out, const double* verts, const int32_t* tris, 
     h.rec = rec.data();
     h.nodes = out.nodes.data();
     host_tree_core(h, verts, tris, nt, threads);
-    out.tri9.resize(9 * n);
+    out.tri9.resize(with_tri9 ? 9 * n : 0);
     out.tri_id.resize(n);
     host_parallel_for(n, threads, [&](size_t lo, size_t hi) {
         for (size_t sl = lo; sl < hi; ++sl)
         {
             const int32_t ti = rec[sl].id;
             out.tri_id[sl] = ti;
+            if (!with_tri9) continue;
             for (int v = 0; v < 3; ++v)
                 for (int q = 0; q < 3; ++q)
                     out.tri9[9 * sl + 3 * v + q] = verts[3 * (size_t)tris[3 * (size_t)ti + v] + q];
