@@ -217,8 +217,36 @@ int sdfo_device_cache(int64_t limit, int64_t* held);
 /* Status word the kernels with bounded waits set instead of hanging (bit 0:
  * a bulk-copy wait of the backward pipeline ran out; bit 1: one of the
  * pipelined query kernel); synchronous read,
- * cleared when `clear` != 0.  0 in normal operation. */
+ * cleared when `clear` != 0.  0 in normal operation.  The synchronous host
+ * entry points (sdfo_query_host, sdfo_query_host_static) read bit 1 in
+ * stream order themselves and return SDFO_ERR_DEVICE_STATUS (clearing it)
+ * when it is set; after the asynchronous calls (sdfo_query,
+ * sdfo_query_linearize, sdfo_query_backward_saved on device buffers) the
+ * caller checks this word once the stream has finished. */
 int sdfo_device_status(uint32_t* flags, int32_t clear);
+
+/* Test-only (no reference counterpart): shortens the main-loop wait of the
+ * two bulk-copy pipelines (k_query_pipe, k_backward_saved_bulk) to
+ * `wait_limit` try-wait iterations (0 = the built-in limit) and, when
+ * `withhold_first_tile` != 0, makes every CTA skip the bulk load of its first
+ * tile so that the wait for it runs out.  The kernel then sets its status bit,
+ * waits for the loads it did issue and returns; nothing faults or hangs.
+ * Process-wide; sdfo_debug_wait_test(0, 0) restores normal operation. */
+int sdfo_debug_wait_test(uint32_t wait_limit, int32_t withhold_first_tile);
+
+/* Process-wide tuning knobs (no reference counterpart; the reference has no
+ * device code to tune).  Zero selects the default of a field.  The autotuner
+ * (sdfo/tune.py) times candidates on the caller's data and stores its picks
+ * keyed by GPU and workload shape. */
+typedef struct
+{
+    int32_t host_chunk_queries; /* sdfo_query_host with pinned buffers: queries per
+                                   pipelined chunk (rounded up to 256; default
+                                   131072); one chunk = no pipelining */
+    int32_t fill_ctas_per_sm;   /* batched brick fill: CTAs per SM (0 = as many as fit) */
+} sdfo_tuning;
+int sdfo_set_tuning(const sdfo_tuning* t);
+int sdfo_get_tuning(sdfo_tuning* t);
 
 void sdfo_build_params_default(sdfo_build_params* p);
 void sdfo_sparse_build_params_default(sdfo_sparse_build_params* p);
@@ -408,7 +436,12 @@ int sdfo_query(const sdfo_grid* g, int32_t mode, const void* d_points, int32_t p
                uint8_t* d_valid, float* d_hess, void* stream);
 
 /* Same with host buffers (pageable or pinned): copies in, queries, copies
- * out; synchronous. */
+ * out; synchronous.  With pinned buffers and more than
+ * sdfo_tuning.host_chunk_queries points the batch runs as a pipeline over
+ * chunks: copies in and queries on `stream`, copies out on a stream of the
+ * handle, so that both directions of the bus are busy at once.  Calls on one
+ * handle serialise.  Returns SDFO_ERR_DEVICE_STATUS when the pipelined query
+ * kernel reports a wait that ran out (see sdfo_device_status). */
 int sdfo_query_host(const sdfo_grid* g, int32_t mode, const void* h_points, int32_t points_f64,
                     int64_t n, float* h_gap, float* h_grad, float* h_unit, float* h_witness,
                     uint8_t* h_valid, void* stream);
@@ -427,7 +460,9 @@ int sdfo_query_host(const sdfo_grid* g, int32_t mode, const void* h_points, int3
  * should come before any stream capture.  Every call shares the array and
  * leaves its contents behind: calls that overlap on the GPU (from several
  * host threads or streams at once) race on it, so callers must serialise
- * them.  Synchronous; the grid's device must be current. */
+ * them.  Synchronous; the grid's device must be current.  Returns
+ * SDFO_ERR_DEVICE_STATUS, and no results, when the pipelined query kernel
+ * reports a wait that ran out (see sdfo_device_status). */
 #define SDFO_STATIC_STAGING_BYTES (32u << 20)
 int sdfo_query_host_static(const sdfo_grid* g, int32_t mode, const void* h_points,
                            int32_t points_f64, int64_t n, float* h_gap, float* h_grad,

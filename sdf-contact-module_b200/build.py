@@ -33,7 +33,7 @@ PER_FILE = {"build.cu": ["-fmad=false"], "batch.cu": ["-fmad=false"], "ca_build.
             "ca_query.cu": ["-fmad=false"], "be_step.cu": ["-fmad=false"]}
 SOURCES = ["grid.cu", "capi.cu", "query.cu", "build.cu", "batch.cu", "batch_query.cu",
            "ca_build.cu", "ca_query.cu", "contact.cu", "static_staging.cu", "sdfo_file.cu",
-           "contact_pair.cu", "be_step.cu", "stream_bwd.cu"]
+           "contact_pair.cu", "be_step.cu", "stream_bwd.cu", "host_query.cu"]
 HEADERS = ["sdfo_internal.cuh", "interp.cuh", "build_common.cuh", "bulk.cuh"]
 
 

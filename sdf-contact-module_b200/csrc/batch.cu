@@ -140,9 +140,7 @@ __global__ void k_batch_hessian(const BatchMeta* __restrict__ meta,
 // Grid size for a grid-stride launch: enough CTAs to fill every SM.
 unsigned stride_blocks(int64_t work, int threads)
 {
-    int dev = 0, sms = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess)
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int sms = current_sm_count();
     const int64_t want = (work + threads - 1) / threads;
     const int64_t cap = (int64_t)sms * 16;
     return (unsigned)std::max<int64_t>(1, std::min(want, cap));
@@ -168,6 +166,7 @@ T* carve(unsigned char*& p, size_t count)
 } // namespace
 
 void set_fill_ctas_per_sm(int k) { g_fill_ctas_per_sm.store(k); }
+int fill_ctas_per_sm() { return g_fill_ctas_per_sm.load(); }
 
 std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n, cudaStream_t s)
 {
@@ -388,9 +387,8 @@ std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n
     {
         DeviceBuffer<unsigned long long> counter(1);
         SDFO_CUDA(cudaMemsetAsync(counter.get(), 0, sizeof(unsigned long long), s));
-        int dev = 0, sms = 148, per_sm = 1;
-        SDFO_CUDA(cudaGetDevice(&dev));
-        SDFO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const int sms = current_sm_count();
+        int per_sm = 1;
         if (mode == SDFO_BVH_REFERENCE)
         {
             SDFO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(

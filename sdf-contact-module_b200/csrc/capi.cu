@@ -245,58 +245,6 @@ int sdfo_query(const sdfo_grid* g, int32_t mode, const void* d_points, int32_t p
     });
 }
 
-int sdfo_query_host(const sdfo_grid* g, int32_t mode, const void* h_points, int32_t points_f64,
-                    int64_t n, float* h_gap, float* h_grad, float* h_unit, float* h_witness,
-                    uint8_t* h_valid, void* stream)
-{
-    return guarded([&] {
-        check_grid(g);
-        SDFO_REQUIRE(n >= 0, SDFO_ERR_INVALID_ARGUMENT, "negative query count");
-        if (n == 0) return;
-        SDFO_REQUIRE(h_points && h_gap, SDFO_ERR_INVALID_ARGUMENT, "points and gap are required");
-        SDFO_REQUIRE(mode >= SDFO_FIRST_ORDER && mode <= SDFO_CONTACT_AWARE,
-                     SDFO_ERR_INVALID_ARGUMENT, "unknown query mode");
-        cudaStream_t s = as_stream(stream);
-        // one staging allocation per handle, 256-byte aligned sub-buffers
-        auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
-        const size_t pb = (size_t)n * 3 * (points_f64 ? sizeof(double) : sizeof(float));
-        const size_t gb = sizeof(float) * (size_t)n, vb = sizeof(float) * 3 * (size_t)n;
-        const size_t need = up(pb) + up(gb) + (h_grad ? up(vb) : 0) + (h_unit ? up(vb) : 0) +
-                            (h_witness ? up(vb) : 0) + (h_valid ? up((size_t)n) : 0);
-        std::lock_guard<std::mutex> lock(g->ws_mutex);
-        if (g->ws_bytes < need)
-        {
-            SDFO_CUDA(cudaStreamSynchronize(s));
-            device_free(g->ws);
-            g->ws = nullptr;
-            g->ws_bytes = 0;
-            g->ws = device_alloc(need);
-            g->ws_bytes = need;
-        }
-        unsigned char* base = static_cast<unsigned char*>(g->ws);
-        auto take = [&](size_t b) {
-            unsigned char* p = base;
-            base += up(b);
-            return p;
-        };
-        void* pts = take(pb);
-        float* gap = reinterpret_cast<float*>(take(gb));
-        float* grad = h_grad ? reinterpret_cast<float*>(take(vb)) : nullptr;
-        float* unit = h_unit ? reinterpret_cast<float*>(take(vb)) : nullptr;
-        float* wit = h_witness ? reinterpret_cast<float*>(take(vb)) : nullptr;
-        uint8_t* valid = h_valid ? take((size_t)n) : nullptr;
-        SDFO_CUDA(cudaMemcpyAsync(pts, h_points, pb, cudaMemcpyHostToDevice, s));
-        const QueryOutputs o{gap, grad, unit, wit, valid, nullptr};
-        launch_query(make_view(g), mode, pts, points_f64 != 0, n, o, s);
-        SDFO_CUDA(cudaMemcpyAsync(h_gap, gap, gb, cudaMemcpyDeviceToHost, s));
-        if (h_grad) SDFO_CUDA(cudaMemcpyAsync(h_grad, grad, vb, cudaMemcpyDeviceToHost, s));
-        if (h_unit) SDFO_CUDA(cudaMemcpyAsync(h_unit, unit, vb, cudaMemcpyDeviceToHost, s));
-        if (h_witness) SDFO_CUDA(cudaMemcpyAsync(h_witness, wit, vb, cudaMemcpyDeviceToHost, s));
-        if (h_valid) SDFO_CUDA(cudaMemcpyAsync(h_valid, valid, (size_t)n, cudaMemcpyDeviceToHost, s));
-        SDFO_CUDA(cudaStreamSynchronize(s));
-    });
-}
-
 int sdfo_query_backward(const sdfo_grid* g, int32_t mode, const float* d_points, int64_t n,
                         const float* d_dgap, const float* d_dgrad, float* d_dpoints,
                         float* d_dgrid, void* stream)

@@ -1,5 +1,6 @@
 // Grid handles: creation from host SdfData / SparseSdfData arrays, export,
 // device views and the FP16 re-encoding of sparse payloads.
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,6 +27,33 @@ void throw_cuda(cudaError_t e, const char* what, const char* file, int line)
                   cudaGetErrorString(e), what, file, line);
     if (e == cudaErrorMemoryAllocation) throw Error(SDFO_ERR_OUT_OF_MEMORY, buf);
     throw Error(SDFO_ERR_CUDA, buf);
+}
+
+// ---------------------------------------------------------------------------
+// Multiprocessor counts, one slot per device ordinal, filled on first use.
+// Two threads filling the same slot store the same value; the slots are
+// atomics so that the unsynchronised read is well defined.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kMaxSmDevices = 64;
+std::atomic<int> g_sm_count[kMaxSmDevices];
+} // namespace
+
+int device_sm_count(int dev)
+{
+    SDFO_REQUIRE(dev >= 0 && dev < kMaxSmDevices, SDFO_ERR_UNSUPPORTED, "device ordinal too large");
+    int v = g_sm_count[dev].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+    SDFO_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+    g_sm_count[dev].store(v, std::memory_order_relaxed);
+    return v;
+}
+
+int current_sm_count()
+{
+    int dev = 0;
+    SDFO_CUDA(cudaGetDevice(&dev));
+    return device_sm_count(dev);
 }
 
 // ---------------------------------------------------------------------------
@@ -385,6 +413,7 @@ void encode_fp16(const sdfo_grid* src, sdfo_grid* dst, cudaStream_t s)
 sdfo_grid::~sdfo_grid()
 {
     using sdfo::device_free;
+    sdfo::destroy_host_pipe(host_pipe);
     device_free(ws);
     if (borrowed) return;
     device_free(d.phin);

@@ -1,0 +1,244 @@
+// sdfo_query_host: the query with host buffers (SdfOracle::queryBatch over
+// caller-owned host arrays, SdfOracle.cpp:434-444), and the process-wide
+// tuning knobs (sdfo_set_tuning).
+//
+// With pinned host buffers and more than one chunk of points, the call is a
+// two-stream pipeline over chunks of `host_chunk_queries` points: on the
+// caller's stream each chunk is copied in and queried, then an event hands
+// the chunk to the handle's copy-out stream, which copies its results back
+// while the next chunks are copied in and queried.  Host-to-device and
+// device-to-host copies then run at the same time on separate copy engines,
+// so a step costs about the larger of the two transfers instead of their
+// sum.  Pageable buffers (whose copies the driver stages synchronously) and
+// batches of one chunk take one copy in, one launch and one copy out on the
+// caller's stream.
+//
+// The call is synchronous.  Before it returns it reads the pipelined query
+// kernel's status word in stream order; a bounded wait that ran out in a
+// launch since the word was last cleared is reported as
+// SDFO_ERR_DEVICE_STATUS (the word is then cleared), so stale staging
+// contents are never returned as results.
+#include <algorithm>
+#include <atomic>
+#include <string>
+
+#include "sdfo_internal.cuh"
+
+namespace sdfo {
+
+namespace {
+
+constexpr int kMaxChunks = 64;
+constexpr int64_t kDefaultHostChunk = 131072;
+std::atomic<int64_t> g_host_chunk{kDefaultHostChunk};
+
+int64_t round_up256(int64_t v) { return (v + 255) & ~int64_t(255); }
+
+bool is_pinned(const void* p)
+{
+    if (p == nullptr) return true;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess)
+    {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+} // namespace
+
+struct HostPipe
+{
+    cudaStream_t out = nullptr; // device-to-host copies of finished chunks
+    cudaEvent_t ready[kMaxChunks] = {};
+    unsigned* status = nullptr; // pinned host copy of the query status word
+};
+
+void destroy_host_pipe(HostPipe* p)
+{
+    if (!p) return;
+    for (cudaEvent_t& e : p->ready)
+        if (e) cudaEventDestroy(e);
+    if (p->out) cudaStreamDestroy(p->out);
+    if (p->status) cudaFreeHost(p->status);
+    delete p;
+}
+
+namespace {
+
+// The handle's pipe (created on its first host query; the caller holds
+// ws_mutex).
+HostPipe* host_pipe(const sdfo_grid* g)
+{
+    if (g->host_pipe) return g->host_pipe;
+    auto* p = new HostPipe();
+    try
+    {
+        SDFO_CUDA(cudaStreamCreateWithFlags(&p->out, cudaStreamNonBlocking));
+        for (cudaEvent_t& e : p->ready) SDFO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        SDFO_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&p->status), sizeof(unsigned), cudaHostAllocDefault));
+        *p->status = 0;
+    }
+    catch (...)
+    {
+        destroy_host_pipe(p);
+        throw;
+    }
+    g->host_pipe = p;
+    return p;
+}
+
+struct Staging
+{
+    unsigned char* pts;
+    float* gap;
+    float* grad;
+    float* unit;
+    float* wit;
+    uint8_t* valid;
+};
+
+} // namespace
+
+} // namespace sdfo
+
+using namespace sdfo;
+
+extern "C" {
+
+int sdfo_query_host(const sdfo_grid* g, int32_t mode, const void* h_points, int32_t points_f64,
+                    int64_t n, float* h_gap, float* h_grad, float* h_unit, float* h_witness,
+                    uint8_t* h_valid, void* stream)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(g != nullptr, SDFO_ERR_INVALID_ARGUMENT, "grid is NULL");
+        SDFO_REQUIRE(g->stored_voxels > 0 || g->info.layout == SDFO_LAYOUT_SPARSE,
+                     SDFO_ERR_INVALID_ARGUMENT, "grid is empty");
+        SDFO_REQUIRE(n >= 0, SDFO_ERR_INVALID_ARGUMENT, "negative query count");
+        if (n == 0) return;
+        SDFO_REQUIRE(h_points && h_gap, SDFO_ERR_INVALID_ARGUMENT, "points and gap are required");
+        SDFO_REQUIRE(mode >= SDFO_FIRST_ORDER && mode <= SDFO_CONTACT_AWARE,
+                     SDFO_ERR_INVALID_ARGUMENT, "unknown query mode");
+        SDFO_REQUIRE(n <= (int64_t)65535 * 256 * 4096, SDFO_ERR_INVALID_ARGUMENT, "too many queries");
+        cudaStream_t s = as_stream(stream);
+        const size_t ep = points_f64 ? sizeof(double) : sizeof(float);
+        // one staging allocation per handle, 256-byte aligned sub-buffers
+        auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+        const size_t pb = (size_t)n * 3 * ep;
+        const size_t gb = sizeof(float) * (size_t)n, vb = sizeof(float) * 3 * (size_t)n;
+        const size_t need = up(pb) + up(gb) + (h_grad ? up(vb) : 0) + (h_unit ? up(vb) : 0) +
+                            (h_witness ? up(vb) : 0) + (h_valid ? up((size_t)n) : 0);
+        std::lock_guard<std::mutex> lock(g->ws_mutex);
+        HostPipe* hp = host_pipe(g);
+        if (g->ws_bytes < need)
+        {
+            SDFO_CUDA(cudaStreamSynchronize(s));
+            device_free(g->ws);
+            g->ws = nullptr;
+            g->ws_bytes = 0;
+            g->ws = device_alloc(need);
+            g->ws_bytes = need;
+        }
+        unsigned char* base = static_cast<unsigned char*>(g->ws);
+        auto take = [&](size_t b) {
+            unsigned char* p = base;
+            base += up(b);
+            return p;
+        };
+        Staging d{};
+        d.pts = take(pb);
+        d.gap = reinterpret_cast<float*>(take(gb));
+        d.grad = h_grad ? reinterpret_cast<float*>(take(vb)) : nullptr;
+        d.unit = h_unit ? reinterpret_cast<float*>(take(vb)) : nullptr;
+        d.wit = h_witness ? reinterpret_cast<float*>(take(vb)) : nullptr;
+        d.valid = h_valid ? take((size_t)n) : nullptr;
+        const GridView view = make_view(g);
+        unsigned* status_dev = query_pipe_status_address();
+
+        int64_t chunk = round_up256(std::max<int64_t>(256, g_host_chunk.load()));
+        const bool pinned = is_pinned(h_points) && is_pinned(h_gap) && is_pinned(h_grad) &&
+                            is_pinned(h_unit) && is_pinned(h_witness) && is_pinned(h_valid);
+        // outputs of `m` queries starting at q0, to host on stream `t`
+        auto copy_out = [&](int64_t q0, int64_t m, cudaStream_t t) {
+            const size_t f = sizeof(float);
+            SDFO_CUDA(cudaMemcpyAsync(h_gap + q0, d.gap + q0, f * m, cudaMemcpyDeviceToHost, t));
+            if (h_grad)
+                SDFO_CUDA(cudaMemcpyAsync(h_grad + 3 * q0, d.grad + 3 * q0, 3 * f * m, cudaMemcpyDeviceToHost, t));
+            if (h_unit)
+                SDFO_CUDA(cudaMemcpyAsync(h_unit + 3 * q0, d.unit + 3 * q0, 3 * f * m, cudaMemcpyDeviceToHost, t));
+            if (h_witness)
+                SDFO_CUDA(cudaMemcpyAsync(h_witness + 3 * q0, d.wit + 3 * q0, 3 * f * m, cudaMemcpyDeviceToHost,
+                                          t));
+            if (h_valid) SDFO_CUDA(cudaMemcpyAsync(h_valid + q0, d.valid + q0, (size_t)m, cudaMemcpyDeviceToHost, t));
+        };
+        auto query = [&](int64_t q0, int64_t m, cudaStream_t t) {
+            const QueryOutputs o{d.gap + q0,
+                                 d.grad ? d.grad + 3 * q0 : nullptr,
+                                 d.unit ? d.unit + 3 * q0 : nullptr,
+                                 d.wit ? d.wit + 3 * q0 : nullptr,
+                                 d.valid ? d.valid + q0 : nullptr,
+                                 nullptr};
+            launch_query(view, mode, d.pts + (size_t)q0 * 3 * ep, points_f64 != 0, m, o, t);
+        };
+        cudaStream_t last = s;
+        if (!pinned || n <= chunk)
+        {
+            SDFO_CUDA(cudaMemcpyAsync(d.pts, h_points, pb, cudaMemcpyHostToDevice, s));
+            query(0, n, s);
+            copy_out(0, n, s);
+        }
+        else
+        {
+            if ((n + chunk - 1) / chunk > kMaxChunks) chunk = round_up256((n + kMaxChunks - 1) / kMaxChunks);
+            const unsigned char* hp_pts = static_cast<const unsigned char*>(h_points);
+            int c = 0;
+            for (int64_t q0 = 0; q0 < n; q0 += chunk, ++c)
+            {
+                const int64_t m = std::min(chunk, n - q0);
+                SDFO_CUDA(cudaMemcpyAsync(d.pts + (size_t)q0 * 3 * ep, hp_pts + (size_t)q0 * 3 * ep,
+                                          (size_t)m * 3 * ep, cudaMemcpyHostToDevice, s));
+                query(q0, m, s);
+                SDFO_CUDA(cudaEventRecord(hp->ready[c], s));
+                SDFO_CUDA(cudaStreamWaitEvent(hp->out, hp->ready[c], 0));
+                copy_out(q0, m, hp->out);
+            }
+            last = hp->out;
+        }
+        // the status word after the last launch, in stream order
+        SDFO_CUDA(cudaMemcpyAsync(hp->status, status_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, last));
+        SDFO_CUDA(cudaStreamSynchronize(last));
+        if (*hp->status & kPipeStatusWaitAbort)
+        {
+            SDFO_CUDA(cudaMemsetAsync(status_dev, 0, sizeof(unsigned), s));
+            SDFO_CUDA(cudaStreamSynchronize(s));
+            throw Error(SDFO_ERR_DEVICE_STATUS,
+                        "a bounded wait of the pipelined query kernel ran out; the results are incomplete");
+        }
+    });
+}
+
+int sdfo_set_tuning(const sdfo_tuning* t)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(t != nullptr, SDFO_ERR_INVALID_ARGUMENT, "tuning is NULL");
+        SDFO_REQUIRE(t->host_chunk_queries >= 0, SDFO_ERR_INVALID_ARGUMENT,
+                     "host_chunk_queries must be >= 0");
+        SDFO_REQUIRE(t->fill_ctas_per_sm >= 0 && t->fill_ctas_per_sm <= 64, SDFO_ERR_INVALID_ARGUMENT,
+                     "CTAs per SM out of range");
+        g_host_chunk.store(t->host_chunk_queries > 0 ? t->host_chunk_queries : kDefaultHostChunk);
+        set_fill_ctas_per_sm(t->fill_ctas_per_sm);
+    });
+}
+
+int sdfo_get_tuning(sdfo_tuning* t)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(t != nullptr, SDFO_ERR_INVALID_ARGUMENT, "tuning is NULL");
+        *t = sdfo_tuning{};
+        t->host_chunk_queries = (int32_t)g_host_chunk.load();
+        t->fill_ctas_per_sm = fill_ctas_per_sm();
+    });
+}
+
+} // extern "C"

@@ -363,6 +363,9 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 
 constexpr int kPipeStages = 3;
 constexpr unsigned kPipeWaitLimit = 1u << 24;
 __device__ unsigned int g_pipe_status = 0;
+// Test-only: {main-loop wait limit (0 = kPipeWaitLimit), withhold the first
+// tile's load in every CTA}; both 0 in normal operation.
+__device__ unsigned int g_pipe_test[2] = {0u, 0u};
 
 template <bool HESS>
 struct PipeLayout
@@ -384,6 +387,8 @@ __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS>())
     __shared__ __align__(8) uint64_t bars[kPipeStages];
     __shared__ int s_abort;
     __shared__ long long s_kabort;
+    __shared__ unsigned s_limit;
+    __shared__ int s_withhold;
     unsigned char* stages = smem;
     unsigned char* outs = smem + kPipeStages * L::pts;
     const int64_t tiles = n / kThreads;
@@ -418,10 +423,13 @@ __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS>())
     if (threadIdx.x == 0)
     {
         s_abort = 0;
+        s_limit = g_pipe_test[0] ? g_pipe_test[0] : kPipeWaitLimit;
+        s_withhold = g_pipe_test[1] != 0u;
         for (int st = 0; st < kPipeStages; ++st) mbar_init(&bars[st], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         for (int k = 0; k < kPipeStages && k < mine; ++k)
         {
+            if (k == 0 && s_withhold) continue; // test: tile 0's barrier never completes
             mbar_expect_tx(&bars[k], L::pts);
             bulk_load(stages + k * L::pts, pts + 3 * (first + k * step) * kThreads, L::pts, &bars[k]);
         }
@@ -433,7 +441,7 @@ __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS>())
         const unsigned parity = (unsigned)((k / kPipeStages) & 1);
         unsigned it = 0;
         while (!mbar_try_wait(&bars[st], parity))
-            if (++it >= kPipeWaitLimit)
+            if (++it >= s_limit)
             {
                 s_abort = 1;
                 s_kabort = k;
@@ -490,9 +498,13 @@ __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS>())
     {
         if (s_abort)
         {
-            atomicOr(&g_pipe_status, 2u);
+            atomicOr(&g_pipe_status, kPipeStatusWaitAbort);
+            // the tiles issued but not consumed complete into this CTA's
+            // shared memory: wait for them (bounded, the full limit) before
+            // the CTA exits; a withheld tile has nothing in flight
             for (long long j = s_kabort; j < s_kabort + kPipeStages && j < mine; ++j)
             {
+                if (j == 0 && s_withhold) continue;
                 unsigned it = 0;
                 while (!mbar_try_wait(&bars[j % kPipeStages], (unsigned)((j / kPipeStages) & 1)) &&
                        ++it < kPipeWaitLimit)
@@ -514,13 +526,7 @@ bool launch_pipe(const GridView& v, const float* pts, int64_t n, const QueryOutp
     if (n < kThreads || o.unit || o.witness || o.hess || !o.gap || !aligned16(pts) || !aligned16(o.gap) ||
         !aligned16(o.grad) || !aligned16(o.valid) || !aligned16(o.hess6))
         return false;
-    static int sms = 0;
-    if (sms == 0)
-    {
-        int dev = 0;
-        SDFO_CUDA(cudaGetDevice(&dev));
-        SDFO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    }
+    const int sms = current_sm_count();
     const int64_t tiles = n / kThreads;
     const int64_t rem = n % kThreads ? 1 : 0; // one more CTA, for the remainder
     if (o.hess6)
@@ -621,6 +627,32 @@ void launch_saved_mode(const GridView& v, const SavedBackward& b, cudaStream_t s
 }
 
 } // namespace
+
+namespace {
+std::mutex g_status_mutex;
+unsigned* g_status_addr[64] = {};
+} // namespace
+
+unsigned* query_pipe_status_address()
+{
+    int dev = 0;
+    SDFO_CUDA(cudaGetDevice(&dev));
+    SDFO_REQUIRE(dev >= 0 && dev < 64, SDFO_ERR_UNSUPPORTED, "device ordinal too large");
+    std::lock_guard<std::mutex> lock(g_status_mutex);
+    if (!g_status_addr[dev])
+    {
+        void* p = nullptr;
+        SDFO_CUDA(cudaGetSymbolAddress(&p, g_pipe_status));
+        g_status_addr[dev] = static_cast<unsigned*>(p);
+    }
+    return g_status_addr[dev];
+}
+
+void set_query_pipe_wait_test(unsigned limit, int withhold_first_tile)
+{
+    const unsigned v[2] = {limit, withhold_first_tile ? 1u : 0u};
+    SDFO_CUDA(cudaMemcpyToSymbol(g_pipe_test, v, sizeof(v)));
+}
 
 unsigned query_pipe_status(bool clear)
 {

@@ -69,6 +69,12 @@ int guarded(F&& f)
     }
 }
 
+// Multiprocessor count of device `dev`, looked up once per device
+// (thread-safe; grid.cu).
+int device_sm_count(int dev);
+// ... of the current device.
+int current_sm_count();
+
 // Device allocation owned by a grid handle.
 void* device_alloc(size_t bytes);
 void device_free(void* p);
@@ -139,6 +145,11 @@ struct GridStorage
     int32_t* ca_branch = nullptr;
 };
 
+// Streams, events and the pinned status word of the chunked host-buffer
+// query path (capi.cu), created on a handle's first host query.
+struct HostPipe;
+void destroy_host_pipe(HostPipe* p);
+
 } // namespace sdfo
 
 struct sdfo_grid
@@ -159,6 +170,7 @@ struct sdfo_grid
     mutable std::mutex ws_mutex;
     mutable void* ws = nullptr;
     mutable size_t ws_bytes = 0;
+    mutable sdfo::HostPipe* host_pipe = nullptr;
     ~sdfo_grid();
 };
 
@@ -271,6 +283,18 @@ struct CandidateOutputs
 // Status bits of the pipelined query kernel (query.cu), read and optionally
 // cleared by sdfo_device_status.
 unsigned query_pipe_status(bool clear);
+// Device address of that status word on the current device (looked up once
+// per device), for stream-ordered reads by the synchronous host paths.
+unsigned* query_pipe_status_address();
+// Bit of the status word that k_query_pipe sets when a bounded wait runs out.
+constexpr unsigned kPipeStatusWaitAbort = 2u;
+// Test-only settings of the bounded waits (query.cu, stream_bwd.cu): the
+// main-loop wait limit in try-wait iterations (0 = the built-in limit) and
+// whether every CTA withholds the bulk load of its first tile, so that the
+// wait for it can only run out.  Process-wide; 0, 0 restores normal
+// operation.
+void set_query_pipe_wait_test(unsigned limit, int withhold_first_tile);
+void set_backward_bulk_wait_test(unsigned limit, int withhold_first_tile);
 // dL/dp of the saved backward for all n queries as a bulk-copy pipeline
 // (stream_bwd.cu); false (nothing launched) when n < 256 or the pointers are
 // not 16-byte aligned.
@@ -312,6 +336,7 @@ void count_dense_traversal(const double* verts, int64_t nv, const int32_t* tris,
 // Batched sparse build (batch.cu): one grid per mesh, storage in one arena.
 std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n, cudaStream_t s);
 void set_fill_ctas_per_sm(int k);
+int fill_ctas_per_sm();
 // Contact-aware build (ca_build.cu).
 sdfo_grid* build_contact_aware(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
                                const double* cnormals, const sdfo_contact_aware_params& p,

@@ -95,16 +95,28 @@ extern "C" int sdfo_query_host_static(const sdfo_grid* g, int32_t mode, const vo
         float* gap = reinterpret_cast<float*>(take(gb));
         float* grad = h_grad ? reinterpret_cast<float*>(take(vb)) : nullptr;
         uint8_t* valid = h_valid ? take((size_t)n) : nullptr;
-        // Every output element is written by the kernel, so nothing in the
-        // array has to start at zero; stale contents of earlier calls are
-        // overwritten before they are read.
+        // A launch that completes writes every output element, so nothing in
+        // the array has to start at zero.  A pipelined launch whose bounded
+        // wait ran out stops early and leaves earlier calls' contents in
+        // part of the outputs: the status word, read below in stream order,
+        // turns that into SDFO_ERR_DEVICE_STATUS instead of results.
         cudaStream_t s = as_stream(stream);
+        unsigned* status_dev = query_pipe_status_address();
         SDFO_CUDA(cudaMemcpyAsync(pts, h_points, pb, cudaMemcpyHostToDevice, s));
         const QueryOutputs o{gap, grad, nullptr, nullptr, valid, nullptr};
         launch_query(make_view(g), mode, pts, points_f64 != 0, n, o, s);
         SDFO_CUDA(cudaMemcpyAsync(h_gap, gap, gb, cudaMemcpyDeviceToHost, s));
         if (h_grad) SDFO_CUDA(cudaMemcpyAsync(h_grad, grad, vb, cudaMemcpyDeviceToHost, s));
         if (h_valid) SDFO_CUDA(cudaMemcpyAsync(h_valid, valid, (size_t)n, cudaMemcpyDeviceToHost, s));
+        unsigned status = 0;
+        SDFO_CUDA(cudaMemcpyAsync(&status, status_dev, sizeof(status), cudaMemcpyDeviceToHost, s));
         SDFO_CUDA(cudaStreamSynchronize(s));
+        if (status & kPipeStatusWaitAbort)
+        {
+            SDFO_CUDA(cudaMemsetAsync(status_dev, 0, sizeof(unsigned), s));
+            SDFO_CUDA(cudaStreamSynchronize(s));
+            throw Error(SDFO_ERR_DEVICE_STATUS,
+                        "a bounded wait of the pipelined query kernel ran out; the results are incomplete");
+        }
     });
 }

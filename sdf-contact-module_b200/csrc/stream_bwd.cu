@@ -24,6 +24,9 @@ using namespace bulk;
 constexpr int kTile = 256;   // queries per tile (= threads per CTA)
 constexpr int kStages = 3;
 constexpr unsigned kWaitLimit = 1u << 24;
+// Test-only: {main-loop wait limit (0 = kWaitLimit), withhold the first
+// tile's loads in every CTA}; both 0 in normal operation.
+__device__ unsigned int g_bwd_test[2] = {0u, 0u};
 
 // Shared-memory layout of one input stage (bytes): dgap | dgrad | grad | hess6.
 constexpr int kOffDgap = 0;
@@ -55,6 +58,8 @@ __global__ void __launch_bounds__(kTile) k_backward_saved_bulk(int64_t n, const 
     __shared__ __align__(8) uint64_t bars[kStages];
     __shared__ int s_abort;
     __shared__ long long s_kabort; // the tile whose wait ran out
+    __shared__ unsigned s_limit;
+    __shared__ int s_withhold;
     unsigned char* stages = smem;
     unsigned char* outs = smem + kStages * kStageBytes;
     const int64_t tiles = n / kTile;
@@ -80,9 +85,11 @@ __global__ void __launch_bounds__(kTile) k_backward_saved_bulk(int64_t n, const 
     if (threadIdx.x == 0)
     {
         s_abort = 0;
+        s_limit = g_bwd_test[0] ? g_bwd_test[0] : kWaitLimit;
+        s_withhold = g_bwd_test[1] != 0u;
         for (int s = 0; s < kStages; ++s) mbar_init(&bars[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        for (int k = 0; k < kStages && k < mine; ++k)
+        for (int k = s_withhold ? 1 : 0; k < kStages && k < mine; ++k)
             issue_tile(stages + k * kStageBytes, &bars[k], (first + k * step) * kTile, dgap, dgrad, grad, hess6);
     }
     __syncthreads();
@@ -92,7 +99,7 @@ __global__ void __launch_bounds__(kTile) k_backward_saved_bulk(int64_t n, const 
         const unsigned parity = (unsigned)((k / kStages) & 1);
         unsigned it = 0;
         while (!mbar_try_wait(&bars[s], parity))
-            if (++it >= kWaitLimit)
+            if (++it >= s_limit)
             {
                 s_abort = 1; // benign race: every writer stores the same values
                 s_kabort = k;
@@ -141,6 +148,7 @@ __global__ void __launch_bounds__(kTile) k_backward_saved_bulk(int64_t n, const 
             // (bounded) before the CTA exits
             for (long long j = s_kabort; j < s_kabort + kStages && j < mine; ++j)
             {
+                if (j == 0 && s_withhold) continue; // nothing in flight
                 unsigned it = 0;
                 while (!mbar_try_wait(&bars[j % kStages], (unsigned)((j / kStages) & 1)) && ++it < kWaitLimit)
                 {
@@ -162,13 +170,7 @@ bool launch_backward_saved_bulk(int64_t n, const float* grad, const float* hess6
         (dgap && !a16(dgap)) || (dgrad && !a16(dgrad)))
         return false;
     const int64_t tiles = n / kTile;
-    static int sms = 0;
-    if (sms == 0)
-    {
-        int dev = 0;
-        SDFO_CUDA(cudaGetDevice(&dev));
-        SDFO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    }
+    const int sms = current_sm_count();
     const int smem = kStages * kStageBytes + 2 * kOutBytes; // 45 KB
     const int64_t rem = n % kTile ? 1 : 0; // one more CTA, for the remainder
     const int64_t ctas = std::min<int64_t>(tiles, (int64_t)sms * 4 - rem) + rem;
@@ -177,7 +179,21 @@ bool launch_backward_saved_bulk(int64_t n, const float* grad, const float* hess6
     return true;
 }
 
+void set_backward_bulk_wait_test(unsigned limit, int withhold_first_tile)
+{
+    const unsigned v[2] = {limit, withhold_first_tile ? 1u : 0u};
+    SDFO_CUDA(cudaMemcpyToSymbol(g_bwd_test, v, sizeof(v)));
+}
+
 } // namespace sdfo
+
+extern "C" int sdfo_debug_wait_test(uint32_t wait_limit, int32_t withhold_first_tile)
+{
+    return sdfo::guarded([&] {
+        sdfo::set_query_pipe_wait_test(wait_limit, withhold_first_tile);
+        sdfo::set_backward_bulk_wait_test(wait_limit, withhold_first_tile);
+    });
+}
 
 extern "C" int sdfo_device_status(uint32_t* flags, int32_t clear)
 {

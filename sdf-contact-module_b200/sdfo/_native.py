@@ -101,6 +101,10 @@ class TraversalStats(ctypes.Structure):
                 ("ray_nodes", _I64), ("ray_triangles", _I64)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("host_chunk_queries", _I32), ("fill_ctas_per_sm", _I32)]
+
+
 class DeviceViews(ctypes.Structure):
     _fields_ = [("phin", _P), ("hessian6", _P), ("table", _P), ("block_ijk", _P),
                 ("stored_voxels", _I64), ("table_dims", _I32 * 3), ("reserved0", _I32)]
@@ -147,6 +151,9 @@ SIGNATURES = [
     ("sdfo_grid_destroy", ctypes.c_int, [_P]),
     ("sdfo_file_probe", ctypes.c_int, [ctypes.c_char_p, _P, _P]),
     ("sdfo_device_status", ctypes.c_int, [_P, _I32]),
+    ("sdfo_debug_wait_test", ctypes.c_int, [ctypes.c_uint32, _I32]),
+    ("sdfo_set_tuning", ctypes.c_int, [ctypes.POINTER(Tuning)]),
+    ("sdfo_get_tuning", ctypes.c_int, [ctypes.POINTER(Tuning)]),
     ("sdfo_contact_pair_create", ctypes.c_int, [_P, _P, _P, _I64, _I32, _D, _I32, _P]),
     ("sdfo_contact_pair_export_bvh", ctypes.c_int, [_P, _P, _P, _P, _P]),
     ("sdfo_contact_pair_eval", ctypes.c_int, [_P, _I32, _P, _I64, _P, _P, _P, _P, _P, _P]),
@@ -226,6 +233,25 @@ def last_error() -> str:
 def check(code: int) -> None:
     if code != SDFO_OK:
         raise SdfoError(code, last_error())
+
+
+def get_tuning() -> dict:
+    """The process-wide tuning knobs (sdfo_get_tuning) as a dict."""
+    t = Tuning()
+    check(load().sdfo_get_tuning(ctypes.byref(t)))
+    return {name: int(getattr(t, name)) for name, _ in Tuning._fields_}
+
+
+def set_tuning(**fields) -> dict:
+    """Sets the named tuning knobs (others keep their values); returns the
+    resulting settings."""
+    cur = get_tuning()
+    unknown = set(fields) - set(cur)
+    if unknown:
+        raise ValueError(f"unknown tuning fields {sorted(unknown)}")
+    cur.update({k: int(v) for k, v in fields.items()})
+    check(load().sdfo_set_tuning(ctypes.byref(Tuning(**cur))))
+    return get_tuning()
 
 
 def mode_id(mode) -> int:

@@ -3,7 +3,10 @@
 Run in a container where the reference checkout is present:
 
     make -C oracle ref port
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference PATH]
+
+PATH defaults to $SDFO_REFERENCE_ROOT, else a directory named ``reference``
+beside this repository.
 
 Sources of truth (nothing here is restated):
   * the reference C++ SdfOracle sources, compiled unmodified into
@@ -80,7 +83,9 @@ def ref_queries(g, pts):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    default_ref = os.environ.get("SDFO_REFERENCE_ROOT") or os.path.join(
+        os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference")
+    ap.add_argument("--reference", default=default_ref)
     ap.add_argument("--only", choices=["all", "contact_aware", "broadphase", "be"], default="all")
     a = ap.parse_args()
     ms = meshes()

@@ -71,8 +71,9 @@ def _row_of(st, rg):
 def _close(out, ref, tol, atol=1e-15):
     """Elementwise |out - ref| <= tol |ref| + atol (equal infinities pass)."""
     both_inf = np.isinf(out) & np.isinf(ref) & (np.sign(out) == np.sign(ref))
-    err = np.where(both_inf, 0.0, np.abs(out - ref))
-    return np.all(err <= tol * np.abs(np.where(both_inf, 0.0, ref)) + atol)
+    o = np.where(both_inf, 0.0, out)
+    r = np.where(both_inf, 0.0, ref)
+    return np.all(np.abs(o - r) <= tol * np.abs(r) + atol)
 
 
 @pytest.mark.parametrize("name", SCENES)

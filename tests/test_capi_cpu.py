@@ -142,3 +142,26 @@ def test_device_check_without_gpu(lib):
 
     assert lib.sdfo_device_check(0) == -7
     assert "no CUDA device" in N.last_error()
+
+
+def test_tuning_round_trip(lib):
+    """sdfo_set_tuning / sdfo_get_tuning: host-only state; zero restores a
+    field's default; out-of-range values are rejected."""
+    from sdfo import _native as N
+
+    before = N.get_tuning()
+    try:
+        t = N.set_tuning(host_chunk_queries=65536, fill_ctas_per_sm=2)
+        assert t == {"host_chunk_queries": 65536, "fill_ctas_per_sm": 2}
+        t = N.set_tuning(host_chunk_queries=0)
+        assert t["host_chunk_queries"] == 131072 and t["fill_ctas_per_sm"] == 2
+        bad = N.Tuning(host_chunk_queries=-1, fill_ctas_per_sm=0)
+        assert lib.sdfo_set_tuning(ctypes.byref(bad)) == -1
+        bad = N.Tuning(host_chunk_queries=0, fill_ctas_per_sm=65)
+        assert lib.sdfo_set_tuning(ctypes.byref(bad)) == -1
+        assert lib.sdfo_set_tuning(None) == -1
+        with pytest.raises(ValueError):
+            N.set_tuning(no_such_knob=1)
+    finally:
+        N.set_tuning(**before)
+    assert N.get_tuning() == before
