@@ -567,30 +567,44 @@ def be_section(torch, dev, stream, steps, warmup, cpu_ok):
     implicit_be.py operation for operation) on the first scenes."""
     from sdfo import SdfGrid
     from sdfo import workloads as W
-    from sdfo.be import BEStepper
+    from sdfo.be import BEStepper, default_params
 
     c = W.be_ring_drops(2048)
     grid = SdfGrid.build_dense(*c["slab"], **c["build"])
     p = c["params"]
-    st = BEStepper(grid, c["quad_x"], c["quad_w"], c["mass"], c["inertia"], p["stiffness"],
-                   order=p["order"], damping=p["damping"], friction=p["friction"],
-                   regularizer=p["regularizer"], activation_distance=p["activation_distance"],
-                   narrow_margin=0.01, max_scenes=len(c["r"]))
-    warm = st.scenes(c["r"], c["R"], c["v"], c["w"])
-    for _ in range(max(1, warmup)):
-        st.step(warm, 1e-3)
-    scenes = st.scenes(c["r"], c["R"], c["v"], c["w"])
-    graph_scenes = scenes.clone()
+
+    def stepper(tangent):
+        return BEStepper(grid, c["quad_x"], c["quad_w"], c["mass"], c["inertia"], p["stiffness"],
+                         order=p["order"], damping=p["damping"], friction=p["friction"],
+                         regularizer=p["regularizer"], activation_distance=p["activation_distance"],
+                         narrow_margin=0.01, max_scenes=len(c["r"]),
+                         params=default_params(tangent=tangent))
+
+    def run(st):
+        warm = st.scenes(c["r"], c["R"], c["v"], c["w"])
+        for _ in range(max(1, warmup)):
+            st.step(warm, 1e-3)
+        scenes = st.scenes(c["r"], c["R"], c["v"], c["w"])
+        torch.cuda.synchronize()
+        st.stats(reset=True)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        for a, b in evs:
+            a.record(stream)
+            st.step(scenes, 1e-3, stream=stream)
+            b.record(stream)
+        torch.cuda.synchronize()
+        return scenes, [a.elapsed_time(b) for a, b in evs], st.stats()
+
+    # the exact-Newton mode (exact contact every residual, analytic tangent)
+    st_ex = stepper("exact")
+    scenes_ex, ms_ex, stats_ex = run(st_ex)
+    u_ex = st_ex.unpack(scenes_ex)
+    st_ex.close()
+    st = stepper("reference")
+    scenes, ms, stats_ref = run(st)
+    graph_scenes = st.scenes(c["r"], c["R"], c["v"], c["w"])
     torch.cuda.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(steps)]
-    hs = []
-    for a, b in evs:
-        a.record(stream)
-        hs.append(st.step(scenes, 1e-3, stream=stream))
-        b.record(stream)
-    torch.cuda.synchronize()
-    ms = [a.elapsed_time(b) for a, b in evs]
     # the same steps as integrate runs them: one CUDA graph of `steps`
     # launches (t_end far enough that every step is the full 1 ms request)
     start = graph_scenes.clone()
@@ -606,9 +620,26 @@ def be_section(torch, dev, stream, steps, warmup, cpu_ok):
     torch.cuda.synchronize()
     u = st.unpack(scenes)
     n = len(c["r"])
+    same_t = u["t"] == u_ex["t"]
+    dr = np.abs(u["r"] - u_ex["r"]).max(axis=1)[same_t]
     out = {"workload": "ring_drops_on_slab_2048_scenes_7680_points_dt1ms",
            "scenes": n, "steps": steps, "step_ms": ms,
            "scene_steps_per_s": n * steps / (sum(ms) * 1e-3),
+           "tangent": "reference (linearisation cache + heuristic diagonal tangent)",
+           "newton_iterations": stats_ref["newton_iterations"],
+           "residual_evaluations": stats_ref["residual_evaluations"],
+           "be_solves": stats_ref["be_solves"],
+           "newton_per_solve": stats_ref["newton_iterations"] / max(1, stats_ref["be_solves"]),
+           "exact": {"tangent": "exact contact every residual + analytic dR/dV",
+                     "step_ms": ms_ex, "scene_steps_per_s": n * steps / (sum(ms_ex) * 1e-3),
+                     "newton_iterations": stats_ex["newton_iterations"],
+                     "residual_evaluations": stats_ex["residual_evaluations"],
+                     "be_solves": stats_ex["be_solves"],
+                     "newton_per_solve": stats_ex["newton_iterations"] / max(1, stats_ex["be_solves"]),
+                     "scenes_same_time_as_reference": int(same_t.sum()),
+                     "max_abs_dr_vs_reference_m": float(dr.max()) if dr.size else None,
+                     "phases_after": {str(k): int((u_ex["phase"] == k).sum())
+                                      for k in sorted(set(u_ex["phase"].tolist()))}},
            "graph_ms": ga.elapsed_time(gb),
            "graph_matches_steps": bool(torch.equal(graph_scenes, scenes)),
            "simulated_time_per_scene_s": float(u["t"].mean()),

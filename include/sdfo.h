@@ -612,6 +612,21 @@ int sdfo_contact_pair_eval(const sdfo_contact_pair* p, int32_t mode,
 int sdfo_contact_pair_destroy(sdfo_contact_pair* p);
 
 /* ---- Backward-Euler contact steps ---------------------------------------- */
+/* Newton tangent of the BE solve (sdfo_be_params.tangent).
+ * REFERENCE: the reference's method -- contact forces inside a step reuse
+ *   the linearisation cache g + grad . dt of its first evaluation
+ *   (contacts_sdf.py:306-326) and Newton uses the heuristic diagonal contact
+ *   stiffness (_contact_tangent / _tangent, implicit_be.py:606-687).
+ * EXACT (no reference counterpart): every residual evaluates contact exactly
+ *   and Newton uses the analytic dR/dV -- M/h, the rotational inertia and
+ *   gyroscopic terms differentiated through R(w), and the contact block
+ *   Jv + Jp diag(h I, h J_l(h w)) from the force law differentiated per
+ *   quadrature point (Jp: w.r.t. the pose, R <- exp([dtheta]x) R, at fixed
+ *   velocities; Jv: w.r.t. (v, w) at a fixed pose; J_l the SO(3) left
+ *   Jacobian).  It converges to the exact BE solution of each step. */
+#define SDFO_BE_TANGENT_REFERENCE 0
+#define SDFO_BE_TANGENT_EXACT 1
+
 /* BackwardEulerIntegrator parameters (implicit_be.py:60-107 defaults via
  * sdfo_be_params_default). */
 typedef struct
@@ -621,7 +636,7 @@ typedef struct
     int32_t max_toi_bisect_iter; /* 60 */
     int32_t stable_steps;        /* contact_stable_steps, 5 */
     int32_t release_steps;       /* contact_release_steps, 3 */
-    int32_t reserved0;
+    int32_t tangent;             /* SDFO_BE_TANGENT_*, default REFERENCE */
     double tol;                  /* 1e-8 */
     double pen_max;              /* contact_penetration_tol, 1e-6 */
     double dt_min;               /* contact_dt_min, 1e-8 */
@@ -714,6 +729,12 @@ int sdfo_be_stepper_integrate(sdfo_be_stepper* st, sdfo_be_scene* d_scenes, int6
                               const double* d_t_end, double dt, int32_t launches_per_check,
                               int64_t max_launches, int64_t* launches_out,
                               int32_t* unfinished_out, void* stream);
+
+/* Work counters summed over every launch since creation or the last reset
+ * (no reference counterpart): out[0] Newton iterations, out[1] residual
+ * evaluations, out[2] BE solves (_step_be calls, trial steps included).
+ * Synchronises the device; reset != 0 zeroes them after the read. */
+int sdfo_be_stepper_stats(sdfo_be_stepper* st, uint64_t* out, int32_t reset);
 
 int sdfo_be_stepper_destroy(sdfo_be_stepper* st);
 

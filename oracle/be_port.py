@@ -28,6 +28,18 @@ joints or drives, and the SDFContactEngine it drives
     the stored gradient and validity.
 The measure the in-residual `any_contact` flag takes (:592-601) is unused by
 the reference and not restated.
+
+Params.tangent = "exact" selects the exact Newton method that replaces the
+reference's cache and heuristic tangent: every residual evaluates contact
+exactly (no linearisation cache), and the tangent is the analytic Jacobian
+dR/dV of the residual -- M/h, the derivatives of the rotational inertia and
+gyroscopic terms through R(w), and the contact block dQ/dV = Jv + Jp
+diag(h I, h J_l(h w)), where Jp is d(F, tau)/d(dx, dtheta) at fixed
+velocities (R <- exp([dtheta]x) R), Jv is d(F, tau)/d(v, w) at a fixed pose,
+and J_l is the left Jacobian of SO(3).  The per-point derivatives are the
+force law's (contacts_sdf.py:329-385) differentiated by hand, with the
+trilinear interpolant's Hessian (Scene.hess_batch).  `jacobians_fd` and
+`tangent_fd` give the same matrices by central differences for the tests.
 """
 from __future__ import annotations
 
@@ -58,6 +70,7 @@ class Params:
     stable_steps: int = 5
     release_steps: int = 3
     max_toi_bisect_iter: int = 60
+    tangent: str = "reference"  # or "exact"
 
     @property
     def release_gap(self):
@@ -109,6 +122,7 @@ class Scene:
     rB: np.ndarray = field(default_factory=lambda: np.zeros(3))
     RB: np.ndarray = field(default_factory=lambda: np.eye(3))
     bvh: tuple = None
+    hess_batch: object = None  # Y (N,3) -> (N,3,3) interpolant Hessian ("exact" tangent)
 
     def __post_init__(self):
         if self.bvh is None:
@@ -131,22 +145,26 @@ class Integrator:
         self.cache = Cache()
         self._M = None
         self._temp = None
+        self.newton_iterations = 0
 
     # -------------------------------------------------------------- engine
     def _cull(self, st):
         return B.cull_indices(self.s.X, self.s.bvh, self.s.bmin, self.s.bmax, st.r, st.R,
                               self.s.narrow_margin)
 
-    def evaluate(self, st):
-        """SDFContactEngine.evaluate (contacts_sdf.py:225-385) with the cache."""
+    def evaluate(self, st, jac=False):
+        """SDFContactEngine.evaluate (contacts_sdf.py:225-385) with the cache;
+        with jac, also (Jp, Jv): the 6x6 Jacobians of (F, tau) w.r.t. the
+        pose (dx, dtheta) and the velocities (v, w)."""
         s, c = self.s, self.cache
         idx = self._cull(st)
         R_sdf = s.RB.T @ st.R
         t_sdf = s.RB.T @ (st.r - s.rB)
         Y = (R_sdf @ s.X[idx].T + t_sdf[:, None]).T
         local = np.nonzero(np.abs(Y[:, 2]) < s.narrow_margin)[0]
+        zero = (np.zeros(3), np.zeros(3)) + ((np.zeros((6, 6)), np.zeros((6, 6))) if jac else ())
         if len(local) == 0:
-            return np.zeros(3), np.zeros(3)
+            return zero
         act_idx = idx[local]
         use = c.enabled and not c.cleared and c.lactive_len is not None and len(local) == c.lactive_len
         if use:
@@ -164,7 +182,7 @@ class Integrator:
         p_all = s.k * np.maximum(-g, 0.0) ** s.order
         vm = valid & (p_all > 1e-30)
         if not np.any(vm):
-            return np.zeros(3), np.zeros(3)
+            return zero
         gi = act_idx[vm]
         gv = g[vm]
         p = s.k * np.maximum(-gv, 0.0) ** s.order
@@ -193,7 +211,73 @@ class Integrator:
         if np.any(a):
             ft[a] = -s.mu * phat[a, None] * ut[a] / den[a, None]
         fq = fn + ft
-        return np.sum(wv[:, None] * fq, axis=0), np.sum(wv[:, None] * np.cross(off, fq), axis=0)
+        F = np.sum(wv[:, None] * fq, axis=0)
+        tau = np.sum(wv[:, None] * np.cross(off, fq), axis=0)
+        if not jac:
+            return F, tau
+        Hs = s.hess_batch(Y[local][vm])
+        Hw = np.einsum("ij,njk,lk->nil", s.RB, Hs, s.RB)
+        dlt = -gv
+        pp = -s.k * s.order * dlt ** (s.order - 1.0)      # dp/dg
+        I3 = np.eye(3)[None]
+        udn = np.sum(u * un, axis=1)
+        P = I3 - un[:, :, None] * un[:, None, :]
+        Mt = (I3 - ut[:, :, None] * ut[:, None, :] / den[:, None, None] ** 2) / den[:, None, None]
+        fr = (s.mu * phat > 0).astype(float)[:, None, None]
+        dm = 1.0 if s.damping > 0 else 0.0
+        # dfq/dg, dfq/d(world gradient), dfq/du
+        a_g = pp[:, None] * rg - fr[:, :, 0] * s.mu * (gnv * pp)[:, None] * ut / den[:, None]
+        B = p[:, None, None] * I3 \
+            - dm * s.damping * (rg[:, :, None] * u[:, None, :] + vn[:, None, None] * I3) \
+            + fr * (-s.mu * p[:, None, None] * ut[:, :, None] * un[:, None, :] / den[:, None, None]
+                    + s.mu * p[:, None, None] * Mt @ ((udn[:, None, None] * I3
+                                                       + un[:, :, None] * u[:, None, :]) @ P))
+        U = -dm * s.damping * rg[:, :, None] * rg[:, None, :] - fr * s.mu * phat[:, None, None] * (Mt @ P)
+        G = a_g[:, :, None] * rg[:, None, :] + B @ Hw
+        Gt = G - U @ _skew(wB)[None]
+        Ox = _skew_n(off)
+        Fx = _skew_n(fq)
+        Wx = _skew(st.w)[None]
+        Dth = -Gt @ Ox - U @ Wx @ Ox
+        W = wv[:, None, None]
+        Jp = np.zeros((6, 6))
+        Jv = np.zeros((6, 6))
+        Jp[:3, :3] = np.sum(W * Gt, 0)
+        Jp[:3, 3:] = np.sum(W * Dth, 0)
+        Jp[3:, :3] = np.sum(W * (Ox @ Gt), 0)
+        Jp[3:, 3:] = np.sum(W * (Ox @ Dth + Fx @ Ox), 0)
+        Jv[:3, :3] = np.sum(W * U, 0)
+        Jv[:3, 3:] = np.sum(W * (-U @ Ox), 0)
+        Jv[3:, :3] = np.sum(W * (Ox @ U), 0)
+        Jv[3:, 3:] = np.sum(W * (-Ox @ U @ Ox), 0)
+        return F, tau, Jp, Jv
+
+    def jacobians_fd(self, st, hx=1e-8, hth=1e-8, hv=1e-6):
+        """Central differences of evaluate (no cache): (Jp, Jv)."""
+        Jp = np.zeros((6, 6))
+        Jv = np.zeros((6, 6))
+
+        def ev(q):
+            F, t = self.evaluate(q)
+            return np.concatenate([F, t])
+
+        for k in range(6):
+            a, b = st.copy(), st.copy()
+            if k < 3:
+                a.r[k] += hx
+                b.r[k] -= hx
+                Jp[:, k] = (ev(a) - ev(b)) / (2 * hx)
+            else:
+                e = np.zeros(3)
+                e[k - 3] = hth
+                a.R = _expm(e) @ st.R
+                b.R = _expm(-e) @ st.R
+                Jp[:, k] = (ev(a) - ev(b)) / (2 * hth)
+            a, b = st.copy(), st.copy()
+            (a.v if k < 3 else a.w)[k % 3] += hv
+            (b.v if k < 3 else b.w)[k % 3] -= hv
+            Jv[:, k] = (ev(a) - ev(b)) / (2 * hv)
+        return Jp, Jv
 
     def measure(self, st):
         """measure_pair (contacts_sdf.py:171-214), uncached."""
@@ -241,6 +325,36 @@ class Integrator:
         self._M = M
         return M @ (z - V0) / dt + C - Q
 
+    def tangent_exact(self, z, q0, dt, allowed):
+        """The analytic dR/dV at z (module docstring)."""
+        s = self.s
+        st = self.kinematic_update(q0, z, dt)
+        Iw = st.R @ s.inertia @ st.R.T
+        w = st.w
+        dw = w - q0.w
+        Jl = left_jacobian(dt * w)
+        K = np.zeros((6, 6))
+        K[:3, :3] = s.mass / dt * np.eye(3)
+        K[3:, 3:] = Iw / dt + (-_skew(Iw @ dw) + Iw @ _skew(dw)) @ Jl
+        K[3:, 3:] += -_skew(Iw @ w) + _skew(w) @ Iw + dt * _skew(w) @ (-_skew(Iw @ w) + Iw @ _skew(w)) @ Jl
+        if allowed:
+            _, _, Jp, Jv = self.evaluate(st, jac=True)
+            T = np.zeros((6, 6))
+            T[:3, :3] = dt * np.eye(3)
+            T[3:, 3:] = dt * Jl
+            K -= Jv + Jp @ T
+        return K
+
+    def tangent_fd(self, z, q0, dt, allowed, eps=1e-7):
+        """Central differences of the residual (exact contact) in V."""
+        K = np.zeros((6, 6))
+        for i in range(6):
+            zp, zm = z.copy(), z.copy()
+            zp[i] += eps
+            zm[i] -= eps
+            K[:, i] = (self.residual(zp, q0, dt, allowed) - self.residual(zm, q0, dt, allowed)) / (2 * eps)
+        return K
+
     def tangent(self, dt, allowed):
         s = self.s
         K = self._M / dt
@@ -261,15 +375,20 @@ class Integrator:
         """_step_be: state advanced in place; `allowed` = contact forces on."""
         q0 = state.copy()
         z = np.concatenate([q0.v, q0.w])
-        self.cache.enabled = allowed
+        exact = self.p.tangent == "exact"
+        self.cache.enabled = allowed and not exact
         self.cache.cleared = True
         try:
             R = self.residual(z, q0, dt, allowed)
             for _ in range(self.p.max_iter):
                 if np.max(np.abs(R)) < self.p.tol:
                     break
-                K = self.tangent(dt, allowed)
-                dz = np.linalg.lstsq(K, -R, rcond=1e-12)[0]
+                self.newton_iterations += 1
+                if exact:
+                    dz = np.linalg.solve(self.tangent_exact(z, q0, dt, allowed), -R)
+                else:
+                    K = self.tangent(dt, allowed)
+                    dz = np.linalg.lstsq(K, -R, rcond=1e-12)[0]
                 alpha = 1.0
                 if self.p.line_search:
                     r0 = np.linalg.norm(R)
@@ -394,6 +513,39 @@ class Integrator:
         else:
             rg.phase = ACTIVE
             rg.dt_current = max(p.dt_contact, p.dt_min)
+
+
+def _skew(a):
+    return np.array([[0.0, -a[2], a[1]], [a[2], 0.0, -a[0]], [-a[1], a[0], 0.0]])
+
+
+def _skew_n(a):
+    S = np.zeros((len(a), 3, 3))
+    S[:, 0, 1], S[:, 0, 2] = -a[:, 2], a[:, 1]
+    S[:, 1, 0], S[:, 1, 2] = a[:, 2], -a[:, 0]
+    S[:, 2, 0], S[:, 2, 1] = -a[:, 1], a[:, 0]
+    return S
+
+
+def _expm(phi):
+    n = np.linalg.norm(phi)
+    if n < 1e-300:
+        return np.eye(3)
+    K = _skew(phi / n)
+    return np.eye(3) + np.sin(n) * K + (1 - np.cos(n)) * K @ K
+
+
+def left_jacobian(phi):
+    """J_l(phi) of SO(3): exp(phi + d) = exp([J_l(phi) d]x) exp(phi) + O(d^2)."""
+    t = np.linalg.norm(phi)
+    S = _skew(phi)
+    if t < 1e-4:
+        a = 0.5 - t * t / 24.0
+        b = 1.0 / 6.0 - t * t / 120.0
+    else:
+        a = (1.0 - np.cos(t)) / (t * t)
+        b = (t - np.sin(t)) / (t * t * t)
+    return np.eye(3) + a * S + b * S @ S
 
 
 def clone(integ: Integrator) -> Integrator:

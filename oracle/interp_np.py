@@ -92,3 +92,40 @@ def query(spec, phi, normal, mode, Y, cells=None):
     gap = np.where(valid, gap, 0.0)
     grad = np.where(valid[:, None], grad, 0.0)
     return gap, grad, valid, cells
+
+
+def trilinear_hessian(spec, phi, Y):
+    """Hessian (N,3,3) of the trilinear interpolant of query() mode 2 at Y
+    (its cell's bilinear mixed partials; the diagonal is zero); zero where
+    the point is invalid.  Used by the exact Newton tangent of the BE
+    restatement."""
+    Y = np.asarray(Y, np.float64).reshape(-1, 3)
+    bmin = np.asarray(spec["bmin"], np.float64)
+    vox = np.asarray(spec["voxel"], np.float64)
+    nx, ny, nz = [int(s) for s in spec["shape"]]
+    f = (Y - bmin) / vox - 0.5
+    with np.errstate(invalid="ignore"):
+        ok = np.all(np.isfinite(f), axis=1)
+        c = np.floor(np.where(np.isfinite(f), f, 0.0)).astype(np.int64)
+    valid = ok & (c[:, 0] >= 0) & (c[:, 0] + 1 < nx) & (c[:, 1] >= 0) & (c[:, 1] + 1 < ny) \
+        & (c[:, 2] >= 0) & (c[:, 2] + 1 < nz)
+    u = f - c
+    c = np.where(valid[:, None], c, 0)
+
+    def P(di, dj, dk):
+        return phi[(c[:, 0] + di) + nx * ((c[:, 1] + dj) + ny * (c[:, 2] + dk))]
+
+    p000, p100, p010, p110 = P(0, 0, 0), P(1, 0, 0), P(0, 1, 0), P(1, 1, 0)
+    p001, p101, p011, p111 = P(0, 0, 1), P(1, 0, 1), P(0, 1, 1), P(1, 1, 1)
+    hxy = ((p110 - p010 - p100 + p000) * (1 - u[:, 2]) + (p111 - p011 - p101 + p001) * u[:, 2]) \
+        / (vox[0] * vox[1])
+    hxz = ((p101 - p001 - p100 + p000) * (1 - u[:, 1]) + (p111 - p011 - p110 + p010) * u[:, 1]) \
+        / (vox[0] * vox[2])
+    hyz = ((p011 - p001 - p010 + p000) * (1 - u[:, 0]) + (p111 - p101 - p110 + p100) * u[:, 0]) \
+        / (vox[1] * vox[2])
+    H = np.zeros((len(Y), 3, 3))
+    H[:, 0, 1] = H[:, 1, 0] = hxy
+    H[:, 0, 2] = H[:, 2, 0] = hxz
+    H[:, 1, 2] = H[:, 2, 1] = hyz
+    H[~valid] = 0.0
+    return H

@@ -23,6 +23,20 @@
 // with the SDF-frame translation; later evaluations with the same number of
 // narrow-filtered points use g + grad . (t - t_ref).
 //
+// Tangent modes (sdfo_be_params.tangent):
+//   * SDFO_BE_TANGENT_REFERENCE: the reference's method as above -- the
+//     linearisation cache inside a step and the heuristic diagonal tangent;
+//   * SDFO_BE_TANGENT_EXACT: every residual evaluates contact exactly (no
+//     cache) and Newton uses the analytic dR/dV: M/h, the derivatives of the
+//     rotational inertia and gyroscopic terms through R(w), and the contact
+//     block Jv + Jp diag(h I, h J_l(h w)), where Jp = d(F, tau)/d(dx, dtheta)
+//     (R <- exp([dtheta]x) R) at fixed velocities and Jv = d(F, tau)/d(v, w)
+//     at a fixed pose come from the force law differentiated per point with
+//     the trilinear Hessian, reduced in FP64 in a fixed order (warp shuffles,
+//     then warps in order), and the 6x6 system is solved by Gaussian
+//     elimination with partial pivoting.  Each mode is its own kernel
+//     instantiation, so the reference mode keeps its register budget.
+//
 // Grid samples are FP64 trilinear on the grid's FP64 values, written as the
 // prototype's TrilinearSDFGrid.query_batch (prototype/src/sdf_grid.py:
 // 138-204); this translation unit is compiled with -fmad=false so that every
@@ -79,7 +93,10 @@ struct BeView
     double* cg;               // cache scratch, nq per scene
     double* cgrad;            // 3 nq per scene
     unsigned char* cvalid;    // nq per scene
+    unsigned long long* stats; // Newton iterations, residual evaluations, BE solves
 };
+
+constexpr int kJac = 72; // Jp (36) then Jv (36), row-major 6x6 each
 
 struct MinRec
 {
@@ -114,6 +131,10 @@ struct Shared
     int scene;                  // index of the scene in the batch
     double alpha;               // line search
     int found;
+    // rows of per-warp partial sums of the contact Jacobians (one row per
+    // warp of the scene; after the reduction row 0 holds Jp then Jv)
+    double* jred;
+    int n_newton, n_resid, n_solves; // this launch's counts for the scene
 };
 
 // ---------------------------------------------------------------- helpers
@@ -180,8 +201,10 @@ struct Grp<true>
     __device__ static int warps() { return 1; }
 };
 
-// TrilinearSDFGrid.query_batch for one point (sdf_grid.py:138-204).
-__device__ bool sample64(const BeView& b, const double Y[3], double& g, double grad[3])
+// TrilinearSDFGrid.query_batch for one point (sdf_grid.py:138-204); with
+// `hess`, also the interpolant's mixed second derivatives {xy, xz, yz} (its
+// diagonal is zero).
+__device__ bool sample64(const BeView& b, const double Y[3], double& g, double grad[3], double* hess = nullptr)
 {
     const int n[3] = {b.g.nx, b.g.ny, b.g.nz};
     int c[3];
@@ -211,6 +234,12 @@ __device__ bool sample64(const BeView& b, const double Y[3], double& g, double g
                (p111 - p101) * uv * wv) * ihy;
     grad[2] = ((p001 - p000) * one_u * one_v + (p101 - p100) * uv * one_v + (p011 - p010) * one_u * vv +
                (p111 - p110) * uv * vv) * ihz;
+    if (hess)
+    {
+        hess[0] = ((p110 - p010 - p100 + p000) * one_w + (p111 - p011 - p101 + p001) * wv) * (ihx * ihy);
+        hess[1] = ((p101 - p001 - p100 + p000) * one_v + (p111 - p011 - p110 + p010) * vv) * (ihx * ihz);
+        hess[2] = ((p011 - p001 - p010 + p000) * one_u + (p111 - p101 - p110 + p100) * uv) * (ihy * ihz);
+    }
     return true;
 }
 
@@ -322,12 +351,151 @@ __device__ __forceinline__ int chunk_scan(Shared& s, bool flag, int& total)
     return off + __popc(bal & ((1u << lane) - 1u));
 }
 
-// SDFContactEngine.evaluate for s.cur with the cache (F, tau into shared).
-template <bool W>
+// 3x3 helpers for the Jacobian (row-major).
+__device__ __forceinline__ void skew3(const double a[3], double S[9])
+{
+    S[0] = 0.0;
+    S[1] = -a[2];
+    S[2] = a[1];
+    S[3] = a[2];
+    S[4] = 0.0;
+    S[5] = -a[0];
+    S[6] = -a[1];
+    S[7] = a[0];
+    S[8] = 0.0;
+}
+
+__device__ __forceinline__ void mat3mul(const double A[9], const double B[9], double C[9])
+{
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            C[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
+}
+
+// Per-point derivatives of the force law (contacts_sdf.py:329-385) for the
+// exact tangent: Gt = d fq / d(material point displacement, world) at fixed
+// A velocities, U = d fq / d(relative velocity u).  Inputs as in eval_pass;
+// H3 = the SDF-frame mixed partials {xy, xz, yz}.
+__device__ void point_jacobian(const BeView& b, const double rg[3], const double H3[3], double g, double p,
+                               double gn, const double u[3], bool damp, bool fric, double phat, const double un[3],
+                               const double ut[3], double den, double Gt[9], double U[9])
+{
+    // world Hessian Hw = RB Hs RB^T
+    const double Hs[9] = {0.0, H3[0], H3[1], H3[0], 0.0, H3[2], H3[1], H3[2], 0.0};
+    double T[9], Hw[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            T[3 * i + j] = b.RB[3 * i] * Hs[j] + b.RB[3 * i + 1] * Hs[3 + j] + b.RB[3 * i + 2] * Hs[6 + j];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            Hw[3 * i + j] = T[3 * i] * b.RB[3 * j] + T[3 * i + 1] * b.RB[3 * j + 1] + T[3 * i + 2] * b.RB[3 * j + 2];
+    const double dl = -g;
+    const double pp = -b.c.stiffness * b.c.order *
+                      (b.c.order == 2.0 ? dl : b.c.order == 1.0 ? 1.0 : pow(dl, b.c.order - 1.0)); // dp/dg
+    const double vn = u[0] * rg[0] + u[1] * rg[1] + u[2] * rg[2];
+    const double udn = u[0] * un[0] + u[1] * un[1] + u[2] * un[2];
+    const double mu = b.c.friction, c = b.c.damping;
+    double ag[3], B[9];
+    for (int i = 0; i < 3; ++i)
+    {
+        ag[i] = pp * rg[i];
+        if (fric) ag[i] = ag[i] - mu * gn * pp * ut[i] / den;
+        for (int j = 0; j < 3; ++j)
+        {
+            const double I = i == j ? 1.0 : 0.0;
+            B[3 * i + j] = p * I;
+            if (damp) B[3 * i + j] = B[3 * i + j] - c * (rg[i] * u[j] + vn * I);
+            U[3 * i + j] = damp ? -c * rg[i] * rg[j] : 0.0;
+        }
+    }
+    if (fric)
+    {
+        // Mt = (I - ut ut^T / den^2) / den, P = I - un un^T
+        double Mt[9], P[9], Q[9], QP[9], MQ[9], MP[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+            {
+                const double I = i == j ? 1.0 : 0.0;
+                Mt[3 * i + j] = (I - ut[i] * ut[j] / (den * den)) / den;
+                P[3 * i + j] = I - un[i] * un[j];
+                Q[3 * i + j] = udn * I + un[i] * u[j];
+            }
+        mat3mul(Q, P, QP);
+        mat3mul(Mt, QP, MQ);
+        mat3mul(Mt, P, MP);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+            {
+                B[3 * i + j] = B[3 * i + j] - mu * p * ut[i] * un[j] / den + mu * p * MQ[3 * i + j];
+                U[3 * i + j] = U[3 * i + j] - mu * phat * MP[3 * i + j];
+            }
+    }
+    // G = ag rg^T + B Hw, Gt = G - U [wB]x
+    double BH[9], Wb[9], UW[9];
+    mat3mul(B, Hw, BH);
+    skew3(b.wB, Wb);
+    mat3mul(U, Wb, UW);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Gt[3 * i + j] = ag[i] * rg[j] + BH[3 * i + j] - UW[3 * i + j];
+}
+
+// Adds the point's weighted contributions to Jp and Jv into the warp's row
+// (every lane of the warp calls it; inactive lanes pass w = 0).  Column by
+// column: for each of the 12 columns the 6 entries are warp-summed and lane
+// 0 adds them to its row in chunk order.
+__device__ void add_point_jacobian(double* row, double w, const double Gt[9], const double U[9],
+                                   const double off[3], const double fq[3], const double wA[3])
+{
+    const int lane = (int)(threadIdx.x & 31);
+    double Ox[9], Wx[9], Fx[9], A[9], UW[9];
+    skew3(off, Ox);
+    skew3(wA, Wx);
+    skew3(fq, Fx);
+    // A = Gt + U [w]x, so that dfq/dtheta = -A [off]x
+    mat3mul(U, Wx, UW);
+    for (int k = 0; k < 9; ++k) A[k] = Gt[k] + UW[k];
+#pragma unroll 1
+    for (int col = 0; col < 12; ++col)
+    {
+        const int m = col / 6, cc = col % 6, c3 = cc % 3;
+        double f[3], t[3];
+        const double ox[3] = {Ox[c3], Ox[3 + c3], Ox[6 + c3]}; // column c3 of [off]x
+        if (m == 0 && cc < 3)
+            for (int i = 0; i < 3; ++i) f[i] = Gt[3 * i + c3];
+        else if (m == 0)
+            for (int i = 0; i < 3; ++i) f[i] = -(A[3 * i] * ox[0] + A[3 * i + 1] * ox[1] + A[3 * i + 2] * ox[2]);
+        else if (cc < 3)
+            for (int i = 0; i < 3; ++i) f[i] = U[3 * i + c3];
+        else
+            for (int i = 0; i < 3; ++i) f[i] = -(U[3 * i] * ox[0] + U[3 * i + 1] * ox[1] + U[3 * i + 2] * ox[2]);
+        for (int i = 0; i < 3; ++i) t[i] = Ox[3 * i] * f[0] + Ox[3 * i + 1] * f[1] + Ox[3 * i + 2] * f[2];
+        if (m == 0 && cc >= 3)
+            for (int i = 0; i < 3; ++i)
+                t[i] = t[i] + (Fx[3 * i] * ox[0] + Fx[3 * i + 1] * ox[1] + Fx[3 * i + 2] * ox[2]);
+        for (int i = 0; i < 3; ++i)
+        {
+            const double vf = warp_dsum(w * f[i]);
+            const double vt = warp_dsum(w * t[i]);
+            if (lane == 0)
+            {
+                row[36 * m + 6 * i + cc] += vf;
+                row[36 * m + 6 * (3 + i) + cc] += vt;
+            }
+        }
+    }
+}
+
+// SDFContactEngine.evaluate for s.cur with the cache (F, tau into shared);
+// JAC: also Jp and Jv (row 0 of s.jred) for the exact tangent.
+template <bool W, bool JAC>
 __device__ void eval_pass(const BeView& b, Shared& s)
 {
     broad_phase<W>(b, s);
     const double narrow = b.cull ? b.narrow : INFINITY;
+    const int warp = Grp<W>::warp(), lane = (int)(threadIdx.x & 31);
+    double* jrow = JAC ? s.jred + kJac * warp : nullptr;
+    if (JAC && lane == 0)
+        for (int e = 0; e < kJac; ++e) jrow[e] = 0.0;
     // the number of narrow-filtered points decides whether the cache is used
     int L = 0;
     for (int c0 = 0; c0 < b.nq; c0 += Grp<W>::size())
@@ -362,73 +530,90 @@ __device__ void eval_pass(const BeView& b, Shared& s)
             int total;
             const int pos = base + chunk_scan<W>(s, f, total);
             base += total;
-            if (!f) continue;
-            double g, gr[3];
-            bool valid;
-            const int64_t ci = base_c + pos;
-            if (use)
+            bool act = false;
+            double fq[3] = {0.0, 0.0, 0.0}, off[3] = {0.0, 0.0, 0.0};
+            double Gt[9], U[9];
+            if (f)
             {
-                const double dt3[3] = {tsdf[0] - s.c_tref[0], tsdf[1] - s.c_tref[1], tsdf[2] - s.c_tref[2]};
-                gr[0] = b.cgrad[3 * ci];
-                gr[1] = b.cgrad[3 * ci + 1];
-                gr[2] = b.cgrad[3 * ci + 2];
-                g = b.cg[ci] + (gr[0] * dt3[0] + gr[1] * dt3[1] + gr[2] * dt3[2]);
-                valid = b.cvalid[ci] != 0;
-            }
-            else
-            {
-                valid = sample64(b, Y, g, gr);
-                if (!valid)
+                double g, gr[3], H3[3] = {0.0, 0.0, 0.0};
+                bool valid;
+                const int64_t ci = base_c + pos;
+                if (use)
                 {
-                    g = 0.0;
-                    gr[0] = gr[1] = gr[2] = 0.0;
+                    const double dt3[3] = {tsdf[0] - s.c_tref[0], tsdf[1] - s.c_tref[1], tsdf[2] - s.c_tref[2]};
+                    gr[0] = b.cgrad[3 * ci];
+                    gr[1] = b.cgrad[3 * ci + 1];
+                    gr[2] = b.cgrad[3 * ci + 2];
+                    g = b.cg[ci] + (gr[0] * dt3[0] + gr[1] * dt3[1] + gr[2] * dt3[2]);
+                    valid = b.cvalid[ci] != 0;
                 }
-                if (store)
+                else
                 {
-                    b.cg[ci] = g;
-                    b.cgrad[3 * ci] = gr[0];
-                    b.cgrad[3 * ci + 1] = gr[1];
-                    b.cgrad[3 * ci + 2] = gr[2];
-                    b.cvalid[ci] = valid ? 1 : 0;
+                    valid = sample64(b, Y, g, gr, JAC ? H3 : nullptr);
+                    if (!valid)
+                    {
+                        g = 0.0;
+                        gr[0] = gr[1] = gr[2] = 0.0;
+                    }
+                    if (store)
+                    {
+                        b.cg[ci] = g;
+                        b.cgrad[3 * ci] = gr[0];
+                        b.cgrad[3 * ci + 1] = gr[1];
+                        b.cgrad[3 * ci + 2] = gr[2];
+                        b.cvalid[ci] = valid ? 1 : 0;
+                    }
+                }
+                const double delta = -g > 0.0 ? -g : 0.0;
+                const double p = b.c.stiffness *
+                                 (b.c.order == 2.0 ? delta * delta : b.c.order == 1.0 ? delta : pow(delta, b.c.order));
+                if (valid && p > 1e-30)
+                {
+                    act = true;
+                    // force law (contacts_sdf.py:329-385)
+                    double rg[3], xw[3], uA[3], uB[3], u[3], t3[3];
+                    matvec(b.RB, gr, rg);
+                    const double gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
+                    matvec(s.cur.R, X, off);
+                    for (int a = 0; a < 3; ++a) xw[a] = s.cur.r[a] + off[a];
+                    for (int a = 0; a < 3; ++a) fq[a] = p * rg[a];
+                    const double phat = p * gn;
+                    cross3(s.cur.w, off, t3);
+                    for (int a = 0; a < 3; ++a) uA[a] = s.cur.v[a] + t3[a];
+                    double offB[3] = {xw[0] - b.rB[0], xw[1] - b.rB[1], xw[2] - b.rB[2]};
+                    cross3(b.wB, offB, t3);
+                    for (int a = 0; a < 3; ++a) uB[a] = b.vB[a] + t3[a];
+                    for (int a = 0; a < 3; ++a) u[a] = uA[a] - uB[a];
+                    const bool damp = b.c.damping > 0.0 && g < 0.0;
+                    if (damp)
+                    {
+                        const double vn = u[0] * rg[0] + u[1] * rg[1] + u[2] * rg[2];
+                        for (int a = 0; a < 3; ++a) fq[a] = fq[a] + b.c.damping * (-vn) * rg[a];
+                    }
+                    const double gs = gn > 1e-30 ? gn : 1e-30;
+                    double un[3] = {rg[0] / gs, rg[1] / gs, rg[2] / gs};
+                    const double udn = u[0] * un[0] + u[1] * un[1] + u[2] * un[2];
+                    double ut[3] = {u[0] - udn * un[0], u[1] - udn * un[1], u[2] - udn * un[2]};
+                    const double utn = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
+                    const double den = sqrt(utn * utn + b.c.regularizer * b.c.regularizer);
+                    const bool fric = b.c.friction * phat > 0.0;
+                    if (fric)
+                        for (int a = 0; a < 3; ++a) fq[a] = fq[a] + -b.c.friction * phat * ut[a] / den;
+                    double tq[3];
+                    cross3(off, fq, tq);
+                    for (int a = 0; a < 3; ++a)
+                    {
+                        acc[a] += w * fq[a];
+                        acc[3 + a] += w * tq[a];
+                    }
+                    if (JAC) point_jacobian(b, rg, H3, g, p, gn, u, damp, fric, phat, un, ut, den, Gt, U);
                 }
             }
-            const double delta = -g > 0.0 ? -g : 0.0;
-            const double p = b.c.stiffness *
-                             (b.c.order == 2.0 ? delta * delta : b.c.order == 1.0 ? delta : pow(delta, b.c.order));
-            if (!(valid && p > 1e-30)) continue;
-            // force law (contacts_sdf.py:329-385)
-            double rg[3], off[3], xw[3], uA[3], uB[3], u[3], t3[3];
-            matvec(b.RB, gr, rg);
-            const double gn = sqrt(gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2]);
-            matvec(s.cur.R, X, off);
-            for (int a = 0; a < 3; ++a) xw[a] = s.cur.r[a] + off[a];
-            double fq[3] = {p * rg[0], p * rg[1], p * rg[2]};
-            const double phat = p * gn;
-            cross3(s.cur.w, off, t3);
-            for (int a = 0; a < 3; ++a) uA[a] = s.cur.v[a] + t3[a];
-            double offB[3] = {xw[0] - b.rB[0], xw[1] - b.rB[1], xw[2] - b.rB[2]};
-            cross3(b.wB, offB, t3);
-            for (int a = 0; a < 3; ++a) uB[a] = b.vB[a] + t3[a];
-            for (int a = 0; a < 3; ++a) u[a] = uA[a] - uB[a];
-            if (b.c.damping > 0.0 && g < 0.0)
+            if (JAC && __any_sync(0xffffffffu, act))
             {
-                const double vn = u[0] * rg[0] + u[1] * rg[1] + u[2] * rg[2];
-                for (int a = 0; a < 3; ++a) fq[a] = fq[a] + b.c.damping * (-vn) * rg[a];
-            }
-            const double gs = gn > 1e-30 ? gn : 1e-30;
-            double un[3] = {rg[0] / gs, rg[1] / gs, rg[2] / gs};
-            const double udn = u[0] * un[0] + u[1] * un[1] + u[2] * un[2];
-            double ut[3] = {u[0] - udn * un[0], u[1] - udn * un[1], u[2] - udn * un[2]};
-            const double utn = sqrt(ut[0] * ut[0] + ut[1] * ut[1] + ut[2] * ut[2]);
-            const double den = sqrt(utn * utn + b.c.regularizer * b.c.regularizer);
-            if (b.c.friction * phat > 0.0)
-                for (int a = 0; a < 3; ++a) fq[a] = fq[a] + -b.c.friction * phat * ut[a] / den;
-            double tq[3];
-            cross3(off, fq, tq);
-            for (int a = 0; a < 3; ++a)
-            {
-                acc[a] += w * fq[a];
-                acc[3 + a] += w * tq[a];
+                if (!act)
+                    for (int k = 0; k < 9; ++k) Gt[k] = U[k] = 0.0;
+                add_point_jacobian(jrow, act ? w : 0.0, Gt, U, off, fq, s.cur.w);
             }
         }
         if (Grp<W>::rank() == 0 && store)
@@ -438,7 +623,6 @@ __device__ void eval_pass(const BeView& b, Shared& s)
             s.c_cleared = 0;
         }
     }
-    const int warp = Grp<W>::warp(), lane = (int)(threadIdx.x & 31);
     for (int q = 0; q < 6; ++q)
     {
         const double v = warp_dsum(acc[q]);
@@ -456,6 +640,9 @@ __device__ void eval_pass(const BeView& b, Shared& s)
             else
                 s.tau[q - 3] = v;
         }
+        if (JAC)
+            for (int wp = 1; wp < Grp<W>::warps(); ++wp)
+                for (int e = 0; e < kJac; ++e) s.jred[e] += s.jred[kJac * wp + e];
     }
     Grp<W>::sync();
 }
@@ -582,13 +769,18 @@ __device__ void kinematic(const Body& q0, const double V[6], double dt, Body& ou
     out.t = q0.t;
 }
 
-// _residual at V = z (implicit_be.py:536-604): s.res, s.err, s.Iw, s.cur.
-template <bool W>
+// _residual at V = z (implicit_be.py:536-604): s.res, s.err, s.Iw, s.cur;
+// JAC: also the contact Jacobians of the exact tangent (s.jred).
+template <bool W, bool JAC>
 __device__ void residual(const BeView& b, Shared& s, const double* z, double dt, bool allowed)
 {
-    if (Grp<W>::rank() == 0) kinematic(s.q0, z, dt, s.cur);
+    if (Grp<W>::rank() == 0)
+    {
+        kinematic(s.q0, z, dt, s.cur);
+        s.n_resid += 1;
+    }
     Grp<W>::sync();
-    if (allowed) eval_pass<W>(b, s);
+    if (allowed) eval_pass<W, JAC>(b, s);
     if (Grp<W>::rank() == 0)
     {
         double RI[9];
@@ -629,9 +821,119 @@ __device__ void residual(const BeView& b, Shared& s, const double* z, double dt,
     Grp<W>::sync();
 }
 
+// Left Jacobian of SO(3): exp(phi + d) = exp([J_l(phi) d]x) exp(phi) + O(d^2).
+__device__ void left_jacobian(const double phi[3], double J[9])
+{
+    const double t = sqrt(phi[0] * phi[0] + phi[1] * phi[1] + phi[2] * phi[2]);
+    double a, c;
+    if (t < 1e-4)
+    {
+        a = 0.5 - t * t / 24.0;
+        c = 1.0 / 6.0 - t * t / 120.0;
+    }
+    else
+    {
+        a = (1.0 - cos(t)) / (t * t);
+        c = (t - sin(t)) / (t * t * t);
+    }
+    double S[9], S2[9];
+    skew3(phi, S);
+    mat3mul(S, S, S2);
+    for (int k = 0; k < 9; ++k) J[k] = (k % 4 == 0 ? 1.0 : 0.0) + a * S[k] + c * S2[k];
+}
+
+// The exact tangent dR/dV at the state of the last residual (s.cur, s.Iw,
+// s.jred) and the Newton step s.dz = -K^-1 res; thread 0.  Returns false
+// when K is singular (no usable pivot).
+__device__ bool exact_newton_step(const BeView& b, Shared& s, double dt, bool allowed)
+{
+    double K[36];
+    for (int k = 0; k < 36; ++k) K[k] = 0.0;
+    for (int a = 0; a < 3; ++a) K[7 * a] = b.mass / dt;
+    const double* w = s.cur.w;
+    double dw[3] = {w[0] - s.q0.w[0], w[1] - s.q0.w[1], w[2] - s.q0.w[2]};
+    const double phi[3] = {dt * w[0], dt * w[1], dt * w[2]};
+    double Jl[9], Iw_dw[3], Iw_w[3], S1[9], S2[9], S3[9], S4[9], A1[9], A2[9], A3[9], T1[9], T3[9];
+    left_jacobian(phi, Jl);
+    matvec(s.Iw, dw, Iw_dw);
+    matvec(s.Iw, w, Iw_w);
+    // A1 = -[Iw dw]x + Iw [dw]x (inertia term through R(w))
+    skew3(Iw_dw, S1);
+    skew3(dw, S2);
+    mat3mul(s.Iw, S2, T1);
+    for (int k = 0; k < 9; ++k) A1[k] = -S1[k] + T1[k];
+    // A2 = -[Iw w]x + [w]x Iw (gyroscopic term, explicit w)
+    skew3(Iw_w, S3);
+    skew3(w, S4);
+    mat3mul(S4, s.Iw, T1);
+    for (int k = 0; k < 9; ++k) A2[k] = -S3[k] + T1[k];
+    // A3 = h [w]x (-[Iw w]x + Iw [w]x) (gyroscopic term through R(w))
+    mat3mul(s.Iw, S4, T1);
+    for (int k = 0; k < 9; ++k) T1[k] = -S3[k] + T1[k];
+    mat3mul(S4, T1, T3);
+    for (int k = 0; k < 9; ++k) A3[k] = dt * T3[k];
+    double B[9];
+    for (int k = 0; k < 9; ++k) B[k] = A1[k] + A3[k];
+    mat3mul(B, Jl, T1);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) K[6 * (3 + i) + 3 + j] = s.Iw[3 * i + j] / dt + T1[3 * i + j] + A2[3 * i + j];
+    if (allowed)
+    {
+        // K -= Jv + Jp diag(h I, h J_l)
+        const double* Jp = s.jred;
+        const double* Jv = s.jred + 36;
+        for (int i = 0; i < 6; ++i)
+        {
+            for (int j = 0; j < 3; ++j) K[6 * i + j] = K[6 * i + j] - (Jv[6 * i + j] + dt * Jp[6 * i + j]);
+            for (int j = 0; j < 3; ++j)
+            {
+                const double jr = Jp[6 * i + 3] * Jl[j] + Jp[6 * i + 4] * Jl[3 + j] + Jp[6 * i + 5] * Jl[6 + j];
+                K[6 * i + 3 + j] = K[6 * i + 3 + j] - (Jv[6 * i + 3 + j] + dt * jr);
+            }
+        }
+    }
+    // Gaussian elimination with partial pivoting on [K | -res]
+    double x[6];
+    for (int a = 0; a < 6; ++a) x[a] = -s.res[a];
+    for (int c = 0; c < 6; ++c)
+    {
+        int piv = c;
+        for (int r = c + 1; r < 6; ++r)
+            if (fabs(K[6 * r + c]) > fabs(K[6 * piv + c])) piv = r;
+        if (!(fabs(K[6 * piv + c]) > 0.0)) return false;
+        if (piv != c)
+        {
+            for (int j = 0; j < 6; ++j)
+            {
+                const double t = K[6 * c + j];
+                K[6 * c + j] = K[6 * piv + j];
+                K[6 * piv + j] = t;
+            }
+            const double t = x[c];
+            x[c] = x[piv];
+            x[piv] = t;
+        }
+        for (int r = c + 1; r < 6; ++r)
+        {
+            const double f = K[6 * r + c] / K[6 * c + c];
+            for (int j = c; j < 6; ++j) K[6 * r + j] = K[6 * r + j] - f * K[6 * c + j];
+            x[r] = x[r] - f * x[c];
+        }
+    }
+    for (int c = 5; c >= 0; --c)
+    {
+        double v = x[c];
+        for (int j = c + 1; j < 6; ++j) v = v - K[6 * c + j] * x[j];
+        x[c] = v / K[6 * c + c];
+    }
+    for (int a = 0; a < 6; ++a) s.dz[a] = x[a];
+    return true;
+}
+
 // _step_be (implicit_be.py:468-505): src -> dst (thread-0 copies), contact
-// forces of the pair when `allowed`.
-template <bool W>
+// forces of the pair when `allowed`.  EXACT: exact contact every residual
+// and the analytic tangent (see the file comment).
+template <bool W, bool EXACT>
 __device__ void step_be(const BeView& b, Shared& s, const Body* src, Body* dst, double dt, bool allowed)
 {
     if (Grp<W>::rank() == 0)
@@ -642,16 +944,29 @@ __device__ void step_be(const BeView& b, Shared& s, const Body* src, Body* dst, 
             s.z[a] = src->v[a];
             s.z[3 + a] = src->w[a];
         }
-        s.c_enabled = allowed ? 1 : 0;
+        s.c_enabled = (allowed && !EXACT) ? 1 : 0;
         s.c_cleared = 1;
+        s.n_solves += 1;
     }
     Grp<W>::sync();
-    residual<W>(b, s, s.z, dt, allowed);
+    residual<W, EXACT>(b, s, s.z, dt, allowed);
     for (int it = 0; it < b.p.max_iter; ++it)
     {
         if (s.err < b.p.tol) break;
-        if (Grp<W>::rank() == 0)
+        if (Grp<W>::rank() == 0 && EXACT)
         {
+            s.n_newton += 1;
+            if (!exact_newton_step(b, s, dt, allowed))
+                for (int a = 0; a < 6; ++a) s.dz[a] = 0.0;
+            double nr = 0.0;
+            for (int a = 0; a < 6; ++a) nr += s.res[a] * s.res[a];
+            s.r0 = sqrt(nr);
+            s.found = 0;
+            s.alpha = 1.0;
+        }
+        else if (Grp<W>::rank() == 0)
+        {
+            s.n_newton += 1;
             // tangent (_tangent / _contact_tangent): M/h + diag(Kc) on the
             // translational rows; the two diagonal blocks solved exactly
             double ktt = b.mass / dt;
@@ -697,7 +1012,7 @@ __device__ void step_be(const BeView& b, Shared& s, const Body* src, Body* dst, 
             {
                 if (Grp<W>::rank() < 6) s.zt[Grp<W>::rank()] = s.z[Grp<W>::rank()] + alphas[k] * s.dz[Grp<W>::rank()];
                 Grp<W>::sync();
-                residual<W>(b, s, s.zt, dt, allowed);
+                residual<W, false>(b, s, s.zt, dt, allowed);
                 if (Grp<W>::rank() == 0)
                 {
                     double nr = 0.0;
@@ -718,7 +1033,7 @@ __device__ void step_be(const BeView& b, Shared& s, const Body* src, Body* dst, 
             for (int a = 0; a < 6; ++a) s.z[a] = s.z[a] + alpha * s.dz[a];
         }
         Grp<W>::sync();
-        residual<W>(b, s, s.z, dt, allowed);
+        residual<W, EXACT>(b, s, s.z, dt, allowed);
     }
     if (Grp<W>::rank() == 0)
     {
@@ -797,21 +1112,31 @@ __device__ void refresh(const BeView& b, Shared& s)
     }
 }
 
+// Dynamic shared memory of the exact-tangent kernels: T / 32 rows of kJac.
+template <int T>
+constexpr int jac_smem_bytes() { return (T / 32) * kJac * (int)sizeof(double); }
+
 // T threads per CTA; W: one warp per scene (T / 32 scenes per CTA), else
 // the whole CTA on one scene.
-template <int T, bool W>
+template <int T, bool W, bool EXACT>
 __global__ void __launch_bounds__(T, (W || T == 256) ? 3 : 4) k_be_step(BeView b, sdfo_be_scene* __restrict__ scenes, int n,
                                                 const double* __restrict__ dt_req, double* __restrict__ h_out,
                                                 const double* __restrict__ t_end, double dt_max,
                                                 int* __restrict__ unfinished)
 {
     __shared__ Shared shared_scenes[W ? T / 32 : 1];
+    // exact tangent: one row of Jacobian partial sums per warp, in dynamic
+    // shared memory (jac_smem_bytes<T>(); the warp-per-scene variant's static
+    // state alone nearly fills the 48 KB static limit)
+    extern __shared__ double jred_rows[];
     const int sc = W ? (int)(blockIdx.x * (T / 32) + (threadIdx.x >> 5)) : (int)blockIdx.x;
     if (sc >= n) return; // (warps) whole warps past the last scene
     Shared& s = shared_scenes[W ? (threadIdx.x >> 5) : 0];
     const sdfo_be_params& p = b.p;
     if (Grp<W>::rank() == 0)
     {
+        s.jred = EXACT ? jred_rows + (W ? (int)(threadIdx.x >> 5) * kJac : 0) : nullptr;
+        s.n_newton = s.n_resid = s.n_solves = 0;
         s.scene = sc;
         const sdfo_be_scene& in = scenes[sc];
         for (int a = 0; a < 3; ++a)
@@ -865,7 +1190,7 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 3 : 4) k_be_step(BeView b
     // _find_earliest_new_contact
     if (s.phase == kInactive && h_cap > 0.0)
     {
-        step_be<W>(b, s, &s.q, &s.tr, h_cap, false);
+        step_be<W, EXACT>(b, s, &s.q, &s.tr, h_cap, false);
         measure_body<W>(b, s, s.tr);
         if (Grp<W>::rank() == 0)
             s.flag = (s.m0_gap > 0.0 && (s.m_gap <= 0.0 || s.m_pen > p.pen_max)) ? 1 : 0;
@@ -887,7 +1212,7 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 3 : 4) k_be_step(BeView b
                 Grp<W>::sync();
                 if (s.hit) break;
                 const double mid = 0.5 * (s.lo + s.hi);
-                step_be<W>(b, s, &s.q, &s.tr, mid, false);
+                step_be<W, EXACT>(b, s, &s.q, &s.tr, mid, false);
                 measure_body<W>(b, s, s.tr);
                 if (Grp<W>::rank() == 0)
                 {
@@ -909,7 +1234,7 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 3 : 4) k_be_step(BeView b
                     s.hit = 1;
                 }
                 Grp<W>::sync();
-                step_be<W>(b, s, &s.q, &s.tr, s.hi, false);
+                step_be<W, EXACT>(b, s, &s.q, &s.tr, s.hi, false);
                 measure_body<W>(b, s, s.tr);
                 if (Grp<W>::rank() == 0) s.hm_pen = s.m_pen;
                 Grp<W>::sync();
@@ -931,7 +1256,7 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 3 : 4) k_be_step(BeView b
     if (s.event)
     {
         h = s.toi;
-        step_be<W>(b, s, &s.q, &s.q, h, region_active(s.phase));
+        step_be<W, EXACT>(b, s, &s.q, &s.q, h, region_active(s.phase));
         if (Grp<W>::rank() == 0)
         {
             s.phase = kImpacting;
@@ -951,7 +1276,7 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 3 : 4) k_be_step(BeView b
     else
     {
         h = h_cap;
-        step_be<W>(b, s, &s.q, &s.q, h, region_active(s.phase));
+        step_be<W, EXACT>(b, s, &s.q, &s.q, h, region_active(s.phase));
         measure_body<W>(b, s, s.q);
         if (Grp<W>::rank() == 0) refresh(b, s);
     }
@@ -961,7 +1286,7 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 3 : 4) k_be_step(BeView b
         // the integrate loop's zero-progress fail-safe (implicit_be.py:124-127):
         // one plain BE step of min(dt_min, t_end - t), nothing re-measured
         h = fmin(p.dt_min, t_end[sc] - s.q.t);
-        step_be<W>(b, s, &s.q, &s.q, h, region_active(s.phase));
+        step_be<W, EXACT>(b, s, &s.q, &s.q, h, region_active(s.phase));
         Grp<W>::sync();
     }
     if (Grp<W>::rank() == 0)
@@ -986,6 +1311,12 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 3 : 4) k_be_step(BeView b
         out.min_dt_hits = s.min_dt_hits;
         if (h_out) h_out[sc] = h;
         if (unfinished && s.q.t < t_end[sc] - 1e-15) atomicAdd(unfinished, 1);
+        if (b.stats)
+        {
+            atomicAdd(b.stats, (unsigned long long)s.n_newton);
+            atomicAdd(b.stats + 1, (unsigned long long)s.n_resid);
+            atomicAdd(b.stats + 2, (unsigned long long)s.n_solves);
+        }
     }
 }
 
@@ -1031,6 +1362,7 @@ struct sdfo_be_stepper
         sdfo::device_free(view.cg);
         sdfo::device_free(view.cgrad);
         sdfo::device_free(view.cvalid);
+        sdfo::device_free(view.stats);
     }
 };
 
@@ -1040,13 +1372,25 @@ namespace {
 void launch_step(const sdfo_be_stepper* st, sdfo_be_scene* scenes, int64_t n, const double* dt, double* h,
                  const double* t_end, double dt_max, int* unfinished, cudaStream_t s)
 {
-    if (st->threads == 32)
-        k_be_step<256, true><<<(unsigned)((n + 7) / 8), 256, 0, s>>>(st->view, scenes, (int)n, dt, h, t_end, dt_max,
-                                                                      unfinished);
-    else if (st->threads == 128)
-        k_be_step<128, false><<<(unsigned)n, 128, 0, s>>>(st->view, scenes, (int)n, dt, h, t_end, dt_max, unfinished);
+#define SDFO_BE_LAUNCH(EX)                                                                                  \
+    if (st->threads == 32)                                                                                  \
+        k_be_step<256, true, EX><<<(unsigned)((n + 7) / 8), 256, EX ? jac_smem_bytes<256>() : 0, s>>>(     \
+            st->view, scenes, (int)n, dt, h, t_end, dt_max, unfinished);                                    \
+    else if (st->threads == 128)                                                                            \
+        k_be_step<128, false, EX><<<(unsigned)n, 128, EX ? jac_smem_bytes<128>() : 0, s>>>(                 \
+            st->view, scenes, (int)n, dt, h, t_end, dt_max, unfinished);                                    \
+    else                                                                                                    \
+        k_be_step<256, false, EX><<<(unsigned)n, 256, EX ? jac_smem_bytes<256>() : 0, s>>>(                 \
+            st->view, scenes, (int)n, dt, h, t_end, dt_max, unfinished);
+    if (st->view.p.tangent == SDFO_BE_TANGENT_EXACT)
+    {
+        SDFO_BE_LAUNCH(true)
+    }
     else
-        k_be_step<256, false><<<(unsigned)n, 256, 0, s>>>(st->view, scenes, (int)n, dt, h, t_end, dt_max, unfinished);
+    {
+        SDFO_BE_LAUNCH(false)
+    }
+#undef SDFO_BE_LAUNCH
     SDFO_CHECK_LAUNCH();
 }
 
@@ -1119,7 +1463,7 @@ void sdfo_be_params_default(sdfo_be_params* p)
     p->max_toi_bisect_iter = 60;
     p->stable_steps = 5;
     p->release_steps = 3;
-    p->reserved0 = 0;
+    p->tangent = SDFO_BE_TANGENT_REFERENCE;
     p->tol = 1e-8;
     p->pen_max = 1e-6;
     p->dt_min = 1e-8;
@@ -1158,6 +1502,8 @@ int sdfo_be_stepper_create(const sdfo_contact_pair* pair, const sdfo_contact_par
         SDFO_REQUIRE(params->max_iter >= 0 && params->max_toi_bisect_iter >= 0, SDFO_ERR_INVALID_ARGUMENT,
                      "negative iteration count");
         SDFO_REQUIRE(body_a->mass > 0.0, SDFO_ERR_INVALID_ARGUMENT, "body mass must be positive");
+        SDFO_REQUIRE(params->tangent == SDFO_BE_TANGENT_REFERENCE || params->tangent == SDFO_BE_TANGENT_EXACT,
+                     SDFO_ERR_INVALID_ARGUMENT, "unknown tangent mode");
         std::unique_ptr<sdfo_be_stepper> st(new sdfo_be_stepper());
         st->pair = pair;
         BeView& b = st->view;
@@ -1206,6 +1552,18 @@ int sdfo_be_stepper_create(const sdfo_contact_pair* pair, const sdfo_contact_par
         b.cg = dalloc<double>(slots);
         b.cgrad = dalloc<double>(3 * slots);
         b.cvalid = dalloc<unsigned char>(slots);
+        if (params->tangent == SDFO_BE_TANGENT_EXACT)
+        {
+            // static + dynamic shared memory above 48 KB needs the opt-in
+            SDFO_CUDA(cudaFuncSetAttribute(k_be_step<256, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           jac_smem_bytes<256>()));
+            SDFO_CUDA(cudaFuncSetAttribute(k_be_step<256, false, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, jac_smem_bytes<256>()));
+            SDFO_CUDA(cudaFuncSetAttribute(k_be_step<128, false, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, jac_smem_bytes<128>()));
+        }
+        b.stats = dalloc<unsigned long long>(3);
+        SDFO_CUDA(cudaMemset(b.stats, 0, 3 * sizeof(unsigned long long)));
         *out = st.release();
     });
 }
@@ -1284,6 +1642,18 @@ int sdfo_be_stepper_set_threads(sdfo_be_stepper* st, int32_t threads)
         SDFO_REQUIRE(threads == 32 || threads == 128 || threads == 256, SDFO_ERR_INVALID_ARGUMENT,
                      "threads per scene must be 32, 128 or 256");
         st->threads = threads;
+    });
+}
+
+int sdfo_be_stepper_stats(sdfo_be_stepper* st, uint64_t* out, int32_t reset)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(st != nullptr && out != nullptr, SDFO_ERR_INVALID_ARGUMENT, "NULL argument");
+        unsigned long long v[3] = {0, 0, 0};
+        SDFO_CUDA(cudaDeviceSynchronize());
+        SDFO_CUDA(cudaMemcpy(v, st->view.stats, sizeof(v), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < 3; ++k) out[k] = (uint64_t)v[k];
+        if (reset) SDFO_CUDA(cudaMemset(st->view.stats, 0, sizeof(v)));
     });
 }
 

@@ -20,6 +20,7 @@ FIRST_ORDER, SECOND_ORDER, TRILINEAR, TRICUBIC, CONTACT_AWARE = 0, 1, 2, 3, 4
 LAYOUT_DENSE, LAYOUT_SPARSE = 1, 2
 STORAGE_FP32, STORAGE_FP16 = 0, 1
 BVH_REFERENCE, BVH_LBVH = 0, 1
+BE_TANGENT_REFERENCE, BE_TANGENT_EXACT = 0, 1
 
 MODE_NAMES = {"first_order": FIRST_ORDER, "second_order": SECOND_ORDER,
               "trilinear": TRILINEAR, "tricubic": TRICUBIC, "contact_aware": CONTACT_AWARE,
@@ -77,7 +78,7 @@ class ContactParams(ctypes.Structure):
 
 class BEParams(ctypes.Structure):
     _fields_ = [("max_iter", _I32), ("line_search", _I32), ("max_toi_bisect_iter", _I32),
-                ("stable_steps", _I32), ("release_steps", _I32), ("reserved0", _I32),
+                ("stable_steps", _I32), ("release_steps", _I32), ("tangent", _I32),
                 ("tol", _D), ("pen_max", _D), ("dt_min", _D), ("dt_impact", _D),
                 ("dt_contact", _D), ("dt_max_contact", _D), ("dt_normal", _D), ("dt_growth", _D)]
 
@@ -166,6 +167,7 @@ SIGNATURES = [
     ("sdfo_be_stepper_advance", ctypes.c_int, [_P, _P, _I64, _P, ctypes.c_double, _I32, _P, _P]),
     ("sdfo_be_stepper_integrate", ctypes.c_int,
      [_P, _P, _I64, _P, ctypes.c_double, _I32, _I64, _P, _P, _P]),
+    ("sdfo_be_stepper_stats", ctypes.c_int, [_P, _P, _I32]),
     ("sdfo_be_stepper_destroy", ctypes.c_int, [_P]),
     ("sdfo_grid_load_file", ctypes.c_int, [ctypes.c_char_p, _I32, _P, _P]),
     ("sdfo_grid_save_file", ctypes.c_int, [_P, ctypes.c_char_p, _P]),

@@ -33,11 +33,18 @@ PHASE_NAMES = {0: "INACTIVE", 1: "APPROACHING", 2: "IMPACTING", 3: "ACTIVE", 4: 
                5: "LEAVING"}
 
 
+TANGENTS = {"reference": N.BE_TANGENT_REFERENCE, "exact": N.BE_TANGENT_EXACT}
+
+
 def default_params(**overrides) -> N.BEParams:
     """BackwardEulerIntegrator's defaults (implicit_be.py:60-107), with
-    keyword overrides by field name (max_iter, tol, pen_max, dt_min, ...)."""
+    keyword overrides by field name (max_iter, tol, pen_max, dt_min, ...).
+    tangent: "reference" (the reference's linearisation cache and diagonal
+    tangent) or "exact" (exact contact every residual, analytic dR/dV)."""
     p = N.BEParams()
     N.load().sdfo_be_params_default(ctypes.byref(p))
+    if isinstance(overrides.get("tangent"), str):
+        overrides["tangent"] = TANGENTS[overrides["tangent"]]
     for k, v in overrides.items():
         if not hasattr(p, k):
             raise ValueError(f"unknown BE parameter {k!r}")
@@ -185,6 +192,14 @@ class BEStepper:
         if left.value:
             raise RuntimeError(f"{left.value} scenes short of their end time after {made.value} launches")
         return made.value
+
+    def stats(self, reset=False) -> dict:
+        """Newton iterations, residual evaluations and BE solves of every
+        launch since creation or the last reset (synchronises the device)."""
+        out = (ctypes.c_uint64 * 3)()
+        N.check(N.load().sdfo_be_stepper_stats(self._h, out, 1 if reset else 0))
+        return {"newton_iterations": int(out[0]), "residual_evaluations": int(out[1]),
+                "be_solves": int(out[2])}
 
     @staticmethod
     def _check(scenes):

@@ -321,3 +321,120 @@ def test_gpu_threads_per_scene_agree(cuda):
     for k in (1, 2):
         assert np.array_equal(outs[0][0], outs[k][0])
         assert _close(outs[0][1], outs[k][1], 1e-12, atol=1e-18)
+
+
+def _port_scene_exact(d, name):
+    from oracle import interp_np
+
+    sc = _port_scene(d, name)
+    spec = dict(bmin=d["bmin"], voxel=d["voxel"], shape=tuple(d["shape"]))
+    sc.hess_batch = lambda Y: interp_np.trilinear_hessian(spec, d["phi"], Y)
+    return sc
+
+
+def _stepper_exact(d, name, max_scenes):
+    from sdfo import SdfGrid
+    from sdfo.be import BEStepper, default_params
+
+    a = _scene_args(d, name)
+    spec = dict(bmin=d["bmin"], bmax=d["bmax"], voxel=d["voxel"], shape=tuple(d["shape"]))
+    grid = SdfGrid.from_dense(spec, d["phi"], d["normal"])
+    st = BEStepper(grid, d["quad_x"], d["quad_w"], a["mass"], a["inertia"], a["k"], order=a["order"],
+                   damping=a["damping"], friction=a["mu"], regularizer=a["reg"],
+                   activation_distance=1e-5, narrow_margin=0.01, max_scenes=max_scenes,
+                   params=default_params(tangent="exact"))
+    return grid, st
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", SCENES)
+def test_gpu_exact_tangent_steps_match_port(cuda, name):
+    """Exact-tangent mode (exact contact every residual, analytic dR/dV):
+    every recorded state of the prototype stepped once on the GPU, all as
+    scenes of one launch, against the restatement's exact Newton from the
+    same state: the step taken and the phase and counters exactly, body
+    state and region measurements within 1e-9 relative; the GPU's Newton
+    iteration count equals the restatement's."""
+    import torch
+
+    from oracle import be_port as P
+
+    d = golden("be_steps.npz")
+    a = d[name]
+    grid, st = _stepper_exact(d, name, max_scenes=len(a))
+    scenes = _rows_to_scenes(st, a[:-1])
+    st.stats(reset=True)
+    h = st.step(scenes, 1e-3)
+    torch.cuda.synchronize()
+    stats = st.stats()
+    out = _scenes_to_rows(st, scenes)
+    h = h.cpu().numpy()
+    sc = _port_scene_exact(d, name)
+    iters = 0
+    for k in range(len(a) - 1):
+        integ = P.Integrator(sc, P.Params(tangent="exact"))
+        s = _load_row(integ, a[k])
+        hk = integ.step(s, 1e-3)
+        iters += integ.newton_iterations
+        ref = _row_of(s, integ.region)
+        assert abs(h[k] - hk) <= 1e-12 * hk, (k, h[k], hk)
+        assert out[k][19] == ref[19] and np.all(out[k][21:24] == ref[21:24]), (k, out[k][19:24], ref[19:24])
+        assert _close(out[k], ref, 1e-9), (k, out[k] - ref)
+    assert stats["newton_iterations"] == iters
+    assert stats["be_solves"] >= len(a) - 1
+
+
+@pytest.mark.gpu
+def test_gpu_exact_tangent_trajectories_and_iterations(cuda):
+    """Eight random drops per contact law advanced 60 steps in both tangent
+    modes: the exact mode's trajectories against the restatement's exact
+    Newton (steps and phases equal, states within 1e-7 relative) with no
+    more Newton iterations than the reference mode; the three thread
+    layouts give the same exact-mode states (to the last bits: they sum
+    the points in different orders)."""
+    import torch
+
+    from oracle import be_port as P
+
+    d = golden("be_steps.npz")
+    rng = np.random.default_rng(11)
+    for name in SCENES:
+        r = np.zeros((8, 3))
+        R = np.zeros((8, 3, 3))
+        for i in range(8):
+            ax = rng.normal(size=3)
+            ax /= np.linalg.norm(ax)
+            ang = rng.uniform(0, 0.4)
+            K = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+            R[i] = np.eye(3) + np.sin(ang) * K + (1 - np.cos(ang)) * K @ K
+            r[i] = [rng.uniform(-0.05, 0.05), rng.uniform(-0.05, 0.05),
+                    -(R[i] @ d["quad_x"].T)[2].min() + rng.uniform(0.0005, 0.003)]
+        v = np.column_stack([rng.normal(size=(8, 2)) * 0.05, -rng.uniform(0.05, 0.3, 8)])
+        w = rng.normal(size=(8, 3)) * 0.5
+        runs = {}
+        for mode, threads in (("exact", 256), ("exact", 128), ("exact", 32), ("reference", 256)):
+            grid, st = (_stepper_exact(d, name, 8) if mode == "exact" else _stepper(d, name, 8))
+            from sdfo import _native as N
+
+            N.check(N.load().sdfo_be_stepper_set_threads(st._h, threads))
+            scenes = st.scenes(r, R, v, w)
+            hs = [st.step(scenes, 1e-3).cpu().numpy() for _ in range(60)]
+            torch.cuda.synchronize()
+            runs[(mode, threads)] = (_scenes_to_rows(st, scenes), hs, st.stats())
+        ex, hs_ex, stats_ex = runs[("exact", 256)]
+        for t in (128, 32):
+            # the layouts sum the points in different orders: last bits only
+            assert np.array_equal(runs[("exact", t)][0][:, 19], ex[:, 19]), t
+            assert all(_close(runs[("exact", t)][0][i][:19], ex[i][:19], 1e-9) for i in range(8)), t
+        rf, _, stats_rf = runs[("reference", 256)]
+        assert stats_ex["newton_iterations"] <= stats_rf["newton_iterations"], (stats_ex, stats_rf)
+        sc = _port_scene_exact(d, name)
+        for i in range(8):
+            integ = P.Integrator(sc, P.Params(tangent="exact"))
+            s = P.BodyState(r[i].copy(), R[i].copy(), v[i].copy(), w[i].copy(), 0.0)
+            for k in range(60):
+                h = integ.step(s, 1e-3)
+                assert abs(h - hs_ex[k][i]) <= 1e-9 * h, (name, i, k, h, hs_ex[k][i])
+            ref = _row_of(s, integ.region)
+            assert ex[i][19] == ref[19], (name, i)
+            assert _close(ex[i][:19], ref[:19], 1e-7), (name, i, ex[i][:19] - ref[:19])
