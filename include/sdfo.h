@@ -71,6 +71,18 @@ extern "C" {
                                 index, so witness/normal at such ties and the
                                 face-normal sign fallback may differ */
 
+/* Inside/outside sign rule of the builders. */
+#define SDFO_SIGN_RAY_PARITY 0   /* the reference's: parity of the hits of one
+                                    fixed ray, the nearest triangle's face
+                                    normal when it hits nothing
+                                    (KdTree.h:143-165, 330-441) */
+#define SDFO_SIGN_PSEUDONORMAL 1 /* angle-weighted pseudo-normal of the
+                                    closest point's feature (vertex, edge or
+                                    face); needs a closed, consistently
+                                    oriented mesh; no parity ray; the sign
+                                    does not depend on which of several
+                                    equidistant triangles is kept */
+
 /* Point precision for query inputs. */
 #define SDFO_POINTS_F32 0
 #define SDFO_POINTS_F64 1
@@ -240,10 +252,17 @@ int sdfo_debug_wait_test(uint32_t wait_limit, int32_t withhold_first_tile);
  * keyed by GPU and workload shape. */
 typedef struct
 {
-    int32_t host_chunk_queries; /* sdfo_query_host with pinned buffers: queries per
-                                   pipelined chunk (rounded up to 256; default
-                                   131072); one chunk = no pipelining */
+    int32_t host_chunk_queries; /* sdfo_query_host with pinned buffers: queries of the
+                                   first pipelined chunk (rounded up to 256;
+                                   default 32768); n <= this: no pipelining */
     int32_t fill_ctas_per_sm;   /* batched brick fill: CTAs per SM (0 = as many as fit) */
+    int32_t fill_tile_log2_x;   /* dense fill: voxel tile of a 256-thread CTA is */
+    int32_t fill_tile_log2_y;   /* 2^x by 2^y by 256/2^(x+y), x fastest (0 = 3: 8x8x4) */
+    int32_t lbvh_traversal;     /* SDFO_BVH_LBVH traversals: 1 = per-thread stack,
+                                   2 = stackless (parent links); 0 = default (1);
+                                   same results and work either way */
+    int32_t host_chunk_growth_pct; /* each next pipelined chunk is this percent of
+                                      the previous (100..400; 0 = default 130) */
 } sdfo_tuning;
 int sdfo_set_tuning(const sdfo_tuning* t);
 int sdfo_get_tuning(sdfo_tuning* t);
@@ -322,6 +341,9 @@ typedef struct
     int64_t nearest_triangles; /* closest-point tests */
     int64_t ray_nodes;         /* ray-box tests */
     int64_t ray_triangles;     /* ray-triangle tests */
+    int64_t nearest_triangles_exact; /* closest-point tests run in FP64: those
+                                        not skipped by the conservative FP32
+                                        triangle-box cull (reference-order tree) */
 } sdfo_traversal_stats;
 int sdfo_build_traversal_stats(const double* h_verts, int64_t nv, const int32_t* h_tris, int64_t nt,
                                const sdfo_build_params* p, void* stream, sdfo_traversal_stats* out);
@@ -331,6 +353,14 @@ int sdfo_build_traversal_stats(const double* h_verts, int64_t nv, const int32_t*
  * only its own tree. */
 int sdfo_set_bvh_mode(int32_t mode);
 int sdfo_get_bvh_mode(void);
+
+/* Selects the sign rule of subsequent builds (process-wide; default
+ * SDFO_SIGN_RAY_PARITY, the reference's).  SDFO_SIGN_PSEUDONORMAL has no
+ * reference counterpart: distances, closest points and the sparse block set
+ * are unchanged; only the sign rule differs.  The per-triangle pseudo-normals
+ * are computed on the host at each build (an edge hash map: O(triangles)). */
+int sdfo_set_sign_mode(int32_t mode);
+int sdfo_get_sign_mode(void);
 
 /* ---- grid from / to host data (SdfData / SparseSdfData, SdfData.h) ------- */
 /* SdfOracle(SdfData) (SdfOracle.cpp:154-157): dense FP64 arrays, x-fastest:
@@ -438,8 +468,9 @@ int sdfo_query(const sdfo_grid* g, int32_t mode, const void* d_points, int32_t p
 /* Same with host buffers (pageable or pinned): copies in, queries, copies
  * out; synchronous.  With pinned buffers and more than
  * sdfo_tuning.host_chunk_queries points the batch runs as a pipeline over
- * chunks: copies in and queries on `stream`, copies out on a stream of the
- * handle, so that both directions of the bus are busy at once.  Calls on one
+ * growing chunks: copies in on `stream`, queries and copies out on two
+ * streams of the handle, so that both directions of the bus are busy at
+ * once.  Calls on one
  * handle serialise.  Returns SDFO_ERR_DEVICE_STATUS when the pipelined query
  * kernel reports a wait that ran out (see sdfo_device_status). */
 int sdfo_query_host(const sdfo_grid* g, int32_t mode, const void* h_points, int32_t points_f64,

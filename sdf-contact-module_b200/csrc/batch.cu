@@ -221,6 +221,9 @@ std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n
     // concatenation, or one device LBVH per mesh
     DeviceBuffer<RefNode> ref_nodes;
     DeviceBuffer<double> ref_tri9;
+    DeviceBuffer<float4> ref_tbox;
+    DeviceBuffer<double> ref_pn; // pseudo-normal sign mode only
+    const bool pseudo = sign_mode() == SDFO_SIGN_PSEUDONORMAL;
     DeviceBuffer<int32_t> ref_tri_id;
     std::vector<std::unique_ptr<DeviceLbvh>> lbvh;
     std::vector<RefTreeView> ref_views;
@@ -272,6 +275,7 @@ std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n
         }
         ref_nodes.reset(nodes.size());
         ref_tri9.reset((size_t)tri_off[(size_t)n] * 9);
+        ref_tbox.reset((size_t)tri_off[(size_t)n] * 2);
         ref_tri_id.reset(tri_id.size());
         SDFO_CUDA(cudaMemcpyAsync(ref_nodes.get(), nodes.data(), sizeof(RefNode) * nodes.size(),
                                   cudaMemcpyHostToDevice, s));
@@ -296,6 +300,9 @@ std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n
                 dverts.get() + 3 * vert_off[(size_t)m], dtris.get() + 3 * tri_off[(size_t)m],
                 ref_tri_id.get() + tri_off[(size_t)m], (int)nt_m, ref_tri9.get() + 9 * tri_off[(size_t)m]);
             SDFO_CHECK_LAUNCH();
+            k_tri_boxes<<<(unsigned)((nt_m + 255) / 256), 256, 0, s>>>(
+                ref_tri9.get() + 9 * tri_off[(size_t)m], (int)nt_m, ref_tbox.get() + 2 * tri_off[(size_t)m]);
+            SDFO_CHECK_LAUNCH();
         }
         ref_views.resize((size_t)n);
         for (int m = 0; m < n; ++m)
@@ -307,6 +314,23 @@ std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n
             v.n = (int)meshes[m].nt;
             v.nnodes = (int)host[(size_t)m].nodes.size();
             parity_ray(v.dir);
+            v.tbox = ref_tbox.get() + 2 * tri_off[(size_t)m];
+            set_cull_margins(v, scene_extent(meshes[m].h_verts, meshes[m].nv, info[(size_t)m]));
+        }
+        if (pseudo)
+        {
+            ref_pn.reset((size_t)tri_off[(size_t)n] * 18);
+            for (int m = 0; m < n; ++m)
+            {
+                if (meshes[m].nt <= 0) continue;
+                DeviceBuffer<double> one;
+                upload_pseudo_normals(one, meshes[m].h_verts, meshes[m].nv, meshes[m].h_tris, meshes[m].nt,
+                                      ref_tri_id.get() + tri_off[(size_t)m], s);
+                SDFO_CUDA(cudaMemcpyAsync(ref_pn.get() + 18 * tri_off[(size_t)m], one.get(),
+                                          sizeof(double) * 18 * (size_t)meshes[m].nt, cudaMemcpyDeviceToDevice, s));
+                SDFO_CUDA(cudaStreamSynchronize(s));
+                ref_views[(size_t)m].pn = ref_pn.get() + 18 * tri_off[(size_t)m];
+            }
         }
         // the host vectors are freed on return from this block
         SDFO_CUDA(cudaStreamSynchronize(s));
@@ -320,6 +344,9 @@ std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n
             lbvh[(size_t)m].reset(new DeviceLbvh());
             build_lbvh(*lbvh[(size_t)m], meshes[m].h_verts, meshes[m].nv, meshes[m].h_tris,
                        meshes[m].nt, scene_extent(meshes[m].h_verts, meshes[m].nv, info[(size_t)m]), s);
+            if (pseudo)
+                upload_pseudo_normals(lbvh[(size_t)m]->pn, meshes[m].h_verts, meshes[m].nv, meshes[m].h_tris,
+                                      meshes[m].nt, lbvh[(size_t)m]->tri_id.get(), s);
             lbvh_views[(size_t)m] = lbvh[(size_t)m]->view();
             total_nodes += meshes[m].nt > 1 ? meshes[m].nt - 1 : 0;
         }

@@ -89,10 +89,33 @@ sdfo_grid_info setup_grid(const double* verts, int64_t nv, const sdfo_build_para
 
 namespace {
 std::atomic<int> g_bvh_mode{SDFO_BVH_REFERENCE};
+std::atomic<int> g_fill_tile{(3 << 8) | 3}; // log2 x << 8 | log2 y: 8 x 8 x 4
+FillTile fill_tile()
+{
+    const int v = g_fill_tile.load();
+    return FillTile{v >> 8, v & 255};
+}
 } // namespace
 
 int bvh_mode() { return g_bvh_mode.load(); }
 void set_bvh_mode(int m) { g_bvh_mode.store(m); }
+namespace {
+std::atomic<int> g_sign_mode{SDFO_SIGN_RAY_PARITY};
+} // namespace
+int sign_mode() { return g_sign_mode.load(); }
+void set_sign_mode(int m) { g_sign_mode.store(m); }
+namespace {
+std::atomic<int> g_lbvh_stackless{0};
+} // namespace
+int lbvh_stackless() { return g_lbvh_stackless.load(); }
+void set_lbvh_stackless(int on) { g_lbvh_stackless.store(on ? 1 : 0); }
+void set_fill_tile(int lx, int ly) { g_fill_tile.store(((lx > 0 ? lx : 3) << 8) | (ly > 0 ? ly : 3)); }
+void get_fill_tile(int* lx, int* ly)
+{
+    const FillTile t = fill_tile();
+    *lx = t.lx;
+    *ly = t.ly;
+}
 
 
 sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
@@ -122,10 +145,10 @@ sdfo_grid* build_dense(const double* verts, int64_t nv, const int32_t* tris, int
     g->stats.bvh_nodes = tree.node_count(nt);
     g->stats.bvh_ms = tm.lap();
     const SpecD sp = spec_of(g->info);
-    const dim3 grid((sp.n[0] + 7) / 8, (sp.n[1] + 7) / 8, (sp.n[2] + 3) / 4);
+    const FillTile tile = fill_tile();
     tree.visit([&](auto view) {
-        k_dense_fill<<<grid, 256, 0, s>>>(view, sp, g->d.phi64, g->d.n64, g->d.w64, g->d.phin,
-                                          status.get());
+        k_dense_fill<<<tile.grid(sp), 256, 0, s>>>(view, sp, tile, g->d.phi64, g->d.n64, g->d.w64, g->d.phin,
+                                                   status.get());
     });
     SDFO_CHECK_LAUNCH();
     g->stats.fill_ms = tm.lap();
@@ -147,14 +170,16 @@ void count_dense_traversal(const double* verts, int64_t nv, const int32_t* tris,
     AnyTree tree{bvh_mode()};
     tree.build(verts, nv, tris, nt, scene_extent(verts, nv, info), s);
     DeviceBuffer<int> status(1);
-    DeviceBuffer<unsigned long long> sums(4);
+    DeviceBuffer<unsigned long long> sums(5);
     SDFO_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), s));
-    SDFO_CUDA(cudaMemsetAsync(sums.get(), 0, 4 * sizeof(unsigned long long), s));
+    SDFO_CUDA(cudaMemsetAsync(sums.get(), 0, 5 * sizeof(unsigned long long), s));
     const SpecD sp = spec_of(info);
-    const dim3 grid((sp.n[0] + 7) / 8, (sp.n[1] + 7) / 8, (sp.n[2] + 3) / 4);
-    tree.visit([&](auto view) { k_dense_count<<<grid, 256, 0, s>>>(view, sp, sums.get(), status.get()); });
+    const FillTile tile = fill_tile();
+    tree.visit([&](auto view) {
+        k_dense_count<<<tile.grid(sp), 256, 0, s>>>(view, sp, tile, sums.get(), status.get());
+    });
     SDFO_CHECK_LAUNCH();
-    unsigned long long h[4] = {0, 0, 0, 0};
+    unsigned long long h[5] = {0, 0, 0, 0, 0};
     SDFO_CUDA(cudaMemcpyAsync(h, sums.get(), sizeof(h), cudaMemcpyDeviceToHost, s));
     check_status(status, s); // synchronises s
     out->voxels = (int64_t)info.shape[0] * info.shape[1] * info.shape[2];
@@ -162,6 +187,7 @@ void count_dense_traversal(const double* verts, int64_t nv, const int32_t* tris,
     out->nearest_triangles = (int64_t)h[1];
     out->ray_nodes = (int64_t)h[2];
     out->ray_triangles = (int64_t)h[3];
+    out->nearest_triangles_exact = (int64_t)h[4];
 }
 
 sdfo_grid* build_sparse(const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
@@ -199,7 +225,7 @@ sdfo_grid* build_sparse(const double* verts, int64_t nv, const int32_t* tris, in
     SDFO_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), s));
     const SpecD sp = spec_of(g->info);
     DeviceBuffer<int32_t> flags(total), slots(total);
-    const int T = 256;
+    const int T = spread_threads(total);
     tree.visit([&](auto view) {
         k_sparse_activate<<<(total + T - 1) / T, T, 0, s>>>(view, sp, bd, g->nb[0], g->nb[1], g->nb[2],
                                                              activation, flags.get(), status.get());

@@ -10,7 +10,9 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <array>
 #include <thread>
+#include <unordered_map>
 #include <cfloat>
 #include <chrono>
 #include <cmath>
@@ -43,36 +45,66 @@ __device__ __forceinline__ d3 cross(const d3& a, const d3& b)
     return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
 
-// closestPointOnTriangle (KdTree.h:26-74): Ericson's Voronoi-region method.
-__device__ d3 closest_point(const d3& p, const d3& a, const d3& b, const d3& c)
+// Voronoi region of a closest point: the vertices a, b, c, the edges ab, ac,
+// bc, or the face (the pseudo-normal sign picks its normal by it).
+enum : int
+{
+    kRegionA = 0,
+    kRegionB = 1,
+    kRegionC = 2,
+    kRegionAB = 3,
+    kRegionAC = 4,
+    kRegionBC = 5,
+    kRegionFace = 6
+};
+
+// closestPointOnTriangle (KdTree.h:26-74): Ericson's Voronoi-region method;
+// *region (may be NULL) receives the region whose branch returned.
+__device__ d3 closest_point(const d3& p, const d3& a, const d3& b, const d3& c, int* region = nullptr)
 {
     const d3 ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
     const double d1 = dot(ab, ap), d2 = dot(ac, ap);
-    if (d1 <= 0.0 && d2 <= 0.0) return a;
+    if (d1 <= 0.0 && d2 <= 0.0)
+    {
+        if (region) *region = kRegionA;
+        return a;
+    }
     const d3 bp = sub(p, b);
     const double d3_ = dot(ab, bp), d4 = dot(ac, bp);
-    if (d3_ >= 0.0 && d4 <= d3_) return b;
+    if (d3_ >= 0.0 && d4 <= d3_)
+    {
+        if (region) *region = kRegionB;
+        return b;
+    }
     const double vc = d1 * d4 - d3_ * d2;
     if (vc <= 0.0 && d1 >= 0.0 && d3_ <= 0.0)
     {
+        if (region) *region = kRegionAB;
         const double v = d1 / (d1 - d3_);
         return mk(a.x + v * ab.x, a.y + v * ab.y, a.z + v * ab.z);
     }
     const d3 cp = sub(p, c);
     const double d5 = dot(ab, cp), d6 = dot(ac, cp);
-    if (d6 >= 0.0 && d5 <= d6) return c;
+    if (d6 >= 0.0 && d5 <= d6)
+    {
+        if (region) *region = kRegionC;
+        return c;
+    }
     const double vb = d5 * d2 - d1 * d6;
     if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0)
     {
+        if (region) *region = kRegionAC;
         const double w = d2 / (d2 - d6);
         return mk(a.x + w * ac.x, a.y + w * ac.y, a.z + w * ac.z);
     }
     const double va = d3_ * d6 - d5 * d4;
     if (va <= 0.0 && (d4 - d3_) >= 0.0 && (d5 - d6) >= 0.0)
     {
+        if (region) *region = kRegionBC;
         const double w = (d4 - d3_) / ((d4 - d3_) + (d5 - d6));
         return mk(b.x + w * (c.x - b.x), b.y + w * (c.y - b.y), b.z + w * (c.z - b.z));
     }
+    if (region) *region = kRegionFace;
     const double denom = 1.0 / (va + vb + vc);
     const double v = vb * denom, w = vc * denom;
     return mk(a.x + ab.x * v + ac.x * w, a.y + ab.y * v + ac.y * w, a.z + ab.z * v + ac.z * w);
@@ -117,6 +149,10 @@ struct LbvhView
     int n;                 // triangles
     double dir[3];         // parity ray direction (FP64)
     float inv_dir[3];
+    // pseudo-normal sign mode: 18 doubles per slot (vertex a, b, c, edge ab,
+    // ac, bc pseudo-normals); NULL: the reference's parity ray
+    const double* pn;
+    int stackless; // traverse by parent links (no per-thread stack)
 };
 
 template <class Tree>
@@ -260,8 +296,8 @@ __global__ void k_refit(int n, const int2* __restrict__ children, const int32_t*
 
 // Pack internal nodes: {L.lo, L.hi, R.lo, R.hi} in FP32 rounded outward and
 // widened by `margin`; children as node index (internal) or ~slot (leaf).
-__global__ void k_pack(int n, const int2* __restrict__ children, const double* __restrict__ box64,
-                       double margin, float4* __restrict__ nodes)
+__global__ void k_pack(int n, const int2* __restrict__ children, const int32_t* __restrict__ parent,
+                       const double* __restrict__ box64, double margin, float4* __restrict__ nodes)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
@@ -279,7 +315,9 @@ __global__ void k_pack(int n, const int2* __restrict__ children, const double* _
     o[0] = make_float4(f[0], f[1], f[2], f[3]);
     o[1] = make_float4(f[4], f[5], f[6], f[7]);
     o[2] = make_float4(f[8], f[9], f[10], f[11]);
-    o[3] = make_float4(__int_as_float(enc[0]), __int_as_float(enc[1]), 0.f, 0.f);
+    // children (leaves as ~slot) and the parent (-1 at the root), for the
+    // stackless traversals
+    o[3] = make_float4(__int_as_float(enc[0]), __int_as_float(enc[1]), __int_as_float(parent[i]), 0.f);
 }
 
 // ---------------------------------------------------------------------------
@@ -300,12 +338,14 @@ struct Nearest
     int slot;
     int id;
     d3 cp;
+    int region; // Voronoi region of cp on the triangle
 };
 
 __device__ __forceinline__ void test_triangle(const LbvhView& b, const d3& p, int slot, Nearest& best)
 {
     const d3 a = tri_vertex(b, slot, 0), bb = tri_vertex(b, slot, 1), c = tri_vertex(b, slot, 2);
-    const d3 cp = closest_point(p, a, bb, c);
+    int region;
+    const d3 cp = closest_point(p, a, bb, c, &region);
     const d3 d = sub(p, cp);
     const double sq = dot(d, d);
     const int id = __ldg(b.tri_id + slot);
@@ -315,6 +355,7 @@ __device__ __forceinline__ void test_triangle(const LbvhView& b, const d3& p, in
         best.slot = slot;
         best.id = id;
         best.cp = cp;
+        best.region = region;
     }
 }
 
@@ -325,6 +366,7 @@ __device__ __forceinline__ void test_triangle(const LbvhView& b, const d3& p, in
 struct TravCount
 {
     int nearest_nodes = 0, nearest_tris = 0, ray_nodes = 0, ray_tris = 0;
+    int nearest_exact = 0; // closest-point tests left after the box cull
 };
 
 // Upper bound used for FP32 culling: bestSq rounded up, plus a relative slack
@@ -332,6 +374,77 @@ struct TravCount
 __device__ __forceinline__ float cull_limit(double sq)
 {
     return sq >= 3.0e38 ? INFINITY : __double2float_ru(sq) * 1.000002f;
+}
+
+// The stackless form of the LBVH nearest search: the same near-first order
+// and the same pruning decisions as the stack form below, taken at the same
+// moments, by walking parent links.  At a node the walk knows where it came
+// from: from the parent (try the near child, else the far one), from the
+// near child (try the far one) or from the far child (go up); a child is
+// entered when its box distance is within the cull limit of the current
+// best, which is when the stack form pushes or pops it.  Leaf children are
+// tested in place.  Returns the same triangle (the lowest id at equal
+// distance does not depend on the order) and counts the same work.
+template <bool COUNT>
+__device__ void nearest_stackless(const LbvhView& b, const d3& p, const float pf[3], Nearest& best,
+                                  TravCount* tc)
+{
+    enum : int
+    {
+        kFromParent = 0,
+        kFromNear = 1,
+        kFromFar = 2,
+        kFromChild = 3
+    };
+    int node = 0, state = kFromParent, child = -1;
+    while (true)
+    {
+        if constexpr (COUNT)
+            if (state == kFromParent) ++tc->nearest_nodes;
+        const float4 n0 = __ldg(b.nodes + 4 * (int64_t)node);
+        const float4 n1 = __ldg(b.nodes + 4 * (int64_t)node + 1);
+        const float4 n2 = __ldg(b.nodes + 4 * (int64_t)node + 2);
+        const float4 n3 = __ldg(b.nodes + 4 * (int64_t)node + 3);
+        const float dl = box_dist2(pf, n0.x, n0.y, n0.z, n0.w, n1.x, n1.y);
+        const float dr = box_dist2(pf, n1.z, n1.w, n2.x, n2.y, n2.z, n2.w);
+        const int cl = __float_as_int(n3.x), cr = __float_as_int(n3.y);
+        const bool lfirst = dl <= dr;
+        const int nearc = lfirst ? cl : cr, farc = lfirst ? cr : cl;
+        const float dn = lfirst ? dl : dr, df = lfirst ? dr : dl;
+        if (state == kFromChild) state = child == nearc ? kFromNear : kFromFar;
+        const float lim = cull_limit(best.sq);
+        int next = 0;
+        bool go = false;
+        if (state == kFromParent && dn <= lim)
+        {
+            next = nearc;
+            go = true;
+        }
+        else if (state != kFromFar && df <= lim)
+        {
+            next = farc;
+            go = true;
+        }
+        if (go)
+        {
+            const bool is_near = state == kFromParent && next == nearc;
+            if (next < 0)
+            {
+                if constexpr (COUNT) ++tc->nearest_tris;
+                test_triangle(b, p, ~next, best);
+                state = is_near ? kFromNear : kFromFar;
+                continue;
+            }
+            node = next;
+            state = kFromParent;
+            continue;
+        }
+        const int parent = __float_as_int(n3.z);
+        if (parent < 0) break;
+        child = node;
+        node = parent;
+        state = kFromChild;
+    }
 }
 
 // init_sq: a triangle is recorded only below it (default +inf).
@@ -344,10 +457,17 @@ __device__ Nearest tree_nearest(const LbvhView& b, const d3& p, int* status, Tra
     best.slot = -1;
     best.id = 0x7fffffff;
     best.cp = p;
+    best.region = kRegionFace;
     if (b.n == 1)
     {
         if constexpr (COUNT) ++tc->nearest_tris;
         test_triangle(b, p, 0, best);
+        return best;
+    }
+    if (b.stackless)
+    {
+        const float pf[3] = {(float)p.x, (float)p.y, (float)p.z};
+        nearest_stackless<COUNT>(b, p, pf, best, tc);
         return best;
     }
     const float pf[3] = {(float)p.x, (float)p.y, (float)p.z};
@@ -435,6 +555,59 @@ __device__ __forceinline__ bool ray_box(const float o[3], const float inv[3], fl
     return tmax >= tmin;
 }
 
+// The parity ray's count by parent links (left child first; the count does
+// not depend on the order): from the parent try the left child, else the
+// right; from the left child try the right; from the right go up.
+template <bool COUNT>
+__device__ int ray_count_stackless(const LbvhView& b, const d3& p, const d3& dir, const float o[3], TravCount* tc)
+{
+    int node = 0, state = 0, child = -1, hits = 0; // state: 0 from parent, 1 from left, 2 from right, 3 from a child
+    while (true)
+    {
+        if constexpr (COUNT)
+            if (state == 0) ++tc->ray_nodes;
+        const float4 n0 = __ldg(b.nodes + 4 * (int64_t)node);
+        const float4 n1 = __ldg(b.nodes + 4 * (int64_t)node + 1);
+        const float4 n2 = __ldg(b.nodes + 4 * (int64_t)node + 2);
+        const float4 n3 = __ldg(b.nodes + 4 * (int64_t)node + 3);
+        const int cl = __float_as_int(n3.x), cr = __float_as_int(n3.y);
+        if (state == 3) state = child == cl ? 1 : 2;
+        int next = 0;
+        bool go = false;
+        if (state == 0 && ray_box(o, b.inv_dir, n0.x, n0.y, n0.z, n0.w, n1.x, n1.y))
+        {
+            next = cl;
+            go = true;
+        }
+        else if (state != 2 && ray_box(o, b.inv_dir, n1.z, n1.w, n2.x, n2.y, n2.z, n2.w))
+        {
+            next = cr;
+            go = true;
+        }
+        if (go)
+        {
+            const bool left = state == 0 && next == cl;
+            if (next < 0)
+            {
+                if constexpr (COUNT) ++tc->ray_tris;
+                const int s = ~next;
+                hits += ray_hits(p, dir, tri_vertex(b, s, 0), tri_vertex(b, s, 1), tri_vertex(b, s, 2)) ? 1 : 0;
+                state = left ? 1 : 2;
+                continue;
+            }
+            node = next;
+            state = 0;
+            continue;
+        }
+        const int parent = __float_as_int(n3.z);
+        if (parent < 0) break;
+        child = node;
+        node = parent;
+        state = 3;
+    }
+    return hits;
+}
+
 // countRayIntersections (KdTree.h:398-441): number of triangles the fixed
 // ray hits (exact FP64 test on every triangle whose widened box it crosses).
 template <bool COUNT = false>
@@ -447,6 +620,7 @@ __device__ int tree_ray_count(const LbvhView& b, const d3& p, int* status, TravC
         return ray_hits(p, dir, tri_vertex(b, 0, 0), tri_vertex(b, 0, 1), tri_vertex(b, 0, 2)) ? 1 : 0;
     }
     const float o[3] = {(float)p.x, (float)p.y, (float)p.z};
+    if (b.stackless) return ray_count_stackless<COUNT>(b, p, dir, o, tc);
     int stack[kStackDepth];
     int sp = 0;
     int node = 0;
@@ -516,7 +690,77 @@ struct RefTreeView
     int n;
     int nnodes;
     double dir[3];
+    // Per-triangle FP32 boxes for the cull ahead of the FP64 closest-point
+    // test (2 float4 per slot: lo, hi; NULL: no cull) and its margins, set
+    // from the scene extent E: cull_m = 2^-21 E (rounded up), cull_abs =
+    // (2^-20 E)^2.
+    const float4* tbox;
+    float cull_m;
+    double cull_abs;
+    const double* pn; // pseudo-normals per slot as in LbvhView (NULL: parity ray)
 };
+
+// Cull margins of a scene whose points and vertices lie within |x| <= E.
+inline void set_cull_margins(RefTreeView& v, double extent)
+{
+    v.cull_m = (float)std::ldexp(extent, -20); // >= 2^-21 E after rounding
+    const double a = std::ldexp(extent, -20);
+    v.cull_abs = a * a;
+}
+
+// Conservative FP32 box of each triangle in slot order (lo rounded down, hi
+// rounded up, so it contains the FP64 triangle).  A near-degenerate triangle
+// -- |ab x ac|^2 <= 2^-20 (longest edge)^4, where the closest point's
+// barycentric division is ill-conditioned -- gets an unbounded box and is
+// never culled.
+__global__ void k_tri_boxes(const double* __restrict__ tri9, int n, float4* __restrict__ tbox)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const double* t = tri9 + 9 * (int64_t)s;
+    const d3 a = mk(t[0], t[1], t[2]), b = mk(t[3], t[4], t[5]), c = mk(t[6], t[7], t[8]);
+    const d3 ab = sub(b, a), ac = sub(c, a), bc = sub(c, b);
+    const d3 cr = cross(ab, ac);
+    const double e2 = fmax(dot(ab, ab), fmax(dot(ac, ac), dot(bc, bc)));
+    const bool degenerate = !(dot(cr, cr) > 0x1p-20 * e2 * e2);
+    float4 lo, hi;
+    if (degenerate)
+    {
+        lo = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+        hi = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+    }
+    else
+    {
+        lo = make_float4(__double2float_rd(fmin(a.x, fmin(b.x, c.x))), __double2float_rd(fmin(a.y, fmin(b.y, c.y))),
+                         __double2float_rd(fmin(a.z, fmin(b.z, c.z))), 0.f);
+        hi = make_float4(__double2float_ru(fmax(a.x, fmax(b.x, c.x))), __double2float_ru(fmax(a.y, fmax(b.y, c.y))),
+                         __double2float_ru(fmax(a.z, fmax(b.z, c.z))), 0.f);
+    }
+    tbox[2 * (int64_t)s] = lo;
+    tbox[2 * (int64_t)s + 1] = hi;
+}
+
+// The cull bound for a best squared distance `sq`: a triangle whose FP32 box
+// lower bound exceeds it cannot produce a computed squared distance below
+// `sq` (the reference's strict update), by the margins above: FP32 rounding
+// of the point and the box gap (< 2^-21 E per axis, taken off each gap),
+// FP32 rounding of the squares and sum (the factor 1 - 2^-19), and the
+// rounding of the FP64 closest point of a well-conditioned triangle
+// (covered by 2^-16 relative and (2^-20 E)^2 absolute on `sq`).
+__device__ __forceinline__ float cull_bound(const RefTreeView& b, double sq)
+{
+    return __double2float_ru(sq * (1.0 + 0x1p-16) + b.cull_abs);
+}
+
+__device__ __forceinline__ bool box_culled(const RefTreeView& b, int s, const float pf[3], float bound)
+{
+    const float4 lo = __ldg(b.tbox + 2 * (int64_t)s), hi = __ldg(b.tbox + 2 * (int64_t)s + 1);
+    const float gx = fmaxf(fmaxf(fmaxf(lo.x - pf[0], pf[0] - hi.x), 0.f) - b.cull_m, 0.f);
+    const float gy = fmaxf(fmaxf(fmaxf(lo.y - pf[1], pf[1] - hi.y), 0.f) - b.cull_m, 0.f);
+    const float gz = fmaxf(fmaxf(fmaxf(lo.z - pf[2], pf[2] - hi.z), 0.f) - b.cull_m, 0.f);
+    const float sum = gx * gx + gy * gy + gz * gz;
+    return sum * (1.f - 0x1p-19f) > bound;
+}
 
 __device__ __forceinline__ void load_box(const RefNode* nd, double lo[3], double hi[3])
 {
@@ -568,7 +812,10 @@ __device__ Nearest tree_nearest(const RefTreeView& b, const d3& p, int* status, 
     best.slot = -1;
     best.id = -1;
     best.cp = mk(0.0, 0.0, 0.0);
+    best.region = kRegionFace;
     if (b.nnodes == 0) return best;
+    const float pf[3] = {(float)p.x, (float)p.y, (float)p.z};
+    float bound = cull_bound(b, init_sq);
     int stack[kStackDepth];
     double sdist[kStackDepth];
     int sp = 0;
@@ -592,8 +839,13 @@ __device__ Nearest tree_nearest(const RefTreeView& b, const d3& p, int* status, 
             if constexpr (COUNT) tc->nearest_tris += meta.w;
             for (int s = meta.z; s < meta.z + meta.w; ++s)
             {
+                // exact-decision cull: a triangle skipped here could not
+                // have replaced the best (see cull_bound)
+                if (b.tbox && box_culled(b, s, pf, bound)) continue;
+                if constexpr (COUNT) ++tc->nearest_exact;
                 const d3 a = tri_vertex(b, s, 0), bb = tri_vertex(b, s, 1), c = tri_vertex(b, s, 2);
-                const d3 cp = closest_point(p, a, bb, c);
+                int region;
+                const d3 cp = closest_point(p, a, bb, c, &region);
                 const d3 d = sub(p, cp);
                 const double sq = dot(d, d);
                 if (sq < best.sq)
@@ -601,6 +853,8 @@ __device__ Nearest tree_nearest(const RefTreeView& b, const d3& p, int* status, 
                     best.sq = sq;
                     best.slot = s;
                     best.cp = cp;
+                    best.region = region;
+                    bound = cull_bound(b, sq);
                 }
             }
             continue;
@@ -715,6 +969,22 @@ __device__ SignedResult signed_nearest(const Tree& b, const d3& p, int* status, 
     r.fn = best.slot >= 0 ? face_normal(tri_vertex(b, best.slot, 0), tri_vertex(b, best.slot, 1),
                                         tri_vertex(b, best.slot, 2))
                           : mk(0.0, 0.0, 1.0);
+    if (b.pn && best.slot >= 0)
+    {
+        // pseudo-normal sign: the normal of the closest point's feature --
+        // the face normal in the face, else the angle-weighted vertex or the
+        // edge pseudo-normal, which every triangle sharing that vertex or
+        // edge carries alike, so the sign does not depend on which of the
+        // equidistant triangles the search kept
+        d3 n = r.fn;
+        if (best.region < kRegionFace)
+        {
+            const double* q = b.pn + 18 * (int64_t)best.slot + 3 * best.region;
+            n = mk(__ldg(q), __ldg(q + 1), __ldg(q + 2));
+        }
+        r.sd = dot(sub(p, r.cp), n) >= 0.0 ? dist : -dist;
+        return r;
+    }
     const int hits = tree_ray_count<COUNT>(b, p, status, tc);
     if (hits > 0)
         r.sd = (hits % 2) == 1 ? -dist : dist;
@@ -753,16 +1023,37 @@ __device__ __forceinline__ d3 voxel_center(const SpecD& s, int i, int j, int k)
 #define SDFO_FILL_MIN_BLOCKS 1
 #endif
 
-// Dense fill: CTA = 8x8x4 voxel tile (coherent traversals), thread = voxel.
+// Voxel tile of a 256-thread fill CTA: 2^lx x 2^ly x 256 / 2^(lx+ly) voxels,
+// x fastest, so a warp covers a 2^lx x min(2^ly, 32 / 2^lx) x .. patch
+// (default 8 x 8 x 4: warps of 8 x 4 x 1; 4 x 4 x 16: warps of 4 x 4 x 2).
+struct FillTile
+{
+    int lx, ly;
+    __host__ __device__ int x() const { return 1 << lx; }
+    __host__ __device__ int y() const { return 1 << ly; }
+    __host__ __device__ int z() const { return 256 >> (lx + ly); }
+    dim3 grid(const SpecD& s) const
+    {
+        return dim3((s.n[0] + x() - 1) / x(), (s.n[1] + y() - 1) / y(), (s.n[2] + z() - 1) / z());
+    }
+    __device__ void voxel(int& i, int& j, int& k) const
+    {
+        const int tx = threadIdx.x;
+        i = blockIdx.x * x() + (tx & (x() - 1));
+        j = blockIdx.y * y() + ((tx >> lx) & (y() - 1));
+        k = blockIdx.z * z() + (tx >> (lx + ly));
+    }
+};
+
+// Dense fill: CTA = one voxel tile (coherent traversals), thread = voxel.
 template <class Tree>
-__global__ void __launch_bounds__(256, SDFO_FILL_MIN_BLOCKS) k_dense_fill(Tree b, SpecD s, double* __restrict__ phi64,
+__global__ void __launch_bounds__(256, SDFO_FILL_MIN_BLOCKS) k_dense_fill(Tree b, SpecD s, FillTile t,
+                                                    double* __restrict__ phi64,
                                                     double* __restrict__ n64, double* __restrict__ w64,
                                                     float4* __restrict__ phin, int* status)
 {
-    const int tx = threadIdx.x;
-    const int i = blockIdx.x * 8 + (tx & 7);
-    const int j = blockIdx.y * 8 + ((tx >> 3) & 7);
-    const int k = blockIdx.z * 4 + (tx >> 6);
+    int i, j, k;
+    t.voxel(i, j, k);
     if (i >= s.n[0] || j >= s.n[1] || k >= s.n[2]) return;
     const int64_t idx = i + (int64_t)s.n[0] * (j + (int64_t)s.n[1] * k);
     const d3 c = voxel_center(s, i, j, k);
@@ -784,19 +1075,20 @@ __global__ void __launch_bounds__(256, SDFO_FILL_MIN_BLOCKS) k_dense_fill(Tree b
 // The dense fill's traversals over the same voxels and tiles, counted
 // (TravCount) and summed into out[4] instead of stored.
 template <class Tree>
-__global__ void __launch_bounds__(256) k_dense_count(Tree b, SpecD s, unsigned long long* out, int* status)
+__global__ void __launch_bounds__(256) k_dense_count(Tree b, SpecD s, FillTile t, unsigned long long* out,
+                                                     int* status)
 {
     const int tx = threadIdx.x;
-    const int i = blockIdx.x * 8 + (tx & 7);
-    const int j = blockIdx.y * 8 + ((tx >> 3) & 7);
-    const int k = blockIdx.z * 4 + (tx >> 6);
+    int i, j, k;
+    t.voxel(i, j, k);
     TravCount tc;
     if (i < s.n[0] && j < s.n[1] && k < s.n[2])
         (void)signed_nearest<Tree, true>(b, voxel_center(s, i, j, k), status, &tc);
-    unsigned long long v[4] = {(unsigned long long)tc.nearest_nodes, (unsigned long long)tc.nearest_tris,
-                               (unsigned long long)tc.ray_nodes, (unsigned long long)tc.ray_tris};
+    unsigned long long v[5] = {(unsigned long long)tc.nearest_nodes, (unsigned long long)tc.nearest_tris,
+                               (unsigned long long)tc.ray_nodes, (unsigned long long)tc.ray_tris,
+                               (unsigned long long)tc.nearest_exact};
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < 5; ++q)
     {
         for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
         if ((tx & 31) == 0) atomicAdd(out + q, v[q]);
@@ -1044,6 +1336,7 @@ struct DeviceLbvh
     DeviceBuffer<float4> nodes;
     DeviceBuffer<double> tri9;
     DeviceBuffer<int32_t> tri_id;
+    DeviceBuffer<double> pn; // pseudo-normal sign mode only
     int n = 0;
     LbvhView view() const
     {
@@ -1054,9 +1347,106 @@ struct DeviceLbvh
         v.n = n;
         parity_ray(v.dir);
         for (int a = 0; a < 3; ++a) v.inv_dir[a] = (float)(1.0 / v.dir[a]);
+        v.pn = pn.get();
+        v.stackless = lbvh_stackless();
         return v;
     }
 };
+
+// Angle-weighted pseudo-normals of a triangle mesh (Baerentzen and Aanaes,
+// "Signed distance computation using the angle weighted pseudonormal",
+// IEEE TVCG 2005), in FP64, per triangle in input order: the vertex normals
+// of its corners a, b, c (sum over incident triangles of the corner angle
+// times the unit face normal) and the normals of its edges ab, ac, bc (sum of
+// the unit face normals of the triangles sharing the edge), each normalised.
+// A degenerate triangle (|cross| <= 1e-15, the face-normal rule) contributes
+// nothing.  For a closed, consistently oriented mesh, the sign of
+// (p - closest point) . (the normal of the closest point's feature) is the
+// inside/outside sign.
+std::vector<double> pseudo_normals(const double* verts, int64_t nv, const int32_t* tris, int64_t nt)
+{
+    std::vector<double> vn((size_t)nv * 3, 0.0), fnorm((size_t)nt * 3, 0.0);
+    std::unordered_map<uint64_t, std::array<double, 3>> en;
+    en.reserve((size_t)nt * 2);
+    auto key = [](int32_t u, int32_t v) {
+        const uint32_t a = (uint32_t)std::min(u, v), b = (uint32_t)std::max(u, v);
+        return ((uint64_t)a << 32) | b;
+    };
+    for (int64_t t = 0; t < nt; ++t)
+    {
+        const int32_t* ix = tris + 3 * t;
+        double P[3][3];
+        for (int k = 0; k < 3; ++k)
+            for (int a = 0; a < 3; ++a) P[k][a] = verts[3 * (int64_t)ix[k] + a];
+        const double e1[3] = {P[1][0] - P[0][0], P[1][1] - P[0][1], P[1][2] - P[0][2]};
+        const double e2[3] = {P[2][0] - P[0][0], P[2][1] - P[0][1], P[2][2] - P[0][2]};
+        const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                              e1[0] * e2[1] - e1[1] * e2[0]};
+        const double len = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+        if (!(len > 1e-15)) continue;
+        double* f = fnorm.data() + 3 * t;
+        for (int a = 0; a < 3; ++a) f[a] = cr[a] / len;
+        for (int k = 0; k < 3; ++k)
+        {
+            const double* o = P[k];
+            const double* q1 = P[(k + 1) % 3];
+            const double* q2 = P[(k + 2) % 3];
+            const double u[3] = {q1[0] - o[0], q1[1] - o[1], q1[2] - o[2]};
+            const double w[3] = {q2[0] - o[0], q2[1] - o[1], q2[2] - o[2]};
+            const double lu = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+            const double lw = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+            if (!(lu > 0.0 && lw > 0.0)) continue;
+            const double c = std::max(-1.0, std::min(1.0, (u[0] * w[0] + u[1] * w[1] + u[2] * w[2]) / (lu * lw)));
+            const double ang = std::acos(c);
+            for (int a = 0; a < 3; ++a) vn[3 * (int64_t)ix[k] + a] += ang * f[a];
+        }
+        const int32_t e[3][2] = {{ix[0], ix[1]}, {ix[0], ix[2]}, {ix[1], ix[2]}};
+        for (int k = 0; k < 3; ++k)
+        {
+            auto& acc = en[key(e[k][0], e[k][1])];
+            for (int a = 0; a < 3; ++a) acc[a] += f[a];
+        }
+    }
+    auto put = [](double* out, const double* v) {
+        const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        for (int a = 0; a < 3; ++a) out[a] = l > 0.0 ? v[a] / l : 0.0;
+    };
+    std::vector<double> out((size_t)nt * 18, 0.0);
+    for (int64_t t = 0; t < nt; ++t)
+    {
+        const int32_t* ix = tris + 3 * t;
+        double* o = out.data() + 18 * t;
+        for (int k = 0; k < 3; ++k) put(o + 3 * k, vn.data() + 3 * (int64_t)ix[k]);
+        const int32_t e[3][2] = {{ix[0], ix[1]}, {ix[0], ix[2]}, {ix[1], ix[2]}};
+        for (int k = 0; k < 3; ++k) put(o + 9 + 3 * k, en[key(e[k][0], e[k][1])].data());
+    }
+    return out;
+}
+
+// Pseudo-normals in slot order: out[slot] = in[tri_id[slot]] (18 doubles).
+__global__ void k_gather_pn(const double* __restrict__ in, const int32_t* __restrict__ ids, int n,
+                            double* __restrict__ out)
+{
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= 18 * (int64_t)n) return;
+    const int64_t s = q / 18;
+    out[q] = in[18 * (int64_t)ids[s] + q % 18];
+}
+
+// Uploads the pseudo-normals of (verts, tris) and gathers them into the slot
+// order of a tree whose slot -> triangle map is `tri_id` (device).
+void upload_pseudo_normals(DeviceBuffer<double>& pn, const double* verts, int64_t nv, const int32_t* tris,
+                           int64_t nt, const int32_t* tri_id, cudaStream_t s)
+{
+    const std::vector<double> h = pseudo_normals(verts, nv, tris, nt);
+    DeviceBuffer<double> tmp(h.size());
+    SDFO_CUDA(cudaMemcpyAsync(tmp.get(), h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, s));
+    pn.reset(h.size());
+    const int64_t total = 18 * nt;
+    k_gather_pn<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(tmp.get(), tri_id, (int)nt, pn.get());
+    SDFO_CHECK_LAUNCH();
+    SDFO_CUDA(cudaStreamSynchronize(s)); // tmp and h are released on return
+}
 
 // Host build of the reference's tree (KdTree::build / buildRecursive,
 // KdTree.h:91-121, 188-242): median split of the centroids on the longest
@@ -1216,8 +1606,11 @@ struct DeviceRefTree
     DeviceBuffer<RefNode> nodes;
     DeviceBuffer<double> tri9;
     DeviceBuffer<int32_t> tri_id;
+    DeviceBuffer<float4> tbox;
+    DeviceBuffer<double> pn; // pseudo-normal sign mode only
     int n = 0;
     int nnodes = 0;
+    double extent = 1.0;
     RefTreeView view() const
     {
         RefTreeView v{};
@@ -1227,6 +1620,9 @@ struct DeviceRefTree
         v.n = n;
         v.nnodes = nnodes;
         parity_ray(v.dir);
+        v.tbox = tbox.get();
+        set_cull_margins(v, extent);
+        v.pn = pn.get();
         return v;
     }
 };
@@ -1329,8 +1725,9 @@ __global__ void k_gather_tri9(const double* __restrict__ verts, const int32_t* _
 }
 
 void build_ref_tree(DeviceRefTree& t, const double* verts, int64_t nv, const int32_t* tris, int64_t nt,
-                    cudaStream_t s)
+                    double extent, cudaStream_t s)
 {
+    t.extent = extent;
     const size_t n = (size_t)nt;
     HostRefTree h;
     const size_t nnodes = (size_t)h.subtree_nodes(nt);
@@ -1369,6 +1766,9 @@ void build_ref_tree(DeviceRefTree& t, const double* verts, int64_t nv, const int
     SDFO_CUDA(cudaMemcpyAsync(dtris.get(), tris, sizeof(int32_t) * 3 * n, cudaMemcpyHostToDevice, s));
     k_gather_tri9<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(dverts.get(), dtris.get(), t.tri_id.get(), (int)nt,
                                                              t.tri9.get());
+    SDFO_CHECK_LAUNCH();
+    t.tbox.reset(2 * n);
+    k_tri_boxes<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(t.tri9.get(), (int)nt, t.tbox.get());
     SDFO_CHECK_LAUNCH();
     // the staging block is reused by the next build and the temporaries are
     // freed on return: finish the copies and the gather first
@@ -1423,11 +1823,13 @@ void build_lbvh(DeviceLbvh& bvh, const double* h_verts, int64_t nv, const int32_
     SDFO_CHECK_LAUNCH();
     bvh.nodes.reset((size_t)(n - 1) * 4);
     const double margin = 4.0e-6 * extent;
-    k_pack<<<(n - 1 + T - 1) / T, T, 0, s>>>(n, children.get(), box64.get(), margin, bvh.nodes.get());
+    k_pack<<<(n - 1 + T - 1) / T, T, 0, s>>>(n, children.get(), parent.get(), box64.get(), margin,
+                                             bvh.nodes.get());
     SDFO_CHECK_LAUNCH();
 }
 
-// The acceleration structure selected by sdfo_set_bvh_mode.
+// The acceleration structure selected by sdfo_set_bvh_mode, with the
+// pseudo-normals when sdfo_set_sign_mode selects that sign.
 struct AnyTree
 {
     int mode;
@@ -1436,10 +1838,17 @@ struct AnyTree
     void build(const double* verts, int64_t nv, const int32_t* tris, int64_t nt, double extent,
                cudaStream_t s)
     {
+        const bool pseudo = sign_mode() == SDFO_SIGN_PSEUDONORMAL;
         if (mode == SDFO_BVH_LBVH)
+        {
             build_lbvh(lbvh, verts, nv, tris, nt, extent, s);
+            if (pseudo) upload_pseudo_normals(lbvh.pn, verts, nv, tris, nt, lbvh.tri_id.get(), s);
+        }
         else
-            build_ref_tree(ref, verts, nv, tris, nt, s);
+        {
+            build_ref_tree(ref, verts, nv, tris, nt, extent, s);
+            if (pseudo) upload_pseudo_normals(ref.pn, verts, nv, tris, nt, ref.tri_id.get(), s);
+        }
     }
     int node_count(int64_t nt) const
     {
@@ -1454,6 +1863,18 @@ struct AnyTree
             f(ref.view());
     }
 };
+
+// Threads per CTA of a one-candidate-per-thread launch over `total`
+// candidates: 256, or fewer (a multiple of 32, at least 32) so that small
+// launches still spread over two CTAs per SM instead of a handful of SMs
+// (the hollow cylinder's 2,048 candidate blocks: 64 CTAs of 32, not 8 of 256).
+int spread_threads(int64_t total)
+{
+    const int64_t want = 2 * (int64_t)current_sm_count();
+    int t = 256;
+    while (t > 32 && (total + t - 1) / t < want) t -= 32;
+    return t;
+}
 
 double scene_extent(const double* verts, int64_t nv, const sdfo_grid_info& info)
 {

@@ -787,8 +787,9 @@ sdfo_grid* build_contact_aware(const double* verts, int64_t nv, const int32_t* t
         const int total = g->nb[0] * g->nb[1] * g->nb[2];
         g->stats.candidate_blocks = total;
         DeviceBuffer<int32_t> flags(total), slots(total);
+        const int TA = spread_threads(total);
         tree.visit([&](auto view) {
-            k_ca_sparse_activate<<<(total + T - 1) / T, T, 0, s>>>(v, view, sp, bd, g->nb[0], g->nb[1],
+            k_ca_sparse_activate<<<(total + TA - 1) / TA, TA, 0, s>>>(v, view, sp, bd, g->nb[0], g->nb[1],
                                                                   g->nb[2], activation, flags.get(),
                                                                   status.get());
         });

@@ -228,6 +228,17 @@ int sdfo_set_bvh_mode(int32_t mode)
 
 int sdfo_get_bvh_mode(void) { return bvh_mode(); }
 
+int sdfo_set_sign_mode(int32_t mode)
+{
+    return guarded([&] {
+        SDFO_REQUIRE(mode == SDFO_SIGN_RAY_PARITY || mode == SDFO_SIGN_PSEUDONORMAL, SDFO_ERR_INVALID_ARGUMENT,
+                     "unknown sign mode");
+        set_sign_mode(mode);
+    });
+}
+
+int sdfo_get_sign_mode(void) { return sign_mode(); }
+
 int sdfo_query(const sdfo_grid* g, int32_t mode, const void* d_points, int32_t points_f64,
                int64_t n, float* d_gap, float* d_grad, float* d_unit, float* d_witness,
                uint8_t* d_valid, float* d_hess, void* stream)

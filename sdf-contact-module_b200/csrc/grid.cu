@@ -232,6 +232,10 @@ GridView make_view(const sdfo_grid* g)
     v.bd = g->info.block_dim;
     v.phin16 = g->d.phin16;
     v.brick_affine = g->d.brick_affine;
+    {
+        const void* pool = g->info.storage == SDFO_STORAGE_FP16 ? (const void*)g->d.phin16 : (const void*)g->d.phin;
+        v.phin_a32 = pool != nullptr && (reinterpret_cast<uintptr_t>(pool) & 31) == 0;
+    }
     v.xpair = g->d.xpair;
     v.cell8 = g->d.cell8;
     v.ca_stride = g->ca_stride;

@@ -2,16 +2,21 @@
 // caller-owned host arrays, SdfOracle.cpp:434-444), and the process-wide
 // tuning knobs (sdfo_set_tuning).
 //
-// With pinned host buffers and more than one chunk of points, the call is a
-// two-stream pipeline over chunks of `host_chunk_queries` points: on the
-// caller's stream each chunk is copied in and queried, then an event hands
-// the chunk to the handle's copy-out stream, which copies its results back
-// while the next chunks are copied in and queried.  Host-to-device and
-// device-to-host copies then run at the same time on separate copy engines,
-// so a step costs about the larger of the two transfers instead of their
-// sum.  Pageable buffers (whose copies the driver stages synchronously) and
-// batches of one chunk take one copy in, one launch and one copy out on the
-// caller's stream.
+// With pinned host buffers and more points than one chunk, the call is a
+// three-stream pipeline over chunks: the caller's stream copies the chunks'
+// points in back to back, the handle's query stream runs each chunk's query
+// once its points have arrived, and the handle's copy-out stream copies each
+// chunk's results back once its query is done (events between the streams).
+// Host-to-device and device-to-host copies then run at the same time on
+// separate copy engines, so a step costs about the larger of the two
+// transfers instead of their sum.  The first chunk has
+// `host_chunk_queries` points and each next one `host_chunk_growth_pct`
+// percent of the previous: a small first chunk starts the copy-out early,
+// larger later ones keep the number of copies (each with a fixed cost) low,
+// and the copy-out (the larger transfer: 17 bytes per query against 12) is
+// never left waiting.  Pageable buffers (whose copies the driver stages
+// synchronously) and batches of one chunk take one copy in, one launch and
+// one copy out on the caller's stream.
 //
 // The call is synchronous.  Before it returns it reads the pipelined query
 // kernel's status word in stream order; a bounded wait that ran out in a
@@ -29,8 +34,10 @@ namespace sdfo {
 namespace {
 
 constexpr int kMaxChunks = 64;
-constexpr int64_t kDefaultHostChunk = 131072;
+constexpr int64_t kDefaultHostChunk = 32768;
+constexpr int kDefaultChunkGrowth = 130; // percent
 std::atomic<int64_t> g_host_chunk{kDefaultHostChunk};
+std::atomic<int> g_chunk_growth{kDefaultChunkGrowth};
 
 int64_t round_up256(int64_t v) { return (v + 255) & ~int64_t(255); }
 
@@ -50,8 +57,11 @@ bool is_pinned(const void* p)
 
 struct HostPipe
 {
-    cudaStream_t out = nullptr; // device-to-host copies of finished chunks
-    cudaEvent_t ready[kMaxChunks] = {};
+    cudaStream_t comp = nullptr; // the chunks' queries
+    cudaStream_t out = nullptr;  // device-to-host copies of finished chunks
+    cudaEvent_t start = nullptr; // the caller's stream reached the call
+    cudaEvent_t in[kMaxChunks] = {};    // chunk's points copied in
+    cudaEvent_t ready[kMaxChunks] = {}; // chunk's results written
     unsigned* status = nullptr; // pinned host copy of the query status word
 };
 
@@ -60,6 +70,10 @@ void destroy_host_pipe(HostPipe* p)
     if (!p) return;
     for (cudaEvent_t& e : p->ready)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t& e : p->in)
+        if (e) cudaEventDestroy(e);
+    if (p->start) cudaEventDestroy(p->start);
+    if (p->comp) cudaStreamDestroy(p->comp);
     if (p->out) cudaStreamDestroy(p->out);
     if (p->status) cudaFreeHost(p->status);
     delete p;
@@ -75,8 +89,11 @@ HostPipe* host_pipe(const sdfo_grid* g)
     auto* p = new HostPipe();
     try
     {
+        SDFO_CUDA(cudaStreamCreateWithFlags(&p->comp, cudaStreamNonBlocking));
         SDFO_CUDA(cudaStreamCreateWithFlags(&p->out, cudaStreamNonBlocking));
+        SDFO_CUDA(cudaEventCreateWithFlags(&p->start, cudaEventDisableTiming));
         for (cudaEvent_t& e : p->ready) SDFO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        for (cudaEvent_t& e : p->in) SDFO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         SDFO_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&p->status), sizeof(unsigned), cudaHostAllocDefault));
         *p->status = 0;
     }
@@ -190,16 +207,34 @@ int sdfo_query_host(const sdfo_grid* g, int32_t mode, const void* h_points, int3
         }
         else
         {
-            if ((n + chunk - 1) / chunk > kMaxChunks) chunk = round_up256((n + kMaxChunks - 1) / kMaxChunks);
-            const unsigned char* hp_pts = static_cast<const unsigned char*>(h_points);
-            int c = 0;
-            for (int64_t q0 = 0; q0 < n; q0 += chunk, ++c)
+            // chunk boundaries: growing by g percent from `chunk`, multiples
+            // of 256 (whole tiles of the pipelined kernel), the last chunk
+            // taking the rest once kMaxChunks - 1 are placed
+            const int g = std::max(100, g_chunk_growth.load());
+            int64_t bounds[kMaxChunks + 1];
+            int nc = 0;
+            bounds[0] = 0;
+            for (double size = (double)chunk; bounds[nc] < n;)
             {
-                const int64_t m = std::min(chunk, n - q0);
+                int64_t m = nc + 1 == kMaxChunks ? n - bounds[nc] : round_up256((int64_t)size);
+                m = std::min(m, n - bounds[nc]);
+                bounds[nc + 1] = bounds[nc] + m;
+                ++nc;
+                size = size * g / 100.0;
+            }
+            const unsigned char* hp_pts = static_cast<const unsigned char*>(h_points);
+            SDFO_CUDA(cudaEventRecord(hp->start, s));
+            SDFO_CUDA(cudaStreamWaitEvent(hp->comp, hp->start, 0));
+            SDFO_CUDA(cudaStreamWaitEvent(hp->out, hp->start, 0));
+            for (int c = 0; c < nc; ++c)
+            {
+                const int64_t q0 = bounds[c], m = bounds[c + 1] - q0;
                 SDFO_CUDA(cudaMemcpyAsync(d.pts + (size_t)q0 * 3 * ep, hp_pts + (size_t)q0 * 3 * ep,
                                           (size_t)m * 3 * ep, cudaMemcpyHostToDevice, s));
-                query(q0, m, s);
-                SDFO_CUDA(cudaEventRecord(hp->ready[c], s));
+                SDFO_CUDA(cudaEventRecord(hp->in[c], s));
+                SDFO_CUDA(cudaStreamWaitEvent(hp->comp, hp->in[c], 0));
+                query(q0, m, hp->comp);
+                SDFO_CUDA(cudaEventRecord(hp->ready[c], hp->comp));
                 SDFO_CUDA(cudaStreamWaitEvent(hp->out, hp->ready[c], 0));
                 copy_out(q0, m, hp->out);
             }
@@ -226,8 +261,20 @@ int sdfo_set_tuning(const sdfo_tuning* t)
                      "host_chunk_queries must be >= 0");
         SDFO_REQUIRE(t->fill_ctas_per_sm >= 0 && t->fill_ctas_per_sm <= 64, SDFO_ERR_INVALID_ARGUMENT,
                      "CTAs per SM out of range");
+        SDFO_REQUIRE(t->fill_tile_log2_x >= 0 && t->fill_tile_log2_y >= 0 &&
+                         (t->fill_tile_log2_x > 0 ? t->fill_tile_log2_x : 3) +
+                                 (t->fill_tile_log2_y > 0 ? t->fill_tile_log2_y : 3) <=
+                             8,
+                     SDFO_ERR_INVALID_ARGUMENT, "fill tile must hold at most 256 voxels in x and y");
+        SDFO_REQUIRE(t->host_chunk_growth_pct == 0 || (t->host_chunk_growth_pct >= 100 && t->host_chunk_growth_pct <= 400),
+                     SDFO_ERR_INVALID_ARGUMENT, "host_chunk_growth_pct must be 0 or in [100, 400]");
         g_host_chunk.store(t->host_chunk_queries > 0 ? t->host_chunk_queries : kDefaultHostChunk);
+        g_chunk_growth.store(t->host_chunk_growth_pct > 0 ? t->host_chunk_growth_pct : kDefaultChunkGrowth);
         set_fill_ctas_per_sm(t->fill_ctas_per_sm);
+        set_fill_tile(t->fill_tile_log2_x, t->fill_tile_log2_y);
+        SDFO_REQUIRE(t->lbvh_traversal >= 0 && t->lbvh_traversal <= 2, SDFO_ERR_INVALID_ARGUMENT,
+                     "unknown LBVH traversal");
+        set_lbvh_stackless(t->lbvh_traversal == 2);
     });
 }
 
@@ -237,7 +284,13 @@ int sdfo_get_tuning(sdfo_tuning* t)
         SDFO_REQUIRE(t != nullptr, SDFO_ERR_INVALID_ARGUMENT, "tuning is NULL");
         *t = sdfo_tuning{};
         t->host_chunk_queries = (int32_t)g_host_chunk.load();
+        t->host_chunk_growth_pct = g_chunk_growth.load();
         t->fill_ctas_per_sm = fill_ctas_per_sm();
+        int lx = 3, ly = 3;
+        get_fill_tile(&lx, &ly);
+        t->fill_tile_log2_x = lx;
+        t->fill_tile_log2_y = ly;
+        t->lbvh_traversal = lbvh_stackless() ? 2 : 1;
     });
 }
 

@@ -230,7 +230,8 @@ struct GridView
     int nx, ny, nz;
     int layout;  // SDFO_LAYOUT_*
     int storage; // SDFO_STORAGE_*
-    int phin_a32; // FP32 payload on a 32-byte boundary (256-bit corner-pair loads)
+    int phin_a32; // the query payload (phin, or phin16 for FP16 storage) starts on a
+                  // 32-byte boundary: 256-bit loads of sparse brick rows
     int has_hessian;
     const float4* phin;
     const float* hess6;
@@ -343,6 +344,16 @@ sdfo_grid* build_contact_aware(const double* verts, int64_t nv, const int32_t* t
                                cudaStream_t s);
 int bvh_mode();
 void set_bvh_mode(int m);
+// Inside/outside sign rule of subsequent builds (build.cu).
+int sign_mode();
+void set_sign_mode(int m);
+// Voxel tile of the dense fill CTAs, as log2 extents in x and y (z takes the
+// rest of 256 threads); 0 selects the default 3 (8 x 8 x 4) (build.cu).
+void set_fill_tile(int lx, int ly);
+void get_fill_tile(int* lx, int* ly);
+// LBVH traversals by parent links instead of a per-thread stack (build.cu).
+int lbvh_stackless();
+void set_lbvh_stackless(int on);
 
 // Contact (contact.cu).
 // The culling of SDFContactEngine.evaluate / measure_pair: a point BVH over

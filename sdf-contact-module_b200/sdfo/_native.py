@@ -21,6 +21,7 @@ LAYOUT_DENSE, LAYOUT_SPARSE = 1, 2
 STORAGE_FP32, STORAGE_FP16 = 0, 1
 BVH_REFERENCE, BVH_LBVH = 0, 1
 BE_TANGENT_REFERENCE, BE_TANGENT_EXACT = 0, 1
+SIGN_RAY_PARITY, SIGN_PSEUDONORMAL = 0, 1
 
 MODE_NAMES = {"first_order": FIRST_ORDER, "second_order": SECOND_ORDER,
               "trilinear": TRILINEAR, "tricubic": TRICUBIC, "contact_aware": CONTACT_AWARE,
@@ -99,11 +100,12 @@ class BuildStats(ctypes.Structure):
 
 class TraversalStats(ctypes.Structure):
     _fields_ = [("voxels", _I64), ("nearest_nodes", _I64), ("nearest_triangles", _I64),
-                ("ray_nodes", _I64), ("ray_triangles", _I64)]
+                ("ray_nodes", _I64), ("ray_triangles", _I64), ("nearest_triangles_exact", _I64)]
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("host_chunk_queries", _I32), ("fill_ctas_per_sm", _I32)]
+    _fields_ = [("host_chunk_queries", _I32), ("fill_ctas_per_sm", _I32), ("fill_tile_log2_x", _I32),
+                ("fill_tile_log2_y", _I32), ("lbvh_traversal", _I32), ("host_chunk_growth_pct", _I32)]
 
 
 class DeviceViews(ctypes.Structure):
@@ -136,6 +138,8 @@ SIGNATURES = [
      [_P, _I64, _P, _I64, _P, _P, ctypes.POINTER(TraversalStats)]),
     ("sdfo_set_bvh_mode", ctypes.c_int, [_I32]),
     ("sdfo_get_bvh_mode", ctypes.c_int, []),
+    ("sdfo_set_sign_mode", ctypes.c_int, [_I32]),
+    ("sdfo_get_sign_mode", ctypes.c_int, []),
     ("sdfo_grid_create_dense", ctypes.c_int,
      [ctypes.POINTER(GridInfo), _P, _P, _P, _P, _P, ctypes.POINTER(_P)]),
     ("sdfo_grid_create_sparse", ctypes.c_int,

@@ -135,7 +135,8 @@ class SdfGrid:
                 "nearest_nodes_per_voxel": st.nearest_nodes / n,
                 "nearest_triangle_tests_per_voxel": st.nearest_triangles / n,
                 "ray_box_tests_per_voxel": st.ray_nodes / n,
-                "ray_triangle_tests_per_voxel": st.ray_triangles / n}
+                "ray_triangle_tests_per_voxel": st.ray_triangles / n,
+                "exact_triangle_tests_per_voxel": st.nearest_triangles_exact / n}
 
     @classmethod
     def build_sparse(cls, verts, tris, padding=0.1, voxel_size=0.0, target_resolution=128,

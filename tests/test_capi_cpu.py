@@ -151,13 +151,24 @@ def test_tuning_round_trip(lib):
 
     before = N.get_tuning()
     try:
-        t = N.set_tuning(host_chunk_queries=65536, fill_ctas_per_sm=2)
-        assert t == {"host_chunk_queries": 65536, "fill_ctas_per_sm": 2}
-        t = N.set_tuning(host_chunk_queries=0)
-        assert t["host_chunk_queries"] == 131072 and t["fill_ctas_per_sm"] == 2
+        t = N.set_tuning(host_chunk_queries=65536, fill_ctas_per_sm=2, fill_tile_log2_x=2,
+                         fill_tile_log2_y=2, host_chunk_growth_pct=150)
+        assert t == {"host_chunk_queries": 65536, "fill_ctas_per_sm": 2, "fill_tile_log2_x": 2,
+                     "fill_tile_log2_y": 2, "lbvh_traversal": 1, "host_chunk_growth_pct": 150}
+        assert N.set_tuning(lbvh_traversal=2)["lbvh_traversal"] == 2
+        assert N.set_tuning(lbvh_traversal=0)["lbvh_traversal"] == 1
+        t = N.set_tuning(host_chunk_queries=0, fill_tile_log2_x=0, fill_tile_log2_y=0,
+                         host_chunk_growth_pct=0)
+        assert t["host_chunk_queries"] == 32768 and t["fill_ctas_per_sm"] == 2
+        assert t["host_chunk_growth_pct"] == 130
+        bad = N.Tuning(host_chunk_growth_pct=99)
+        assert lib.sdfo_set_tuning(ctypes.byref(bad)) == -1
+        assert (t["fill_tile_log2_x"], t["fill_tile_log2_y"]) == (3, 3)
         bad = N.Tuning(host_chunk_queries=-1, fill_ctas_per_sm=0)
         assert lib.sdfo_set_tuning(ctypes.byref(bad)) == -1
         bad = N.Tuning(host_chunk_queries=0, fill_ctas_per_sm=65)
+        assert lib.sdfo_set_tuning(ctypes.byref(bad)) == -1
+        bad = N.Tuning(fill_tile_log2_x=6, fill_tile_log2_y=3)
         assert lib.sdfo_set_tuning(ctypes.byref(bad)) == -1
         assert lib.sdfo_set_tuning(None) == -1
         with pytest.raises(ValueError):
@@ -165,3 +176,27 @@ def test_tuning_round_trip(lib):
     finally:
         N.set_tuning(**before)
     assert N.get_tuning() == before
+
+
+def test_tuning_cache_round_trip(lib, tmp_path):
+    """TuningCache stores knobs per (GPU, workload) in JSON and applies the
+    sdfo_tuning ones through sdfo_set_tuning."""
+    from sdfo import _native as N
+    from sdfo.tune import TuningCache, workload_key
+
+    before = N.get_tuning()
+    try:
+        path = str(tmp_path / "tuning.json")
+        c = TuningCache(path)
+        key = workload_key("dense_fill", (128, 128, 64), tris=34816)
+        assert key == "dense_fill:128x128x64:tris=34816"
+        assert c.get("NVIDIA B200", key) is None and not c.apply("NVIDIA B200", key)
+        c.put("NVIDIA B200", key, {"fill_tile_log2_x": 2, "fill_tile_log2_y": 2, "threads": 256})
+        c2 = TuningCache(path)
+        assert c2.get("NVIDIA B200", key)["threads"] == 256
+        assert c2.apply("NVIDIA B200", key)
+        t = N.get_tuning()
+        assert (t["fill_tile_log2_x"], t["fill_tile_log2_y"]) == (2, 2)
+        assert c2.get("other GPU", key) is None
+    finally:
+        N.set_tuning(**before)

@@ -237,3 +237,59 @@ def test_build_stats(cuda):
     s = g.build_stats()
     assert s["voxels_filled"] == np.prod(g.shape)
     assert s["triangles"] == len(t) and s["bvh_nodes"] > 0
+
+
+@pytest.mark.parametrize("tile", [(2, 2), (4, 2), (2, 3), (4, 1), (5, 3)])
+def test_dense_fill_tile_shapes_bit_identical(cuda, port, tile):
+    """Every voxel tile of the dense fill CTAs (a tuning knob) builds the
+    oracle's grid bit for bit, with the same device-counted traversal work."""
+    from sdfo import SdfGrid
+    from sdfo import _native as N
+
+    _set_mode(0)
+    before = N.get_tuning()
+    v, t = _meshes()["gear"]
+    P = port.build_dense(v, t, padding=0.1, target_resolution=64, max_resolution=64)
+    base = SdfGrid.traversal_stats(v, t, padding=0.1, target_resolution=64, max_resolution=64)
+    try:
+        N.set_tuning(fill_tile_log2_x=tile[0], fill_tile_log2_y=tile[1])
+        g = SdfGrid.build_dense(v, t, padding=0.1, target_resolution=64, max_resolution=64)
+        d = g.export_dense()
+        for k in ("phi", "normal", "witness", "hessian"):
+            assert np.array_equal(d[k], P[k]), k
+        st = SdfGrid.traversal_stats(v, t, padding=0.1, target_resolution=64, max_resolution=64)
+        assert st["totals"] == base["totals"]
+    finally:
+        N.set_tuning(**before)
+
+
+@pytest.mark.parametrize("name,res", [("gear", 64), ("torus", 40), ("one_triangle", 16),
+                                      ("degenerate", 24)])
+def test_lbvh_stackless_equals_stack(cuda, name, res):
+    """The stackless LBVH traversals (parent links) give the stack
+    traversals' grid bit for bit, dense and sparse, with the same
+    device-counted work."""
+    from sdfo import SdfGrid
+    from sdfo import _native as N
+
+    v, t = _meshes()[name]
+    kw = dict(padding=0.1, target_resolution=res, max_resolution=res)
+    before = N.get_tuning()
+    out = {}
+    try:
+        _set_mode(1)
+        for mode in (1, 2):
+            N.set_tuning(lbvh_traversal=mode)
+            d = SdfGrid.build_dense(v, t, **kw).export_dense()
+            sp = SdfGrid.build_sparse(v, t, band_voxels=3, **kw).export_sparse()
+            st = SdfGrid.traversal_stats(v, t, **kw)["totals"]
+            out[mode] = (d, sp, st)
+    finally:
+        _set_mode(0)
+        N.set_tuning(**before)
+    (d1, s1, c1), (d2, s2, c2) = out[1], out[2]
+    for k in ("phi", "normal", "witness", "hessian"):
+        assert np.array_equal(d1[k], d2[k]), k
+    for k in ("ijk", "phi", "normal"):
+        assert np.array_equal(s1[k], s2[k]), k
+    assert c1 == c2

@@ -1,10 +1,11 @@
-"""sdfo_query_host with pinned buffers runs as a chunked two-stream pipeline
-(copy-in and query on the caller's stream, copy-out on the handle's own
-stream).  Its results must equal the device-buffer query bit for bit: the
+"""sdfo_query_host with pinned buffers runs as a chunked three-stream
+pipeline (copy-in on the caller's stream, query and copy-out on two streams
+of the handle).  Its results must equal the device-buffer query bit for bit: the
 chunks run the same kernels on the same points.  Covered: a remainder chunk
-shorter than a CTA tile, more chunks than the pipeline keeps events for
-(the chunk grows), float64 points, every optional output, pageable buffers
-(single-shot path) and repeated calls on one handle."""
+shorter than a CTA tile, growing chunks, more chunks than the pipeline keeps
+events for (the last one takes the rest), float64 points, every optional
+output, pageable buffers (single-shot path) and repeated calls on one
+handle."""
 import ctypes
 
 import numpy as np
@@ -51,9 +52,10 @@ def _device_query(grid, pts, mode, outputs):
     return {k: v.cpu().numpy() for k, v in out.items()}
 
 
-@pytest.mark.parametrize("chunk,n", [(4096, 50_077), (4096, 300_000), (256, 1000)])
+@pytest.mark.parametrize("chunk,growth,n", [(4096, 130, 50_077), (4096, 100, 300_000),
+                                             (256, 100, 1000), (32768, 200, 300_000)])
 @pytest.mark.parametrize("outputs", [("grad", "valid"), ("grad", "unit", "witness", "valid")])
-def test_pipelined_host_query_equals_device_query(cuda, chunk, n, outputs):
+def test_pipelined_host_query_equals_device_query(cuda, chunk, growth, n, outputs):
     from sdfo import _native as N
 
     lib = N.load()
@@ -62,7 +64,7 @@ def test_pipelined_host_query_equals_device_query(cuda, chunk, n, outputs):
     pts = rng.uniform(g["bmin"], g["bmax"], (n, 3)).astype(np.float32)
     before = N.get_tuning()
     try:
-        N.set_tuning(host_chunk_queries=chunk)
+        N.set_tuning(host_chunk_queries=chunk, host_chunk_growth_pct=growth)
         for mode in (2, 3):
             host = _pinned_query(lib, grid, pts, mode, outputs)
             dev = _device_query(grid, pts, mode, outputs)
