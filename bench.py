@@ -1003,7 +1003,9 @@ def run_ours(args, rank, world, local_rank):
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": 12 * n,
                 "d2h_bytes_per_step": 17 * n,
-                "path": "sdfo_query_host, pinned host buffers, synchronous"},
+                "path": "sdfo_query_host, pinned host buffers, synchronous; default host io: the "
+                        "query kernel reads the points from and writes the results to the pinned "
+                        "buffers (mapped into the device) while it runs, both bus directions at once"},
         "gpu_launches": args.steps,
         "step_us": {"min": 1e3 * min(head_steps), "median": 1e3 * float(np.median(head_steps)),
                     "max": 1e3 * max(head_steps)},

@@ -259,10 +259,23 @@ typedef struct
     int32_t fill_tile_log2_x;   /* dense fill: voxel tile of a 256-thread CTA is */
     int32_t fill_tile_log2_y;   /* 2^x by 2^y by 256/2^(x+y), x fastest (0 = 3: 8x8x4) */
     int32_t lbvh_traversal;     /* SDFO_BVH_LBVH traversals: 1 = per-thread stack,
-                                   2 = stackless (parent links); 0 = default (1);
+                                   2 = stackless (parent links); 0 = default (2);
                                    same results and work either way */
     int32_t host_chunk_growth_pct; /* each next pipelined chunk is this percent of
                                       the previous (100..400; 0 = default 130) */
+    int32_t host_io_mode;       /* sdfo_query_host with pinned buffers: 1 = staged in
+                                   device memory, copied in and out per chunk;
+                                   2 = points copied in per chunk, results written
+                                   by the query straight into the caller's buffers;
+                                   3 = one query launch reads the points from and
+                                   writes the results to the caller's buffers (both
+                                   mapped into the device), no staging; modes 2 and
+                                   3 fall back to 1 for unmapped buffers; 0 = default
+                                   (3) */
+    int32_t triangle_cull;      /* reference-order tree: 1 = a conservative FP32
+                                   triangle-box test skips closest-point tests that
+                                   cannot replace the best (same results), 2 = off;
+                                   0 = default (1) */
 } sdfo_tuning;
 int sdfo_set_tuning(const sdfo_tuning* t);
 int sdfo_get_tuning(sdfo_tuning* t);

@@ -56,13 +56,23 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     hdr = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "sdfo.h"),
                                                     os.path.abspath(__file__)]
+    # extra nvcc flags from the environment (e.g. -DSDFO_QUERY_SPARSE_MIN_BLOCKS=4
+    # to try another register budget); they are part of the objects' inputs,
+    # so a change forces a rebuild
+    env_flags = os.environ.get("SDFO_NVCC_FLAGS", "").split()
+    stamp = os.path.join(BUILD, "flags.txt")
+    flags_now = " ".join(env_flags + (extra_flags or []))
+    if not os.path.exists(stamp) or open(stamp).read() != flags_now:
+        force = True
+        with open(stamp, "w") as f:
+            f.write(flags_now)
     objs = []
     for src in SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _newer(o, [s] + hdr):
-            cmd = [nvcc(), "-c", s, "-o", o] + ARCH + COMMON + PER_FILE.get(src, []) + (extra_flags or [])
+            cmd = [nvcc(), "-c", s, "-o", o] + ARCH + COMMON + PER_FILE.get(src, []) + env_flags + (extra_flags or [])
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)

@@ -314,7 +314,7 @@ std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n
             v.n = (int)meshes[m].nt;
             v.nnodes = (int)host[(size_t)m].nodes.size();
             parity_ray(v.dir);
-            v.tbox = ref_tbox.get() + 2 * tri_off[(size_t)m];
+            v.tbox = triangle_cull() ? ref_tbox.get() + 2 * tri_off[(size_t)m] : nullptr;
             set_cull_margins(v, scene_extent(meshes[m].h_verts, meshes[m].nv, info[(size_t)m]));
         }
         if (pseudo)

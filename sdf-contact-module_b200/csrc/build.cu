@@ -105,9 +105,16 @@ std::atomic<int> g_sign_mode{SDFO_SIGN_RAY_PARITY};
 int sign_mode() { return g_sign_mode.load(); }
 void set_sign_mode(int m) { g_sign_mode.store(m); }
 namespace {
-std::atomic<int> g_lbvh_stackless{0};
+// stackless by default: the same results; 1.31M-triangle icosphere sparse
+// fill 70.6 ms against 89.0 with the per-thread stack, hollow cylinder even
+std::atomic<int> g_lbvh_stackless{1};
 } // namespace
 int lbvh_stackless() { return g_lbvh_stackless.load(); }
+namespace {
+std::atomic<int> g_triangle_cull{1};
+} // namespace
+int triangle_cull() { return g_triangle_cull.load(); }
+void set_triangle_cull(int on) { g_triangle_cull.store(on ? 1 : 0); }
 void set_lbvh_stackless(int on) { g_lbvh_stackless.store(on ? 1 : 0); }
 void set_fill_tile(int lx, int ly) { g_fill_tile.store(((lx > 0 ? lx : 3) << 8) | (ly > 0 ? ly : 3)); }
 void get_fill_tile(int* lx, int* ly)

@@ -10,9 +10,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
-#include <array>
 #include <thread>
-#include <unordered_map>
 #include <cfloat>
 #include <chrono>
 #include <cmath>
@@ -1355,97 +1353,147 @@ struct DeviceLbvh
 
 // Angle-weighted pseudo-normals of a triangle mesh (Baerentzen and Aanaes,
 // "Signed distance computation using the angle weighted pseudonormal",
-// IEEE TVCG 2005), in FP64, per triangle in input order: the vertex normals
-// of its corners a, b, c (sum over incident triangles of the corner angle
-// times the unit face normal) and the normals of its edges ab, ac, bc (sum of
-// the unit face normals of the triangles sharing the edge), each normalised.
-// A degenerate triangle (|cross| <= 1e-15, the face-normal rule) contributes
-// nothing.  For a closed, consistently oriented mesh, the sign of
-// (p - closest point) . (the normal of the closest point's feature) is the
-// inside/outside sign.
-std::vector<double> pseudo_normals(const double* verts, int64_t nv, const int32_t* tris, int64_t nt)
+// IEEE TVCG 2005), in FP64, on the device: per triangle the unit face normal
+// (none for a degenerate triangle, |cross| <= 1e-15, the face-normal rule);
+// per vertex the sum over incident triangles of the corner angle times the
+// face normal; per edge the sum of the face normals of the triangles sharing
+// it; each normalised.  The corner and edge records are sorted by vertex and
+// by edge with a stable radix sort, so every sum runs over its triangles in
+// triangle order (deterministic).  For a closed, consistently oriented mesh
+// the sign of (p - closest point) . (the normal of the closest point's
+// feature) is the inside/outside sign.
+__global__ void k_pn_records(const double* __restrict__ verts, const int32_t* __restrict__ tris, int nt,
+                             uint32_t* __restrict__ vkey, uint64_t* __restrict__ ekey, int32_t* __restrict__ val,
+                             double* __restrict__ fn, double* __restrict__ vcontrib)
 {
-    std::vector<double> vn((size_t)nv * 3, 0.0), fnorm((size_t)nt * 3, 0.0);
-    std::unordered_map<uint64_t, std::array<double, 3>> en;
-    en.reserve((size_t)nt * 2);
-    auto key = [](int32_t u, int32_t v) {
-        const uint32_t a = (uint32_t)std::min(u, v), b = (uint32_t)std::max(u, v);
-        return ((uint64_t)a << 32) | b;
-    };
-    for (int64_t t = 0; t < nt; ++t)
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    const int32_t ix[3] = {tris[3 * (int64_t)t], tris[3 * (int64_t)t + 1], tris[3 * (int64_t)t + 2]};
+    d3 P[3];
+    for (int k = 0; k < 3; ++k)
+        P[k] = mk(verts[3 * (int64_t)ix[k]], verts[3 * (int64_t)ix[k] + 1], verts[3 * (int64_t)ix[k] + 2]);
+    const d3 cr = cross(sub(P[1], P[0]), sub(P[2], P[0]));
+    const double len = sqrt(dot(cr, cr));
+    const bool ok = len > 1e-15;
+    const d3 f = ok ? mk(cr.x / len, cr.y / len, cr.z / len) : mk(0.0, 0.0, 0.0);
+    fn[3 * (int64_t)t] = f.x;
+    fn[3 * (int64_t)t + 1] = f.y;
+    fn[3 * (int64_t)t + 2] = f.z;
+    const int e[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+    for (int k = 0; k < 3; ++k)
     {
-        const int32_t* ix = tris + 3 * t;
-        double P[3][3];
-        for (int k = 0; k < 3; ++k)
-            for (int a = 0; a < 3; ++a) P[k][a] = verts[3 * (int64_t)ix[k] + a];
-        const double e1[3] = {P[1][0] - P[0][0], P[1][1] - P[0][1], P[1][2] - P[0][2]};
-        const double e2[3] = {P[2][0] - P[0][0], P[2][1] - P[0][1], P[2][2] - P[0][2]};
-        const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
-                              e1[0] * e2[1] - e1[1] * e2[0]};
-        const double len = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
-        if (!(len > 1e-15)) continue;
-        double* f = fnorm.data() + 3 * t;
-        for (int a = 0; a < 3; ++a) f[a] = cr[a] / len;
-        for (int k = 0; k < 3; ++k)
-        {
-            const double* o = P[k];
-            const double* q1 = P[(k + 1) % 3];
-            const double* q2 = P[(k + 2) % 3];
-            const double u[3] = {q1[0] - o[0], q1[1] - o[1], q1[2] - o[2]};
-            const double w[3] = {q2[0] - o[0], q2[1] - o[1], q2[2] - o[2]};
-            const double lu = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-            const double lw = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
-            if (!(lu > 0.0 && lw > 0.0)) continue;
-            const double c = std::max(-1.0, std::min(1.0, (u[0] * w[0] + u[1] * w[1] + u[2] * w[2]) / (lu * lw)));
-            const double ang = std::acos(c);
-            for (int a = 0; a < 3; ++a) vn[3 * (int64_t)ix[k] + a] += ang * f[a];
-        }
-        const int32_t e[3][2] = {{ix[0], ix[1]}, {ix[0], ix[2]}, {ix[1], ix[2]}};
-        for (int k = 0; k < 3; ++k)
-        {
-            auto& acc = en[key(e[k][0], e[k][1])];
-            for (int a = 0; a < 3; ++a) acc[a] += f[a];
-        }
+        const int64_t r = 3 * (int64_t)t + k;
+        vkey[r] = (uint32_t)ix[k];
+        val[r] = (int32_t)r;
+        const uint32_t a = (uint32_t)ix[e[k][0]], b = (uint32_t)ix[e[k][1]];
+        ekey[r] = ((uint64_t)min(a, b) << 32) | max(a, b);
+        const d3 u = sub(P[(k + 1) % 3], P[k]), w = sub(P[(k + 2) % 3], P[k]);
+        const double lu = sqrt(dot(u, u)), lw = sqrt(dot(w, w));
+        double ang = 0.0;
+        if (ok && lu > 0.0 && lw > 0.0) ang = acos(fmax(-1.0, fmin(1.0, dot(u, w) / (lu * lw))));
+        vcontrib[3 * r] = ang * f.x;
+        vcontrib[3 * r + 1] = ang * f.y;
+        vcontrib[3 * r + 2] = ang * f.z;
     }
-    auto put = [](double* out, const double* v) {
-        const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-        for (int a = 0; a < 3; ++a) out[a] = l > 0.0 ? v[a] / l : 0.0;
-    };
-    std::vector<double> out((size_t)nt * 18, 0.0);
-    for (int64_t t = 0; t < nt; ++t)
-    {
-        const int32_t* ix = tris + 3 * t;
-        double* o = out.data() + 18 * t;
-        for (int k = 0; k < 3; ++k) put(o + 3 * k, vn.data() + 3 * (int64_t)ix[k]);
-        const int32_t e[3][2] = {{ix[0], ix[1]}, {ix[0], ix[2]}, {ix[1], ix[2]}};
-        for (int k = 0; k < 3; ++k) put(o + 9 + 3 * k, en[key(e[k][0], e[k][1])].data());
-    }
-    return out;
 }
 
-// Pseudo-normals in slot order: out[slot] = in[tri_id[slot]] (18 doubles).
-__global__ void k_gather_pn(const double* __restrict__ in, const int32_t* __restrict__ ids, int n,
-                            double* __restrict__ out)
+__device__ __forceinline__ void put_unit(double* out, double x, double y, double z)
+{
+    const double l = sqrt(x * x + y * y + z * z);
+    out[0] = l > 0.0 ? x / l : 0.0;
+    out[1] = l > 0.0 ? y / l : 0.0;
+    out[2] = l > 0.0 ? z / l : 0.0;
+}
+
+// Vertex normals: the thread at the start of each vertex's run of sorted
+// corner records sums the run in order and writes the unit normal for every
+// corner of the run (out: 3 doubles per corner record, by record index).
+__global__ void k_pn_vertex(int64_t m, const uint32_t* __restrict__ key, const int32_t* __restrict__ val,
+                            const double* __restrict__ vcontrib, double* __restrict__ out)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || (i > 0 && key[i] == key[i - 1])) return;
+    double x = 0.0, y = 0.0, z = 0.0;
+    int64_t j = i;
+    for (; j < m && key[j] == key[i]; ++j)
+    {
+        const int64_t r = val[j];
+        x += vcontrib[3 * r];
+        y += vcontrib[3 * r + 1];
+        z += vcontrib[3 * r + 2];
+    }
+    for (int64_t q = i; q < j; ++q) put_unit(out + 3 * (int64_t)val[q], x, y, z);
+}
+
+// Edge normals: the same over runs of sorted edge records, summing the face
+// normals of the records' triangles.
+__global__ void k_pn_edge(int64_t m, const uint64_t* __restrict__ key, const int32_t* __restrict__ val,
+                          const double* __restrict__ fn, double* __restrict__ out)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || (i > 0 && key[i] == key[i - 1])) return;
+    double x = 0.0, y = 0.0, z = 0.0;
+    int64_t j = i;
+    for (; j < m && key[j] == key[i]; ++j)
+    {
+        const int64_t t = val[j] / 3;
+        x += fn[3 * t];
+        y += fn[3 * t + 1];
+        z += fn[3 * t + 2];
+    }
+    for (int64_t q = i; q < j; ++q) put_unit(out + 3 * (int64_t)val[q], x, y, z);
+}
+
+// Slot-order pseudo-normals: vertex normals of corners a, b, c then edge
+// normals of ab, ac, bc of triangle tri_id[slot] (18 doubles per slot).
+__global__ void k_pn_assemble(int n, const int32_t* __restrict__ ids, const double* __restrict__ vn,
+                              const double* __restrict__ en, double* __restrict__ out)
 {
     const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= 18 * (int64_t)n) return;
-    const int64_t s = q / 18;
-    out[q] = in[18 * (int64_t)ids[s] + q % 18];
+    const int64_t s = q / 18, r = q % 18;
+    const int64_t t = ids[s];
+    out[q] = r < 9 ? vn[9 * t + r] : en[9 * t + (r - 9)];
 }
 
-// Uploads the pseudo-normals of (verts, tris) and gathers them into the slot
-// order of a tree whose slot -> triangle map is `tri_id` (device).
+// The pseudo-normals of (verts, tris) (host arrays) in the slot order of a
+// tree whose slot -> triangle map is `tri_id` (device).
 void upload_pseudo_normals(DeviceBuffer<double>& pn, const double* verts, int64_t nv, const int32_t* tris,
                            int64_t nt, const int32_t* tri_id, cudaStream_t s)
 {
-    const std::vector<double> h = pseudo_normals(verts, nv, tris, nt);
-    DeviceBuffer<double> tmp(h.size());
-    SDFO_CUDA(cudaMemcpyAsync(tmp.get(), h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, s));
-    pn.reset(h.size());
-    const int64_t total = 18 * nt;
-    k_gather_pn<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(tmp.get(), tri_id, (int)nt, pn.get());
+    const int64_t m = 3 * nt;
+    DeviceBuffer<double> dverts((size_t)nv * 3);
+    DeviceBuffer<int32_t> dtris((size_t)m);
+    SDFO_CUDA(cudaMemcpyAsync(dverts.get(), verts, sizeof(double) * 3 * (size_t)nv, cudaMemcpyHostToDevice, s));
+    SDFO_CUDA(cudaMemcpyAsync(dtris.get(), tris, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+    DeviceBuffer<uint32_t> vkey((size_t)m), vkey2((size_t)m);
+    DeviceBuffer<uint64_t> ekey((size_t)m), ekey2((size_t)m);
+    DeviceBuffer<int32_t> val((size_t)m), vval((size_t)m), eval((size_t)m);
+    DeviceBuffer<double> fn((size_t)nt * 3), vcontrib((size_t)m * 3), vn((size_t)m * 3), en((size_t)m * 3);
+    const int T = 256;
+    k_pn_records<<<(unsigned)((nt + T - 1) / T), T, 0, s>>>(dverts.get(), dtris.get(), (int)nt, vkey.get(),
+                                                           ekey.get(), val.get(), fn.get(), vcontrib.get());
     SDFO_CHECK_LAUNCH();
-    SDFO_CUDA(cudaStreamSynchronize(s)); // tmp and h are released on return
+    int vbits = 1;
+    while (vbits < 32 && (int64_t(1) << vbits) < nv) ++vbits;
+    size_t t1 = 0, t2 = 0;
+    SDFO_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t1, vkey.get(), vkey2.get(), val.get(), vval.get(), (int)m,
+                                              0, vbits, s));
+    SDFO_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t2, ekey.get(), ekey2.get(), val.get(), eval.get(), (int)m,
+                                              0, 32 + vbits, s));
+    DeviceBuffer<unsigned char> tmp(std::max(t1, t2));
+    SDFO_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), t1, vkey.get(), vkey2.get(), val.get(), vval.get(), (int)m,
+                                              0, vbits, s));
+    SDFO_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), t2, ekey.get(), ekey2.get(), val.get(), eval.get(), (int)m,
+                                              0, 32 + vbits, s));
+    k_pn_vertex<<<(unsigned)((m + T - 1) / T), T, 0, s>>>(m, vkey2.get(), vval.get(), vcontrib.get(), vn.get());
+    SDFO_CHECK_LAUNCH();
+    k_pn_edge<<<(unsigned)((m + T - 1) / T), T, 0, s>>>(m, ekey2.get(), eval.get(), fn.get(), en.get());
+    SDFO_CHECK_LAUNCH();
+    pn.reset((size_t)nt * 18);
+    k_pn_assemble<<<(unsigned)((18 * nt + T - 1) / T), T, 0, s>>>((int)nt, tri_id, vn.get(), en.get(), pn.get());
+    SDFO_CHECK_LAUNCH();
+    SDFO_CUDA(cudaStreamSynchronize(s)); // the temporaries are released on return
 }
 
 // Host build of the reference's tree (KdTree::build / buildRecursive,
@@ -1620,7 +1668,7 @@ struct DeviceRefTree
         v.n = n;
         v.nnodes = nnodes;
         parity_ray(v.dir);
-        v.tbox = tbox.get();
+        v.tbox = triangle_cull() ? tbox.get() : nullptr;
         set_cull_margins(v, extent);
         v.pn = pn.get();
         return v;

@@ -242,6 +242,9 @@ __device__ __forceinline__ bool gather_rows_b8(const GridView& g, const Cell& c,
          s[1][1][1]) < 0)
         return false;
     const bool fp16 = g.storage == SDFO_STORAGE_FP16;
+    // FP16: the affine phi map of the cell's first brick, read once; rows in
+    // other bricks (cells on a brick face) read theirs
+    const float2 aff000 = fp16 ? __ldg(g.brick_affine + s[0][0][0]) : make_float2(0.f, 0.f);
 #pragma unroll
     for (int r = 0; r < 4; ++r)
     {
@@ -265,7 +268,7 @@ __device__ __forceinline__ bool gather_rows_b8(const GridView& g, const Cell& c,
         }
         else
         {
-            const float2 af0 = __ldg(g.brick_affine + s0);
+            const float2 af0 = s0 == s[0][0][0] ? aff000 : __ldg(g.brick_affine + s0);
             float4 lo, hi; // halves of voxels (li & ~3) .. (li & ~3) + 3
             ld256(reinterpret_cast<const float4*>(g.phin16 + row0 + (li & ~3)), lo, hi);
             const int m = li & 3;
@@ -279,7 +282,7 @@ __device__ __forceinline__ bool gather_rows_b8(const GridView& g, const Cell& c,
             else
             {
                 const int64_t i1 = cx ? (int64_t)s1 * V + bd * (ly + bd * lz) : row0 + li + 1;
-                const float2 af1 = cx ? __ldg(g.brick_affine + s1) : af0;
+                const float2 af1 = s1 == s0 ? af0 : __ldg(g.brick_affine + s1);
                 b = decode_fp16(__ldg(g.phin16 + i1), af1);
             }
         }

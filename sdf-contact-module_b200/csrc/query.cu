@@ -156,14 +156,23 @@ __device__ __forceinline__ void scatter_grid_gradient(const GridView& g, const C
 #ifndef SDFO_QUERY_MIN_BLOCKS
 #define SDFO_QUERY_MIN_BLOCKS 5
 #endif
+// Sparse gathers: 4 CTAs per SM (64 registers) measured faster than 5 (48
+// registers, with spills) and 6 on the 512^3 icosphere: FP32 23.8 against
+// 23.2 and 17.2 G queries/s, FP16 20.7 against 19.5 and 14.8.
+#ifndef SDFO_QUERY_SPARSE_MIN_BLOCKS
+#define SDFO_QUERY_SPARSE_MIN_BLOCKS 4
+#endif
 #ifndef SDFO_QUERY_HESS_MIN_BLOCKS
 #define SDFO_QUERY_HESS_MIN_BLOCKS 4
 #endif
-template <bool HESS>
-constexpr int query_min_blocks() { return HESS ? SDFO_QUERY_HESS_MIN_BLOCKS : SDFO_QUERY_MIN_BLOCKS; }
+template <bool HESS, bool SPARSE = false>
+constexpr int query_min_blocks()
+{
+    return HESS ? SDFO_QUERY_HESS_MIN_BLOCKS : SPARSE ? SDFO_QUERY_SPARSE_MIN_BLOCKS : SDFO_QUERY_MIN_BLOCKS;
+}
 
 template <int MODE, bool SPARSE, int BD, typename PT, bool HESS, bool STAGED>
-__global__ void __launch_bounds__(kThreads, query_min_blocks<HESS>())
+__global__ void __launch_bounds__(kThreads, query_min_blocks<HESS, SPARSE>())
     k_query(GridView g, const PT* __restrict__ pts, int64_t n, QueryOutputs o)
 {
     __shared__ __align__(16) float sbuf[STAGED ? (HESS ? 6 : 3) * kThreads : 1];
@@ -523,7 +532,7 @@ __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS>())
 template <int MODE, bool SPARSE, int BD>
 bool launch_pipe(const GridView& v, const float* pts, int64_t n, const QueryOutputs& o, cudaStream_t s)
 {
-    if (n < kThreads || o.unit || o.witness || o.hess || !o.gap || !aligned16(pts) || !aligned16(o.gap) ||
+    if (n < kThreads || o.host_mapped || o.unit || o.witness || o.hess || !o.gap || !aligned16(pts) || !aligned16(o.gap) ||
         !aligned16(o.grad) || !aligned16(o.valid) || !aligned16(o.hess6))
         return false;
     const int sms = current_sm_count();

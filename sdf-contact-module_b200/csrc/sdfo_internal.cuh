@@ -269,6 +269,9 @@ struct QueryOutputs
     uint8_t* valid;
     float* hess;            // 9 per query (full 3x3), or NULL
     float* hess6 = nullptr; // 6 per query (xx, xy, xz, yy, yz, zz), or NULL
+    // outputs live in host memory mapped into the device: plain stores only
+    // (no bulk-copy stores)
+    bool host_mapped = false;
 };
 void launch_query(const GridView& v, int mode, const void* pts, bool f64, int64_t n,
                   const QueryOutputs& o, cudaStream_t s);
@@ -354,6 +357,10 @@ void get_fill_tile(int* lx, int* ly);
 // LBVH traversals by parent links instead of a per-thread stack (build.cu).
 int lbvh_stackless();
 void set_lbvh_stackless(int on);
+// The FP32 triangle-box cull ahead of the FP64 closest-point test of the
+// reference-order tree (build.cu; on by default).
+int triangle_cull();
+void set_triangle_cull(int on);
 
 // Contact (contact.cu).
 // The culling of SDFContactEngine.evaluate / measure_pair: a point BVH over

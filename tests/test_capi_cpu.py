@@ -154,9 +154,16 @@ def test_tuning_round_trip(lib):
         t = N.set_tuning(host_chunk_queries=65536, fill_ctas_per_sm=2, fill_tile_log2_x=2,
                          fill_tile_log2_y=2, host_chunk_growth_pct=150)
         assert t == {"host_chunk_queries": 65536, "fill_ctas_per_sm": 2, "fill_tile_log2_x": 2,
-                     "fill_tile_log2_y": 2, "lbvh_traversal": 1, "host_chunk_growth_pct": 150}
+                     "fill_tile_log2_y": 2, "lbvh_traversal": 2, "host_chunk_growth_pct": 150,
+                     "host_io_mode": 3, "triangle_cull": 1}
+        assert N.set_tuning(triangle_cull=2)["triangle_cull"] == 2
+        assert N.set_tuning(triangle_cull=0)["triangle_cull"] == 1
+        assert N.set_tuning(host_io_mode=3)["host_io_mode"] == 3
+        assert N.set_tuning(host_io_mode=1)["host_io_mode"] == 1
+        assert N.set_tuning(host_io_mode=0)["host_io_mode"] == 3
         assert N.set_tuning(lbvh_traversal=2)["lbvh_traversal"] == 2
-        assert N.set_tuning(lbvh_traversal=0)["lbvh_traversal"] == 1
+        assert N.set_tuning(lbvh_traversal=1)["lbvh_traversal"] == 1
+        assert N.set_tuning(lbvh_traversal=0)["lbvh_traversal"] == 2
         t = N.set_tuning(host_chunk_queries=0, fill_tile_log2_x=0, fill_tile_log2_y=0,
                          host_chunk_growth_pct=0)
         assert t["host_chunk_queries"] == 32768 and t["fill_ctas_per_sm"] == 2

@@ -293,3 +293,33 @@ def test_lbvh_stackless_equals_stack(cuda, name, res):
     for k in ("ijk", "phi", "normal"):
         assert np.array_equal(s1[k], s2[k]), k
     assert c1 == c2
+
+
+def test_triangle_cull_off_equals_on(cuda, port):
+    """The FP32 triangle-box cull only skips closest-point tests that cannot
+    replace the best: with it off (a tuning knob) the grid is the same bit
+    for bit, and the device counts more FP64 tests."""
+    from sdfo import SdfGrid
+    from sdfo import _native as N
+
+    _set_mode(0)
+    v, t = _meshes()["gear"]
+    kw = dict(padding=0.1, target_resolution=64, max_resolution=64)
+    before = N.get_tuning()
+    out = {}
+    try:
+        for cull in (1, 2):
+            N.set_tuning(triangle_cull=cull)
+            out[cull] = (SdfGrid.build_dense(v, t, **kw).export_dense(),
+                         SdfGrid.build_sparse(v, t, band_voxels=3, **kw).export_sparse(),
+                         SdfGrid.traversal_stats(v, t, **kw))
+    finally:
+        N.set_tuning(**before)
+    for k in ("phi", "normal", "witness", "hessian"):
+        assert np.array_equal(out[1][0][k], out[2][0][k]), k
+    for k in ("ijk", "phi", "normal", "hessian"):
+        assert np.array_equal(out[1][1][k], out[2][1][k]), k
+    on, off = out[1][2], out[2][2]
+    assert on["totals"] == off["totals"]
+    assert off["exact_triangle_tests_per_voxel"] == off["nearest_triangle_tests_per_voxel"]
+    assert on["exact_triangle_tests_per_voxel"] < off["exact_triangle_tests_per_voxel"]

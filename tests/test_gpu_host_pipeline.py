@@ -55,7 +55,8 @@ def _device_query(grid, pts, mode, outputs):
 @pytest.mark.parametrize("chunk,growth,n", [(4096, 130, 50_077), (4096, 100, 300_000),
                                              (256, 100, 1000), (32768, 200, 300_000)])
 @pytest.mark.parametrize("outputs", [("grad", "valid"), ("grad", "unit", "witness", "valid")])
-def test_pipelined_host_query_equals_device_query(cuda, chunk, growth, n, outputs):
+@pytest.mark.parametrize("out_mode", [1, 2, 3])
+def test_pipelined_host_query_equals_device_query(cuda, chunk, growth, n, outputs, out_mode):
     from sdfo import _native as N
 
     lib = N.load()
@@ -64,7 +65,7 @@ def test_pipelined_host_query_equals_device_query(cuda, chunk, growth, n, output
     pts = rng.uniform(g["bmin"], g["bmax"], (n, 3)).astype(np.float32)
     before = N.get_tuning()
     try:
-        N.set_tuning(host_chunk_queries=chunk, host_chunk_growth_pct=growth)
+        N.set_tuning(host_chunk_queries=chunk, host_chunk_growth_pct=growth, host_io_mode=out_mode)
         for mode in (2, 3):
             host = _pinned_query(lib, grid, pts, mode, outputs)
             dev = _device_query(grid, pts, mode, outputs)
