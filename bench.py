@@ -325,7 +325,21 @@ def c5_section(torch, lib, N, dev, stream, flush, steps, warmup, peak):
     st_l = gl.build_stats()
     same_occupancy = bool(gl.block_count == g32.block_count)
     gl.close()
+    tuning0 = N.get_tuning()
+    N.set_tuning(lbvh_traversal=1)
+    gl = SdfGrid.build_sparse(c["verts"], c["tris"], mode=TRICUBIC, **c["sparse"])
+    st_stack = gl.build_stats()
+    gl.close()
+    N.set_tuning(**tuning0)
     N.check(lib.sdfo_set_bvh_mode(N.BVH_REFERENCE))
+    # the pseudo-normal sign rule (no parity ray), reference-order tree
+    N.check(lib.sdfo_set_sign_mode(N.SIGN_PSEUDONORMAL))
+    t0 = time.perf_counter()
+    gp = SdfGrid.build_sparse(c["verts"], c["tris"], mode=TRICUBIC, **c["sparse"])
+    t_pseudo = time.perf_counter() - t0
+    st_p = gp.build_stats()
+    gp.close()
+    N.check(lib.sdfo_set_sign_mode(N.SIGN_RAY_PARITY))
     g16 = g32.to_fp16()
     h = float(g32.voxel[0])
     pts = torch.tensor(W.c5_points(c["verts"], c["tris"], h), device=dev)
@@ -415,6 +429,9 @@ def c5_section(torch, lib, N, dev, stream, flush, steps, warmup, peak):
         "build_stored_voxels_per_s": g32.stored_voxels / t_build,
         "build_candidate_blocks": st["candidate_blocks"],
         "lbvh_build_ms": 1e3 * t_lbvh, "lbvh_fill_ms": st_l["fill_ms"],
+        "lbvh_stack_fill_ms": st_stack["fill_ms"],
+        "pseudonormal_build_ms": 1e3 * t_pseudo, "pseudonormal_fill_ms": st_p["fill_ms"],
+        "pseudonormal_bvh_ms": st_p["bvh_ms"],
         "lbvh_same_block_count": same_occupancy,
         "queries_per_s": rate,
         "ad_vs_fd_speedup_fp32": ms["fd_fp32"] / ms["ad_points_fp32"],
@@ -815,6 +832,31 @@ def run_ours(args, rank, world, local_rank):
     lb.close()
     N.check(lib.sdfo_set_bvh_mode(N.BVH_REFERENCE))
     n_vox = int(np.prod(dense.shape))
+    # build knobs on this box (each result bit-identical, per the tests):
+    # the FP32 triangle cull on/off, the LBVH walk with a stack or stackless
+    knobs = {}
+    tuning0 = N.get_tuning()
+
+    def fill_ms(kind, **kw):
+        out = []
+        for _ in range(3):
+            g = (SdfGrid.build_dense if kind == "dense" else SdfGrid.build_sparse)(
+                c["verts"], c["tris"], **(c["dense"] if kind == "dense" else c["sparse"]))
+            out.append(g.build_stats()["fill_ms"])
+            g.close()
+        return float(np.median(out))
+
+    for cull in (1, 2):
+        N.set_tuning(triangle_cull=cull)
+        key = "cull_on" if cull == 1 else "cull_off"
+        knobs[key] = {"dense_fill_ms": fill_ms("dense"), "sparse_fill_ms": fill_ms("sparse")}
+    N.set_tuning(**tuning0)
+    N.check(lib.sdfo_set_bvh_mode(N.BVH_LBVH))
+    for trav in (1, 2):
+        N.set_tuning(lbvh_traversal=trav)
+        knobs["lbvh_stack" if trav == 1 else "lbvh_stackless"] = {"dense_fill_ms": fill_ms("dense")}
+    N.set_tuning(**tuning0)
+    N.check(lib.sdfo_set_bvh_mode(N.BVH_REFERENCE))
     # traversal work per voxel of the dense fill (instrumented copy, untimed)
     trav = SdfGrid.traversal_stats(c["verts"], c["tris"], **c["dense"])
     trav.pop("totals")
@@ -934,6 +976,20 @@ def run_ours(args, rank, world, local_rank):
         e = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(e, op=torch.distributed.ReduceOp.MAX)
         e2e_value = world * args.steps * n / float(e.item())
+    # the same call with each host io mode (sdfo_tuning.host_io_mode): staged
+    # copies per growing chunk, results written in place, both ways in place
+    tuning0 = N.get_tuning()
+    e2e_modes = {}
+    for name, io in (("staged_copies", 1), ("results_in_place", 2), ("zero_copy", 3)):
+        N.set_tuning(host_io_mode=io)
+        for _ in range(args.warmup):
+            e2e_step()
+        reps = max(20, min(args.steps, 200))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            e2e_step()
+        e2e_modes[name] = reps * n / (time.perf_counter() - t0)
+    N.set_tuning(**tuning0)
 
     # ---- contact: ring on cube, 4096 poses, forward + 6x6 Jacobian ----
     cc = W.c3_ring_cube(n_poses=4096)
@@ -1002,7 +1058,7 @@ def run_ours(args, rank, world, local_rank):
                              "counts gather-model bytes, DRAM traffic is lower"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": 12 * n,
-                "d2h_bytes_per_step": 17 * n,
+                "d2h_bytes_per_step": 17 * n, "by_host_io_mode": e2e_modes,
                 "path": "sdfo_query_host, pinned host buffers, synchronous; default host io: the "
                         "query kernel reads the points from and writes the results to the pinned "
                         "buffers (mapped into the device) while it runs, both bus directions at once"},
@@ -1023,6 +1079,7 @@ def run_ours(args, rank, world, local_rank):
             "sparse_fill_ms": st_sparse["fill_ms"],
             "cpu_reference_dense_voxels_per_s": cpu_build,
             "dense_fill_traversal": trav,
+            "knobs_fill_ms": knobs,
         },
         "queries": {
             "dense_tricubic_fwd_per_s": n / per_launch_s,

@@ -276,6 +276,14 @@ typedef struct
                                    triangle-box test skips closest-point tests that
                                    cannot replace the best (same results), 2 = off;
                                    0 = default (1) */
+    int32_t sparse_pair_records; /* sparse FP32 grids with 8^3 bricks created from
+                                    now on keep a 32-byte record {voxel, +x
+                                    neighbour} per stored voxel (one 256-bit load
+                                    per Tricubic row; twice the payload's memory):
+                                    0 = when the payload is at most 48 MB (the
+                                    records then stay in L2; larger pools gather
+                                    from DRAM, where the doubled footprint costs
+                                    more), 1 = always, 2 = never */
 } sdfo_tuning;
 int sdfo_set_tuning(const sdfo_tuning* t);
 int sdfo_get_tuning(sdfo_tuning* t);

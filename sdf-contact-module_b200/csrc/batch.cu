@@ -479,8 +479,10 @@ std::vector<sdfo_grid*> build_sparse_batched(const sdfo_mesh_desc* meshes, int n
             g->stats.triangles = (int32_t)meshes[m].nt;
             g->stats.bvh_nodes = mode == SDFO_BVH_REFERENCE ? ref_views[(size_t)m].nnodes
                                                             : (int32_t)(meshes[m].nt > 1 ? meshes[m].nt - 1 : 0);
+            build_stencil_layouts(g.get(), s);
             out.push_back(g.release());
         }
+        SDFO_CUDA(cudaStreamSynchronize(s));
     }
     catch (...)
     {

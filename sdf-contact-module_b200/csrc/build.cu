@@ -272,6 +272,7 @@ sdfo_grid* build_sparse(const double* verts, int64_t nv, const int32_t* tris, in
             sp, bd, g->nb[0], g->nb[1], stored, g->d.ijk, g->d.table, g->d.phin, g->d.hess6);
         SDFO_CHECK_LAUNCH();
     }
+    build_stencil_layouts(g.get(), s);
     g->stats.hessian_ms = tm.lap();
     check_status(status, s);
     g->stats.voxels_filled = (int64_t)B * V;

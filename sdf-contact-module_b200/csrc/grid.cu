@@ -375,26 +375,52 @@ __global__ void k_sparse_stencil_layouts(const float4* __restrict__ phin,
     };
     xpair[2 * v] = self;
     xpair[2 * v + 1] = at(1, 0, 0);
+    if (!cell8) return;
     cell8[2 * v] = make_float4(self.x, at(1, 0, 0).x, at(0, 1, 0).x, at(1, 1, 0).x);
     cell8[2 * v + 1] = make_float4(at(0, 0, 1).x, at(1, 0, 1).x, at(0, 1, 1).x, at(1, 1, 1).x);
 }
 
 } // namespace
 
+namespace {
+// 0 automatic, 1 always, 2 never
+std::atomic<int> g_sparse_pairs{0};
+// Pools up to this size get pair records automatically: with the records
+// (twice the pool) they stay mostly in the 126 MB L2, where one load per row
+// pays (hollow cylinder 6.8 MB pool: 23.1 -> 24.4 G queries/s; 256 gears, each
+// queried in turn: 15.8 -> 17.7).  A larger pool is gathered from DRAM at
+// random, where the doubled footprint costs more than the saved loads (the
+// 162 MB icosphere pool: 23.8 -> 20.1).
+constexpr int64_t kAutoPairPoolBytes = int64_t(48) << 20;
+} // namespace
+
+int sparse_pair_records() { return g_sparse_pairs.load(); }
+void set_sparse_pair_records(int mode) { g_sparse_pairs.store(mode); }
+
 void build_stencil_layouts(sdfo_grid* g, cudaStream_t s)
 {
     if (g->stored_voxels == 0 || g->info.storage != SDFO_STORAGE_FP32 || g->d.phin == nullptr)
         return;
     const int64_t N = g->stored_voxels;
-    if (!g->d.xpair) g->d.xpair = dalloc<float4>((size_t)N * 2);
-    if (!g->d.cell8) g->d.cell8 = dalloc<float4>((size_t)N * 2);
     if (g->info.layout == SDFO_LAYOUT_DENSE)
+    {
+        if (!g->d.xpair) g->d.xpair = dalloc<float4>((size_t)N * 2);
+        if (!g->d.cell8) g->d.cell8 = dalloc<float4>((size_t)N * 2);
         k_stencil_layouts<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
             g->d.phin, g->info.shape[0], g->info.shape[1], g->info.shape[2], g->d.xpair, g->d.cell8);
+    }
     else
+    {
+        // sparse 8^3 bricks: the x-pair records only (Tricubic rows, one
+        // 256-bit load each, the +x neighbour read across the brick face)
+        const int mode = sparse_pair_records();
+        const bool want = mode == 1 || (mode == 0 && N * (int64_t)sizeof(float4) <= kAutoPairPoolBytes);
+        if (g->info.block_dim != 8 || !want) return;
+        if (!g->d.xpair) g->d.xpair = dalloc<float4>((size_t)N * 2);
         k_sparse_stencil_layouts<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
             g->d.phin, g->d.ijk, g->d.table, g->info.shape[0], g->info.shape[1], g->info.shape[2],
-            g->info.block_dim, g->nb[0], g->nb[1], N, g->d.xpair, g->d.cell8);
+            g->info.block_dim, g->nb[0], g->nb[1], N, g->d.xpair, nullptr);
+    }
     SDFO_CHECK_LAUNCH();
 }
 
@@ -419,6 +445,10 @@ sdfo_grid::~sdfo_grid()
     using sdfo::device_free;
     sdfo::destroy_host_pipe(host_pipe);
     device_free(ws);
+    // stencil records belong to the handle (views have none; the grids of a
+    // batched build allocate theirs outside the shared arena)
+    device_free(d.xpair);
+    device_free(d.cell8);
     if (borrowed) return;
     device_free(d.phin);
     device_free(d.hess6);
@@ -430,8 +460,6 @@ sdfo_grid::~sdfo_grid()
     device_free(d.ijk);
     device_free(d.phin16);
     device_free(d.brick_affine);
-    device_free(d.xpair);
-    device_free(d.cell8);
     device_free(d.ca_count);
     device_free(d.ca_phi64);
     device_free(d.ca_n64);
@@ -559,6 +587,7 @@ int sdfo_grid_create_sparse(const sdfo_grid_info* info, const int32_t* h_block_i
                 SDFO_CUDA(cudaMemcpyAsync(g->d.hess6, h_hessian6, sizeof(float) * 6 * B * V, cudaMemcpyHostToDevice, s));
             }
         }
+        build_stencil_layouts(g.get(), s);
         SDFO_CUDA(cudaStreamSynchronize(s));
         *out = g.release();
     });

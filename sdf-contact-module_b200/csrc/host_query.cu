@@ -338,6 +338,9 @@ int sdfo_set_tuning(const sdfo_tuning* t)
         SDFO_REQUIRE(t->triangle_cull >= 0 && t->triangle_cull <= 2, SDFO_ERR_INVALID_ARGUMENT,
                      "triangle_cull must be 0, 1 or 2");
         set_triangle_cull(t->triangle_cull != 2);
+        SDFO_REQUIRE(t->sparse_pair_records >= 0 && t->sparse_pair_records <= 2, SDFO_ERR_INVALID_ARGUMENT,
+                     "sparse_pair_records must be 0, 1 or 2");
+        set_sparse_pair_records(t->sparse_pair_records);
         set_fill_ctas_per_sm(t->fill_ctas_per_sm);
         set_fill_tile(t->fill_tile_log2_x, t->fill_tile_log2_y);
         SDFO_REQUIRE(t->lbvh_traversal >= 0 && t->lbvh_traversal <= 2, SDFO_ERR_INVALID_ARGUMENT,
@@ -355,6 +358,7 @@ int sdfo_get_tuning(sdfo_tuning* t)
         t->host_chunk_growth_pct = g_chunk_growth.load();
         t->host_io_mode = g_output_mode.load() + 1;
         t->triangle_cull = triangle_cull() ? 1 : 2;
+        t->sparse_pair_records = sparse_pair_records();
         t->fill_ctas_per_sm = fill_ctas_per_sm();
         int lx = 3, ly = 3;
         get_fill_tile(&lx, &ly);

@@ -205,8 +205,10 @@ __device__ __forceinline__ bool gather_corners(const GridView& g, const Cell& c,
 // The 8 cell corners of a sparse 8^3-brick grid as rows: for each (dj, dk)
 // the x-pair (i0, i0 + 1).  Each distinct brick the cell touches is looked
 // up once (1.42 lookups per uniformly placed cell, instead of one per corner
-// when the cell crosses a brick face).  FP32: a pair starting on an even x
-// is one 256-bit load, otherwise two 128-bit loads.  FP16: the 32-byte chunk
+// when the cell crosses a brick face).  FP32 with the grid's x-pair records
+// (GridView::xpair, 32 bytes per stored voxel): one 256-bit load per row;
+// without them a pair starting on an even x is one 256-bit load, otherwise
+// two 128-bit loads.  FP16: the 32-byte chunk
 // of four voxels holding i0 is one 256-bit load; i0 mod 4 == 3 needs a second,
 // 64-bit load for i0 + 1; the brick's affine phi map is read once per brick.
 // Needs the pool on a 32-byte boundary (GridView::phin_a32).  Same values and
@@ -256,7 +258,13 @@ __device__ __forceinline__ bool gather_rows_b8(const GridView& g, const Cell& c,
         const int64_t row0 = (int64_t)s0 * V + bd * (ly + bd * lz);
         float4& a = out[2 * r];
         float4& b = out[2 * r + 1];
-        if (!fp16)
+        if (!fp16 && g.xpair)
+        {
+            // the row's pair record {v, v + x}, the +x voxel taken across the
+            // brick face (validity from the table lookups above)
+            ld256(g.xpair + 2 * (row0 + li), a, b);
+        }
+        else if (!fp16)
         {
             if ((li & 1) == 0)
                 ld256(g.phin + row0 + li, a, b);

@@ -914,6 +914,7 @@ sdfo_grid* load_sparse(const File& f, const Header& h, cudaStream_t s)
         g->ca_stride = s_ca;
         g->info.candidate_stride = s_ca;
     }
+    build_stencil_layouts(g.get(), s);
     SDFO_CUDA(cudaStreamSynchronize(s));
     g->stats.hessian_ms = tm.lap();
     g->stats.total_ms = tm.total();

@@ -256,7 +256,13 @@ struct GridView
 };
 
 GridView make_view(const sdfo_grid* g);
-// Fills the dense stencil layouts from phin (grid.cu).
+// Which sparse 8^3-brick FP32 grids created from now on get x-pair records
+// (2x the payload's memory): 0 those with pools up to 48 MB, 1 all, 2 none
+// (grid.cu).
+int sparse_pair_records();
+void set_sparse_pair_records(int mode);
+// Fills the stencil layouts from phin (grid.cu): dense xpair and cell8;
+// sparse 8^3 FP32 bricks: xpair as sparse_pair_records() selects.
 void build_stencil_layouts(sdfo_grid* g, cudaStream_t s);
 
 // Query launch (query.cu).

@@ -155,7 +155,10 @@ def test_tuning_round_trip(lib):
                          fill_tile_log2_y=2, host_chunk_growth_pct=150)
         assert t == {"host_chunk_queries": 65536, "fill_ctas_per_sm": 2, "fill_tile_log2_x": 2,
                      "fill_tile_log2_y": 2, "lbvh_traversal": 2, "host_chunk_growth_pct": 150,
-                     "host_io_mode": 3, "triangle_cull": 1}
+                     "host_io_mode": 3, "triangle_cull": 1, "sparse_pair_records": 0}
+        assert N.set_tuning(sparse_pair_records=2)["sparse_pair_records"] == 2
+        assert N.set_tuning(sparse_pair_records=1)["sparse_pair_records"] == 1
+        assert N.set_tuning(sparse_pair_records=0)["sparse_pair_records"] == 0
         assert N.set_tuning(triangle_cull=2)["triangle_cull"] == 2
         assert N.set_tuning(triangle_cull=0)["triangle_cull"] == 1
         assert N.set_tuning(host_io_mode=3)["host_io_mode"] == 3

@@ -223,3 +223,35 @@ def test_pipelined_dense_query_is_bit_identical(cuda, mode, n):
     assert torch.equal(lin["gap"], h["gap"]) and torch.equal(lin["grad"], h["grad"])
     H = h["hess"].reshape(n, 9)[:, [0, 1, 2, 4, 5, 8]]
     assert torch.equal(lin["hess6"], H)
+
+
+@pytest.mark.parametrize("mode", [2, 3])
+def test_sparse_pair_records_bit_identical(cuda, mode):
+    """Sparse grids with the x-pair records (one 256-bit load per Tricubic
+    row) and without them (a tuning knob) answer every query bit for bit
+    alike, including cells on brick faces and next to missing bricks."""
+    import torch
+
+    from sdfo import SdfGrid
+    from sdfo import _native as N
+
+    g = golden("sparse_cyl.npz")
+    spec = dict(bmin=g["bmin"], bmax=g["bmax"], voxel=g["voxel"], shape=tuple(g["shape"]))
+    before = N.get_tuning()
+    out = {}
+    rng = np.random.default_rng(5)
+    pts = np.concatenate([g["pts"], rng.uniform(g["bmin"], g["bmax"], (60_000, 3))]).astype(np.float32)
+    x = torch.tensor(pts, device="cuda")
+    try:
+        for pairs in (1, 2):
+            N.set_tuning(sparse_pair_records=pairs)
+            grid = SdfGrid.from_sparse(spec, int(g["block_dim"]), g["ijk"], g["phi"], g["normal"],
+                                       g["hessian"])
+            o = grid.query_tensors(x, mode=mode, unit=True, witness=True, valid=True, hess=True)
+            torch.cuda.synchronize()
+            out[pairs] = {k: v.cpu().numpy() for k, v in o.items()}
+    finally:
+        N.set_tuning(**before)
+    assert out[1]["valid"].sum() > 1000
+    for k in out[1]:
+        assert np.array_equal(out[1][k], out[2][k], equal_nan=True), k
