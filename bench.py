@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--kernels-once", choices=["c2", "c5", "ca", "be", "build", "build5", "contact"],
+    ap.add_argument("--kernels-once", choices=["c2", "c4", "c5", "ca", "be", "build", "build5", "contact"],
                     default=None,
                     help="one launch of each query kernel on the workload (for ncu), then exit")
     ap.add_argument("--skip-ca", action="store_true",
@@ -785,6 +785,7 @@ def c4_section(torch, lib, N, dev, stream, flush, steps, warmup, peak):
         "per_grid_launches_queries_per_s": total / (per_grid_ms * 1e-3),
         "graph_vs_per_grid_speedup": per_grid_ms / graph_ms,
         "autotuned_threads": tuned["threads"],
+        "autotuned_run_tiles": tuned["run"],
         "autotune_ms": {str(k): v for k, v in tuned["ms"].items()},
     }
     qb.close()
@@ -1121,6 +1122,8 @@ def kernels_once(which):
     sparse (band 3) reference-order build of the hollow cylinder
     (k_dense_fill, k_dense_hessian, k_sparse_activate, k_sparse_fill);
     "build5": the same sparse build of the 1.31M-triangle icosphere at 512³.
+    "c4": the first 16 gears of the 256-gear set, one batched query launch
+    (16 x 65,536 points, identity poses).
     "contact": the ring-on-cube contact batch (4096 poses x 7680 points),
     one Trilinear forward, one Trilinear forward + Jacobian and one
     Tricubic forward + Jacobian launch."""
@@ -1133,6 +1136,29 @@ def kernels_once(which):
     from sdfo import workloads as W
 
     lib = N.load()
+    if which == "c4":
+        # the first 16 gears of the 256-gear set, one batched build and ONE
+        # posed Tricubic batch launch over 16 x 65,536 near-surface points
+        from sdfo.batch import QueryBatch, pack_poses
+
+        gears = W.c4_gears()[:16]
+        grids = SdfGrid.build_sparse_batched(
+            [dict(verts=g["verts"], tris=g["tris"], **g["sparse"]) for g in gears], mode=TRICUBIC)
+        rng = np.random.default_rng(3)
+        pts = []
+        for g, grid in zip(gears, grids):
+            pts.append(W.near_surface_points(g["verts"], g["tris"], float(grid.voxel[0]), 65_536,
+                                             int(rng.integers(1 << 30))))
+        x = torch.tensor(np.concatenate(pts).astype(np.float32), device="cuda")
+        poses = pack_poses(np.array([np.eye(3)] * len(grids)), np.zeros((len(grids), 3)), device="cuda")
+        qb = QueryBatch(grids, [65_536] * len(grids))
+        out = qb.outputs(x.device)
+        torch.empty(64 << 20, dtype=torch.uint8, device="cuda").zero_()
+        qb.run(x, poses, TRICUBIC, out)
+        torch.cuda.synchronize()
+        print(json.dumps({"kernels_once": which, "grids": len(grids), "queries": int(x.shape[0]),
+                          "pool_mb": round(16 * sum(g.stored_voxels for g in grids) / 2**20, 1)}))
+        return
     if which == "contact":
         from sdfo.contact import ContactBatch, pack_states
 

@@ -318,6 +318,7 @@ int sdfo_query_host(const sdfo_grid* g, int32_t mode, const void* h_points, int3
 int sdfo_set_tuning(const sdfo_tuning* t)
 {
     return guarded([&] {
+        // every field is checked before any is applied
         SDFO_REQUIRE(t != nullptr, SDFO_ERR_INVALID_ARGUMENT, "tuning is NULL");
         SDFO_REQUIRE(t->host_chunk_queries >= 0, SDFO_ERR_INVALID_ARGUMENT,
                      "host_chunk_queries must be >= 0");
@@ -330,22 +331,25 @@ int sdfo_set_tuning(const sdfo_tuning* t)
                      SDFO_ERR_INVALID_ARGUMENT, "fill tile must hold at most 256 voxels in x and y");
         SDFO_REQUIRE(t->host_chunk_growth_pct == 0 || (t->host_chunk_growth_pct >= 100 && t->host_chunk_growth_pct <= 400),
                      SDFO_ERR_INVALID_ARGUMENT, "host_chunk_growth_pct must be 0 or in [100, 400]");
-        g_host_chunk.store(t->host_chunk_queries > 0 ? t->host_chunk_queries : kDefaultHostChunk);
-        g_chunk_growth.store(t->host_chunk_growth_pct > 0 ? t->host_chunk_growth_pct : kDefaultChunkGrowth);
         SDFO_REQUIRE(t->host_io_mode >= 0 && t->host_io_mode <= 3, SDFO_ERR_INVALID_ARGUMENT,
                      "unknown host io mode");
-        g_output_mode.store(t->host_io_mode == 0 ? kDefaultIoMode : t->host_io_mode - 1);
         SDFO_REQUIRE(t->triangle_cull >= 0 && t->triangle_cull <= 2, SDFO_ERR_INVALID_ARGUMENT,
                      "triangle_cull must be 0, 1 or 2");
-        set_triangle_cull(t->triangle_cull != 2);
         SDFO_REQUIRE(t->sparse_pair_records >= 0 && t->sparse_pair_records <= 2, SDFO_ERR_INVALID_ARGUMENT,
                      "sparse_pair_records must be 0, 1 or 2");
+        SDFO_REQUIRE(t->lbvh_traversal >= 0 && t->lbvh_traversal <= 2, SDFO_ERR_INVALID_ARGUMENT,
+                     "unknown LBVH traversal");
+        SDFO_REQUIRE(t->sparse_query_walk >= 0 && t->sparse_query_walk <= 2, SDFO_ERR_INVALID_ARGUMENT,
+                     "sparse_query_walk must be 0, 1 or 2");
+        g_host_chunk.store(t->host_chunk_queries > 0 ? t->host_chunk_queries : kDefaultHostChunk);
+        g_chunk_growth.store(t->host_chunk_growth_pct > 0 ? t->host_chunk_growth_pct : kDefaultChunkGrowth);
+        g_output_mode.store(t->host_io_mode == 0 ? kDefaultIoMode : t->host_io_mode - 1);
+        set_triangle_cull(t->triangle_cull != 2);
         set_sparse_pair_records(t->sparse_pair_records);
         set_fill_ctas_per_sm(t->fill_ctas_per_sm);
         set_fill_tile(t->fill_tile_log2_x, t->fill_tile_log2_y);
-        SDFO_REQUIRE(t->lbvh_traversal >= 0 && t->lbvh_traversal <= 2, SDFO_ERR_INVALID_ARGUMENT,
-                     "unknown LBVH traversal");
         set_lbvh_stackless(t->lbvh_traversal != 1);
+        set_sparse_query_walk(t->sparse_query_walk != 1);
     });
 }
 
@@ -365,6 +369,7 @@ int sdfo_get_tuning(sdfo_tuning* t)
         t->fill_tile_log2_x = lx;
         t->fill_tile_log2_y = ly;
         t->lbvh_traversal = lbvh_stackless() ? 2 : 1;
+        t->sparse_query_walk = sparse_query_walk() ? 2 : 1;
     });
 }
 

@@ -14,6 +14,10 @@
 #include "bulk.cuh"
 #include "interp.cuh"
 
+#include <algorithm>
+#include <atomic>
+#include <mutex>
+
 namespace sdfo {
 namespace {
 
@@ -230,6 +234,89 @@ __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS, SPARSE>())
     }
 }
 
+// Persistent variant of k_query for FP32 points on sparse grids: CTA c walks
+// the contiguous tile range [ntiles c / G, ntiles (c + 1) / G) of kThreads
+// queries (measured 10% faster than grid-stride order on random points over
+// one grid; points sorted in space stay coherent within a CTA's range).  Each
+// thread loads the point of its next tile before it evaluates the current
+// one, and loads and stores go straight to global memory, so warps never wait
+// for one another (k_query stages points and records through shared memory
+// between CTA barriers).  Selected by sdfo_tuning.sparse_query_walk.
+template <int MODE, int BD, bool HESS>
+__global__ void __launch_bounds__(kThreads, query_min_blocks<HESS, true>())
+    k_query_walk(GridView g, const float* __restrict__ pts, int64_t n, QueryOutputs o)
+{
+    const int64_t ntiles = (n + kThreads - 1) / kThreads;
+    const int64_t t_begin = ntiles * blockIdx.x / gridDim.x;
+    const int64_t t_end = ntiles * (blockIdx.x + 1) / gridDim.x;
+    int64_t q = t_begin * kThreads + threadIdx.x;
+    float xn[3] = {0.f, 0.f, 0.f};
+    if (t_begin < t_end && q < n)
+        for (int a = 0; a < 3; ++a) xn[a] = __ldcs(pts + 3 * q + a);
+    const bool want_unit = o.unit != nullptr || o.witness != nullptr;
+    for (int64_t t = t_begin; t < t_end; ++t)
+    {
+        const int64_t qc = q;
+        const double p[3] = {xn[0], xn[1], xn[2]};
+        q += kThreads;
+        if (t + 1 < t_end && q < n)
+            for (int a = 0; a < 3; ++a) xn[a] = __ldcs(pts + 3 * q + a);
+        if (qc >= n) continue; // the tail of the last tile
+        Interp r;
+        float unit[3] = {1.f, 0.f, 0.f};
+        const bool valid = evaluate<MODE, true, BD, HESS>(g, p, r, unit, want_unit);
+        if (!valid)
+        {
+            r.gap = 0.f;
+            r.g[0] = r.g[1] = r.g[2] = 0.f;
+            unit[0] = 1.f;
+            unit[1] = unit[2] = 0.f;
+#pragma unroll
+            for (int a = 0; a < 6; ++a) r.H[a] = 0.f;
+        }
+        __stcs(o.gap + qc, r.gap);
+        if (o.valid) o.valid[qc] = valid ? 1 : 0;
+        if (o.grad)
+            for (int a = 0; a < 3; ++a) __stcs(o.grad + 3 * qc + a, r.g[a]);
+        if (o.unit)
+            for (int a = 0; a < 3; ++a) __stcs(o.unit + 3 * qc + a, unit[a]);
+        if (o.witness)
+            for (int a = 0; a < 3; ++a)
+                __stcs(o.witness + 3 * qc + a, valid ? (float)(p[a] - (double)r.gap * unit[a]) : 0.f);
+        if (HESS && o.hess6)
+            for (int a = 0; a < 6; ++a) __stcs(o.hess6 + 6 * qc + a, r.H[a]);
+        if (HESS && o.hess)
+        {
+            const float H9[9] = {r.H[0], r.H[1], r.H[2], r.H[1], r.H[3], r.H[4], r.H[2], r.H[4], r.H[5]};
+#pragma unroll
+            for (int a = 0; a < 9; ++a) __stcs(o.hess + 9 * qc + a, H9[a]);
+        }
+    }
+}
+
+template <int MODE, int BD, bool HESS>
+void launch_walk(const GridView& v, const float* pts, int64_t n, const QueryOutputs& o, cudaStream_t s)
+{
+    static std::mutex mu;
+    static int per_sm[64] = {0};
+    int dev = 0;
+    SDFO_CUDA(cudaGetDevice(&dev));
+    int b;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (per_sm[dev & 63] == 0)
+        {
+            int r = 0;
+            SDFO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_query_walk<MODE, BD, HESS>, kThreads, 0));
+            per_sm[dev & 63] = r > 0 ? r : 1;
+        }
+        b = per_sm[dev & 63];
+    }
+    const int64_t ntiles = (n + kThreads - 1) / kThreads;
+    const unsigned blocks = (unsigned)std::min<int64_t>(ntiles, (int64_t)current_sm_count() * b);
+    k_query_walk<MODE, BD, HESS><<<blocks, kThreads, 0, s>>>(v, pts, n, o);
+}
+
 // Reverse mode from the linearisation the forward saved (grad, symmetric
 // Hessian, valid flag): dL/dp = dgap * grad + H dgrad is elementwise, and the
 // grid gradient needs only the corner weights, which depend on the point
@@ -359,6 +446,15 @@ void launch_pt2(const GridView& v, const void* pts, bool f64, bool staged, int64
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+std::atomic<bool> g_sparse_query_walk{true};
+
+} // namespace
+
+bool sparse_query_walk() { return g_sparse_query_walk.load(); }
+void set_sparse_query_walk(bool on) { g_sparse_query_walk.store(on); }
+
+namespace {
 
 // Persistent, bulk-copy-pipelined variant of k_query for FP32 points on dense
 // grids and the outputs gap, raw gradient, valid flag and (HESS) the
@@ -563,6 +659,17 @@ void launch_pt(const GridView& v, const void* pts, bool f64, int64_t n, const Qu
     if constexpr (!SPARSE && (MODE == SDFO_TRILINEAR || MODE == SDFO_TRICUBIC))
     {
         if (!f64 && launch_pipe<MODE, SPARSE, BD>(v, static_cast<const float*>(pts), n, o, s)) return;
+    }
+    if constexpr (SPARSE && (MODE == SDFO_TRILINEAR || MODE == SDFO_TRICUBIC))
+    {
+        if (!f64 && sparse_query_walk())
+        {
+            if (o.hess || o.hess6)
+                launch_walk<MODE, BD, true>(v, static_cast<const float*>(pts), n, o, s);
+            else
+                launch_walk<MODE, BD, false>(v, static_cast<const float*>(pts), n, o, s);
+            return;
+        }
     }
     const bool staged = !f64 && aligned16(pts) && aligned16(o.grad) && aligned16(o.unit) &&
                         aligned16(o.witness) && aligned16(o.hess6);

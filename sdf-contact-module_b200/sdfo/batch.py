@@ -48,11 +48,18 @@ class QueryBatch:
                                                   ctypes.byref(out)))
         self.handle = out.value
         self.total = int(self.counts.sum())
-        self.threads = 256
+        self.threads = 128
+        self.run_tiles = 4
 
     def set_threads(self, threads: int) -> None:
         N.check(self._lib.sdfo_query_batch_set_threads(self.handle, int(threads)))
         self.threads = int(threads)
+
+    def set_run(self, tiles: int) -> None:
+        """Consecutive tiles each persistent CTA takes before it strides
+        (a power of two, 1..64)."""
+        N.check(self._lib.sdfo_query_batch_set_run(self.handle, int(tiles)))
+        self.run_tiles = int(tiles)
 
     def outputs(self, device="cuda"):
         """Preallocated (gap, grad, valid) for run(..., out=...), e.g. for a

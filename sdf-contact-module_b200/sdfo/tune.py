@@ -1,7 +1,7 @@
 """Autotuner: picks launch shapes and the brick size by timing the candidates
 on the caller's own data with CUDA events (no reference counterpart).
 
-  tune_query_batch  threads per CTA of the batched query launch
+  tune_query_batch  threads per CTA and tile run length of the batched query launch
                     (128 / 256 / 512), set on the QueryBatch;
   tune_block_dim    sparse brick edge (4 / 8 / 16 voxels) for a mesh and a
                     query set: builds each candidate grid and times its
@@ -44,17 +44,21 @@ def _time(fn, reps, warmup):
 
 
 def tune_query_batch(batch, points, poses=None, mode=N.TRICUBIC, candidates=(128, 256, 512),
-                     reps=20, warmup=3):
-    """Times QueryBatch.run for each CTA size, keeps the fastest on the batch;
-    returns {"threads": best, "ms": {threads: ms}}."""
+                     runs=(1, 2, 4, 8), reps=20, warmup=3):
+    """Times QueryBatch.run for each CTA size and tile run length, keeps the
+    fastest on the batch; returns {"threads": t, "run": r, "ms":
+    {"<t>x<r>": ms}}."""
     out = batch.outputs(points.device)
     ms = {}
     for t in candidates:
         batch.set_threads(t)
-        ms[t] = _time(lambda: batch.run(points, poses, mode, out), reps, warmup)
+        for r in runs:
+            batch.set_run(r)
+            ms[(t, r)] = _time(lambda: batch.run(points, poses, mode, out), reps, warmup)
     best = min(ms, key=ms.get)
-    batch.set_threads(best)
-    return {"threads": best, "ms": ms}
+    batch.set_threads(best[0])
+    batch.set_run(best[1])
+    return {"threads": best[0], "run": best[1], "ms": {f"{t}x{r}": v for (t, r), v in ms.items()}}
 
 
 def tune_block_dim(verts, tris, points, candidates=(4, 8, 16), mode=N.TRICUBIC, reps=20,

@@ -207,6 +207,64 @@ def test_query_batch_identity_pose_equals_single_queries(cuda, port):
         assert torch.allclose(grad[s], one["grad"], rtol=0, atol=1e-6)
 
 
+@pytest.mark.parametrize("kind", ["sparse", "dense"])
+def test_query_batch_ragged_counts(cuda, kind):
+    """The persistent batch kernel walks runs of tiles in grid-stride order:
+    grids with no queries between others, tails shorter than a CTA, more
+    tiles than resident CTAs (several grid changes per CTA) and repeated
+    grids must all answer as the single-grid query does, for every launch
+    shape and run length, and for batches of one layout (the kernel is
+    specialised on it)."""
+    import torch
+
+    from sdfo import SdfGrid
+    from sdfo import meshes as M
+    from sdfo import workloads as W
+    from sdfo.batch import QueryBatch
+
+    if kind == "sparse":
+        gears = W.c4_gears(n_gears=3, seed=5)
+        _set_mode(0)
+        base = SdfGrid.build_sparse_batched([_mesh_args(g) for g in gears], mode=3)
+        meshes = [(g["verts"], g["tris"]) for g in gears]
+    else:
+        cv, ct = M.cube(0.1)
+        base = [SdfGrid.build_dense(cv, ct, target_resolution=40, max_resolution=40, mode=3)]
+        meshes = [(cv, ct)]
+    counts = [0, 1, 0, 257, 0, 300_000, 3, 128, 129, 0, 100_000, 0]
+    which = [i % len(base) for i in range(len(counts))]
+    rng = np.random.default_rng(21)
+    pts = []
+    for c, w in zip(counts, which):
+        v, tr = meshes[w]
+        p = W.near_surface_points(v, tr, float(base[w].voxel[0]), max(c, 1), int(rng.integers(1 << 30)))
+        pts.append(p[:c].astype(np.float32))
+    qb = QueryBatch([base[w] for w in which], counts)
+    for bad in (0, 3, 128):
+        with pytest.raises(RuntimeError, match="run length"):
+            qb.set_run(bad)
+    x = torch.tensor(np.concatenate(pts), device="cuda")
+    off = np.concatenate([[0], np.cumsum(counts)])
+    single = []
+    for g, w in enumerate(which):
+        if counts[g]:
+            single.append(base[w].query_tensors(torch.tensor(pts[g], device="cuda"), mode=3, valid=True))
+        else:
+            single.append(None)
+    for threads, run in ((128, 1), (256, 1), (512, 1), (128, 4), (256, 64)):
+        qb.set_threads(threads)
+        qb.set_run(run)
+        gap, grad, valid = qb.run(x)
+        for g, w in enumerate(which):
+            if not counts[g]:
+                continue
+            one, s = single[g], slice(off[g], off[g + 1])
+            h = float(base[w].voxel[0])
+            assert torch.equal(valid[s], one["valid"]), (threads, run, g)
+            assert torch.allclose(gap[s], one["gap"], rtol=0, atol=1e-6 * h), (threads, run, g)
+            assert torch.allclose(grad[s], one["grad"], rtol=0, atol=1e-6), (threads, run, g)
+
+
 def test_query_batch_cuda_graph_and_threads(cuda, port):
     import torch
 
@@ -233,10 +291,13 @@ def test_query_batch_cuda_graph_and_threads(cuda, port):
     # every launch shape gives the same answer; the tuner keeps one of them
     for threads in (128, 256, 512):
         qb.set_threads(threads)
-        for a, b in zip(eager2, qb.run(x, poses)):
-            assert torch.equal(a, b)
+        for run in (1, 2, 8, 64):
+            qb.set_run(run)
+            for a, b in zip(eager2, qb.run(x, poses)):
+                assert torch.equal(a, b)
     res = tune_query_batch(qb, x, poses, reps=3, warmup=1)
     assert res["threads"] in (128, 256, 512) and qb.threads == res["threads"]
+    assert res["run"] in (1, 2, 4, 8) and qb.run_tiles == res["run"]
 
 
 def test_tuners_run(cuda):

@@ -255,3 +255,42 @@ def test_sparse_pair_records_bit_identical(cuda, mode):
     assert out[1]["valid"].sum() > 1000
     for k in out[1]:
         assert np.array_equal(out[1][k], out[2][k], equal_nan=True), k
+
+
+@pytest.mark.parametrize("mode", [2, 3])
+def test_sparse_query_walk_bit_identical(cuda, mode):
+    """The persistent walk kernel for sparse FP32-point queries (the default;
+    a tuning knob) answers every query bit for bit as the staged per-tile
+    kernel does: FP32 and FP16 pools, every output (the full and the
+    symmetric Hessian included), and batch sizes below one tile, between
+    tiles and above the resident CTA count."""
+    import torch
+
+    from sdfo import SdfGrid
+    from sdfo import _native as N
+
+    g = golden("sparse_cyl.npz")
+    spec = dict(bmin=g["bmin"], bmax=g["bmax"], voxel=g["voxel"], shape=tuple(g["shape"]))
+    grid = SdfGrid.from_sparse(spec, int(g["block_dim"]), g["ijk"], g["phi"], g["normal"], g["hessian"])
+    grids = [grid, grid.to_fp16()]
+    rng = np.random.default_rng(8)
+    pts = np.concatenate([g["pts"], rng.uniform(g["bmin"], g["bmax"], (700_000, 3))]).astype(np.float32)
+    before = N.get_tuning()
+    try:
+        for gr in grids:
+            for n in (1, 255, 257, 40_000, len(pts)):
+                x = torch.tensor(pts[:n], device="cuda")
+                out = {}
+                for walk in (1, 2):
+                    N.set_tuning(sparse_query_walk=walk)
+                    o = gr.query_tensors(x, mode=mode, unit=True, witness=True, valid=True)
+                    h = gr.query_tensors(x, mode=mode, valid=True, hess=True)
+                    lin = gr.query_linearize(x, mode=mode)
+                    torch.cuda.synchronize()
+                    out[walk] = {k: v.cpu().numpy() for k, v in o.items()}
+                    out[walk].update({"h_" + k: v.cpu().numpy() for k, v in h.items()})
+                    out[walk].update({"lin_" + k: v.cpu().numpy() for k, v in lin.items()})
+                for k in out[1]:
+                    assert np.array_equal(out[1][k], out[2][k], equal_nan=True), (gr.storage, n, k)
+    finally:
+        N.set_tuning(**before)
