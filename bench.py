@@ -1040,7 +1040,9 @@ def run_ours(args, rank, world, local_rank):
         cpu_build = cpu_build_rate(c)
 
     achieved = BYTES_PER_QUERY * n / per_launch_s / 1e9
-    traffic = ncu_traffic("tricubic_dense_c2")
+    walk = N.get_tuning()["query_walk"] == 2
+    head_kernel = "k_query_walk<Tricubic,dense>" if walk else "k_query_pipe<Tricubic,dense>"
+    traffic = ncu_traffic("tricubic_dense_c2_walk" if walk else "tricubic_dense_c2")
     line = {
         "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -1053,7 +1055,7 @@ def run_ours(args, rank, world, local_rank):
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                     "kernel": "k_query_pipe<Tricubic,dense>",
+                     "kernel": head_kernel,
                      "bytes_per_query": BYTES_PER_QUERY,
                      "note": "16 MB grid is L2-resident after the first touch; achieved "
                              "counts gather-model bytes, DRAM traffic is lower"},

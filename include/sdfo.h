@@ -284,12 +284,17 @@ typedef struct
                                     records then stay in L2; larger pools gather
                                     from DRAM, where the doubled footprint costs
                                     more), 1 = always, 2 = never */
-    int32_t sparse_query_walk;  /* FP32-point queries of sparse grids: 1 = one CTA
-                                   per 256-query tile, points and results staged
-                                   through shared memory, 2 = persistent CTAs over
-                                   contiguous tile ranges, next point prefetched,
-                                   no CTA barriers (same results; 18% faster on
-                                   the 512^3 icosphere); 0 = default (2) */
+    int32_t query_walk;         /* Trilinear / Tricubic queries of FP32 points with
+                                   results in device memory: 2 = persistent CTAs
+                                   over contiguous tile ranges, next point
+                                   prefetched, no CTA barriers (sparse grids: every
+                                   output, 18% faster than 1 on the 512^3
+                                   icosphere; dense grids: without the Hessian, 13%
+                                   faster than the bulk-copy pipeline on the hollow
+                                   cylinder); 1 = per-tile kernels (points and
+                                   results staged through shared memory, or the
+                                   dense bulk-copy pipeline); same results;
+                                   0 = default (2) */
 } sdfo_tuning;
 int sdfo_set_tuning(const sdfo_tuning* t);
 int sdfo_get_tuning(sdfo_tuning* t);

@@ -339,8 +339,8 @@ int sdfo_set_tuning(const sdfo_tuning* t)
                      "sparse_pair_records must be 0, 1 or 2");
         SDFO_REQUIRE(t->lbvh_traversal >= 0 && t->lbvh_traversal <= 2, SDFO_ERR_INVALID_ARGUMENT,
                      "unknown LBVH traversal");
-        SDFO_REQUIRE(t->sparse_query_walk >= 0 && t->sparse_query_walk <= 2, SDFO_ERR_INVALID_ARGUMENT,
-                     "sparse_query_walk must be 0, 1 or 2");
+        SDFO_REQUIRE(t->query_walk >= 0 && t->query_walk <= 2, SDFO_ERR_INVALID_ARGUMENT,
+                     "query_walk must be 0, 1 or 2");
         g_host_chunk.store(t->host_chunk_queries > 0 ? t->host_chunk_queries : kDefaultHostChunk);
         g_chunk_growth.store(t->host_chunk_growth_pct > 0 ? t->host_chunk_growth_pct : kDefaultChunkGrowth);
         g_output_mode.store(t->host_io_mode == 0 ? kDefaultIoMode : t->host_io_mode - 1);
@@ -349,7 +349,7 @@ int sdfo_set_tuning(const sdfo_tuning* t)
         set_fill_ctas_per_sm(t->fill_ctas_per_sm);
         set_fill_tile(t->fill_tile_log2_x, t->fill_tile_log2_y);
         set_lbvh_stackless(t->lbvh_traversal != 1);
-        set_sparse_query_walk(t->sparse_query_walk != 1);
+        set_query_walk(t->query_walk != 1);
     });
 }
 
@@ -369,7 +369,7 @@ int sdfo_get_tuning(sdfo_tuning* t)
         t->fill_tile_log2_x = lx;
         t->fill_tile_log2_y = ly;
         t->lbvh_traversal = lbvh_stackless() ? 2 : 1;
-        t->sparse_query_walk = sparse_query_walk() ? 2 : 1;
+        t->query_walk = query_walk() ? 2 : 1;
     });
 }
 

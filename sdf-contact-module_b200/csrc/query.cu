@@ -234,15 +234,16 @@ __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS, SPARSE>())
     }
 }
 
-// Persistent variant of k_query for FP32 points on sparse grids: CTA c walks
-// the contiguous tile range [ntiles c / G, ntiles (c + 1) / G) of kThreads
-// queries (measured 10% faster than grid-stride order on random points over
-// one grid; points sorted in space stay coherent within a CTA's range).  Each
+// Persistent variant of k_query for FP32 points (sparse grids: every output;
+// dense grids: without the Hessian): CTA c walks the contiguous tile range
+// [ntiles c / G, ntiles (c + 1) / G) of kThreads queries (measured 10%
+// faster than grid-stride order on random points over one grid; points
+// sorted in space stay coherent within a CTA's range).  Each
 // thread loads the point of its next tile before it evaluates the current
 // one, and loads and stores go straight to global memory, so warps never wait
 // for one another (k_query stages points and records through shared memory
-// between CTA barriers).  Selected by sdfo_tuning.sparse_query_walk.
-template <int MODE, int BD, bool HESS, int MINB>
+// between CTA barriers).  Selected by sdfo_tuning.query_walk.
+template <int MODE, bool SPARSE, int BD, bool HESS, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB)
     k_query_walk(GridView g, const float* __restrict__ pts, int64_t n, QueryOutputs o)
 {
@@ -264,7 +265,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
         if (qc >= n) continue; // the tail of the last tile
         Interp r;
         float unit[3] = {1.f, 0.f, 0.f};
-        const bool valid = evaluate<MODE, true, BD, HESS>(g, p, r, unit, want_unit);
+        const bool valid = evaluate<MODE, SPARSE, BD, HESS>(g, p, r, unit, want_unit);
         if (!valid)
         {
             r.gap = 0.f;
@@ -294,7 +295,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
     }
 }
 
-template <int MODE, int BD, bool HESS, int MINB>
+template <int MODE, bool SPARSE, int BD, bool HESS, int MINB>
 void launch_walk(const GridView& v, const float* pts, int64_t n, const QueryOutputs& o, cudaStream_t s)
 {
     static std::mutex mu;
@@ -307,14 +308,14 @@ void launch_walk(const GridView& v, const float* pts, int64_t n, const QueryOutp
         if (per_sm[dev & 63] == 0)
         {
             int r = 0;
-            SDFO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_query_walk<MODE, BD, HESS, MINB>, kThreads, 0));
+            SDFO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_query_walk<MODE, SPARSE, BD, HESS, MINB>, kThreads, 0));
             per_sm[dev & 63] = r > 0 ? r : 1;
         }
         b = per_sm[dev & 63];
     }
     const int64_t ntiles = (n + kThreads - 1) / kThreads;
     const unsigned blocks = (unsigned)std::min<int64_t>(ntiles, (int64_t)current_sm_count() * b);
-    k_query_walk<MODE, BD, HESS, MINB><<<blocks, kThreads, 0, s>>>(v, pts, n, o);
+    k_query_walk<MODE, SPARSE, BD, HESS, MINB><<<blocks, kThreads, 0, s>>>(v, pts, n, o);
 }
 
 // Reverse mode from the linearisation the forward saved (grad, symmetric
@@ -447,12 +448,12 @@ void launch_pt2(const GridView& v, const void* pts, bool f64, bool staged, int64
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
-std::atomic<bool> g_sparse_query_walk{true};
+std::atomic<bool> g_query_walk{true};
 
 } // namespace
 
-bool sparse_query_walk() { return g_sparse_query_walk.load(); }
-void set_sparse_query_walk(bool on) { g_sparse_query_walk.store(on); }
+bool query_walk() { return g_query_walk.load(); }
+void set_query_walk(bool on) { g_query_walk.store(on); }
 
 namespace {
 
@@ -653,31 +654,44 @@ bool launch_pipe(const GridView& v, const float* pts, int64_t n, const QueryOutp
 template <int MODE, bool SPARSE, int BD>
 void launch_pt(const GridView& v, const void* pts, bool f64, int64_t n, const QueryOutputs& o, cudaStream_t s)
 {
-    // Dense grids only: on sparse grids the gathers' latency varies with the
-    // brick lookups, and the per-tile barriers of a persistent CTA then cost
-    // more than the prefetched points save (measured: C5 forward -11%).
+    // The persistent walk (query_walk(), the default) for FP32 points and
+    // results in device memory (results in mapped host memory take the staged
+    // kernel, whose 16-byte accesses suit the bus).  Register budgets
+    // (resident CTAs per SM) measured on the hollow cylinder (dense) and the
+    // 512^3 icosphere (sparse):
+    //   dense, no Hessian: 4 CTAs (64 registers, no spills), 32.5 G queries/s
+    //     against 28.7 for the bulk-copy pipeline; the Hessian-writing dense
+    //     forward stays on the pipeline (25.7 against 22.2 as a walk);
+    //   sparse, no Hessian: 4 CTAs;
+    //   sparse with the Hessian over an FP32 pool: 3 CTAs (80 registers, no
+    //     spills), 19% faster than 4 (linearising forward 19.8 -> 23.5 G/s);
+    //     over an FP16 pool 4 CTAs stay 4% faster.
+    if constexpr (MODE == SDFO_TRILINEAR || MODE == SDFO_TRICUBIC)
+    {
+        const bool hess = o.hess || o.hess6;
+        if (!f64 && !o.host_mapped && query_walk() && (SPARSE || !hess))
+        {
+            const float* p32 = static_cast<const float*>(pts);
+            if (!hess)
+                launch_walk<MODE, SPARSE, BD, false, 4>(v, p32, n, o, s);
+            else if constexpr (SPARSE)
+            {
+                if (v.storage == SDFO_STORAGE_FP32)
+                    launch_walk<MODE, SPARSE, BD, true, 3>(v, p32, n, o, s);
+                else
+                    launch_walk<MODE, SPARSE, BD, true, 4>(v, p32, n, o, s);
+            }
+            return;
+        }
+    }
+    // The bulk-copy pipeline: dense grids, the Hessian-writing forward (and
+    // every forward when the walk is off).  Not on sparse grids: there the
+    // gathers' latency varies with the brick lookups, and the per-tile
+    // barriers of a persistent CTA cost more than the prefetched points save
+    // (measured: C5 forward -11%).
     if constexpr (!SPARSE && (MODE == SDFO_TRILINEAR || MODE == SDFO_TRICUBIC))
     {
         if (!f64 && launch_pipe<MODE, SPARSE, BD>(v, static_cast<const float*>(pts), n, o, s)) return;
-    }
-    if constexpr (SPARSE && (MODE == SDFO_TRILINEAR || MODE == SDFO_TRICUBIC))
-    {
-        if (!f64 && sparse_query_walk())
-        {
-            // Register budgets (resident CTAs per SM) measured on the 512^3
-            // icosphere: the Hessian-writing walk over an FP32 pool runs 80
-            // registers at 3 CTAs without spills, 19% faster than 64 at 4
-            // (linearising forward 19.8 -> 23.5 G queries/s); over an FP16
-            // pool 4 CTAs stay 4% faster.
-            const float* p32 = static_cast<const float*>(pts);
-            if (!(o.hess || o.hess6))
-                launch_walk<MODE, BD, false, query_min_blocks<false, true>()>(v, p32, n, o, s);
-            else if (v.storage == SDFO_STORAGE_FP32)
-                launch_walk<MODE, BD, true, 3>(v, p32, n, o, s);
-            else
-                launch_walk<MODE, BD, true, query_min_blocks<true, true>()>(v, p32, n, o, s);
-            return;
-        }
     }
     const bool staged = !f64 && aligned16(pts) && aligned16(o.grad) && aligned16(o.unit) &&
                         aligned16(o.witness) && aligned16(o.hess6);

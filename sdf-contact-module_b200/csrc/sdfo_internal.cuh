@@ -261,9 +261,9 @@ GridView make_view(const sdfo_grid* g);
 // (grid.cu).
 int sparse_pair_records();
 void set_sparse_pair_records(int mode);
-// FP32-point sparse queries by the persistent walk kernel (query.cu)
-bool sparse_query_walk();
-void set_sparse_query_walk(bool on);
+// FP32-point queries by the persistent walk kernel (query.cu)
+bool query_walk();
+void set_query_walk(bool on);
 // Fills the stencil layouts from phin (grid.cu): dense xpair and cell8;
 // sparse 8^3 FP32 bricks: xpair as sparse_pair_records() selects.
 void build_stencil_layouts(sdfo_grid* g, cudaStream_t s);

@@ -107,7 +107,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [("host_chunk_queries", _I32), ("fill_ctas_per_sm", _I32), ("fill_tile_log2_x", _I32),
                 ("fill_tile_log2_y", _I32), ("lbvh_traversal", _I32), ("host_chunk_growth_pct", _I32),
                 ("host_io_mode", _I32), ("triangle_cull", _I32),
-                ("sparse_pair_records", _I32), ("sparse_query_walk", _I32)]
+                ("sparse_pair_records", _I32), ("query_walk", _I32)]
 
 
 class DeviceViews(ctypes.Structure):

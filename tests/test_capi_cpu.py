@@ -156,11 +156,11 @@ def test_tuning_round_trip(lib):
         assert t == {"host_chunk_queries": 65536, "fill_ctas_per_sm": 2, "fill_tile_log2_x": 2,
                      "fill_tile_log2_y": 2, "lbvh_traversal": 2, "host_chunk_growth_pct": 150,
                      "host_io_mode": 3, "triangle_cull": 1, "sparse_pair_records": 0,
-                     "sparse_query_walk": 2}
-        assert N.set_tuning(sparse_query_walk=1)["sparse_query_walk"] == 1
-        assert N.set_tuning(sparse_query_walk=0)["sparse_query_walk"] == 2
+                     "query_walk": 2}
+        assert N.set_tuning(query_walk=1)["query_walk"] == 1
+        assert N.set_tuning(query_walk=0)["query_walk"] == 2
         # a rejected tuning applies none of its fields
-        bad = N.Tuning(host_chunk_queries=4096, sparse_query_walk=3)
+        bad = N.Tuning(host_chunk_queries=4096, query_walk=3)
         assert lib.sdfo_set_tuning(ctypes.byref(bad)) == -1
         assert N.get_tuning()["host_chunk_queries"] == 65536
         assert N.set_tuning(sparse_pair_records=2)["sparse_pair_records"] == 2

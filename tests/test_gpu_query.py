@@ -258,39 +258,48 @@ def test_sparse_pair_records_bit_identical(cuda, mode):
 
 
 @pytest.mark.parametrize("mode", [2, 3])
-def test_sparse_query_walk_bit_identical(cuda, mode):
-    """The persistent walk kernel for sparse FP32-point queries (the default;
-    a tuning knob) answers every query bit for bit as the staged per-tile
-    kernel does: FP32 and FP16 pools, every output (the full and the
+def test_query_walk_bit_identical(cuda, mode):
+    """The persistent walk kernel for FP32-point queries (the default; a
+    tuning knob) answers every query bit for bit as the per-tile kernels do
+    (staged on sparse grids, the bulk-copy pipeline on dense ones): sparse
+    FP32 and FP16 pools and a dense grid, every output (the full and the
     symmetric Hessian included), and batch sizes below one tile, between
     tiles and above the resident CTA count."""
     import torch
 
     from sdfo import SdfGrid
     from sdfo import _native as N
+    from sdfo import workloads as W
 
     g = golden("sparse_cyl.npz")
     spec = dict(bmin=g["bmin"], bmax=g["bmax"], voxel=g["voxel"], shape=tuple(g["shape"]))
     grid = SdfGrid.from_sparse(spec, int(g["block_dim"]), g["ijk"], g["phi"], g["normal"], g["hessian"])
-    grids = [grid, grid.to_fp16()]
+    c = W.c2_cylinder()
+    dense = SdfGrid.build_dense(c["verts"], c["tris"], mode=3, target_resolution=64, max_resolution=64)
+    grids = [grid, grid.to_fp16(), dense]
     rng = np.random.default_rng(8)
-    pts = np.concatenate([g["pts"], rng.uniform(g["bmin"], g["bmax"], (700_000, 3))]).astype(np.float32)
     before = N.get_tuning()
     try:
         for gr in grids:
+            lo, hi = np.array(gr.bmin), np.array(gr.bmax)
+            pts = np.concatenate([g["pts"], rng.uniform(lo, hi, (700_000, 3))]).astype(np.float32)
             for n in (1, 255, 257, 40_000, len(pts)):
                 x = torch.tensor(pts[:n], device="cuda")
                 out = {}
                 for walk in (1, 2):
-                    N.set_tuning(sparse_query_walk=walk)
+                    N.set_tuning(query_walk=walk)
                     o = gr.query_tensors(x, mode=mode, unit=True, witness=True, valid=True)
+                    fast = gr.query_tensors(x, mode=mode, valid=True)
                     h = gr.query_tensors(x, mode=mode, valid=True, hess=True)
                     lin = gr.query_linearize(x, mode=mode)
                     torch.cuda.synchronize()
                     out[walk] = {k: v.cpu().numpy() for k, v in o.items()}
+                    out[walk].update({"f_" + k: v.cpu().numpy() for k, v in fast.items()})
                     out[walk].update({"h_" + k: v.cpu().numpy() for k, v in h.items()})
                     out[walk].update({"lin_" + k: v.cpu().numpy() for k, v in lin.items()})
+                if n == len(pts):
+                    assert out[1]["valid"].sum() > 1000
                 for k in out[1]:
-                    assert np.array_equal(out[1][k], out[2][k], equal_nan=True), (gr.storage, n, k)
+                    assert np.array_equal(out[1][k], out[2][k], equal_nan=True), (gr.storage, gr.is_sparse, n, k)
     finally:
         N.set_tuning(**before)
