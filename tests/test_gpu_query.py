@@ -198,27 +198,37 @@ def test_fp16_sparse_storage_error_bound(cuda, port):
     assert np.max(np.abs(d["phi"] - g["phi"])) <= bound
 
 
+@pytest.mark.parametrize("walk", [1, 2])
 @pytest.mark.parametrize("mode", [2, 3])
 @pytest.mark.parametrize("n", [255, 256 * 41, 256 * 41 + 97])
-def test_pipelined_dense_query_is_bit_identical(cuda, mode, n):
-    """Float32 points on a dense grid take the persistent bulk-copy pipeline
-    for whole tiles of 256 (the rest through the plain kernel); the same
-    points as float64 (the plain kernel throughout) give bit-identical gap,
-    gradient, valid flags and linearisation Hessians."""
+def test_pipelined_dense_query_is_bit_identical(cuda, mode, n, walk):
+    """Float32 points on a dense grid take the persistent walk kernel (the
+    default) or, with the walk off, the persistent bulk-copy pipeline for
+    whole tiles of 256 (the rest in one extra CTA); the Hessian-writing
+    forward always takes the pipeline.  The same points as float64 (the plain
+    kernel throughout) give bit-identical gap, gradient, valid flags and
+    linearisation Hessians."""
     import torch
 
     from sdfo import SdfGrid
+    from sdfo import _native as N
     from sdfo import meshes as M
 
     v, t = M.torus(0.05, 0.01, 48, 12)
     grid = SdfGrid.build_dense(v, t, target_resolution=40, max_resolution=40)
     rng = np.random.default_rng(n)
     p32 = torch.tensor(rng.uniform(grid.bmin, grid.bmax, (n, 3)).astype(np.float32), device="cuda")
-    a = grid.query_tensors(p32, mode=mode)
+    before = N.get_tuning()
+    try:
+        N.set_tuning(query_walk=walk)
+        a = grid.query_tensors(p32, mode=mode)
+        lin = grid.query_linearize(p32, mode=mode)
+        torch.cuda.synchronize()
+    finally:
+        N.set_tuning(**before)
     b = grid.query_tensors(p32.double(), mode=mode)
     for k in ("gap", "grad", "valid"):
         assert torch.equal(a[k], b[k]), k
-    lin = grid.query_linearize(p32, mode=mode)
     h = grid.query_tensors(p32.double(), mode=mode, hess=True)
     assert torch.equal(lin["gap"], h["gap"]) and torch.equal(lin["grad"], h["grad"])
     H = h["hess"].reshape(n, 9)[:, [0, 1, 2, 4, 5, 8]]

@@ -1,6 +1,7 @@
-"""Bounded waits of the bulk-copy pipelines run out without faulting or
-hanging, set their status bits, and the synchronous host entry points turn
-them into SDFO_ERR_DEVICE_STATUS instead of returning partial results.
+"""Bounded waits of the bulk-copy pipelines (the dense forward with the walk
+kernel off, and the saved backward) run out without faulting or hanging, set
+their status bits, and the synchronous host entry points turn them into
+SDFO_ERR_DEVICE_STATUS instead of returning partial results.
 
 The wait is made to run out through the test-only sdfo_debug_wait_test:
 every CTA skips the bulk load of its first tile (so that tile's mbarrier
@@ -51,7 +52,11 @@ def test_waits_run_out_and_are_reported(cuda):
     ref = {k: v.cpu().numpy() for k, v in ref.items()}
     _status(lib, clear=True)
     p = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    before = N.get_tuning()
     try:
+        # the dense forwards on the bulk-copy pipeline (the walk kernel, the
+        # default, has no bounded wait)
+        N.set_tuning(query_walk=1)
         N.check(lib.sdfo_debug_wait_test(1000, 1))
         # device path: the call is asynchronous and succeeds; the word
         # records the abort of the pipelined forward (bit 1)
@@ -88,6 +93,7 @@ def test_waits_run_out_and_are_reported(cuda):
         assert f & 1 and f & 2
     finally:
         N.check(lib.sdfo_debug_wait_test(0, 0))
+        N.set_tuning(**before)
         _status(lib, clear=True)
     # normal operation again: the same results as before, no status
     out = grid.query_host(pts, mode=3)
