@@ -222,6 +222,7 @@ __device__ __forceinline__ void split_h4(const float4 q, int k, float4& v)
     v = make_float4(a.x, a.y, b.x, b.y);
 }
 
+template <int ST = 0>
 __device__ __forceinline__ bool gather_rows_b8(const GridView& g, const Cell& c, float4 out[8])
 {
     constexpr int bd = 8, V = 512;
@@ -243,7 +244,8 @@ __device__ __forceinline__ bool gather_rows_b8(const GridView& g, const Cell& c,
     if ((s[0][0][0] | s[0][0][1] | s[0][1][0] | s[0][1][1] | s[1][0][0] | s[1][0][1] | s[1][1][0] |
          s[1][1][1]) < 0)
         return false;
-    const bool fp16 = g.storage == SDFO_STORAGE_FP16;
+    // ST: the pool's storage when the caller knows it (1 FP32, 2 FP16), else 0
+    const bool fp16 = ST == 2 || (ST == 0 && g.storage == SDFO_STORAGE_FP16);
     // FP16: the affine phi map of the cell's first brick, read once; rows in
     // other bricks (cells on a brick face) read theirs
     const float2 aff000 = fp16 ? __ldg(g.brick_affine + s[0][0][0]) : make_float2(0.f, 0.f);
@@ -475,7 +477,7 @@ __device__ __forceinline__ void unit_of(const float g[3], float u[3])
 
 // unit (the normalised gradient) is computed only when want_unit is set;
 // otherwise it is left unset for Trilinear / Tricubic.
-template <int MODE, bool SPARSE, int BD, bool HESS>
+template <int MODE, bool SPARSE, int BD, bool HESS, int ST = 0>
 __device__ __forceinline__ bool evaluate(const GridView& g, const double p[3], Interp& r,
                                          float unit[3], bool want_unit = true)
 {
@@ -510,7 +512,7 @@ __device__ __forceinline__ bool evaluate(const GridView& g, const double p[3], I
         }
         else if (SPARSE && BD == 8 && g.phin_a32)
         {
-            if (!gather_rows_b8(g, c, cs)) return false;
+            if (!gather_rows_b8<ST>(g, c, cs)) return false;
         }
         else
         {

@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS, SPARSE>())
 // one, and loads and stores go straight to global memory, so warps never wait
 // for one another (k_query stages points and records through shared memory
 // between CTA barriers).  Selected by sdfo_tuning.query_walk.
-template <int MODE, bool SPARSE, int BD, bool HESS, int MINB>
+template <int MODE, bool SPARSE, int BD, bool HESS, int MINB, int ST>
 __global__ void __launch_bounds__(kThreads, MINB)
     k_query_walk(GridView g, const float* __restrict__ pts, int64_t n, QueryOutputs o)
 {
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
         if (qc >= n) continue; // the tail of the last tile
         Interp r;
         float unit[3] = {1.f, 0.f, 0.f};
-        const bool valid = evaluate<MODE, SPARSE, BD, HESS>(g, p, r, unit, want_unit);
+        const bool valid = evaluate<MODE, SPARSE, BD, HESS, ST>(g, p, r, unit, want_unit);
         if (!valid)
         {
             r.gap = 0.f;
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
     }
 }
 
-template <int MODE, bool SPARSE, int BD, bool HESS, int MINB>
+template <int MODE, bool SPARSE, int BD, bool HESS, int MINB, int ST = 0>
 void launch_walk(const GridView& v, const float* pts, int64_t n, const QueryOutputs& o, cudaStream_t s)
 {
     static std::mutex mu;
@@ -308,14 +308,14 @@ void launch_walk(const GridView& v, const float* pts, int64_t n, const QueryOutp
         if (per_sm[dev & 63] == 0)
         {
             int r = 0;
-            SDFO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_query_walk<MODE, SPARSE, BD, HESS, MINB>, kThreads, 0));
+            SDFO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_query_walk<MODE, SPARSE, BD, HESS, MINB, ST>, kThreads, 0));
             per_sm[dev & 63] = r > 0 ? r : 1;
         }
         b = per_sm[dev & 63];
     }
     const int64_t ntiles = (n + kThreads - 1) / kThreads;
     const unsigned blocks = (unsigned)std::min<int64_t>(ntiles, (int64_t)current_sm_count() * b);
-    k_query_walk<MODE, SPARSE, BD, HESS, MINB><<<blocks, kThreads, 0, s>>>(v, pts, n, o);
+    k_query_walk<MODE, SPARSE, BD, HESS, MINB, ST><<<blocks, kThreads, 0, s>>>(v, pts, n, o);
 }
 
 // Reverse mode from the linearisation the forward saved (grad, symmetric
@@ -672,14 +672,22 @@ void launch_pt(const GridView& v, const void* pts, bool f64, int64_t n, const Qu
         if (!f64 && !o.host_mapped && query_walk() && (SPARSE || !hess))
         {
             const float* p32 = static_cast<const float*>(pts);
+            // sparse 8^3 bricks: the gather specialised on the pool's storage
+            constexpr bool b8 = SPARSE && BD == 8;
+            const bool fp32 = v.storage == SDFO_STORAGE_FP32;
             if (!hess)
-                launch_walk<MODE, SPARSE, BD, false, 4>(v, p32, n, o, s);
+            {
+                if (b8 && fp32)
+                    launch_walk<MODE, SPARSE, BD, false, 4, b8 ? 1 : 0>(v, p32, n, o, s);
+                else
+                    launch_walk<MODE, SPARSE, BD, false, 4, b8 ? 2 : 0>(v, p32, n, o, s);
+            }
             else if constexpr (SPARSE)
             {
-                if (v.storage == SDFO_STORAGE_FP32)
-                    launch_walk<MODE, SPARSE, BD, true, 3>(v, p32, n, o, s);
+                if (fp32)
+                    launch_walk<MODE, SPARSE, BD, true, 3, b8 ? 1 : 0>(v, p32, n, o, s);
                 else
-                    launch_walk<MODE, SPARSE, BD, true, 4>(v, p32, n, o, s);
+                    launch_walk<MODE, SPARSE, BD, true, 4, b8 ? 2 : 0>(v, p32, n, o, s);
             }
             return;
         }
