@@ -41,8 +41,9 @@ struct sdfo_query_batch
     // tile records for 128, 256 and 512 threads per CTA
     sdfo::DeviceBuffer<sdfo::BatchTile> tiles[3];
     int64_t ntiles[3] = {0, 0, 0};
-    // layouts of the grids: 0 all dense, 1 all sparse 8^3 bricks, 2 all other
-    // sparse, 3 mixed (the kernel is specialised on it)
+    // layouts of the grids: 0 all dense, 1 all sparse 8^3 bricks over FP32
+    // pools, 4 all sparse 8^3 bricks over FP16 pools, 2 all other sparse, 3
+    // mixed (the kernel is specialised on it)
     int kind = 3;
 };
 
@@ -81,7 +82,8 @@ template <int KIND, int MODE>
 __device__ __forceinline__ bool evaluate_kind(const GridView& v, const double p[3], Interp& r, float unit[3])
 {
     if constexpr (KIND == 0) return evaluate<MODE, false, 0, false>(v, p, r, unit);
-    else if constexpr (KIND == 1) return evaluate<MODE, true, 8, false>(v, p, r, unit);
+    else if constexpr (KIND == 1) return evaluate<MODE, true, 8, false, 1>(v, p, r, unit);
+    else if constexpr (KIND == 4) return evaluate<MODE, true, 8, false, 2>(v, p, r, unit);
     else if constexpr (KIND == 2) return evaluate<MODE, true, 0, false>(v, p, r, unit);
     else
     {
@@ -204,6 +206,7 @@ void launch_batch2(const sdfo_query_batch* b, int64_t ntiles, const BatchTile* t
     case 0: launch_batch3<MODE, THREADS, 0>(b, ntiles, t, pts, poses, gap, grad, valid, s); break;
     case 1: launch_batch3<MODE, THREADS, 1>(b, ntiles, t, pts, poses, gap, grad, valid, s); break;
     case 2: launch_batch3<MODE, THREADS, 2>(b, ntiles, t, pts, poses, gap, grad, valid, s); break;
+    case 4: launch_batch3<MODE, THREADS, 4>(b, ntiles, t, pts, poses, gap, grad, valid, s); break;
     default: launch_batch3<MODE, THREADS, 3>(b, ntiles, t, pts, poses, gap, grad, valid, s);
     }
 }
@@ -255,7 +258,11 @@ int sdfo_query_batch_create(const sdfo_grid* const* grids, int32_t n, const int6
         }
         SDFO_REQUIRE(ntiles128 < (int64_t(1) << 31), SDFO_ERR_INVALID_ARGUMENT, "too many queries in one batch");
         b->device = grids[0]->device;
-        auto kind_of = [](const GridView& v) { return v.layout == SDFO_LAYOUT_DENSE ? 0 : (v.bd == 8 ? 1 : 2); };
+        auto kind_of = [](const GridView& v) {
+            if (v.layout == SDFO_LAYOUT_DENSE) return 0;
+            if (v.bd != 8) return 2;
+            return v.storage == SDFO_STORAGE_FP16 ? 4 : 1;
+        };
         b->kind = kind_of(views[0]);
         for (int g = 1; g < n; ++g)
             if (kind_of(views[(size_t)g]) != b->kind) b->kind = 3;

@@ -207,7 +207,7 @@ def test_query_batch_identity_pose_equals_single_queries(cuda, port):
         assert torch.allclose(grad[s], one["grad"], rtol=0, atol=1e-6)
 
 
-@pytest.mark.parametrize("kind", ["sparse", "dense"])
+@pytest.mark.parametrize("kind", ["sparse", "sparse16", "dense"])
 def test_query_batch_ragged_counts(cuda, kind):
     """The persistent batch kernel walks runs of tiles in grid-stride order:
     grids with no queries between others, tails shorter than a CTA, more
@@ -222,10 +222,12 @@ def test_query_batch_ragged_counts(cuda, kind):
     from sdfo import workloads as W
     from sdfo.batch import QueryBatch
 
-    if kind == "sparse":
+    if kind in ("sparse", "sparse16"):
         gears = W.c4_gears(n_gears=3, seed=5)
         _set_mode(0)
         base = SdfGrid.build_sparse_batched([_mesh_args(g) for g in gears], mode=3)
+        if kind == "sparse16":
+            base = [b.to_fp16() for b in base]
         meshes = [(g["verts"], g["tris"]) for g in gears]
     else:
         cv, ct = M.cube(0.1)
