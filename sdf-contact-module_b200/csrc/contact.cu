@@ -34,6 +34,11 @@ namespace sdfo {
 namespace {
 
 constexpr int kContactThreads = 256;
+// Jacobian pass: the points of a span of kJacSpan points that are in contact
+// are listed per warp (a warp meets at most kJacSpan / 8 of them), then all
+// warps share the span's list.
+constexpr int kJacSpan = 4096;
+constexpr int kJacPerWarp = kJacSpan / (kContactThreads / 32);
 
 struct v3
 {
@@ -306,7 +311,7 @@ __global__ void __launch_bounds__(kContactThreads,
     __shared__ sdfo_body_state sA, sB;
     __shared__ double red[kWarps][6];
     __shared__ double sjac[JAC ? kWarps : 1][JAC ? 36 : 1];
-    __shared__ int s_list[JAC ? kContactThreads : 1];
+    __shared__ int s_list[JAC ? kJacSpan : 1];
     __shared__ int s_wcnt[kWarps];
     __shared__ unsigned s_mask[EXT ? kMaxCullLeaves / 32 : 1];
     __shared__ double s_box[6];
@@ -378,13 +383,22 @@ __global__ void __launch_bounds__(kContactThreads,
     MinRec best{INFINITY, INT_MAX, -1};
     int nvalid = 0, nactive = 0;
 
-    // block-uniform trip count: the barriers and warp reductions below see
-    // every thread
-    for (int i0 = 0; i0 < nq; i0 += kContactThreads)
+    // Spans of kJacSpan points (one span over all points without the
+    // Jacobian).  First every point's forward; with the Jacobian, each warp
+    // lists its points in contact, in point order, with no barrier.  Then
+    // the span's list is shared out: group k of 32 consecutive entries to
+    // warp k mod 8, so all warps carry the FP64 Jacobian work, and the sums
+    // run in a fixed order (repeated runs are bit-identical).  Block-uniform
+    // trip counts: the barriers and warp reductions below see every thread.
+    for (int s0 = 0; s0 < nq; s0 += JAC ? kJacSpan : nq)
+    {
+    const int s1 = JAC ? min(nq, s0 + kJacSpan) : nq;
+    int wcnt = 0; // this warp's listed points in the span (warp-uniform)
+    for (int i0 = s0; i0 < s1; i0 += kContactThreads)
     {
         const int i = i0 + threadIdx.x;
         bool act = false;
-        if (i < nq)
+        if (i < s1)
         {
             bool sel = true;
             if (EXT && !full)
@@ -418,27 +432,45 @@ __global__ void __launch_bounds__(kContactThreads,
                 }
             }
         }
-        if (!JAC) continue;
-        const unsigned m = __ballot_sync(0xffffffffu, act);
-        if (lane == 0) s_wcnt[warp] = __popc(m);
-        __syncthreads();
-        int off = 0, total = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w)
+        if (JAC)
         {
-            const int c = s_wcnt[w];
-            off += w < warp ? c : 0;
-            total += c;
+            const unsigned m = __ballot_sync(0xffffffffu, act);
+            if (act) s_list[warp * kJacPerWarp + wcnt + __popc(m & ((1u << lane) - 1u))] = i;
+            wcnt += __popc(m);
         }
-        if (act) s_list[off + __popc(m & ((1u << lane) - 1u))] = i;
+    }
+    if (JAC)
+    {
+        if (lane == 0) s_wcnt[warp] = wcnt;
         __syncthreads();
-        if (warp * 32 < total)
+        int total = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) total += s_wcnt[w];
+        for (int k = warp; 32 * k < total; k += kWarps) // warp-uniform
         {
+            const int e = 32 * k + lane;
+            bool mine = e < total;
+            int idx = 0;
+            if (mine)
+            {
+                // entry e of the span's list: warp src's list, position rem
+                int rem = e, src = 0;
+#pragma unroll
+                for (int w = 0; w < kWarps; ++w)
+                {
+                    const int c = s_wcnt[w];
+                    if (src == w && rem >= c)
+                    {
+                        rem -= c;
+                        ++src;
+                    }
+                }
+                idx = s_list[src * kJacPerWarp + rem];
+            }
             PointState st;
             double gap = 0.0;
-            const bool mine = threadIdx.x < total &&
-                              point_state<MODE, SPARSE, BD, true>(g, qx, qw, s_list[threadIdx.x], sA, sB, f,
-                                                                  prm, narrow, false, st, gap) == 2;
+            mine = mine && point_state<MODE, SPARSE, BD, true>(g, qx, qw, idx, sA, sB, f, prm, narrow, false,
+                                                               st, gap) == 2;
 #pragma unroll 1
             for (int j = 0; j < 6; ++j)
             {
@@ -452,7 +484,8 @@ __global__ void __launch_bounds__(kContactThreads,
                 }
             }
         }
-        __syncthreads(); // s_list and s_wcnt are rewritten by the next chunk
+        __syncthreads(); // s_list and s_wcnt are rewritten by the next span
+    }
     }
     if (want_force)
     {
