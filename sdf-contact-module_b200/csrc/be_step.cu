@@ -97,6 +97,11 @@ struct BeView
 };
 
 constexpr int kJac = 72; // Jp (36) then Jv (36), row-major 6x6 each
+// Cache positions without per-chunk barriers (CTA per scene): one count per
+// (chunk, warp) of the narrow-filtered points, then their exclusive prefix;
+// up to kPrefCap entries (32,768 points at 256 threads), larger point sets
+// take the per-chunk block scan.
+constexpr int kPrefCap = 1024;
 
 struct MinRec
 {
@@ -135,6 +140,10 @@ struct Shared
     // warp of the scene; after the reduction row 0 holds Jp then Jv)
     double* jred;
     int n_newton, n_resid, n_solves; // this launch's counts for the scene
+    // (CTA per scene) per-(chunk, warp) filtered-point counts, then their
+    // exclusive prefix, and the total; NULL in the warp-per-scene variant
+    int* pref;
+    int pref_total;
 };
 
 // ---------------------------------------------------------------- helpers
@@ -497,17 +506,62 @@ __device__ void eval_pass(const BeView& b, Shared& s)
     if (JAC && lane == 0)
         for (int e = 0; e < kJac; ++e) jrow[e] = 0.0;
     // the number of narrow-filtered points decides whether the cache is used
+    const int nw = Grp<W>::warps();
+    const bool fast = !W && ((b.nq + Grp<W>::size() - 1) / Grp<W>::size()) * nw <= kPrefCap;
+    const unsigned lt = (1u << lane) - 1u;
     int L = 0;
-    for (int c0 = 0; c0 < b.nq; c0 += Grp<W>::size())
+    if (fast)
     {
-        double X[3], w, Y[3];
-        bool f = false;
-        if (point_at(b, s, c0 + Grp<W>::rank(), X, w))
+        // counts per (chunk, warp), no barrier in the loop
+        for (int c0 = 0, k = 0; c0 < b.nq; c0 += Grp<W>::size(), ++k)
         {
-            to_sdf(s, X, Y);
-            f = fabs(Y[2]) < narrow;
+            double X[3], w, Y[3];
+            bool f = false;
+            if (point_at(b, s, c0 + Grp<W>::rank(), X, w))
+            {
+                to_sdf(s, X, Y);
+                f = fabs(Y[2]) < narrow;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, f);
+            if (lane == 0) s.pref[k * nw + warp] = __popc(bal);
         }
-        L += Grp<W>::count(f);
+        Grp<W>::sync();
+        if (warp == 0)
+        {
+            // exclusive prefix in (chunk, warp) order = point order
+            const int E = ((b.nq + Grp<W>::size() - 1) / Grp<W>::size()) * nw;
+            int carry = 0;
+            for (int e0 = 0; e0 < E; e0 += 32)
+            {
+                const int e = e0 + lane;
+                const int v = e < E ? s.pref[e] : 0;
+                int x = v;
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const int y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += y;
+                }
+                if (e < E) s.pref[e] = carry + x - v;
+                carry += __shfl_sync(0xffffffffu, x, 31);
+            }
+            if (lane == 0) s.pref_total = carry;
+        }
+        Grp<W>::sync();
+        L = s.pref_total;
+    }
+    else
+    {
+        for (int c0 = 0; c0 < b.nq; c0 += Grp<W>::size())
+        {
+            double X[3], w, Y[3];
+            bool f = false;
+            if (point_at(b, s, c0 + Grp<W>::rank(), X, w))
+            {
+                to_sdf(s, X, Y);
+                f = fabs(Y[2]) < narrow;
+            }
+            L += Grp<W>::count(f);
+        }
     }
     double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (L > 0)
@@ -518,7 +572,7 @@ __device__ void eval_pass(const BeView& b, Shared& s)
         matTvec(b.RB, d, tsdf);
         const int64_t base_c = (int64_t)s.scene * b.nq;
         int base = 0;
-        for (int c0 = 0; c0 < b.nq; c0 += Grp<W>::size())
+        for (int c0 = 0, k = 0; c0 < b.nq; c0 += Grp<W>::size(), ++k)
         {
             double X[3], w = 0.0, Y[3];
             bool f = false;
@@ -527,9 +581,18 @@ __device__ void eval_pass(const BeView& b, Shared& s)
                 to_sdf(s, X, Y);
                 f = fabs(Y[2]) < narrow;
             }
-            int total;
-            const int pos = base + chunk_scan<W>(s, f, total);
-            base += total;
+            int pos;
+            if (fast)
+            {
+                // the same flags as the counting loop: position from the prefix
+                pos = s.pref[k * nw + warp] + __popc(__ballot_sync(0xffffffffu, f) & lt);
+            }
+            else
+            {
+                int total;
+                pos = base + chunk_scan<W>(s, f, total);
+                base += total;
+            }
             bool act = false;
             double fq[3] = {0.0, 0.0, 0.0}, off[3] = {0.0, 0.0, 0.0};
             double Gt[9], U[9];
@@ -655,21 +718,20 @@ __device__ void measure_pass(const BeView& b, Shared& s)
     broad_phase<W>(b, s);
     MinRec best{INFINITY, INT_MAX, -1};
     int nv = 0, na = 0;
-    int base = 0;
+    // ties of the minimum go to the first kept point; the list index orders
+    // kept points as their positions among the kept points do, so it serves
+    // as the key and the loop needs no block scan
     for (int c0 = 0; c0 < b.nq; c0 += Grp<W>::size())
     {
         double X[3], w, Y[3];
-        const bool kept = point_at(b, s, c0 + Grp<W>::rank(), X, w);
-        int total;
-        const int pos = base + chunk_scan<W>(s, kept, total);
-        base += total;
-        if (!kept) continue;
+        const int i = c0 + Grp<W>::rank();
+        if (!point_at(b, s, i, X, w)) continue;
         to_sdf(s, X, Y);
         double g, gr[3];
         if (!sample64(b, Y, g, gr)) continue;
         ++nv;
         if (g < 0.0) ++na;
-        if (g < best.gap || (g == best.gap && pos < best.key)) best = MinRec{g, pos, c0 + Grp<W>::rank()};
+        if (g < best.gap || (g == best.gap && i < best.key)) best = MinRec{g, i, i};
     }
     const int warp = Grp<W>::warp(), lane = (int)(threadIdx.x & 31);
     for (int o = 16; o > 0; o >>= 1)
@@ -704,7 +766,7 @@ __device__ void measure_pass(const BeView& b, Shared& s)
         s.m_gap = v ? m.gap : INFINITY;
         s.m_pen = v && m.gap < 0.0 ? -m.gap : 0.0;
         s.m_vn = 0.0;
-        s.count = v ? m.key : -1;
+        s.count = v ? m.key : -1; // the minimum's point index
         s.mi = v ? m.i : -1;
     }
     Grp<W>::sync();
@@ -1125,6 +1187,7 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 3 : 4) k_be_step(BeView b
                                                 int* __restrict__ unfinished)
 {
     __shared__ Shared shared_scenes[W ? T / 32 : 1];
+    __shared__ int pref_table[W ? 1 : kPrefCap];
     // exact tangent: one row of Jacobian partial sums per warp, in dynamic
     // shared memory (jac_smem_bytes<T>(); the warp-per-scene variant's static
     // state alone nearly fills the 48 KB static limit)
@@ -1136,6 +1199,7 @@ __global__ void __launch_bounds__(T, (W || T == 256) ? 3 : 4) k_be_step(BeView b
     if (Grp<W>::rank() == 0)
     {
         s.jred = EXACT ? jred_rows + (W ? (int)(threadIdx.x >> 5) * kJac : 0) : nullptr;
+        s.pref = W ? nullptr : pref_table;
         s.n_newton = s.n_resid = s.n_solves = 0;
         s.scene = sc;
         const sdfo_be_scene& in = scenes[sc];
