@@ -37,7 +37,7 @@ struct BatchMeta
 };
 
 template <class Tree>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, SDFO_FILL_MIN_BLOCKS)
     k_batch_activate(const Tree* __restrict__ trees, const BatchMeta* __restrict__ meta,
                      const int64_t* __restrict__ cand_offs, int n, int bd, int64_t total,
                      int32_t* __restrict__ flags, int* status)
@@ -93,9 +93,10 @@ __global__ void k_batch_table(const BatchMeta* __restrict__ meta, const int64_t*
 }
 
 // Persistent brick fill: CTAs loop taking the next brick from `next` until
-// the bricks run out (the counter only grows, so every CTA ends).
+// the bricks run out (the counter only grows, so every CTA ends).  Register
+// budget as the single-mesh fills (SDFO_FILL_MIN_BLOCKS CTAs per SM).
 template <class Tree>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, SDFO_FILL_MIN_BLOCKS)
     k_batch_fill(const Tree* __restrict__ trees, const BatchMeta* __restrict__ meta,
                  const int64_t* __restrict__ slot_offs, int n, int bd, int64_t nbricks,
                  const int32_t* __restrict__ ijk, float4* __restrict__ phin,
