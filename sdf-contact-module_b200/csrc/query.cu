@@ -243,10 +243,49 @@ __global__ void __launch_bounds__(kThreads, query_min_blocks<HESS, SPARSE>())
 // one, and loads and stores go straight to global memory, so warps never wait
 // for one another (k_query stages points and records through shared memory
 // between CTA barriers).  Selected by sdfo_tuning.query_walk.
+// Records of K floats of a warp's 32 consecutive queries q0 .. q0 + cnt - 1,
+// stored through the warp's slice of shared memory (32 K floats): each lane
+// writes its record, then the warp writes the slice out as contiguous 16-byte
+// stores (a full warp) or contiguous 4-byte stores (the tail of the last
+// tile).  Without this, each of a lane's K strided 4-byte stores touches K
+// cache lines per warp instruction.  `direct`: the output is not 16-byte
+// aligned; each lane stores its record itself.
+template <int K>
+__device__ __forceinline__ void warp_store(float* __restrict__ slice, float* __restrict__ out, int64_t q0,
+                                           int cnt, const float v[K], bool direct)
+{
+    const int lane = (int)(threadIdx.x & 31);
+    if (direct)
+    {
+        if (lane < cnt)
+#pragma unroll
+            for (int a = 0; a < K; ++a) __stcs(out + K * (q0 + lane) + a, v[a]);
+        return;
+    }
+#pragma unroll
+    for (int a = 0; a < K; ++a) slice[K * lane + a] = v[a];
+    __syncwarp();
+    float* dst = out + K * q0;
+    if (cnt == 32)
+    {
+        // 32 K floats = 8 K float4, at a 16-byte aligned address (q0 is a
+        // multiple of 32)
+        const float4* src = reinterpret_cast<const float4*>(slice);
+        for (int i = lane; i < 8 * K; i += 32) __stcs(reinterpret_cast<float4*>(dst) + i, src[i]);
+    }
+    else
+    {
+        for (int i = lane; i < K * cnt; i += 32) __stcs(dst + i, slice[i]);
+    }
+    __syncwarp(); // the slice is rewritten by the next tile
+}
+
 template <int MODE, bool SPARSE, int BD, bool HESS, int MINB, int ST>
 __global__ void __launch_bounds__(kThreads, MINB)
     k_query_walk(GridView g, const float* __restrict__ pts, int64_t n, QueryOutputs o)
 {
+    // Hessian records (6 or 9 floats) leave through per-warp slices
+    __shared__ __align__(16) float stage[HESS ? kThreads * 9 : 1];
     const int64_t ntiles = (n + kThreads - 1) / kThreads;
     const int64_t t_begin = ntiles * blockIdx.x / gridDim.x;
     const int64_t t_end = ntiles * (blockIdx.x + 1) / gridDim.x;
@@ -255,6 +294,10 @@ __global__ void __launch_bounds__(kThreads, MINB)
     if (t_begin < t_end && q < n)
         for (int a = 0; a < 3; ++a) xn[a] = __ldcs(pts + 3 * q + a);
     const bool want_unit = o.unit != nullptr || o.witness != nullptr;
+    const int lane = (int)(threadIdx.x & 31);
+    float* slice = stage + (HESS ? (threadIdx.x >> 5) * 32 * 9 : 0);
+    const bool h6_direct = (reinterpret_cast<uintptr_t>(o.hess6) & 15) != 0;
+    const bool h9_direct = (reinterpret_cast<uintptr_t>(o.hess) & 15) != 0;
     for (int64_t t = t_begin; t < t_end; ++t)
     {
         const int64_t qc = q;
@@ -262,10 +305,13 @@ __global__ void __launch_bounds__(kThreads, MINB)
         q += kThreads;
         if (t + 1 < t_end && q < n)
             for (int a = 0; a < 3; ++a) xn[a] = __ldcs(pts + 3 * q + a);
-        if (qc >= n) continue; // the tail of the last tile
+        // the tail of the last tile: lanes past n skip the work but (HESS)
+        // still take part in their warp's staged stores
+        const bool live = qc < n;
+        if (!HESS && !live) continue;
         Interp r;
         float unit[3] = {1.f, 0.f, 0.f};
-        const bool valid = evaluate<MODE, SPARSE, BD, HESS, ST>(g, p, r, unit, want_unit);
+        const bool valid = live && evaluate<MODE, SPARSE, BD, HESS, ST>(g, p, r, unit, want_unit);
         if (!valid)
         {
             r.gap = 0.f;
@@ -275,22 +321,30 @@ __global__ void __launch_bounds__(kThreads, MINB)
 #pragma unroll
             for (int a = 0; a < 6; ++a) r.H[a] = 0.f;
         }
-        __stcs(o.gap + qc, r.gap);
-        if (o.valid) o.valid[qc] = valid ? 1 : 0;
-        if (o.grad)
-            for (int a = 0; a < 3; ++a) __stcs(o.grad + 3 * qc + a, r.g[a]);
-        if (o.unit)
-            for (int a = 0; a < 3; ++a) __stcs(o.unit + 3 * qc + a, unit[a]);
-        if (o.witness)
-            for (int a = 0; a < 3; ++a)
-                __stcs(o.witness + 3 * qc + a, valid ? (float)(p[a] - (double)r.gap * unit[a]) : 0.f);
-        if (HESS && o.hess6)
-            for (int a = 0; a < 6; ++a) __stcs(o.hess6 + 6 * qc + a, r.H[a]);
-        if (HESS && o.hess)
+        if (live)
         {
-            const float H9[9] = {r.H[0], r.H[1], r.H[2], r.H[1], r.H[3], r.H[4], r.H[2], r.H[4], r.H[5]};
-#pragma unroll
-            for (int a = 0; a < 9; ++a) __stcs(o.hess + 9 * qc + a, H9[a]);
+            __stcs(o.gap + qc, r.gap);
+            if (o.valid) o.valid[qc] = valid ? 1 : 0;
+            if (o.grad)
+                for (int a = 0; a < 3; ++a) __stcs(o.grad + 3 * qc + a, r.g[a]);
+            if (o.unit)
+                for (int a = 0; a < 3; ++a) __stcs(o.unit + 3 * qc + a, unit[a]);
+            if (o.witness)
+                for (int a = 0; a < 3; ++a)
+                    __stcs(o.witness + 3 * qc + a, valid ? (float)(p[a] - (double)r.gap * unit[a]) : 0.f);
+        }
+        if constexpr (HESS)
+        {
+            // warp-uniform: the warp's first query and how many of its 32 exist
+            const int64_t qw = qc - lane;
+            const int64_t left = n - qw;
+            const int cnt = left >= 32 ? 32 : (left > 0 ? (int)left : 0);
+            if (o.hess6) warp_store<6>(slice, o.hess6, qw, cnt, r.H, h6_direct);
+            if (o.hess)
+            {
+                const float H9[9] = {r.H[0], r.H[1], r.H[2], r.H[1], r.H[3], r.H[4], r.H[2], r.H[4], r.H[5]};
+                warp_store<9>(slice, o.hess, qw, cnt, H9, h9_direct);
+            }
         }
     }
 }
@@ -669,7 +723,9 @@ void launch_pt(const GridView& v, const void* pts, bool f64, int64_t n, const Qu
     if constexpr (MODE == SDFO_TRILINEAR || MODE == SDFO_TRICUBIC)
     {
         const bool hess = o.hess || o.hess6;
-        if (!f64 && !o.host_mapped && query_walk() && (SPARSE || !hess))
+        // dense grids: the full 3x3 Hessian too (the bulk-copy pipeline
+        // writes only the 6 unique entries)
+        if (!f64 && !o.host_mapped && query_walk() && (SPARSE || !hess || o.hess))
         {
             const float* p32 = static_cast<const float*>(pts);
             // sparse 8^3 bricks: the gather specialised on the pool's storage
@@ -682,13 +738,10 @@ void launch_pt(const GridView& v, const void* pts, bool f64, int64_t n, const Qu
                 else
                     launch_walk<MODE, SPARSE, BD, false, 4, b8 ? 2 : 0>(v, p32, n, o, s);
             }
-            else if constexpr (SPARSE)
-            {
-                if (fp32)
-                    launch_walk<MODE, SPARSE, BD, true, 3, b8 ? 1 : 0>(v, p32, n, o, s);
-                else
-                    launch_walk<MODE, SPARSE, BD, true, 4, b8 ? 2 : 0>(v, p32, n, o, s);
-            }
+            else if (fp32)
+                launch_walk<MODE, SPARSE, BD, true, 3, b8 ? 1 : 0>(v, p32, n, o, s);
+            else
+                launch_walk<MODE, SPARSE, BD, true, 4, b8 ? 2 : 0>(v, p32, n, o, s);
             return;
         }
     }
