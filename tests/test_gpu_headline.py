@@ -4,7 +4,7 @@
   Tricubic points of the benchmark (surface points offset along the face
   normal by N(0, (2h)^2), seed 1), queried exactly as the benchmark does:
   float32 points, gap + raw gradient + valid, through ``sdfo_query`` (the
-  persistent bulk-copy kernel on dense float32 grids).
+  persistent walk kernel, the default for float32 points).
 * Cube 0.1 m, dense 64^3 with 4 voxels of padding, 100,000 uniform points in
   the grid box (seed 0), Trilinear, same outputs.
 
