@@ -175,3 +175,37 @@ def test_lbvh_mode_contact_aware(cuda):
     b = _gpu_build(g, bvh=1).export_candidates()
     for k in a:
         assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("name", ["ca_dense_torus", "ca_sparse_gear"])
+def test_contact_aware_walk_bit_identical(cuda, name):
+    """The persistent walk kernel for ContactAware queries of float32 points
+    on sparse grids (the default there; sdfo_tuning.query_walk) gives every
+    output and candidate list bit for bit as the one-CTA-per-tile kernel
+    does, for batches below one tile, between tiles and above the resident
+    CTA count; dense grids take the per-tile kernel either way."""
+    import torch
+
+    from sdfo import _native as N
+
+    g = golden(f"{name}.npz")
+    grid = _gpu_build(g)
+    rng = np.random.default_rng(12)
+    lo, hi = np.array(grid.bmin), np.array(grid.bmax)
+    pts = np.concatenate([g["pts"], rng.uniform(lo, hi, (400_000, 3))]).astype(np.float32)
+    before = N.get_tuning()
+    try:
+        for n in (1, 255, 257, len(pts)):
+            x = torch.tensor(pts[:n], device="cuda")
+            out = {}
+            for walk in (1, 2):
+                N.set_tuning(query_walk=walk)
+                c = grid.query_candidates(x, mode=4)
+                q = grid.query_tensors(x, mode=4, unit=True, witness=True, valid=True)
+                torch.cuda.synchronize()
+                out[walk] = {k: v.cpu().numpy() for k, v in c.items()}
+                out[walk].update({"q_" + k: v.cpu().numpy() for k, v in q.items()})
+            for k in out[1]:
+                assert np.array_equal(out[1][k], out[2][k], equal_nan=True), (n, k)
+    finally:
+        N.set_tuning(**before)
