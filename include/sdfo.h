@@ -227,9 +227,11 @@ int sdfo_device_check(int device);
 int sdfo_device_cache(int64_t limit, int64_t* held);
 
 /* Status word the kernels with bounded waits set instead of hanging (bit 0:
- * a bulk-copy wait of the backward pipeline ran out; bit 1: one of the
- * pipelined query kernel); synchronous read,
- * cleared when `clear` != 0.  0 in normal operation.  The synchronous host
+ * a bulk-copy wait of the saved backward's pipeline ran out; bit 1: a wait
+ * of the pipelined dense query kernel ran out -- with the default
+ * sdfo_tuning.query_walk only the dense linearising forward runs that
+ * kernel); synchronous read, cleared when `clear` != 0.  0 in normal
+ * operation.  The synchronous host
  * entry points (sdfo_query_host, sdfo_query_host_static) read bit 1 in
  * stream order themselves and return SDFO_ERR_DEVICE_STATUS (clearing it)
  * when it is set; after the asynchronous calls (sdfo_query,
