@@ -286,7 +286,8 @@ typedef struct
                                     records then stay in L2; larger pools gather
                                     from DRAM, where the doubled footprint costs
                                     more), 1 = always, 2 = never */
-    int32_t query_walk;         /* Trilinear / Tricubic queries (and ContactAware
+    int32_t query_walk;         /* Trilinear / Tricubic queries and their
+                                   regathering backward for dL/dp (and ContactAware
                                    queries of sparse grids) of FP32 points with
                                    results in device memory: 2 = persistent CTAs
                                    over contiguous tile ranges, next point

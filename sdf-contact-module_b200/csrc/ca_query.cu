@@ -229,7 +229,10 @@ void launch_ca2(const GridView& v, const void* pts, bool f64, int64_t n, const Q
     const unsigned blocks = (unsigned)((n + kThreads - 1) / kThreads);
     // sparse grids only: measured on the hollow cylinder's candidate grids
     // (1M points), the walk took sparse queries from 10.2 to 11.6 G/s but
-    // dense ones (FP64 candidates, 4 per voxel) from 13.5 down to 10.4
+    // dense ones (FP64 candidates, 4 per voxel) from 13.5 down to 10.4 (10.7
+    // in grid-stride order): there the work per query varies (voxels without
+    // candidates answer with a FirstOrder query), which fresh CTAs balance
+    // and a fixed persistent assignment does not
     if (SPARSE && !f64 && query_walk())
     {
         static std::mutex mu;

@@ -484,6 +484,92 @@ __global__ void __launch_bounds__(kThreads)
     scatter_grid_gradient<MODE, SPARSE, BD>(g, cell_of(g, p), dG, dg, dgrid);
 }
 
+// Persistent variant of k_query_backward (sdfo_tuning.query_walk): CTA c
+// walks the contiguous tile range [ntiles c / G, ntiles (c + 1) / G) of
+// kThreads queries, and each thread loads the next tile's point and upstream
+// gradients before it regathers the current one.
+template <int MODE, bool SPARSE, int BD, int ST, bool DGRID>
+__global__ void __launch_bounds__(kThreads, 3)
+    k_query_backward_walk(GridView g, const float* __restrict__ pts, int64_t n,
+                          const float* __restrict__ dgap, const float* __restrict__ dgrad,
+                          float* __restrict__ dpts, float* __restrict__ dgrid)
+{
+    const int64_t ntiles = (n + kThreads - 1) / kThreads;
+    const int64_t t_begin = ntiles * blockIdx.x / gridDim.x;
+    const int64_t t_end = ntiles * (blockIdx.x + 1) / gridDim.x;
+    int64_t q = t_begin * kThreads + threadIdx.x;
+    float xn[3] = {0.f, 0.f, 0.f}, dGn = 0.f, dgn[3] = {0.f, 0.f, 0.f};
+    auto fetch = [&](int64_t i) {
+        for (int a = 0; a < 3; ++a) xn[a] = __ldcs(pts + 3 * i + a);
+        if (dgap) dGn = __ldcs(dgap + i);
+        if (dgrad)
+            for (int a = 0; a < 3; ++a) dgn[a] = __ldcs(dgrad + 3 * i + a);
+    };
+    if (t_begin < t_end && q < n) fetch(q);
+    for (int64_t t = t_begin; t < t_end; ++t)
+    {
+        const int64_t qc = q;
+        const double p[3] = {xn[0], xn[1], xn[2]};
+        const float dG = dGn;
+        const float dg[3] = {dgn[0], dgn[1], dgn[2]};
+        q += kThreads;
+        if (t + 1 < t_end && q < n) fetch(q);
+        if (qc >= n) continue; // the tail of the last tile
+        Interp r;
+        float unit[3];
+        const bool ok = evaluate<MODE, SPARSE, BD, true, ST>(g, p, r, unit, false);
+        if (dpts)
+        {
+            const float* H = r.H;
+            float o3[3] = {0.f, 0.f, 0.f};
+            if (ok)
+            {
+                o3[0] = dG * r.g[0] + H[0] * dg[0] + H[1] * dg[1] + H[2] * dg[2];
+                o3[1] = dG * r.g[1] + H[1] * dg[0] + H[3] * dg[1] + H[4] * dg[2];
+                o3[2] = dG * r.g[2] + H[2] * dg[0] + H[4] * dg[1] + H[5] * dg[2];
+            }
+            for (int a = 0; a < 3; ++a) __stcs(dpts + 3 * qc + a, o3[a]);
+        }
+        if (DGRID && ok) scatter_grid_gradient<MODE, SPARSE, BD>(g, cell_of(g, p), dG, dg, dgrid);
+    }
+}
+
+template <int MODE, bool SPARSE, int BD, int ST, bool DGRID>
+void launch_bwd_walk2(const GridView& v, const float* pts, int64_t n, const float* dgap, const float* dgrad,
+                     float* dpts, float* dgrid, cudaStream_t s)
+{
+    static std::mutex mu;
+    static int per_sm[64] = {0};
+    int dev = 0;
+    SDFO_CUDA(cudaGetDevice(&dev));
+    int b;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (per_sm[dev & 63] == 0)
+        {
+            int r = 0;
+            SDFO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &r, k_query_backward_walk<MODE, SPARSE, BD, ST, DGRID>, kThreads, 0));
+            per_sm[dev & 63] = r > 0 ? r : 1;
+        }
+        b = per_sm[dev & 63];
+    }
+    const int64_t ntiles = (n + kThreads - 1) / kThreads;
+    const unsigned blocks = (unsigned)std::min<int64_t>(ntiles, (int64_t)current_sm_count() * b);
+    k_query_backward_walk<MODE, SPARSE, BD, ST, DGRID><<<blocks, kThreads, 0, s>>>(v, pts, n, dgap, dgrad, dpts,
+                                                                                 dgrid);
+}
+
+// points only: the walk with the grid-gradient scatter needs more than 80
+// registers (100-250 bytes of spills), so that backward keeps the per-tile
+// kernel
+template <int MODE, bool SPARSE, int BD, int ST>
+void launch_bwd_walk(const GridView& v, const float* pts, int64_t n, const float* dgap, const float* dgrad,
+                     float* dpts, cudaStream_t s)
+{
+    launch_bwd_walk2<MODE, SPARSE, BD, ST, false>(v, pts, n, dgap, dgrad, dpts, nullptr, s);
+}
+
 template <int MODE, bool SPARSE, int BD, bool HESS>
 void launch_pt2(const GridView& v, const void* pts, bool f64, bool staged, int64_t n,
                 const QueryOutputs& o, cudaStream_t s)
@@ -778,6 +864,18 @@ template <int MODE>
 void launch_bwd_mode(const GridView& v, const float* pts, int64_t n, const float* dgap,
                      const float* dgrad, float* dpts, float* dgrid, cudaStream_t s)
 {
+    if (query_walk() && !dgrid)
+    {
+        if (v.layout == SDFO_LAYOUT_DENSE)
+            launch_bwd_walk<MODE, false, 0, 0>(v, pts, n, dgap, dgrad, dpts, s);
+        else if (v.bd == 8 && v.storage == SDFO_STORAGE_FP32)
+            launch_bwd_walk<MODE, true, 8, 1>(v, pts, n, dgap, dgrad, dpts, s);
+        else if (v.bd == 8)
+            launch_bwd_walk<MODE, true, 8, 2>(v, pts, n, dgap, dgrad, dpts, s);
+        else
+            launch_bwd_walk<MODE, true, 0, 0>(v, pts, n, dgap, dgrad, dpts, s);
+        return;
+    }
     const unsigned blocks = (unsigned)((n + kThreads - 1) / kThreads);
     if (v.layout == SDFO_LAYOUT_DENSE)
         k_query_backward<MODE, false, 0><<<blocks, kThreads, 0, s>>>(v, pts, n, dgap, dgrad, dpts, dgrid);

@@ -173,3 +173,42 @@ def test_bulk_copy_backward_matches_regathered(cuda, port, n):
     flags = ctypes.c_uint32(7)
     N.check(N.load().sdfo_device_status(ctypes.byref(flags), 1))
     assert flags.value == 0
+
+
+def test_regathering_backward_walk_bit_identical(cuda):
+    """The persistent walk kernel of the regathering backward for dL/dp (the
+    default; sdfo_tuning.query_walk) gives dL/dp bit for bit as the
+    one-CTA-per-tile kernel does: dense and sparse FP32 / FP16 grids, each
+    combination of upstream gradients, batch sizes below one tile, between
+    tiles and above the resident CTA count."""
+    import torch
+
+    from conftest import golden
+    from sdfo import SdfGrid
+    from sdfo import _native as N
+    from sdfo import workloads as W
+
+    g = golden("sparse_cyl.npz")
+    spec = dict(bmin=g["bmin"], bmax=g["bmax"], voxel=g["voxel"], shape=tuple(g["shape"]))
+    sparse = SdfGrid.from_sparse(spec, int(g["block_dim"]), g["ijk"], g["phi"], g["normal"], g["hessian"])
+    c = W.c2_cylinder()
+    dense = SdfGrid.build_dense(c["verts"], c["tris"], mode=3, target_resolution=64, max_resolution=64)
+    rng = np.random.default_rng(17)
+    before = N.get_tuning()
+    try:
+        for gr in (sparse, sparse.to_fp16(), dense):
+            lo, hi = np.array(gr.bmin), np.array(gr.bmax)
+            pts = np.concatenate([g["pts"], rng.uniform(lo, hi, (600_000, 3))]).astype(np.float32)
+            for n in (1, 255, 257, len(pts)):
+                x = torch.tensor(pts[:n], device="cuda")
+                gen = torch.Generator(device="cuda").manual_seed(n)
+                dgap = torch.randn(n, device="cuda", generator=gen)
+                dgrad = torch.randn((n, 3), device="cuda", generator=gen)
+                for dg, dr in ((dgap, dgrad), (dgap, None), (None, dgrad)):
+                    out = {}
+                    for walk in (1, 2):
+                        N.set_tuning(query_walk=walk)
+                        out[walk] = gr.query_backward(x, dg, dr, mode=3).cpu().numpy()
+                    assert np.array_equal(out[1], out[2]), (gr.storage, gr.is_sparse, n)
+    finally:
+        N.set_tuning(**before)
