@@ -800,8 +800,13 @@ void launch_pt(const GridView& v, const void* pts, bool f64, int64_t n, const Qu
     // (resident CTAs per SM) measured on the hollow cylinder (dense) and the
     // 512^3 icosphere (sparse):
     //   dense, no Hessian: 4 CTAs (64 registers, no spills), 32.5 G queries/s
-    //     against 28.7 for the bulk-copy pipeline; the Hessian-writing dense
-    //     forward stays on the pipeline (25.7 against 22.2 as a walk);
+    //     against 28.7 for the bulk-copy pipeline;
+    //   dense, full 3x3 Hessian: 3 CTAs, 25.8 G/s against 17.1 for the staged
+    //     kernel (the pipeline writes only the 6 unique entries);
+    //   dense, 6-entry Hessian (the linearising forward): stays on the
+    //     pipeline -- as a walk it ran 24.4-26.4 against 25.7 G/s, but the
+    //     saved backward that follows it in AD then ran slower (AD 18.4
+    //     against 20.0);
     //   sparse, no Hessian: 4 CTAs;
     //   sparse with the Hessian over an FP32 pool: 3 CTAs (80 registers, no
     //     spills), 19% faster than 4 (linearising forward 19.8 -> 23.5 G/s);
@@ -831,8 +836,8 @@ void launch_pt(const GridView& v, const void* pts, bool f64, int64_t n, const Qu
             return;
         }
     }
-    // The bulk-copy pipeline: dense grids, the Hessian-writing forward (and
-    // every forward when the walk is off).  Not on sparse grids: there the
+    // The bulk-copy pipeline: dense grids, the forward that writes the
+    // 6-entry Hessian (and every forward when the walk is off).  Not on sparse grids: there the
     // gathers' latency varies with the brick lookups, and the per-tile
     // barriers of a persistent CTA cost more than the prefetched points save
     // (measured: C5 forward -11%).
