@@ -207,6 +207,19 @@ class TuningCache:
         N.set_tuning(**{k: v for k, v in knobs.items() if k in fields})
         return True
 
+    def apply_batch(self, gpu: str, workload: str, batch) -> bool:
+        """Sets a stored launch shape ("threads", "run": what
+        tune_query_batch picks) on a QueryBatch; returns whether the entry
+        held one."""
+        knobs = self.get(gpu, workload) or {}
+        if "threads" not in knobs and "run" not in knobs:
+            return False
+        if "threads" in knobs:
+            batch.set_threads(int(knobs["threads"]))
+        if "run" in knobs:
+            batch.set_run(int(knobs["run"]))
+        return True
+
 
 def workload_key(kind: str, shape, **extra) -> str:
     """A stable key for a workload shape, e.g. workload_key("dense_fill",

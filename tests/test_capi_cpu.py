@@ -215,5 +215,24 @@ def test_tuning_cache_round_trip(lib, tmp_path):
         t = N.get_tuning()
         assert (t["fill_tile_log2_x"], t["fill_tile_log2_y"]) == (2, 2)
         assert c2.get("other GPU", key) is None
+
+        # a batch launch shape goes to the QueryBatch, not to sdfo_set_tuning
+        class Batch:
+            def __init__(self):
+                self.calls = []
+
+            def set_threads(self, t):
+                self.calls.append(("threads", t))
+
+            def set_run(self, r):
+                self.calls.append(("run", r))
+
+        bkey = workload_key("query_batch", (256,), queries=65536)
+        c2.put("NVIDIA B200", bkey, {"threads": 128, "run": 4})
+        b = Batch()
+        assert TuningCache(path).apply_batch("NVIDIA B200", bkey, b)
+        assert b.calls == [("threads", 128), ("run", 4)]
+        assert not TuningCache(path).apply_batch("other GPU", bkey, Batch())
+        assert not TuningCache(path).apply_batch("NVIDIA B200", key + "x", Batch())
     finally:
         N.set_tuning(**before)
