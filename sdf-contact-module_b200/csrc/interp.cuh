@@ -213,13 +213,13 @@ __device__ __forceinline__ bool gather_corners(const GridView& g, const Cell& c,
 // 64-bit load for i0 + 1; the brick's affine phi map is read once per brick.
 // Needs the pool on a 32-byte boundary (GridView::phin_a32).  Same values and
 // validity as gather_corners.
-__device__ __forceinline__ void split_h4(const float4 q, int k, float4& v)
+// One FP16 voxel {phi, nx, ny, nz} held as two 32-bit words (low half
+// first), decoded as decode_fp16 does.
+__device__ __forceinline__ float4 decode_fp16_words(unsigned w0, unsigned w1, float2 aff)
 {
-    // halves 4k .. 4k+3 of a 32-byte chunk held as {q.lo, q.hi} words
-    const unsigned w0 = __float_as_uint(k == 0 ? q.x : q.z), w1 = __float_as_uint(k == 0 ? q.y : q.w);
     const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&w0));
     const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&w1));
-    v = make_float4(a.x, a.y, b.x, b.y);
+    return make_float4(a.x * aff.x + aff.y, a.y, b.x, b.y);
 }
 
 template <int ST = 0>
@@ -278,19 +278,20 @@ __device__ __forceinline__ bool gather_rows_b8(const GridView& g, const Cell& c,
         }
         else
         {
+            // FP16 voxels of 8 bytes: li even, the pair in one aligned
+            // 16-byte load (li + 1 is in the same brick); li odd, two 8-byte
+            // loads, the second across the brick face when li == 7
             const float2 af0 = s0 == s[0][0][0] ? aff000 : __ldg(g.brick_affine + s0);
-            float4 lo, hi; // halves of voxels (li & ~3) .. (li & ~3) + 3
-            ld256(reinterpret_cast<const float4*>(g.phin16 + row0 + (li & ~3)), lo, hi);
-            const int m = li & 3;
-            split_h4(m < 2 ? lo : hi, m & 1, a);
-            a.x = a.x * af0.x + af0.y;
-            if (m < 3)
+            const ushort4* r16 = g.phin16 + row0 + li;
+            if ((li & 1) == 0)
             {
-                split_h4(m + 1 < 2 ? lo : hi, (m + 1) & 1, b);
-                b.x = b.x * af0.x + af0.y;
+                const uint4 w = __ldg(reinterpret_cast<const uint4*>(r16));
+                a = decode_fp16_words(w.x, w.y, af0);
+                b = decode_fp16_words(w.z, w.w, af0);
             }
             else
             {
+                a = decode_fp16(__ldg(r16), af0);
                 const int64_t i1 = cx ? (int64_t)s1 * V + bd * (ly + bd * lz) : row0 + li + 1;
                 const float2 af1 = s1 == s0 ? af0 : __ldg(g.brick_affine + s1);
                 b = decode_fp16(__ldg(g.phin16 + i1), af1);
