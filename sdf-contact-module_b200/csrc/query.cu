@@ -810,7 +810,8 @@ void launch_pt(const GridView& v, const void* pts, bool f64, int64_t n, const Qu
     //   sparse, no Hessian: 4 CTAs;
     //   sparse with the Hessian over an FP32 pool: 3 CTAs (80 registers, no
     //     spills), 19% faster than 4 (linearising forward 19.8 -> 23.5 G/s);
-    //     over an FP16 pool 4 CTAs stay 4% faster.
+    //     over an FP16 pool 4 CTAs stay faster (21.5 against 19.7 G/s at 3,
+    //     with the 16-byte FP16 row loads).
     if constexpr (MODE == SDFO_TRILINEAR || MODE == SDFO_TRICUBIC)
     {
         const bool hess = o.hess || o.hess6;
