@@ -88,10 +88,6 @@ class RigidBody(ctypes.Structure):
     _fields_ = [("mass", _D), ("inertia", _D * 9), ("gravity", _D * 3)]
 
 
-class BodyState(ctypes.Structure):
-    _fields_ = [("r", _D * 3), ("R", _D * 9), ("v", _D * 3), ("w", _D * 3)]
-
-
 class BuildStats(ctypes.Structure):
     _fields_ = [("setup_ms", _D), ("bvh_ms", _D), ("fill_ms", _D), ("hessian_ms", _D),
                 ("total_ms", _D), ("voxels_filled", _I64), ("candidate_blocks", _I64),
